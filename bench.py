@@ -1,0 +1,358 @@
+"""Benchmark of the batched one-sided Jacobi SVD on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step): the uneven batch of 8192 float32 matrices, n ~ U{8..64},
+m ~ U{n..2n}, entries N(0,1), seed 1 (rank r > 0 of a multi-GPU run uses seed
+1 + 1000 r: independent matrices, same distribution), solved by ONE persistent
+launch replayed from a captured CUDA graph, in the mixed precision that meets
+sigma-rel-err <= 1e-5 against FP64 LAPACK (checked on rank 0 after timing).
+Metric: matrices/s (whole job).  Each step is timed with CUDA events on the
+launching stream; a 256 MiB buffer is written between steps (outside the
+events) so every step starts with a cold L2.
+
+--impl reference: the reference algorithm's CPU implementation, timed on the
+host cores of this machine (the C restatement in oracle/, all threads; the
+reference itself is Python/PyTorch and is not present here), on a bounded
+sample of the same workload.  Under torchrun only rank 0 runs it.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Jacobi SVD matrices/s at sigma-rel-err<=1e-5 vs FP64 (uneven batch)"
+WORKLOAD = "uneven_batch_8192"
+COUNT = 8192
+
+
+def workload_config(n_gpus):
+    return {"workload": WORKLOAD, "matrices_per_gpu": COUNT, "n_range": [8, 64], "m_range": "[n, 2n]",
+            "dtype": "float32", "seed": 1, "tol": "10*eps32 (reference default)", "max_sweeps": 60,
+            "precision": "mixed (FP32 sweeps, then FP64 sweeps from Householder-QR V)",
+            "parallelism": f"dp{n_gpus} (independent matrices per GPU, no collective)",
+            "l2": "256 MiB write between steps, outside the timed events"}
+
+
+def load_matrices(rank):
+    wl = importlib.import_module("pavel-s_svd_b200.workloads")
+    return wl.uneven_batch(COUNT, seed=1 if rank == 0 else 1 + 1000 * rank)
+
+
+def algorithmic(m, n):
+    """Compulsory HBM bytes and FP work of one solve of the batch.
+    bytes: read A, write U (m x k), S (k), Vh (k x n), descriptors (48 B) and
+    status/sweeps (8 B) per matrix.  flop/sweep of one matrix on its tall view
+    (mt x nt): nt(nt-1)/2 pairs x (12 mt + 6 nt)."""
+    m = m.astype(np.int64); n = n.astype(np.int64)
+    k = np.minimum(m, n)
+    nbytes = int((4 * (m * n + m * k + k + k * n) + 48 + 8).sum())
+    mt, nt = np.maximum(m, n), np.minimum(m, n)
+    flop_per_sweep = nt * (nt - 1) // 2 * (12 * mt + 6 * nt)
+    return nbytes, flop_per_sweep
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (every 200 ms)."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_port_sample(mats, seconds=12.0, threads=0):
+    """Time the C oracle on consecutive chunks of the workload until about
+    `seconds` of wall time; returns (matrices/s, matrices solved, threads)."""
+    from oracle import c_oracle
+    B = importlib.import_module("pavel-s_svd_b200.batch")
+    threads = threads or c_oracle.max_threads()
+    done, elapsed, i = 0, 0.0, 0
+    chunk = 256
+    while elapsed < seconds and i < len(mats):
+        part = mats[i:i + chunk]
+        flat, m, n, a_off = B.pack(part)
+        k = np.minimum(m, n)
+        desc = np.zeros(len(part), B.DESC_DTYPE)
+        desc["m"], desc["n"], desc["rank"], desc["a_off"] = m, n, k, a_off
+        desc["u_off"], _ = B._aligned_offsets(m * k)
+        desc["s_off"], _ = B._aligned_offsets(k)
+        desc["v_off"], _ = B._aligned_offsets(k * n)
+        t = time.perf_counter()
+        c_oracle.svd_uneven(flat.numpy(), desc, threads=threads)
+        elapsed += time.perf_counter() - t
+        done += len(part)
+        i += chunk
+    return done / elapsed, done, threads, elapsed
+
+
+def run_reference(args, rank, world):
+    """The CPU reference arm: rank 0 times the oracle port; other ranks exit."""
+    if rank != 0:
+        return
+    mats = load_matrices(0)
+    per_step = []
+    sample = 0
+    threads = 0
+    for step in range(args.warmup + args.steps):
+        rate, done, threads, el = cpu_port_sample(mats, seconds=args.ref_seconds)
+        if step >= args.warmup:
+            per_step.append(rate)
+            sample = done
+    value = statistics.median(per_step)
+    line = {"metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sample / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": workload_config(world), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "matrices/s", "cores": threads, "kind": "port",
+                             "sample": f"first {sample} matrices of the workload per step (~{args.ref_seconds:.0f} s),"
+                                       " C restatement of the reference Jacobi (oracle/), fp32 as the reference"},
+            "e2e": {"value": value, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def check_accuracy(plan, mats, limit=None):
+    """Max relative sigma error vs FP64 LAPACK over values above 2x the
+    reference cut, and the worst reconstruction error, on rank 0."""
+    worst_sig, worst_rec = 0.0, 0.0
+    S = plan.S.cpu().numpy()
+    U = plan.U.cpu().numpy()
+    Vh = plan.Vh.cpu().numpy()
+    idx = range(len(mats)) if limit is None else range(0, len(mats), max(1, len(mats) // limit))
+    for i in idx:
+        a = mats[i].astype(np.float64)
+        m, n = a.shape
+        k = min(m, n)
+        s = S[plan.s_off[i]:plan.s_off[i] + k].astype(np.float64)
+        sr = np.linalg.svd(a, compute_uv=False)
+        sel = sr > 2 * np.finfo(np.float32).eps * max(m, n) * sr[0]
+        worst_sig = max(worst_sig, float(np.max(np.abs(s[sel] - sr[sel]) / sr[sel])))
+        u = U[plan.u_off[i]:plan.u_off[i] + m * k].reshape(m, k).astype(np.float64)
+        vh = Vh[plan.v_off[i]:plan.v_off[i] + k * n].reshape(k, n).astype(np.float64)
+        worst_rec = max(worst_rec, float(np.linalg.norm(a - (u * s) @ vh) / np.linalg.norm(a)))
+    return worst_sig, worst_rec
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    pkg = importlib.import_module("pavel-s_svd_b200")
+    B = importlib.import_module("pavel-s_svd_b200.batch")
+    mats = load_matrices(rank)
+    flat_host, m, n, a_off = B.pack(mats)
+    flat = flat_host.to(dev)
+    plan = B.UnevenBatch(m, n, dev, a_off=a_off, precision=args.precision)
+    nbytes, flop_per_sweep = algorithmic(m, n)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    graph = plan.capture(flat)
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        graph.replay()
+    torch.cuda.synchronize(dev)
+    sweeps = plan.check()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    times = []
+    with ClockSampler(local_rank) as clocks:
+        for step in range(args.steps):
+            flush.fill_(step & 0xff)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            graph.replay()
+            e1.record(stream)
+            times.append((e0, e1))
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in times]
+    total_ms = sum(step_ms)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = COUNT * world / (ms_per_step / 1e3)
+
+    # End to end: pinned host input -> device, solve, outputs -> pinned host,
+    # status read-back (plan.check), all inside the timed region.
+    host_in = flat_host.pin_memory()
+    host_u = torch.empty_like(plan.U, device="cpu").pin_memory()
+    host_s = torch.empty_like(plan.S, device="cpu").pin_memory()
+    host_v = torch.empty_like(plan.Vh, device="cpu").pin_memory()
+    dev_in = torch.empty_like(flat)
+    h2d = host_in.numel() * 4
+    d2h = (host_u.numel() + host_s.numel() + host_v.numel()) * 4 + 8 * COUNT
+
+    def e2e_step():
+        dev_in.copy_(host_in, non_blocking=True)
+        plan.launch(dev_in)
+        host_u.copy_(plan.U, non_blocking=True)
+        host_s.copy_(plan.S, non_blocking=True)
+        host_v.copy_(plan.Vh, non_blocking=True)
+        plan.check()  # synchronises; raises on any failed matrix
+
+    for _ in range(args.warmup):
+        e2e_step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e2e_ev = []
+    for _ in range(args.steps):
+        flush.fill_(3)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_step()
+        e1.record(stream)
+        e2e_ev.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = COUNT * world / (float(t.item()) / args.steps / 1e3)
+
+    if rank != 0:
+        return
+    graph.replay()
+    torch.cuda.synchronize(dev)
+    sweeps = plan.check()
+    sig_err, rec_err = check_accuracy(plan, mats, limit=None if args.full_check else 2048)
+    hbm_peak, peak_kind = peaks()
+    achieved_gbs = nbytes / (ms_per_step / 1e3) / 1e9
+    flop = float((flop_per_sweep * sweeps).sum())
+    fp_tflops = flop / (ms_per_step / 1e3) / 1e12
+    line = {"metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 in/out; f32+f64 sweeps" if args.precision == "mixed" else "f32",
+            "data": "synthetic (seeded, BASELINE config 2 distribution)", "config": workload_config(world),
+            "accuracy": {"max_rel_sigma_err_vs_fp64": sig_err, "max_reconstruction_rel_fro": rec_err,
+                         "matrices_checked": len(mats) if args.full_check else 2048,
+                         "sweeps_mean": float(sweeps.mean()), "sweeps_max": int(sweeps.max())},
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved_gbs / hbm_peak, "peak_kind": peak_kind,
+                         "traffic": args.traffic_bytes,
+                         "algorithmic_bytes_per_launch": nbytes,
+                         "note": "compulsory bytes only; the path is bound by the FP32/FP64 pipes, see fp_pipe"},
+            "fp_pipe": {"achieved_tflops": fp_tflops, "flop_per_launch": flop,
+                        "fp32_nominal_tflops": 74.4, "fp64_nominal_tflops": 37.2,
+                        "note": "algorithmic flop = sum over matrices of sweeps x nt(nt-1)/2 (12 mt + 6 nt)"},
+            "clocks": clocks.summary(), "gpu_launches": args.steps,
+            "e2e": {"value": e2e_value, "unit": "matrices/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}}
+    if not args.no_cpu_baseline:
+        rate, done, threads, el = cpu_port_sample(mats, seconds=args.ref_seconds)
+        line["cpu_baseline"] = {"value": rate, "unit": "matrices/s", "cores": threads, "kind": "port",
+                                "sample": f"first {done} of the 8192 matrices ({el:.1f} s), C restatement of the "
+                                          "reference Jacobi (oracle/), fp32 like the reference"}
+    print(json.dumps(line), flush=True)
+    del graph
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--precision", choices=("mixed", "fp32"), default="mixed")
+    ap.add_argument("--ref-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--full-check", action="store_true")
+    ap.add_argument("--traffic-bytes", type=float, default=None,
+                    help="per-launch DRAM bytes from an ncu capture, reported as roofline.traffic")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("at least 3 warm-up steps")
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,121 @@
+/*
+ * jacobi_b200.h - C ABI of the B200 (sm_100a) one-sided Jacobi SVD library.
+ *
+ * Plain pointers and sizes only: every buffer argument is a DEVICE pointer,
+ * every stream is a cudaStream_t passed as void*.  Every entry point returns
+ * an int status (JB_OK or a JB_E* code) and never aborts the process; it only
+ * enqueues work on the given stream (asynchronous).  Per-matrix outcomes
+ * (converged / not converged / non-finite input / failed null completion /
+ * non-finite output) land in the caller's `status` array on the device.
+ *
+ * Reference interfaces replaced (uncle-Slava/Pavel-s_SVD, paths relative to
+ * that project):
+ *   jb_svd_batched_*     svdbench/standalone/primitives.py:316-367 (jacobi_svd),
+ *                        with solvers.py:224-230 (wide -> tall via adjoint),
+ *                        solvers.py:289-310 (scaling, truncation, full bases)
+ *                        and primitives.py:430-467 (null-space completion)
+ *                        fused into one launch.
+ *   jb_svd_uneven_f32    the per-matrix loop a harness runs over svd(x,'jacobi')
+ *                        for matrices of different shapes (the reference can
+ *                        only batch equal shapes: solvers.py:289-290).
+ */
+#ifndef JACOBI_B200_H
+#define JACOBI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define JB_API __attribute__((visibility("default")))
+#else
+#define JB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- return codes of the entry points ---------------------------------- */
+#define JB_OK               0
+#define JB_EINVAL           1   /* bad argument (null pointer, size, tolerance) */
+#define JB_ETOOBIG          2   /* shape exceeds what the entry point supports  */
+#define JB_EWORKSPACE       3   /* workspace missing or smaller than required   */
+#define JB_ECUDA            4   /* a CUDA runtime call failed                   */
+
+/* ---- per-matrix status words written to `status` ------------------------ */
+#define JB_ST_OK            0   /* converged, outputs written                        */
+#define JB_ST_NOT_CONVERGED 1   /* off > tol after max_sweeps (primitives.py:354-355) */
+#define JB_ST_NONFINITE_IN  2   /* NaN/Inf in the input (solvers.py:291-292)          */
+#define JB_ST_NULL_FAILED   3   /* null completion failed (primitives.py:451-452)     */
+#define JB_ST_NONFINITE_OUT 4   /* NaN/Inf in an output (solvers.py:305-306)          */
+#define JB_ST_BAD_DESC      5   /* descriptor outside the launch's max sizes/flags    */
+
+/* ---- flags ---------------------------------------------------------------- */
+#define JB_FULL_MATRICES    1   /* U is m x m and Vh is n x n (complete_basis)  */
+#define JB_VALUES_ONLY      2   /* write S only; U and Vh may be NULL           */
+
+/* ---- arithmetic of the solve ------------------------------------------- */
+#define JB_PREC_NATIVE      0   /* sweeps in the input precision (f32 or f64)   */
+#define JB_PREC_MIXED       1   /* f32 input: FP32 sweeps, then Householder-QR
+                                   re-orthonormalised V and FP64 sweeps from
+                                   W = A V to the same tolerance; f64 input:
+                                   same as NATIVE                               */
+
+/* One matrix of an uneven batch.  A is row-major m x n at A + a_off.
+ * Outputs (row-major): U at U + u_off (m x ucols), S at S + s_off (k values),
+ * Vh at Vh + v_off (vrows x n), where k = rank, ucols = vrows = rank, or with
+ * JB_FULL_MATRICES ucols = m, vrows = n.  Offsets count elements. */
+typedef struct jb_matrix_desc {
+    int32_t m, n;
+    int32_t rank;       /* 1 <= rank <= min(m, n) */
+    int32_t flags;      /* JB_FULL_MATRICES | JB_VALUES_ONLY */
+    int64_t a_off, u_off, s_off, v_off;
+} jb_matrix_desc;
+
+/* Library version (major*10000 + minor*100 + patch). */
+JB_API int jb_version(void);
+
+/* Number of streaming multiprocessors of the current device, or -1. */
+JB_API int jb_device_sm_count(void);
+
+/* Bytes of device workspace that jb_svd_batched_* / jb_svd_uneven_f32 need
+ * for matrices up to max_m x max_n (either orientation), `count` matrices,
+ * the given precision and flags.  0 is a valid answer. */
+JB_API size_t jb_workspace_bytes(int32_t max_m, int32_t max_n, int64_t count,
+                          int32_t elem_bytes, int32_t precision, int32_t flags);
+
+/* Equal-shape batch: `batch` row-major m x n matrices at A (stride m*n).
+ * U: batch x m x ucols, S: batch x k, Vh: batch x vrows x n (see
+ * jb_matrix_desc).  tol <= 0 selects the reference default 10*eps(dtype)
+ * (primitives.py:325).  sweeps/status: `batch` int32 each (device).
+ * Replaces svd(a, 'jacobi', tol=, max_sweeps=, rank=, full_matrices=,
+ * values_only=) of svdbench/standalone/solvers.py:264-310 for real dtypes. */
+JB_API int jb_svd_batched_f32(const float *A, float *U, float *S, float *Vh,
+                       int64_t batch, int32_t m, int32_t n, int32_t rank,
+                       int32_t flags, double tol, int32_t max_sweeps,
+                       int32_t precision, int32_t *sweeps, int32_t *status,
+                       void *workspace, size_t workspace_bytes, void *stream);
+
+JB_API int jb_svd_batched_f64(const double *A, double *U, double *S, double *Vh,
+                       int64_t batch, int32_t m, int32_t n, int32_t rank,
+                       int32_t flags, double tol, int32_t max_sweeps,
+                       int32_t *sweeps, int32_t *status,
+                       void *workspace, size_t workspace_bytes, void *stream);
+
+/* Uneven batch in ONE persistent launch.  descs: `count` device descriptors;
+ * order: optional device permutation of [0, count) giving the processing
+ * order (largest cost first balances the persistent grid), or NULL.
+ * max_m/max_n bound every descriptor (either orientation).  Replaces a
+ * harness loop of svd(x, 'jacobi') over matrices of different shapes. */
+JB_API int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh,
+                      const jb_matrix_desc *descs, const int32_t *order,
+                      int64_t count, int32_t max_m, int32_t max_n,
+                      double tol, int32_t max_sweeps, int32_t precision,
+                      int32_t *sweeps, int32_t *status,
+                      void *workspace, size_t workspace_bytes, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JACOBI_B200_H */

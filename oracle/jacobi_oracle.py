@@ -1,0 +1,269 @@
+"""CPU oracle: NumPy restatement of the reference one-sided Jacobi SVD path.
+
+TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` may import this
+module, and only as the checker (or the timed CPU baseline).  The product path
+(``pavel-s_svd_b200``) never imports it and has no CPU fallback.
+
+Every function restates the algorithm of the reference project
+(uncle-Slava/Pavel-s_SVD) step by step with NumPy arrays, batched in lock-step
+exactly like the PyTorch original:
+
+  round_robin            svdbench/standalone/primitives.py:309-313
+  jacobi_svd             svdbench/standalone/primitives.py:316-367
+  complete_null_columns  svdbench/standalone/primitives.py:430-455
+  complete_basis         svdbench/standalone/primitives.py:458-467
+  svd                    svdbench/standalone/solvers.py:264-310 ('jacobi' only)
+  raw                    svdbench/standalone/solvers.py:224-230
+  reference / validate   svdbench/metrics.py:6-66 (FP64 LAPACK gesvd truth)
+
+Parity of this restatement is pinned against fixtures produced by the
+reference itself (tests/golden/make_golden.py, tests/test_oracle.py).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+__all__ = ["round_robin", "jacobi_svd", "complete_null_columns", "complete_basis",
+           "svd", "raw", "reference", "validate", "eps"]
+
+
+def _real(dt):
+    dt = np.dtype(dt)
+    return {np.dtype(np.complex64): np.dtype(np.float32),
+            np.dtype(np.complex128): np.dtype(np.float64)}.get(dt, dt)
+
+
+def eps(dt):
+    """Machine epsilon of the real part type (primitives.py:26-31)."""
+    return float(np.finfo(_real(dt)).eps)
+
+
+def tiny(dt):
+    return float(np.finfo(_real(dt)).tiny)
+
+
+def round_robin(n):
+    """Circle-method tournament: n-1 rounds of n//2 disjoint (p<q) pairs.
+
+    Player 0 stays fixed; the last player moves to slot 1 each round
+    (primitives.py:309-313)."""
+    players = list(range(n))
+    for _ in range(n - 1):
+        yield [(min(players[i], players[n - 1 - i]), max(players[i], players[n - 1 - i]))
+               for i in range(n // 2)]
+        players = [players[0]] + [players[-1]] + players[1:-1]
+
+
+def jacobi_svd(A, tol=None, max_sweeps=30):
+    """One-sided Hestenes Jacobi, round-robin ordering, lock-step batch.
+
+    A: (b, m, n) with m >= n.  Returns U (b,m,n), s (b,n) descending, V (b,n,n),
+    sweeps (primitives.py:316-367).  Raises RuntimeError when not converged
+    (primitives.py:354-355)."""
+    A = np.asarray(A)
+    dt = A.dtype
+    rdt = _real(dt)
+    b, m, n = A.shape
+    padded = n % 2 == 1
+    W = A.copy()
+    if padded:                                                    # :320-323
+        W = np.concatenate([W, np.zeros((b, m, 1), dt)], -1)
+        n += 1
+    V = np.broadcast_to(np.eye(n, dtype=dt), (b, n, n)).copy()    # :324
+    e = eps(dt)
+    tol = tol or 10 * e                                           # :325
+    sched = [(np.array([p for p, _ in prs]), np.array([q for _, q in prs])) for prs in round_robin(n)]
+    sweeps = 0
+    off = rdt.type(0)
+    one = rdt.type(1)
+    for sweeps in range(1, max_sweeps + 1):                       # :328
+        off = rdt.type(0)
+        for P, Q in sched:                                        # :330
+            wp, wq = W[:, :, P], W[:, :, Q]
+            app = (np.abs(wp) ** 2).sum(1, dtype=rdt)             # :332
+            aqq = (np.abs(wq) ** 2).sum(1, dtype=rdt)
+            apq = (np.conj(wp) * wq).sum(1, dtype=dt)             # :333
+            den = np.sqrt(app) * np.sqrt(aqq)                     # :334
+            ratio = np.abs(apq) / np.maximum(den, rdt.type(tiny(dt)))     # :335
+            floor = rdt.type(e) ** 2 * np.maximum(app, aqq).max(-1, keepdims=True)   # :337
+            active = (ratio > tol) & (np.minimum(app, aqq) > floor)       # :338
+            off = max(off, np.where(active, ratio, rdt.type(0)).max())    # :339
+            a = np.where(active, np.abs(apq), one)                # :340
+            tau = (aqq - app) / (2 * a)                           # :341
+            t = np.sign(tau) / (np.abs(tau) + np.hypot(tau, one))         # :342
+            t = np.where(tau == 0, one, t).astype(rdt)            # :343
+            c = (one / np.sqrt(one + t * t)).astype(rdt)          # :344
+            s = (t * c).astype(dt) * (apq / a.astype(dt))         # :345
+            c = np.where(active, c, one).astype(dt)               # :346
+            s = np.where(active, s, 0).astype(dt)                 # :347
+            c = c[:, None, :]
+            s = s[:, None, :]
+            W[:, :, P], W[:, :, Q] = c * wp - np.conj(s) * wq, s * wp + c * wq   # :349
+            vp, vq = V[:, :, P], V[:, :, Q]
+            V[:, :, P], V[:, :, Q] = c * vp - np.conj(s) * vq, s * vp + c * vq   # :350-351
+        if off <= tol:                                            # :352
+            break
+    if off > tol:                                                 # :354-355
+        raise RuntimeError(f"one-sided Jacobi did not converge in {max_sweeps} sweeps")
+    s_vals = np.sqrt((np.abs(W) ** 2).sum(1, dtype=rdt))          # :356
+    if padded:                                                    # :357-358
+        W, V, s_vals = W[:, :, :-1], V[:, :-1, :-1], s_vals[:, :-1]
+    order = np.argsort(-s_vals, axis=1, kind="stable")            # :359
+    s_vals = np.take_along_axis(s_vals, order, 1)
+    W = np.take_along_axis(W, order[:, None, :], 2)
+    V = np.take_along_axis(V, order[:, None, :], 2)
+    # n here is the padded width, as in the reference (:319, :323, :362).
+    cut = rdt.type(e) * max(m, n) * s_vals[:, :1]                 # :362
+    keep = s_vals > cut                                           # :363
+    U = W / np.where(keep, s_vals, one)[:, None, :]               # :364
+    U = complete_null_columns(U, keep)                            # :365
+    s_vals = np.where(keep, s_vals, rdt.type(0))                  # :366
+    return U, s_vals, V, sweeps
+
+
+def complete_null_columns(u, keep):
+    """Fill columns with keep==False by projected coordinate vectors
+    (primitives.py:430-455): largest leftover row leverage picks the
+    coordinate, two projections against all columns, normalise."""
+    if keep.all():                                                # :432
+        return u
+    u = np.where(keep[:, None, :], u, 0).astype(u.dtype)          # :434-436
+    b, m, n = u.shape
+    rdt = _real(u.dtype)
+    e = eps(u.dtype)
+    for j in range(n):                                            # :438
+        missing = ~keep[:, j]
+        if not missing.any():
+            continue
+        leverage = 1 - (np.abs(u) ** 2).sum(-1, dtype=rdt)        # :444
+        idx = leverage.argmax(-1)                                 # :445
+        v = np.zeros((b, m, 1), u.dtype)
+        v[np.arange(b), idx, 0] = 1                               # :446-447
+        for _ in range(2):                                        # :448-449
+            v = v - u @ (np.conj(np.swapaxes(u, -1, -2)) @ v)
+        length = np.sqrt((np.abs(v) ** 2).sum(-2, keepdims=True, dtype=rdt))  # :450
+        if (length[missing] < 10 * e).any():                      # :451-452
+            raise RuntimeError("null-space completion failed: supplied live columns are not independent")
+        v = v / np.maximum(length, rdt.type(tiny(u.dtype)))       # :453
+        u[:, :, j] = np.where(missing[:, None], v[:, :, 0], u[:, :, j])   # :454
+    return u
+
+
+def complete_basis(q, size):
+    """Extend an orthonormal basis to `size` columns (primitives.py:458-467)."""
+    if size == q.shape[-1]:
+        return q
+    b, m, k = q.shape
+    if not k <= size <= m:
+        raise ValueError("invalid basis size")
+    z = np.zeros((b, m, size - k), q.dtype)
+    keep = np.broadcast_to(np.arange(size)[None, :] < k, (b, size))
+    return complete_null_columns(np.concatenate([q, z], -1), keep)
+
+
+def raw(x, opts, stats):
+    """Wide inputs are solved through their adjoint (solvers.py:224-230)."""
+    if x.shape[-2] < x.shape[-1]:
+        u, s, v = raw(np.conj(np.swapaxes(x, -1, -2)), opts, stats)
+        return v, s, u
+    u, s, v, sweeps = jacobi_svd(x, tol=opts.get("tol"), max_sweeps=opts.get("max_sweeps", 60))
+    stats["jacobi_sweeps"] = max(stats.get("jacobi_sweeps", 0), sweeps)   # solvers.py:24-27
+    return u, s, v
+
+
+def svd(a, algorithm="jacobi", *, full_matrices=False, values_only=False, return_info=False, **opts):
+    """NumPy restatement of the public entry (solvers.py:264-310), 'jacobi' only."""
+    a = np.asarray(a)
+    if algorithm != "jacobi":
+        raise ValueError("the oracle restates the 'jacobi' family only")
+    if a.ndim < 2 or min(a.shape[-2:]) < 1:
+        raise ValueError("nonempty matrix dimensions required")
+    if a.dtype not in (np.float32, np.float64, np.complex64, np.complex128):
+        raise TypeError("supported dtypes: float32/64, complex64/128")
+    rank = opts.get("rank", min(a.shape[-2:]))
+    if not 1 <= rank <= min(a.shape[-2:]):
+        raise ValueError("rank outside [1,min(m,n)]")
+    if full_matrices and rank != min(a.shape[-2:]):
+        raise ValueError("full_matrices and truncated rank cannot be combined")
+    for key in ("max_iter", "max_sweeps", "leaf_size"):
+        if key in opts and opts[key] < 1:
+            raise ValueError(f"{key} must be positive")
+    for key in ("oversample", "iterations"):
+        if key in opts and opts[key] < 0:
+            raise ValueError(f"{key} must be nonnegative")
+    shape = a.shape[:-2]
+    x = a.reshape(-1, *a.shape[-2:])
+    if not np.isfinite(x).all():
+        raise ValueError("input contains NaN or infinity")
+    scale = np.abs(x).max((-2, -1), keepdims=True)                # solvers.py:294-295
+    scale = np.where(scale > 0, scale, 1).astype(_real(a.dtype))
+    stats = {"algorithm": algorithm, "vendor_factorizations": 0, "converged": True}
+    u, s, v = raw((x / scale).astype(a.dtype), opts, stats)
+    s = s * scale[:, 0, 0][:, None]
+    if full_matrices:
+        u = complete_basis(u, a.shape[-2])
+        v = complete_basis(v, a.shape[-1])
+    else:
+        u, s, v = u[:, :, :rank], s[:, :rank], v[:, :, :rank]
+    if not all(np.isfinite(z).all() for z in (u, s, v)):
+        raise RuntimeError("standalone solver produced nonfinite output")
+    vh = np.conj(np.swapaxes(v, -1, -2))
+    result = (None if values_only else u.reshape(*shape, *u.shape[-2:]),
+              s.reshape(*shape, s.shape[-1]),
+              None if values_only else vh.reshape(*shape, *vh.shape[-2:]))
+    return (*result, stats) if return_info else result
+
+
+def reference(a):
+    """FP64 LAPACK gesvd truth on the rounded input (metrics.py:6-10)."""
+    import scipy.linalg
+    dtype = np.complex128 if np.iscomplexobj(a) else np.float64
+    arrays = a[None] if a.ndim == 2 else a
+    return [scipy.linalg.svd(x.astype(dtype), full_matrices=False, lapack_driver="gesvd",
+                             check_finite=True) for x in arrays]
+
+
+def validate(a, result, refs):
+    """Accuracy metrics against the FP64 truth (metrics.py:13-66): worst case
+    over the batch of each key, plus the per-matrix rows."""
+    u, s, vh = result
+    arrays = a[None] if a.ndim == 2 else a
+    if a.ndim == 2:
+        s = s[None]
+        u, vh = (u[None], vh[None]) if u is not None else (None, None)
+    rows = []
+    for i, (x, (ur, sr, vhr)) in enumerate(zip(arrays, refs)):
+        dtype = np.complex128 if np.iscomplexobj(x) else np.float64
+        x = x.astype(dtype)
+        k = s.shape[-1]
+        si = s[i].astype(np.float64)
+        if not np.isfinite(si).all() or (u is not None and
+                                         (not np.isfinite(u[i]).all() or not np.isfinite(vh[i]).all())):
+            raise ValueError("Non-finite SVD output")
+        norm = np.linalg.norm(x)
+        denom = norm if norm > 0 else 1.0
+        top = sr[0] if sr[0] > 0 else 1.0
+        floor = np.finfo(np.float64).eps * max(x.shape) * top
+        resolved = sr[:k] > floor
+        d = {
+            "spectrum_error_over_sigma1": float(np.max(np.abs(si - sr[:k])) / top),
+            "singular_values_nonnegative_sorted": bool(np.all(si >= 0) and np.all(np.diff(si) <= 0)),
+            "resolved_spectrum_max_relative_error": float(np.max(np.abs(si[resolved] - sr[:k][resolved]) / sr[:k][resolved])) if resolved.any() else None,
+            "reference_tail_relative_fro": float(np.linalg.norm(sr[k:]) / denom),
+        }
+        if u is not None:
+            ui, vi = u[i].astype(dtype), vh[i].astype(dtype)
+            uk, vk = ui[:, :k], vi[:k, :]
+            residual = np.linalg.norm(x - (uk * si) @ vk) / denom
+            d.update({
+                "reconstruction_relative_fro": float(residual),
+                "orthogonality_u_fro_over_sqrt_cols": float(np.linalg.norm(ui.conj().T @ ui - np.eye(ui.shape[1])) / np.sqrt(ui.shape[1])),
+                "orthogonality_v_fro_over_sqrt_rows": float(np.linalg.norm(vi @ vi.conj().T - np.eye(vi.shape[0])) / np.sqrt(vi.shape[0])),
+            })
+        rows.append(d)
+    worst = {}
+    for key in rows[0]:
+        values = [r[key] for r in rows if r[key] is not None]
+        worst[key] = (all(values) if isinstance(values[0], bool) else max(values)) if values else None
+    return {"worst": worst, "per_matrix": rows}

@@ -1,0 +1,83 @@
+"""ctypes binding of the C ABI in include/jacobi_b200.h.
+
+The shared library is built in-tree by ``build.py``.  There is no CPU or
+PyTorch fallback: when the library is missing or a CUDA device is absent,
+``lib()`` raises and every solver call fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+from .build import library_path
+
+# Return codes and per-matrix status words (include/jacobi_b200.h).
+JB_OK, JB_EINVAL, JB_ETOOBIG, JB_EWORKSPACE, JB_ECUDA = 0, 1, 2, 3, 4
+ST_OK, ST_NOT_CONVERGED, ST_NONFINITE_IN, ST_NULL_FAILED, ST_NONFINITE_OUT, ST_BAD_DESC = 0, 1, 2, 3, 4, 5
+FULL_MATRICES, VALUES_ONLY = 1, 2
+PREC_NATIVE, PREC_MIXED = 0, 1
+
+RC_NAMES = {JB_EINVAL: "invalid argument", JB_ETOOBIG: "shape too large for this entry point",
+            JB_EWORKSPACE: "workspace missing or too small", JB_ECUDA: "CUDA runtime error"}
+
+# Exported symbols, in declaration order of include/jacobi_b200.h.
+SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_batched_f32",
+           "jb_svd_batched_f64", "jb_svd_uneven_f32")
+
+
+class MatrixDesc(ctypes.Structure):
+    """jb_matrix_desc: one matrix of an uneven batch (offsets in elements)."""
+    _fields_ = [("m", ctypes.c_int32), ("n", ctypes.c_int32), ("rank", ctypes.c_int32),
+                ("flags", ctypes.c_int32), ("a_off", ctypes.c_int64), ("u_off", ctypes.c_int64),
+                ("s_off", ctypes.c_int64), ("v_off", ctypes.c_int64)]
+
+
+DESC_BYTES = ctypes.sizeof(MatrixDesc)  # 48
+
+_lock = threading.Lock()
+_lib = None
+
+P, I32, I64, F64, SZ = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double, ctypes.c_size_t
+
+
+def _declare(l):
+    l.jb_version.restype = ctypes.c_int
+    l.jb_version.argtypes = []
+    l.jb_device_sm_count.restype = ctypes.c_int
+    l.jb_device_sm_count.argtypes = []
+    l.jb_workspace_bytes.restype = SZ
+    l.jb_workspace_bytes.argtypes = [I32, I32, I64, I32, I32, I32]
+    l.jb_svd_batched_f32.restype = ctypes.c_int
+    l.jb_svd_batched_f32.argtypes = [P, P, P, P, I64, I32, I32, I32, I32, F64, I32, I32, P, P, P, SZ, P]
+    l.jb_svd_batched_f64.restype = ctypes.c_int
+    l.jb_svd_batched_f64.argtypes = [P, P, P, P, I64, I32, I32, I32, I32, F64, I32, P, P, P, SZ, P]
+    l.jb_svd_uneven_f32.restype = ctypes.c_int
+    l.jb_svd_uneven_f32.argtypes = [P, P, P, P, P, P, I64, I32, I32, F64, I32, I32, P, P, P, SZ, P]
+    return l
+
+
+def load(path: Path | None = None):
+    """Load the shared library (no device needed).  Raises if it is missing."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            p = Path(path) if path else library_path()
+            if not p.exists():
+                raise RuntimeError(f"B200 Jacobi library not built: {p} is missing "
+                                   "(run pavel-s_svd_b200/build.py); there is no CPU fallback")
+            _lib = _declare(ctypes.CDLL(str(p)))
+        return _lib
+
+
+def lib():
+    """The loaded library, for compute calls: also requires a CUDA device."""
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("the B200 Jacobi solver needs a CUDA device; there is no CPU fallback")
+    return load()
+
+
+def check(rc: int, what: str):
+    if rc != JB_OK:
+        raise RuntimeError(f"{what} failed: {RC_NAMES.get(rc, rc)} (code {rc})")

@@ -1,0 +1,48 @@
+"""Shared fixtures.  `-m gpu` tests need a CUDA device and the built library;
+everything else runs on CPU."""
+import importlib
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+GOLDEN = ROOT / "tests" / "golden" / "reference_jacobi.npz"
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built sm_100a library")
+
+
+@pytest.fixture(scope="session")
+def pkg():
+    return importlib.import_module("pavel-s_svd_b200")
+
+
+@pytest.fixture(scope="session")
+def golden():
+    z = np.load(GOLDEN, allow_pickle=False)
+    names = [str(x) for x in z["_names"]]
+    cases = {}
+    for n in names:
+        c = {"a": z[f"{n}/a"], "s": z[f"{n}/s"], "sweeps": int(z[f"{n}/sweeps"]), "truth": z[f"{n}/truth"],
+             "kw": eval(str(z[f"{n}/kw"]))}
+        if f"{n}/u" in z.files:
+            c["u"], c["vh"] = z[f"{n}/u"], z[f"{n}/vh"]
+        cases[n] = c
+    return cases
+
+
+@pytest.fixture(scope="session")
+def workloads():
+    return importlib.import_module("pavel-s_svd_b200.workloads")
+
+
+def sigma_tol(dtype):
+    """Agreement bound on sigma (relative to sigma_1) between two correct
+    implementations: single precision 1e-5, double 1e-12."""
+    return 1e-5 if np.dtype(dtype) == np.float32 else 1e-12

@@ -1,0 +1,106 @@
+"""Generate the golden fixtures of the Jacobi path from the reference itself.
+
+Run once, in a container where uncle-Slava/Pavel-s_SVD is checked out (its
+path is given by REFERENCE_ROOT, default /root/reference):
+
+    python tests/golden/make_golden.py
+
+It imports the reference's ``svdbench.standalone.svd`` and
+``svdbench.matrices.make_matrix`` unchanged, runs ``svd(x, 'jacobi', ...)``
+on CPU (1 thread, as the reference's own tests do) and writes
+``tests/golden/reference_jacobi.npz``: for every case the input, the
+reference's U, s, Vh, jacobi_sweeps, and SciPy FP64 singular values.  The
+GPU box never runs this script; tests read only the .npz.
+"""
+from __future__ import annotations
+
+import hashlib
+import importlib.util
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+
+REF = Path(os.environ.get("REFERENCE_ROOT", "/root/reference"))
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parent.parent
+
+
+def _workloads():
+    spec = importlib.util.spec_from_file_location("workloads", REPO / "pavel-s_svd_b200" / "workloads.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def cases(make_matrix):
+    """(name, input array, svd kwargs) -- mirrors the reference's own test
+    inputs (tests/test_standalone.py:47-90, 187-207) in real dtypes, the
+    real-valued byte-exact corpus (corpus/standalone/*.npy) and samples of
+    the BASELINE workloads."""
+    out = []
+    for dt in ("float32", "float64"):
+        for m, n in ((13, 7), (7, 13)):
+            out.append((f"gauss_{dt}_{m}x{n}_b2", make_matrix(dict(m=m, n=n, batch=2, dtype=dt, family="gaussian")), {}))
+    special = [np.zeros((9, 5)), np.eye(7), np.diag([0., 2., 0., 3., 1.]),
+               make_matrix(dict(m=15, n=7, dtype="float64", family="low_rank", rank=3, tail=0)),
+               make_matrix(dict(m=15, n=7, dtype="float64", family="clustered"))]
+    base = make_matrix(dict(m=11, n=5, dtype="float64", family="gaussian"))
+    special += [base * 1e-150, base * 1e150]
+    for i, a in enumerate(special):
+        out.append((f"special{i}", np.ascontiguousarray(a), {}))
+    for shape in ((1, 1), (8, 1), (1, 8), (10, 4), (4, 10)):
+        a = make_matrix(dict(m=shape[0], n=shape[1], family="gaussian", dtype="float64"))
+        out.append((f"full_{shape[0]}x{shape[1]}", a, {"full_matrices": True}))
+        out.append((f"values_{shape[0]}x{shape[1]}", a, {"values_only": True}))
+    out.append(("geometric_24x9", make_matrix(dict(m=24, n=9, dtype="float64", family="geometric", condition=1e8)), {}))
+    out.append(("multidim_2x3x9x5", np.random.default_rng(22).normal(size=(2, 3, 9, 5)), {}))
+    out.append(("rank4_of_13x7", make_matrix(dict(m=13, n=7, dtype="float32", family="gaussian")), {"rank": 4}))
+    out.append(("full_f32_12x5", make_matrix(dict(m=12, n=5, dtype="float32", family="low_rank", rank=2, tail=0)),
+                {"full_matrices": True}))
+    corpus = REF / "corpus" / "standalone"
+    for name in ("square32", "tall256x16", "batch8x16", "condition1e8", "condition1e12", "rank_deficient", "zero",
+                 "square64", "tall2048x32"):
+        p = corpus / f"{name}.npy"
+        if p.exists():
+            out.append((f"corpus_{name}", np.load(p, allow_pickle=False), {}))
+    wl = _workloads()
+    out.append(("plain_single_256x128", wl.plain_single(), {"tol": 1e-6, "max_sweeps": 30}))
+    for i, a in enumerate(wl.uneven_batch(48)):
+        out.append((f"uneven_{i:02d}", a, {}))
+    return out
+
+
+def main():
+    sys.path.insert(0, str(REF))
+    import torch
+    import scipy.linalg
+    from svdbench.standalone import svd
+    from svdbench.matrices import make_matrix
+    torch.set_num_threads(1)
+    blob = {}
+    names = []
+    for name, a, kw in cases(make_matrix):
+        a = np.ascontiguousarray(a)
+        u, s, vh, info = svd(torch.from_numpy(a.copy()), "jacobi", return_info=True, **kw)
+        flat = a.reshape(-1, *a.shape[-2:]).astype(np.float64)
+        truth = np.stack([scipy.linalg.svd(x, compute_uv=False, lapack_driver="gesvd") for x in flat])
+        blob[f"{name}/a"] = a
+        blob[f"{name}/s"] = s.numpy()
+        if u is not None and a.size <= 20000:
+            blob[f"{name}/u"] = u.numpy()
+            blob[f"{name}/vh"] = vh.numpy()
+        blob[f"{name}/sweeps"] = np.array(info["jacobi_sweeps"])
+        blob[f"{name}/truth"] = truth
+        blob[f"{name}/kw"] = np.array(repr(kw))
+        blob[f"{name}/sha256"] = np.array(hashlib.sha256(a.tobytes(order="C")).hexdigest())
+        names.append(name)
+        print(f"{name:28s} {str(a.shape):18s} {a.dtype}  sweeps={info['jacobi_sweeps']}")
+    blob["_names"] = np.array(names)
+    np.savez_compressed(HERE / "reference_jacobi.npz", **blob)
+    print("wrote", HERE / "reference_jacobi.npz")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,64 @@
+"""The C-ABI library loads and exports every entry point include/*.h
+declares -- CPU only, no compute calls."""
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols():
+    names = []
+    for h in sorted((ROOT / "include").glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names += re.findall(r"JB_API\s+[\w\s\*]+?\b(jb_\w+)\s*\(", text)
+    return names
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    assert "jb_svd_batched_f32" in names and "jb_svd_uneven_f32" in names
+    assert len(names) == len(set(names))
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    lib = pkg.native.load()
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+    assert tuple(n for n in declared_symbols() if n in pkg.native.SYMBOLS) == tuple(
+        n for n in pkg.native.SYMBOLS if n in declared_symbols())
+
+
+def test_library_is_sm100a_and_torch_free(pkg):
+    import subprocess
+    so = pkg.native.load()._name
+    deps = subprocess.run(["ldd", so], capture_output=True, text=True).stdout
+    assert "torch" not in deps and "c10" not in deps
+
+
+def test_workspace_query_is_host_only(pkg):
+    lib = pkg.native.load()
+    assert lib.jb_version() >= 100
+    small = lib.jb_workspace_bytes(128, 64, 8192, 4, 1, 0)
+    assert 0 < small < 1 << 20
+    assert lib.jb_workspace_bytes(0, 4, 1, 4, 0, 0) == 0
+    assert lib.jb_workspace_bytes(4, 4, 1, 3, 0, 0) == 0
+
+
+def test_descriptor_layout_matches_header(pkg):
+    B = __import__("importlib").import_module("pavel-s_svd_b200.batch")
+    assert pkg.native.DESC_BYTES == 48 == B.DESC_DTYPE.itemsize
+    assert pkg.native.MatrixDesc.a_off.offset == 16
+
+
+def test_argument_errors_return_codes_without_a_device(pkg):
+    lib = pkg.native.load()
+    # rank 0 and max_sweeps 0 are rejected before any CUDA call
+    assert lib.jb_svd_batched_f32(None, None, None, None, 1, 4, 4, 0, 0, 0.0, 30, 0, None, None, None, 0,
+                                  None) == pkg.native.JB_EINVAL
+    assert lib.jb_svd_batched_f64(None, None, None, None, 1, 4, 4, 4, 0, 0.0, 0, None, None, None, 0,
+                                  None) == pkg.native.JB_EINVAL
+    assert lib.jb_svd_uneven_f32(None, None, None, None, None, None, 1, 4, 4, 0.0, 30, 0, None, None, None, 0,
+                                 None) == pkg.native.JB_EINVAL

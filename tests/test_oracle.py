@@ -1,0 +1,145 @@
+"""The oracle against the reference's own outputs (golden fixtures made by
+tests/golden/make_golden.py from uncle-Slava/Pavel-s_SVD) -- CPU only."""
+import numpy as np
+import pytest
+
+from oracle import jacobi_oracle as O
+from oracle import c_oracle as C
+from conftest import sigma_tol
+
+
+def _cmp_sigma(s, ref, dtype, factor=1.0):
+    s = np.asarray(s, np.float64).reshape(ref.shape)
+    top = max(float(np.abs(ref).max()), np.finfo(np.float64).tiny)
+    err = float(np.abs(s - ref).max()) / top
+    assert err <= factor * sigma_tol(dtype), err
+    return err
+
+
+def _cmp_vectors(u, ref, s, dtype, axis):
+    """Columns (axis=-1) or rows (axis=-2) agree up to sign where the singular
+    value is simple (gap > 1e-3 relative); returns max deviation."""
+    ref = np.asarray(ref, np.float64)
+    ref = ref.reshape(-1, *ref.shape[-2:])
+    u = np.asarray(u, np.float64).reshape(ref.shape)
+    tol = 1e-3 if np.dtype(dtype) == np.float32 else 1e-8
+    s = np.asarray(s, np.float64).reshape(ref.shape[0], -1)
+    worst = 0.0
+    for b in range(u.shape[0]):
+        sb = s[b]
+        ncols = ref.shape[-1] if axis == -1 else ref.shape[-2]
+        for j in range(min(len(sb), ncols)):
+            gap = min([abs(sb[j] - sb[i]) for i in range(len(sb)) if i != j] or [np.inf])
+            if sb[j] == 0 or gap <= 1e-3 * sb[0]:
+                continue
+            x = u[b][:, j] if axis == -1 else u[b][j, :]
+            y = ref[b][:, j] if axis == -1 else ref[b][j, :]
+            d = min(np.abs(x - y).max(), np.abs(x + y).max())
+            worst = max(worst, d)
+    assert worst <= tol, worst
+    return worst
+
+
+def test_numpy_oracle_matches_reference(golden):
+    for name, c in golden.items():
+        a = c["a"]
+        u, s, vh, info = O.svd(a, "jacobi", return_info=True, **c["kw"])
+        _cmp_sigma(s, c["s"], a.dtype)
+        if a.dtype == np.float64:
+            assert info["jacobi_sweeps"] == c["sweeps"], name
+        else:
+            assert abs(info["jacobi_sweeps"] - c["sweeps"]) <= 1, name
+        if "u" in c and u is not None:
+            _cmp_vectors(u, c["u"], c["s"], a.dtype, -1)
+            _cmp_vectors(vh, c["vh"], c["s"], a.dtype, -2)
+
+
+def _c_oracle(a, kw):
+    x = a.reshape(-1, *a.shape[-2:])
+    rank = kw.get("rank")
+    u, s, vh, sweeps, status = C.svd_batched(x, rank=rank, full_matrices=kw.get("full_matrices", False),
+                                             values_only=kw.get("values_only", False), tol=kw.get("tol"),
+                                             max_sweeps=kw.get("max_sweeps", 60))
+    return u, s, vh, sweeps, status
+
+
+def test_c_oracle_matches_reference(golden):
+    for name, c in golden.items():
+        a = c["a"]
+        u, s, vh, sweeps, status = _c_oracle(a, c["kw"])
+        assert (status == 0).all(), name
+        _cmp_sigma(s, c["s"], a.dtype)
+        if a.dtype == np.float64:
+            assert int(sweeps.max()) == c["sweeps"], name
+        else:
+            assert abs(int(sweeps.max()) - c["sweeps"]) <= 1, name
+        if "u" in c and u is not None:
+            _cmp_vectors(u.reshape(c["u"].shape), c["u"], c["s"], a.dtype, -1)
+            _cmp_vectors(vh.reshape(c["vh"].shape), c["vh"], c["s"], a.dtype, -2)
+
+
+def test_oracle_pins_reference_sweeps_of_corpus(golden):
+    """Sweep counts the reference recorded for the byte-exact corpus
+    (results/standalone-hetzner.jsonl lines 5, 23, 59, 77, 95, 131, 149)."""
+    recorded = {"corpus_square32": 8, "corpus_tall256x16": 6, "corpus_batch8x16": 7, "corpus_condition1e8": 12,
+                "corpus_condition1e12": 14, "corpus_rank_deficient": 5, "corpus_zero": 1}
+    for name, sw in recorded.items():
+        assert golden[name]["sweeps"] == sw, name
+        _, _, _, sweeps, _ = _c_oracle(golden[name]["a"], {})
+        assert int(sweeps.max()) == sw, name
+
+
+def test_corpus_inputs_are_the_reference_bytes(golden):
+    """SHA-256 prefixes recorded by the reference (results/standalone-hetzner.jsonl)."""
+    import hashlib
+    recorded = {"corpus_square32": "52d63f80514ec9f0", "corpus_tall256x16": "d6e0fa184b2d7ebd",
+                "corpus_batch8x16": "64f1e958765e61c4", "corpus_condition1e8": "f4e8c3c129a2e86f",
+                "corpus_condition1e12": "d3e0049c7534acfe", "corpus_rank_deficient": "d929a6987cec069d",
+                "corpus_zero": "a1a4f5721c1c4610", "corpus_tall2048x32": "d9e8b9afed4d1eb6"}
+    for name, h in recorded.items():
+        assert hashlib.sha256(golden[name]["a"].tobytes()).hexdigest().startswith(h), name
+
+
+def test_oracle_errors_follow_reference():
+    a = np.random.default_rng(0).normal(size=(12, 9))
+    with pytest.raises(RuntimeError):
+        O.svd(a, "jacobi", max_sweeps=1)
+    with pytest.raises(ValueError):
+        O.svd(a * np.nan)
+    with pytest.raises(ValueError):
+        O.svd(a, rank=0)
+    with pytest.raises(TypeError):
+        O.svd(a.astype(np.int32))
+    _, _, _, _, status = C.svd_batched(a[None], max_sweeps=1)
+    assert status[0] == 1
+    _, _, _, _, status = C.svd_batched((a * np.nan)[None])
+    assert status[0] == 2
+
+
+def test_c_oracle_uneven_matches_batched(workloads):
+    import importlib
+    B = importlib.import_module("pavel-s_svd_b200.batch")
+    mats = workloads.uneven_batch(24)
+    flat, m, n, a_off = B.pack(mats)
+    k = np.minimum(m, n)
+    desc = np.zeros(len(mats), B.DESC_DTYPE)
+    desc["m"], desc["n"], desc["rank"] = m, n, k
+    desc["a_off"] = a_off
+    desc["u_off"], _ = B._aligned_offsets(m * k)
+    desc["s_off"], _ = B._aligned_offsets(k)
+    desc["v_off"], _ = B._aligned_offsets(k * n)
+    u, s, vh, sweeps, status = C.svd_uneven(flat.numpy(), desc)
+    assert (status == 0).all()
+    for i, a in enumerate(mats):
+        _, s1, _, sw1, _ = C.svd_batched(a[None])
+        so = desc["s_off"][i]
+        np.testing.assert_array_equal(s[so:so + k[i]], s1[0])
+        assert sweeps[i] == sw1[0]
+
+
+def test_oracle_threads_do_not_change_results(workloads):
+    x = np.stack(workloads.uneven_batch(1) * 6)
+    r1 = C.svd_batched(x, threads=1)
+    r4 = C.svd_batched(x, threads=4)
+    for p, q in zip(r1, r4):
+        np.testing.assert_array_equal(p, q)
