@@ -53,6 +53,10 @@ extern "C" {
 /* ---- flags ---------------------------------------------------------------- */
 #define JB_FULL_MATRICES    1   /* U is m x m and Vh is n x n (complete_basis)  */
 #define JB_VALUES_ONLY      2   /* write S only; U and Vh may be NULL           */
+#define JB_ROUND_ROBIN      4   /* sweep in the reference's round-robin pair
+                                   order (primitives.py:309-313) instead of the
+                                   register-blocked order; same results within
+                                   rounding, slower                             */
 
 /* ---- arithmetic of the solve ------------------------------------------- */
 #define JB_PREC_NATIVE      0   /* sweeps in the input precision (f32 or f64)   */
@@ -64,12 +68,15 @@ extern "C" {
 /* One matrix of an uneven batch.  A is row-major m x n at A + a_off.
  * Outputs (row-major): U at U + u_off (m x ucols), S at S + s_off (k values),
  * Vh at Vh + v_off (vrows x n), where k = rank, ucols = vrows = rank, or with
- * JB_FULL_MATRICES ucols = m, vrows = n.  Offsets count elements. */
+ * JB_FULL_MATRICES ucols = m, vrows = n.  Offsets count elements.
+ * x_off: offset (in floats) of this matrix's min(m,n)^2 scratch floats inside
+ * the workspace scratch area (used by JB_PREC_MIXED only). */
 typedef struct jb_matrix_desc {
     int32_t m, n;
     int32_t rank;       /* 1 <= rank <= min(m, n) */
-    int32_t flags;      /* JB_FULL_MATRICES | JB_VALUES_ONLY */
+    int32_t flags;      /* JB_FULL_MATRICES | JB_VALUES_ONLY | JB_ROUND_ROBIN */
     int64_t a_off, u_off, s_off, v_off;
+    int64_t x_off;
 } jb_matrix_desc;
 
 /* Library version (major*10000 + minor*100 + patch). */
@@ -78,9 +85,11 @@ JB_API int jb_version(void);
 /* Number of streaming multiprocessors of the current device, or -1. */
 JB_API int jb_device_sm_count(void);
 
-/* Bytes of device workspace that jb_svd_batched_* / jb_svd_uneven_f32 need
- * for matrices up to max_m x max_n (either orientation), `count` matrices,
- * the given precision and flags.  0 is a valid answer. */
+/* Bytes of device workspace that jb_svd_batched_* need for `count` matrices
+ * of max_m x max_n (either orientation), the given precision and flags.
+ * jb_svd_uneven_f32 needs this for its largest shape plus, with
+ * JB_PREC_MIXED, 4 bytes per scratch float addressed by the descriptors'
+ * x_off (see jb_svd_uneven_f32). */
 JB_API size_t jb_workspace_bytes(int32_t max_m, int32_t max_n, int64_t count,
                           int32_t elem_bytes, int32_t precision, int32_t flags);
 
@@ -102,11 +111,15 @@ JB_API int jb_svd_batched_f64(const double *A, double *U, double *S, double *Vh,
                        int32_t *sweeps, int32_t *status,
                        void *workspace, size_t workspace_bytes, void *stream);
 
-/* Uneven batch in ONE persistent launch.  descs: `count` device descriptors;
- * order: optional device permutation of [0, count) giving the processing
- * order (largest cost first balances the persistent grid), or NULL.
- * max_m/max_n bound every descriptor (either orientation).  Replaces a
- * harness loop of svd(x, 'jacobi') over matrices of different shapes. */
+/* Uneven batch in ONE persistent launch per precision phase.  descs: `count`
+ * device descriptors; order: optional device permutation of [0, count)
+ * giving the processing order (largest cost first balances the persistent
+ * grid), or NULL.  max_m/max_n bound every descriptor (either orientation).
+ * Workspace: jb_workspace_bytes(max_m, max_n, count, 4, precision, 0) bytes,
+ * followed (JB_PREC_MIXED) by the scratch floats the descriptors' x_off
+ * address; a descriptor whose scratch does not fit gets JB_ST_BAD_DESC.
+ * Replaces a harness loop of svd(x, 'jacobi') over matrices of different
+ * shapes. */
 JB_API int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh,
                       const jb_matrix_desc *descs, const int32_t *order,
                       int64_t count, int32_t max_m, int32_t max_n,

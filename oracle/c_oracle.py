@@ -20,8 +20,13 @@ _lib = None
 
 
 def build(force=False):
-    if force or not LIB.exists():
+    """make -C oracle (rebuilds when the sources or include/jacobi_b200.h
+    changed).  Without make/gcc an existing library is used as is."""
+    try:
         subprocess.run(["make", "-s", "-C", str(HERE)] + (["-B"] if force else []), check=True)
+    except (OSError, subprocess.CalledProcessError):
+        if not LIB.exists():
+            raise
     return LIB
 
 

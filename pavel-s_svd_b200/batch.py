@@ -17,7 +17,8 @@ from . import native as N
 from .solvers import raise_for_status
 
 DESC_DTYPE = np.dtype([("m", "<i4"), ("n", "<i4"), ("rank", "<i4"), ("flags", "<i4"),
-                       ("a_off", "<i8"), ("u_off", "<i8"), ("s_off", "<i8"), ("v_off", "<i8")])
+                       ("a_off", "<i8"), ("u_off", "<i8"), ("s_off", "<i8"), ("v_off", "<i8"),
+                       ("x_off", "<i8")])
 assert DESC_DTYPE.itemsize == N.DESC_BYTES
 
 
@@ -63,7 +64,10 @@ class UnevenBatch:
         self.m = np.asarray(m, np.int64)
         self.n = np.asarray(n, np.int64)
         self.count = len(self.m)
-        self.device = torch.device(device)
+        dev = torch.device(device)
+        if dev.type == "cuda" and dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
         self.tol = float(tol or 0.0)
         self.max_sweeps = int(max_sweeps)
         if precision not in ("mixed", "fp32"):
@@ -76,25 +80,31 @@ class UnevenBatch:
         self.u_off, ut = _aligned_offsets(self.m * k)
         self.s_off, st = _aligned_offsets(k)
         self.v_off, vt = _aligned_offsets(k * self.n)
+        self.x_off, xt = _aligned_offsets(k * k)
         self.values_only = values_only
         desc = np.zeros(self.count, DESC_DTYPE)
         desc["m"], desc["n"], desc["rank"] = self.m, self.n, k
         desc["flags"] = N.VALUES_ONLY if values_only else 0
         desc["a_off"], desc["u_off"], desc["s_off"], desc["v_off"] = self.a_off, self.u_off, self.s_off, self.v_off
+        desc["x_off"] = self.x_off
         dev = self.device
         self.desc = torch.from_numpy(desc.view(np.uint8).copy()).to(dev)
         self.order_host = cost_order(self.m, self.n) if order == "cost" else np.arange(self.count, dtype=np.int32)
         self.order = torch.from_numpy(self.order_host).to(dev)
         self.max_m = int(max(self.m.max(), self.n.max())) if self.count else 1
         self.max_n = int(np.minimum(self.m, self.n).max()) if self.count else 1
-        self.U = None if values_only else torch.empty(max(ut, 1), dtype=torch.float32, device=dev)
-        self.S = torch.empty(max(st, 1), dtype=torch.float32, device=dev)
-        self.Vh = None if values_only else torch.empty(max(vt, 1), dtype=torch.float32, device=dev)
+        self.U = None if values_only else torch.zeros(max(ut, 1), dtype=torch.float32, device=dev)
+        self.S = torch.zeros(max(st, 1), dtype=torch.float32, device=dev)
+        self.Vh = None if values_only else torch.zeros(max(vt, 1), dtype=torch.float32, device=dev)
         self.info = torch.zeros(2, max(self.count, 1), dtype=torch.int32, device=dev)
         lib = N.lib()
-        ws = lib.jb_workspace_bytes(self.max_m, self.max_n, self.count, 4, self.precision, 0)
+        # Workspace: the base area (ticket counters) followed, in mixed
+        # precision, by the scratch floats the descriptors' x_off address.
+        base = lib.jb_workspace_bytes(self.max_m, self.max_n, self.count, 4, N.PREC_NATIVE, 0)
+        ws = base + (4 * xt if self.precision == N.PREC_MIXED else 0)
         self.workspace = torch.empty(max(int(ws), 256), dtype=torch.uint8, device=dev)
-        self.launches_per_solve = 2  # memset of the work ticket + the persistent kernel
+        # memset of the work tickets + one persistent kernel per precision phase
+        self.kernels_per_solve = 2 if self.precision == N.PREC_MIXED else 1
 
     # -- solving ----------------------------------------------------------------
     def launch(self, a_flat: torch.Tensor, stream=None):

@@ -14,6 +14,7 @@
 #include <string.h>
 #include "jacobi_b200.h"
 #include "jb_device.cuh"
+#include "jb_regblock.cuh"
 
 namespace jb {
 
@@ -54,7 +55,7 @@ __host__ __device__ inline size_t aux_bytes(const Dims &d) {
     const int npairs = d.np / 2;
     const int vecn = (d.mt > d.ncp ? d.mt : d.ncp) + 32;
     return align16((size_t)3 * npairs * 8) + align16((size_t)d.np * 8) + align16((size_t)vecn * 8) +
-           align16((size_t)d.np * 8) + align16((size_t)d.np * 4) + align16(32 * 8) + align16(4 * 4);
+           align16((size_t)d.np * 8) + align16((size_t)d.np * 4) + align16(64 * 8) + align16(4 * 4);
 }
 
 __device__ inline Aux carve_aux(unsigned char *base, const Dims &d) {
@@ -67,7 +68,7 @@ __device__ inline Aux carve_aux(unsigned char *base, const Dims &d) {
     a.vec = (double *)p; p += align16((size_t)vecn * 8);
     a.tau = (double *)p; p += align16((size_t)d.np * 8);
     a.perm = (int *)p; p += align16((size_t)d.np * 4);
-    a.red = (double *)p; p += align16(32 * 8);
+    a.red = (double *)p; p += align16(64 * 8);
     a.flag = (int *)p;
     return a;
 }
@@ -85,9 +86,13 @@ struct Params {
     int32_t max_sweeps32;
     int32_t *sweeps, *status;
     int *counter;                 // NULL: static grid-stride schedule
+    int *counter2;                // ticket of the second (FP64) kernel
     unsigned char *gws;           // NULL: work area in shared memory
     size_t gws_stride;
     Dims maxd;                    // sizing of aux / region (largest matrix)
+    float *x32;                   // mixed scratch (V of the FP32 phase)
+    int64_t x_cap;                // floats available at x32
+    size_t region_cap;            // bytes of the shared-memory work area
 };
 
 __device__ inline jb_matrix_desc desc_of(const Params &p, int64_t mat) {
@@ -100,6 +105,8 @@ __device__ inline jb_matrix_desc desc_of(const Params &p, int64_t mat) {
     d.u_off = mat * (int64_t)p.um * ucols;
     d.s_off = mat * (int64_t)p.urank;
     d.v_off = mat * vrows * (int64_t)p.un;
+    const int64_t nt = p.um < p.un ? p.um : p.un;
+    d.x_off = mat * nt * nt;
     return d;
 }
 
@@ -223,6 +230,337 @@ __global__ void __launch_bounds__(1024, 1) batched_kernel(Params p) {
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Register-tile path (matrices up to 128 x 64 in their tall view).
+// ---------------------------------------------------------------------------
+constexpr int kB32 = 4;   // block width of the FP32 sweeps (8 warps for 64 columns)
+constexpr int kB64 = 2;   // block width of the FP64 sweeps (16 warps for 64 columns)
+constexpr int kT32 = 256, kT64 = 512;  // threads of the two kernels
+constexpr int kMaxR = 4;  // rows per lane: mt <= 128
+constexpr int kMaxRV = 2; // V rows per lane: padded width <= 64
+
+struct RGeo {
+    int R, RV, nb, npb, live, ldw, ldv, ncp;
+};
+
+__host__ __device__ inline RGeo rgeo(int mt, int nt, int B, int flags) {
+    RGeo r;
+    r.R = (mt + 31) / 32;
+    r.nb = 2 * ((nt + 2 * B - 1) / (2 * B));
+    r.npb = r.nb * B;
+    r.RV = (r.npb + 31) / 32;
+    r.live = (nt + B - 1) / B;
+    r.ldw = 32 * r.R;
+    r.ldv = 32 * r.RV;
+    r.ncp = (flags & JB_FULL_MATRICES) ? r.npb + (mt - nt) : r.npb;
+    return r;
+}
+
+__host__ __device__ inline size_t rregion_bytes(const RGeo &r, int elem) {
+    return align16((size_t)r.ldw * r.ncp * elem) + align16((size_t)r.ldv * r.npb * elem);
+}
+
+// FP64 polish of a float32 matrix: W | V | X1 (npb x npb doubles) | X2
+// (npb x npb doubles, or the float32 staging of A, ldw x nt).
+__host__ __device__ inline size_t xbytes(const RGeo &r, int nt) {
+    const size_t a = (size_t)r.ldw * nt * 4, b = (size_t)r.ldv * r.npb * 8;
+    return align16(a > b ? a : b);
+}
+__host__ __device__ inline size_t rregion_mixed64(const RGeo &r, int nt) {
+    return rregion_bytes(r, 8) + align16((size_t)r.ldv * r.npb * 8) + xbytes(r, nt);
+}
+
+// Aux sizing for the register path: np -> padded width, mt -> row stride.
+__host__ __device__ inline Dims raux_dims(const RGeo &r) {
+    Dims d;
+    d.mt = r.ldw; d.nt = r.npb; d.np = r.npb; d.ncp = r.ncp; d.ldw = r.ldw; d.ldv = r.ldv;
+    return d;
+}
+
+__device__ inline bool rdesc_fits(const jb_matrix_desc &d, int B, int elem, const Params &p, bool mixed_scratch) {
+    if (d.m < 1 || d.n < 1) return false;
+    const int mt = d.m > d.n ? d.m : d.n, nt = d.m > d.n ? d.n : d.m;
+    if (d.rank < 1 || d.rank > nt) return false;
+    if ((d.flags & JB_FULL_MATRICES) && d.rank != nt) return false;
+    const RGeo r = rgeo(mt, nt, B, d.flags);
+    if (r.R > kMaxR || r.RV > kMaxRV) return false;
+    const size_t need = (mixed_scratch && elem == 8) ? rregion_mixed64(r, nt) : rregion_bytes(r, elem);
+    if (need > p.region_cap) return false;
+    if (r.ldw > p.maxd.mt || r.npb > p.maxd.np || r.ncp > p.maxd.ncp) return false;
+    if (mixed_scratch && (d.x_off < 0 || d.x_off + (int64_t)nt * nt > p.x_cap)) return false;
+    return true;
+}
+
+template <typename T>
+__device__ void zero_fill(T *X, size_t count) {
+    for (size_t i = threadIdx.x; i < count; i += blockDim.x) X[i] = T(0);
+}
+
+// W = scaled tall view of A (rows < mt, cols < nt); the rest of W and V must
+// already be zero.  V = I on the padded width.
+template <typename T, typename TI>
+__device__ void load_padded(const TI *A, const Geo &g, const RGeo &r, int e, T *W, T *V) {
+    const int total = g.m * g.n;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int row = idx / g.n, col = idx - row * g.n;
+        const int i = g.wide ? col : row, j = g.wide ? row : col;
+        W[(size_t)j * r.ldw + i] = dscale((T)A[idx], -e);
+    }
+    for (int j = threadIdx.x; j < r.npb; j += blockDim.x) V[(size_t)j * r.ldv + j] = T(1);
+}
+
+template <typename T, int B>
+__device__ int rb_dispatch(const RGeo &r, T *W, T *V, T tol, int max_sweeps, bool confirm, double *red,
+                           bool &conv) {
+    return rb_sweeps<T, B, kMaxR, kMaxRV>(W, r.ldw, V, r.ldv, r.nb, r.live, tol, max_sweeps, confirm, red, conv);
+}
+
+__device__ inline Geo reg_geo(const jb_matrix_desc &d, const RGeo &r) {
+    Geo g = make_geo(d.m, d.n, d.rank, d.flags);
+    g.np = r.npb;  // physical width (extra full-basis columns follow it)
+    g.ncp = r.ncp;
+    g.ldw = r.ldw;
+    g.ldv = r.ldv;
+    return g;
+}
+
+__device__ inline bool next_ticket(int *counter, int &s_idx, int64_t &idx) {
+    if (threadIdx.x == 0) s_idx = atomicAdd(counter, 1);
+    __syncthreads();
+    idx = s_idx;
+    __syncthreads();
+    return true;
+}
+
+// K1: FP32 sweeps.  MIXED: store the FP32 V (nt x nt) in the scratch for K2;
+// else run the epilogue and write U, S, Vh.
+template <bool MIXED>
+__global__ void __launch_bounds__(kT32) rb32_kernel(Params p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_idx;
+    Aux ax = carve_aux(smem, p.maxd);
+    unsigned char *region = smem + aux_bytes(p.maxd);
+    for (;;) {
+        int64_t idx;
+        next_ticket(p.counter, s_idx, idx);
+        if (idx >= p.count) break;
+        const int64_t mat = p.order ? (int64_t)p.order[idx] : idx;
+        const jb_matrix_desc d = desc_of(p, mat);
+        if (threadIdx.x < 4) ax.flag[threadIdx.x] = 0;
+        __syncthreads();
+        int ns = 0, st = JB_ST_OK;
+        if (!rdesc_fits(d, kB32, 4, p, MIXED)) {
+            st = JB_ST_BAD_DESC;
+        } else {
+            const RGeo r = rgeo(d.m > d.n ? d.m : d.n, d.m > d.n ? d.n : d.m, kB32, d.flags);
+            const Geo g = reg_geo(d, r);
+            const float *A = (const float *)p.A + d.a_off;
+            float *W = (float *)region;
+            float *V = (float *)(region + align16((size_t)r.ldw * r.ncp * 4));
+            bool bad;
+            const int e = scan_input(A, g.m * g.n, ax, bad);
+            if (bad) {
+                st = JB_ST_NONFINITE_IN;
+            } else {
+                zero_fill(W, (size_t)r.ldw * r.ncp);
+                zero_fill(V, (size_t)r.ldv * r.npb);
+                __syncthreads();
+                load_padded(A, g, r, e, W, V);
+                __syncthreads();
+                const float tol = MIXED ? (p.tol32 > 0 ? (float)p.tol32 : 10.0f * Lim<float>::eps())
+                                        : (p.tol > 0 ? (float)p.tol : 10.0f * Lim<float>::eps());
+                bool conv;
+                ns = rb_dispatch<float, kB32>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true, ax.red, conv);
+                if (MIXED) {
+                    float *x = p.x32 + d.x_off;
+                    const int nt = g.nt;
+                    for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) {
+                        const int c = k / nt, i = k - c * nt;
+                        x[k] = V[(size_t)c * r.ldv + i];
+                    }
+                } else if (!conv) {
+                    st = JB_ST_NOT_CONVERGED;
+                } else {
+                    float *U = p.U ? (float *)p.U + d.u_off : nullptr;
+                    float *Vh = p.Vh ? (float *)p.Vh + d.v_off : nullptr;
+                    st = epilogue<float, float>(W, V, g, e, U, (float *)p.S + d.s_off, Vh, ax);
+                }
+            }
+        }
+        if (threadIdx.x == 0) {
+            if (p.status) p.status[mat] = st;
+            if (p.sweeps) p.sweeps[mat] = ns;
+        }
+        __syncthreads();
+    }
+}
+
+
+// C (M x N) = alpha * A (M x K) * B (K x N), column-major, in shared memory;
+// M and N multiples of 4.  Each thread owns 4 x 4 tiles of C, consecutive
+// lanes take consecutive row tiles (contiguous A loads, B loads broadcast).
+template <typename TA>
+__device__ void gemm_nn(double *C, int ldc, const TA *A, int lda, const double *B, int ldb, int M, int N, int K,
+                        double alpha) {
+    const int tm = M >> 2, tn = N >> 2;
+    for (int t = threadIdx.x; t < tm * tn; t += blockDim.x) {
+        const int i0 = (t % tm) << 2, j0 = (t / tm) << 2;
+        double acc[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+        for (int k = 0; k < K; ++k) {
+            double a[4], b[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) a[r] = (double)A[(size_t)k * lda + i0 + r];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) b[c] = B[(size_t)(j0 + c) * ldb + k];
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) C[(size_t)(j0 + c) * ldc + i0 + r] = alpha * acc[r][c];
+    }
+}
+
+// V <- V (3I - V^T V) / 2 (Newton-Schulz step towards the orthogonal polar
+// factor of V), n x n with ld; VT, H, Vn: n x n scratch (ld).  Returns
+// max |V^T V - I| before the step.
+__device__ double polar_step(double *V, int n, int ld, double *VT, double *H, double *Vn, Aux &ax) {
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+        const int c = k / n, i = k - c * n;
+        VT[(size_t)i * ld + c] = V[(size_t)c * ld + i];
+    }
+    __syncthreads();
+    gemm_nn<double>(H, ld, VT, ld, V, ld, n, n, n, 1.0);
+    __syncthreads();
+    double err = 0.0;
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+        const int c = k / n, i = k - c * n;
+        const double g = H[(size_t)c * ld + i];
+        const double e = g - (i == c ? 1.0 : 0.0);
+        err = fmax(err, fabs(e));
+        H[(size_t)c * ld + i] = (i == c ? 1.0 : 0.0) - 0.5 * e;  // (3I - G) / 2
+    }
+    err = block_max(err, ax.red);
+    gemm_nn<double>(Vn, ld, V, ld, H, ld, n, n, n, 1.0);
+    __syncthreads();
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+        const int c = k / n, i = k - c * n;
+        V[(size_t)c * ld + i] = Vn[(size_t)c * ld + i];
+    }
+    __syncthreads();
+    return err;
+}
+
+// K2: FP64 sweeps.  MIXED (TI = float): start from the FP32 V of K1, made
+// orthogonal to FP64 accuracy by Newton-Schulz polar steps (it is orthogonal
+// to ~1e-5 already), with W = A V recomputed in FP64 from the exact input;
+// native (TI = double): start from V = I.  Runs the epilogue and writes U,
+// S, Vh in TI.
+template <typename TI, bool MIXED>
+__global__ void __launch_bounds__(kT64) rb64_kernel(Params p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_idx;
+    Aux ax = carve_aux(smem, p.maxd);
+    unsigned char *region = smem + aux_bytes(p.maxd);
+    for (;;) {
+        int64_t idx;
+        next_ticket(MIXED ? p.counter2 : p.counter, s_idx, idx);
+        if (idx >= p.count) break;
+        const int64_t mat = p.order ? (int64_t)p.order[idx] : idx;
+        const jb_matrix_desc d = desc_of(p, mat);
+        if (threadIdx.x < 4) ax.flag[threadIdx.x] = 0;
+        __syncthreads();
+        int prev = JB_ST_OK, s1 = 0;
+        if (MIXED && threadIdx.x == 0) { ax.flag[3] = p.status[mat]; ax.flag[2] = p.sweeps[mat]; }
+        __syncthreads();
+        if (MIXED) { prev = ax.flag[3]; s1 = ax.flag[2]; }
+        __syncthreads();
+        if (threadIdx.x == 0) ax.flag[2] = 0;
+        __syncthreads();
+        if (prev != JB_ST_OK) continue;  // K1 already reported this matrix
+        int ns = s1, st = JB_ST_OK;
+        if (!rdesc_fits(d, kB64, 8, p, MIXED)) {
+            st = JB_ST_BAD_DESC;
+        } else {
+            const int mt = d.m > d.n ? d.m : d.n, nt = d.m > d.n ? d.n : d.m;
+            const RGeo r = rgeo(mt, nt, kB64, d.flags);
+            const Geo g = reg_geo(d, r);
+            const TI *A = (const TI *)p.A + d.a_off;
+            double *W = (double *)region;
+            double *V = (double *)(region + align16((size_t)r.ldw * r.ncp * 8));
+            bool bad;
+            const int e = scan_input(A, g.m * g.n, ax, bad);
+            if (bad) {
+                st = JB_ST_NONFINITE_IN;
+            } else {
+                zero_fill(V, (size_t)r.ldv * r.npb);
+                if (!MIXED) zero_fill(W, (size_t)r.ldw * r.ncp);
+                __syncthreads();
+                if (!MIXED) {
+                    load_padded(A, g, r, e, W, V);
+                } else {
+                    double *X1 = (double *)(region + rregion_bytes(r, 8));
+                    unsigned char *X2 = region + rregion_bytes(r, 8) + align16((size_t)r.ldv * r.npb * 8);
+                    const float *x = p.x32 + d.x_off;
+                    for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) {
+                        const int c = k / nt, i = k - c * nt;
+                        V[(size_t)c * r.ldv + i] = (double)x[k];
+                    }
+                    for (int j = nt + threadIdx.x; j < r.npb; j += blockDim.x) V[(size_t)j * r.ldv + j] = 1.0;
+                    __syncthreads();
+                    double err = polar_step(V, r.npb, r.ldv, W, X1, (double *)X2, ax);
+                    if (err > 1e-5 && err < 0.5) err = polar_step(V, r.npb, r.ldv, W, X1, (double *)X2, ax);
+                    if (err >= 0.5) {  // not near-orthogonal: restart from V = I
+                        for (int k = threadIdx.x; k < r.npb * r.ldv; k += blockDim.x) {
+                            const int c = k / r.ldv, i = k - c * r.ldv;
+                            V[k] = (i == c) ? 1.0 : 0.0;
+                        }
+                    }
+                    // A_t (float, ldw x nt, zero rows >= mt) staged in X2.
+                    float *As = (float *)X2;
+                    zero_fill(As, (size_t)r.ldw * nt);
+                    __syncthreads();
+                    const int total = g.m * g.n;
+                    for (int k = threadIdx.x; k < total; k += blockDim.x) {
+                        const int row = k / g.n, col = k - row * g.n;
+                        const int i = g.wide ? col : row, j = g.wide ? row : col;
+                        As[(size_t)j * r.ldw + i] = (float)A[k];
+                    }
+                    __syncthreads();
+                    gemm_nn<float>(W, r.ldw, As, r.ldw, V, r.ldv, r.ldw, r.npb, nt, ldexp(1.0, -e));
+                    for (int j = r.npb; j < r.ncp; ++j)
+                        for (int i = threadIdx.x; i < r.ldw; i += blockDim.x) W[(size_t)j * r.ldw + i] = 0.0;
+                }
+                __syncthreads();
+                const double tol = MIXED ? (p.tol > 0 ? (double)(float)p.tol : (double)(10.0f * Lim<float>::eps()))
+                                         : (p.tol > 0 ? p.tol : 10.0 * Lim<double>::eps());
+                bool conv;
+                ns += rb_dispatch<double, kB64>(r, W, V, tol, p.max_sweeps, true, ax.red, conv);
+                if (!conv) {
+                    st = JB_ST_NOT_CONVERGED;
+                } else {
+                    TI *U = p.U ? (TI *)p.U + d.u_off : nullptr;
+                    TI *Vh = p.Vh ? (TI *)p.Vh + d.v_off : nullptr;
+                    st = epilogue<double, TI>(W, V, g, e, U, (TI *)p.S + d.s_off, Vh, ax);
+                }
+            }
+        }
+        if (threadIdx.x == 0) {
+            if (p.status) p.status[mat] = st;
+            if (p.sweeps) p.sweeps[mat] = ns;
+        }
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Host side.
 // ---------------------------------------------------------------------------
@@ -247,15 +585,22 @@ static int sm_count() {
     return g_dev[dev].sms;
 }
 
+// Launch plan for one batch (sized by its largest tall shape).
 struct Plan {
+    bool reg;             // register-tile path
+    // round-robin path
     Dims d;
     size_t aux, region, smem;
     bool global_region;
     int threads;
+    // register path: one sizing per kernel
+    Dims d32, d64;
+    size_t smem32, smem64, reg32, reg64;
 };
 
 static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags) {
     Plan pl;
+    memset(&pl, 0, sizeof(pl));
     pl.d = dims_of(max_mt, max_nt, flags);
     pl.aux = aux_bytes(pl.d);
     pl.region = region_bytes(pl.d, elem, precision);
@@ -266,56 +611,118 @@ static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags
     if (t < 64) t = 64;
     if (t > 1024) t = 1024;
     pl.threads = t;
+    const RGeo r32 = rgeo(max_mt, max_nt, kB32, flags), r64 = rgeo(max_mt, max_nt, kB64, flags);
+    pl.reg = !(flags & JB_ROUND_ROBIN) && r32.R <= kMaxR && r32.RV <= kMaxRV && r64.RV <= kMaxRV;
+    if (pl.reg) {
+        pl.d32 = raux_dims(r32);
+        pl.d64 = raux_dims(r64);
+        pl.reg32 = rregion_bytes(r32, 4);
+        pl.reg64 = (elem == 4 && precision == JB_PREC_MIXED) ? rregion_mixed64(r64, max_nt) : rregion_bytes(r64, 8);
+        pl.smem32 = aux_bytes(pl.d32) + pl.reg32;
+        pl.smem64 = aux_bytes(pl.d64) + pl.reg64;
+        if (pl.smem64 > kSmemLimit || pl.smem32 > kSmemLimit) pl.reg = false;
+    }
     return pl;
 }
 
-template <typename T, int PREC>
-static int launch(Params &p, const Plan &pl, void *workspace, size_t ws_bytes, bool dynamic, cudaStream_t st) {
-    const int sms = sm_count();
-    if (sms <= 0) return JB_ECUDA;
-    auto kern = batched_kernel<T, PREC>;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem) != cudaSuccess)
-        return JB_ECUDA;
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, pl.threads, pl.smem) != cudaSuccess)
-        return JB_ECUDA;
-    if (per_sm < 1) return JB_ETOOBIG;
-    int64_t grid = (int64_t)sms * per_sm;
-    if (grid > p.count) grid = p.count;
-    if (grid < 1) grid = 1;
-    unsigned char *ws = (unsigned char *)workspace;
-    p.maxd = pl.d;
-    p.counter = nullptr;
-    p.gws = nullptr;
-    p.gws_stride = 0;
-    if (dynamic || pl.global_region) {
-        if (!ws) return JB_EWORKSPACE;
-    }
-    if (dynamic) {
-        p.counter = (int *)ws;
-        if (cudaMemsetAsync(p.counter, 0, sizeof(int), st) != cudaSuccess) return JB_ECUDA;
-    }
-    if (pl.global_region) {
-        const size_t stride = align16(pl.region) + 256;
-        const int64_t max_grid = (int64_t)((ws_bytes - kCounterBytes) / stride);
-        if (ws_bytes < kCounterBytes + stride) return JB_EWORKSPACE;
-        if (grid > max_grid) grid = max_grid;
-        p.gws = ws + kCounterBytes;
-        p.gws_stride = stride;
-    }
-    kern<<<(unsigned)grid, pl.threads, pl.smem, st>>>(p);
-    return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
-}
-
-static size_t workspace_for(const Plan &pl, int64_t count) {
+// Bytes before the mixed-precision scratch: ticket counters and, on the
+// round-robin path, per-CTA global work areas.
+static size_t base_bytes(const Plan &pl, int64_t count) {
     size_t bytes = kCounterBytes;
-    if (pl.global_region) {
+    if (!pl.reg && pl.global_region) {
         const int sms = sm_count();
         int64_t grid = sms > 0 ? sms : 148;
         if (grid > count) grid = count;
         bytes += (size_t)grid * (align16(pl.region) + 256);
     }
     return bytes;
+}
+
+template <typename K>
+static int occupancy_grid(K kern, int threads, size_t smem, int64_t count, int64_t &grid) {
+    const int sms = sm_count();
+    if (sms <= 0) return JB_ECUDA;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return JB_ECUDA;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess)
+        return JB_ECUDA;
+    if (per_sm < 1) return JB_ETOOBIG;
+    grid = (int64_t)sms * per_sm;
+    if (grid > count) grid = count;
+    if (grid < 1) grid = 1;
+    return JB_OK;
+}
+
+template <typename T, int PREC>
+static int launch_rr(Params &p, const Plan &pl, unsigned char *ws, size_t ws_bytes, cudaStream_t st) {
+    auto kern = batched_kernel<T, PREC>;
+    int64_t grid;
+    int rc = occupancy_grid(kern, pl.threads, pl.smem, p.count, grid);
+    if (rc) return rc;
+    p.maxd = pl.d;
+    p.counter = (int *)ws;
+    p.gws = nullptr;
+    p.gws_stride = 0;
+    if (pl.global_region) {
+        const size_t stride = align16(pl.region) + 256;
+        if (ws_bytes < kCounterBytes + stride) return JB_EWORKSPACE;
+        const int64_t max_grid = (int64_t)((ws_bytes - kCounterBytes) / stride);
+        if (grid > max_grid) grid = max_grid;
+        p.gws = ws + kCounterBytes;
+        p.gws_stride = stride;
+    }
+    if (cudaMemsetAsync(p.counter, 0, sizeof(int), st) != cudaSuccess) return JB_ECUDA;
+    kern<<<(unsigned)grid, pl.threads, pl.smem, st>>>(p);
+    return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+}
+
+// elem: 4 (f32 input) or 8 (f64 input).
+static int launch_reg(Params &p, const Plan &pl, int elem, int precision, unsigned char *ws, size_t ws_bytes,
+                      cudaStream_t st) {
+    p.counter = (int *)ws;
+    p.counter2 = (int *)ws + 1;
+    const bool mixed = elem == 4 && precision == JB_PREC_MIXED;
+    if (mixed) {
+        const size_t base = base_bytes(pl, p.count);
+        if (ws_bytes < base) return JB_EWORKSPACE;
+        p.x32 = (float *)(ws + base);
+        p.x_cap = (int64_t)((ws_bytes - base) / 4);
+    }
+    if (cudaMemsetAsync(ws, 0, 2 * sizeof(int), st) != cudaSuccess) return JB_ECUDA;
+    int64_t grid;
+    int rc;
+    if (elem == 4) {
+        auto k1 = mixed ? rb32_kernel<true> : rb32_kernel<false>;
+        if ((rc = occupancy_grid(k1, kT32, pl.smem32, p.count, grid))) return rc;
+        p.maxd = pl.d32;
+        p.region_cap = pl.reg32;
+        k1<<<(unsigned)grid, kT32, pl.smem32, st>>>(p);
+        if (cudaGetLastError() != cudaSuccess) return JB_ECUDA;
+        if (!mixed) return JB_OK;
+        auto k2 = rb64_kernel<float, true>;
+        if ((rc = occupancy_grid(k2, kT64, pl.smem64, p.count, grid))) return rc;
+        p.maxd = pl.d64;
+        p.region_cap = pl.reg64;
+        k2<<<(unsigned)grid, kT64, pl.smem64, st>>>(p);
+        return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+    }
+    auto k2 = rb64_kernel<double, false>;
+    if ((rc = occupancy_grid(k2, kT64, pl.smem64, p.count, grid))) return rc;
+    p.maxd = pl.d64;
+    p.region_cap = pl.reg64;
+    k2<<<(unsigned)grid, kT64, pl.smem64, st>>>(p);
+    return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+}
+
+static int launch_any(Params &p, const Plan &pl, int elem, int precision, void *workspace, size_t ws_bytes,
+                      cudaStream_t st) {
+    unsigned char *ws = (unsigned char *)workspace;
+    if (!ws || ws_bytes < kCounterBytes) return JB_EWORKSPACE;
+    if (pl.reg) return launch_reg(p, pl, elem, precision, ws, ws_bytes, st);
+    if (elem == 8) return launch_rr<double, JB_PREC_NATIVE>(p, pl, ws, ws_bytes, st);
+    return precision == JB_PREC_MIXED ? launch_rr<float, JB_PREC_MIXED>(p, pl, ws, ws_bytes, st)
+                                      : launch_rr<float, JB_PREC_NATIVE>(p, pl, ws, ws_bytes, st);
 }
 
 static int check_common(int64_t count, int32_t m, int32_t n, int32_t rank, int32_t flags, int32_t max_sweeps) {
@@ -327,63 +734,69 @@ static int check_common(int64_t count, int32_t m, int32_t n, int32_t rank, int32
     return JB_OK;
 }
 
+static size_t uniform_workspace(int32_t m, int32_t n, int64_t count, int32_t elem, int32_t precision,
+                                int32_t flags) {
+    const int mt = m > n ? m : n, nt = m > n ? n : m;
+    const int prec = elem == 4 ? precision : JB_PREC_NATIVE;
+    const Plan pl = make_plan(mt, nt, elem, prec, flags);
+    size_t bytes = base_bytes(pl, count);
+    if (pl.reg && prec == JB_PREC_MIXED) bytes += (size_t)count * nt * nt * 4;
+    return bytes;
+}
+
 }  // namespace jb
 
 using namespace jb;
 
 extern "C" {
 
-int jb_version(void) { return 100; }
+int jb_version(void) { return 200; }
 
 int jb_device_sm_count(void) { return sm_count(); }
 
 size_t jb_workspace_bytes(int32_t max_m, int32_t max_n, int64_t count, int32_t elem_bytes, int32_t precision,
                           int32_t flags) {
-    if (max_m < 1 || max_n < 1 || (elem_bytes != 4 && elem_bytes != 8)) return 0;
-    const int mt = max_m > max_n ? max_m : max_n, nt = max_m > max_n ? max_n : max_m;
-    const Plan pl = make_plan(mt, nt, elem_bytes, elem_bytes == 4 ? precision : JB_PREC_NATIVE, flags);
-    return workspace_for(pl, count);
+    if (max_m < 1 || max_n < 1 || count < 0 || (elem_bytes != 4 && elem_bytes != 8)) return 0;
+    return uniform_workspace(max_m, max_n, count, elem_bytes, precision, flags);
 }
 
-int jb_svd_batched_f32(const float *A, float *U, float *S, float *Vh, int64_t batch, int32_t m, int32_t n,
-                       int32_t rank, int32_t flags, double tol, int32_t max_sweeps, int32_t precision,
-                       int32_t *sweeps, int32_t *status, void *workspace, size_t workspace_bytes, void *stream) {
+static int batched_common(const void *A, void *U, void *S, void *Vh, int64_t batch, int32_t m, int32_t n,
+                          int32_t rank, int32_t flags, double tol, int32_t max_sweeps, int32_t precision,
+                          int32_t *sweeps, int32_t *status, void *workspace, size_t workspace_bytes, void *stream,
+                          int elem) {
     int rc = check_common(batch, m, n, rank, flags, max_sweeps);
     if (rc) return rc;
     if (!A || !S || (!(flags & JB_VALUES_ONLY) && (!U || !Vh))) return JB_EINVAL;
     if (precision != JB_PREC_NATIVE && precision != JB_PREC_MIXED) return JB_EINVAL;
     if (batch == 0) return JB_OK;
+    if (workspace_bytes < uniform_workspace(m, n, batch, elem, precision, flags)) return JB_EWORKSPACE;
     Params p;
     memset(&p, 0, sizeof(p));
-    p.A = A; p.U = (flags & JB_VALUES_ONLY) ? nullptr : U; p.S = S; p.Vh = (flags & JB_VALUES_ONLY) ? nullptr : Vh;
-    p.count = batch; p.um = m; p.un = n; p.urank = rank; p.uflags = flags;
+    p.A = A;
+    p.U = (flags & JB_VALUES_ONLY) ? nullptr : U;
+    p.S = S;
+    p.Vh = (flags & JB_VALUES_ONLY) ? nullptr : Vh;
+    p.count = batch; p.um = m; p.un = n; p.urank = rank; p.uflags = flags & ~JB_ROUND_ROBIN;
     p.tol = tol; p.max_sweeps = max_sweeps; p.tol32 = tol; p.max_sweeps32 = max_sweeps;
     p.sweeps = sweeps; p.status = status;
     const int mt = m > n ? m : n, nt = m > n ? n : m;
-    const Plan pl = make_plan(mt, nt, 4, precision, flags);
-    if (workspace && workspace_bytes < workspace_for(pl, batch)) return JB_EWORKSPACE;
-    cudaStream_t st = (cudaStream_t)stream;
-    return precision == JB_PREC_MIXED ? launch<float, JB_PREC_MIXED>(p, pl, workspace, workspace_bytes, false, st)
-                                      : launch<float, JB_PREC_NATIVE>(p, pl, workspace, workspace_bytes, false, st);
+    const int prec = elem == 4 ? precision : JB_PREC_NATIVE;
+    const Plan pl = make_plan(mt, nt, elem, prec, flags);
+    return launch_any(p, pl, elem, prec, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int jb_svd_batched_f32(const float *A, float *U, float *S, float *Vh, int64_t batch, int32_t m, int32_t n,
+                       int32_t rank, int32_t flags, double tol, int32_t max_sweeps, int32_t precision,
+                       int32_t *sweeps, int32_t *status, void *workspace, size_t workspace_bytes, void *stream) {
+    return batched_common(A, U, S, Vh, batch, m, n, rank, flags, tol, max_sweeps, precision, sweeps, status,
+                          workspace, workspace_bytes, stream, 4);
 }
 
 int jb_svd_batched_f64(const double *A, double *U, double *S, double *Vh, int64_t batch, int32_t m, int32_t n,
                        int32_t rank, int32_t flags, double tol, int32_t max_sweeps, int32_t *sweeps,
                        int32_t *status, void *workspace, size_t workspace_bytes, void *stream) {
-    int rc = check_common(batch, m, n, rank, flags, max_sweeps);
-    if (rc) return rc;
-    if (!A || !S || (!(flags & JB_VALUES_ONLY) && (!U || !Vh))) return JB_EINVAL;
-    if (batch == 0) return JB_OK;
-    Params p;
-    memset(&p, 0, sizeof(p));
-    p.A = A; p.U = (flags & JB_VALUES_ONLY) ? nullptr : U; p.S = S; p.Vh = (flags & JB_VALUES_ONLY) ? nullptr : Vh;
-    p.count = batch; p.um = m; p.un = n; p.urank = rank; p.uflags = flags;
-    p.tol = tol; p.max_sweeps = max_sweeps;
-    p.sweeps = sweeps; p.status = status;
-    const int mt = m > n ? m : n, nt = m > n ? n : m;
-    const Plan pl = make_plan(mt, nt, 8, JB_PREC_NATIVE, flags);
-    if (workspace && workspace_bytes < workspace_for(pl, batch)) return JB_EWORKSPACE;
-    return launch<double, JB_PREC_NATIVE>(p, pl, workspace, workspace_bytes, false, (cudaStream_t)stream);
+    return batched_common(A, U, S, Vh, batch, m, n, rank, flags, tol, max_sweeps, JB_PREC_NATIVE, sweeps, status,
+                          workspace, workspace_bytes, stream, 8);
 }
 
 int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh, const jb_matrix_desc *descs,
@@ -395,17 +808,15 @@ int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh, const jb_ma
     const int mt = max_m > max_n ? max_m : max_n, nt = max_m > max_n ? max_n : max_m;
     if (mt > 8192 || nt > 4096) return JB_ETOOBIG;
     if (count == 0) return JB_OK;
+    const Plan pl = make_plan(mt, nt, 4, precision, 0);
+    if (!workspace || workspace_bytes < base_bytes(pl, count)) return JB_EWORKSPACE;
     Params p;
     memset(&p, 0, sizeof(p));
     p.A = A; p.U = U; p.S = S; p.Vh = Vh;
     p.descs = descs; p.order = order; p.count = count;
     p.tol = tol; p.max_sweeps = max_sweeps; p.tol32 = tol; p.max_sweeps32 = max_sweeps;
     p.sweeps = sweeps; p.status = status;
-    const Plan pl = make_plan(mt, nt, 4, precision, 0);
-    if (!workspace || workspace_bytes < workspace_for(pl, count)) return JB_EWORKSPACE;
-    cudaStream_t st = (cudaStream_t)stream;
-    return precision == JB_PREC_MIXED ? launch<float, JB_PREC_MIXED>(p, pl, workspace, workspace_bytes, true, st)
-                                      : launch<float, JB_PREC_NATIVE>(p, pl, workspace, workspace_bytes, true, st);
+    return launch_any(p, pl, 4, precision, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
 }  // extern "C"

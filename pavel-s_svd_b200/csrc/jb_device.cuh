@@ -57,7 +57,7 @@ struct Aux {
     double *vec;              // scratch vector (max(mt, np))
     double *tau;              // Householder scalars (np)
     int *perm;                // sorted position -> physical column (np)
-    double *red;              // 32 reduction slots
+    double *red;              // 64 reduction slots
     int *flag;                // 4 ints: [0] non-finite, [1] null-fail, [2] argmax idx
 };
 
@@ -348,7 +348,8 @@ __device__ int epilogue(T *W, T *V, const Geo &g, int e, TO *U_out, TO *S_out, T
     // cut = eps * max(m, n_padded) * sigma_1 (primitives.py:362; the
     // reference's n is the padded width there).
     const T smax = (T)ax.sig[ax.perm[0]];
-    const T cut = Lim<T>::eps() * (T)(mt > np ? mt : np) * smax;
+    const int npref = nt + (nt & 1);
+    const T cut = Lim<T>::eps() * (T)(mt > npref ? mt : npref) * smax;
     // Normalise kept columns in place, zero the others (primitives.py:364, :436).
     int any_missing = 0;
     for (int r = warp; r < nt; r += nw) {

@@ -1,0 +1,312 @@
+// jb_regblock.cuh - register-resident block-cyclic one-sided Jacobi sweeps.
+//
+// The tall work matrix W (mt x npb, column-major in shared memory, 32*R rows
+// per column, rows >= mt zero) and V (npb x npb, 32*RV rows per column) are
+// split into nb = npb / B blocks of B columns.  Warp w of the CTA holds the two
+// blocks at positions (w, nb-1-w) of a circle-method tournament over blocks
+// in registers: lane l owns rows l, l+32, ... of all 2B columns.  A sweep is
+//   * an intra step: the B-1 circle rounds inside each held block, and
+//   * nb-1 block rounds: each warp meets its block pair with B "shift"
+//     rounds (x_i, y_(i+j) mod B), i.e. all B^2 cross pairs,
+// so every column pair is rotated exactly once per sweep, as in the
+// reference's round-robin sweep (primitives.py:328-351) but with a block
+// ordering: B disjoint pairs per warp step, their 3B dot products reduced
+// together across the warp, and one CTA barrier per block round instead of
+// two per pair round.  Blocks move between warps through shared memory.
+//
+// The rotation, the active test and the convergence test (no active pair in
+// a sweep <=> off <= tol) are the reference's (primitives.py:334-355); the
+// rotation is evaluated in an algebraically equal form (rot_params).  The null-column floor
+// eps^2 * max ||w_j||^2 uses the column norms at the start of each sweep
+// (the reference takes the maximum inside each round: they differ only for
+// columns whose squared norm is within a factor n of eps^2 max).
+#pragma once
+#include "jb_device.cuh"
+
+namespace jb {
+
+template <int N> struct Log2 { static constexpr int value = 1 + Log2<N / 2>::value; };
+template <> struct Log2<1> { static constexpr int value = 0; };
+
+__device__ __forceinline__ int circ(int pos, int r, int n) {
+    if (pos == 0) return 0;
+    int x = (pos - 1 - r) % (n - 1);
+    if (x < 0) x += n - 1;
+    return 1 + x;
+}
+
+template <typename T, int B, int R, int RV>
+struct Tile {
+    T w[2 * B][R];
+    T v[2 * B][RV];
+};
+
+// Warp reduce-scatter of NV (power of two <= 32) values: afterwards x[0] on
+// lane l holds the full warp sum of value index l >> (5 - log2 NV).
+template <typename T, int NV>
+__device__ __forceinline__ void reduce_scatter(T (&x)[NV], int lane) {
+    constexpr int L = Log2<NV>::value;
+#pragma unroll
+    for (int s = 0; s < L; ++s) {
+        const int h = NV >> (s + 1);
+        const int o = 16 >> s;
+        const bool up = (lane & o) != 0;
+#pragma unroll
+        for (int k = 0; k < h; ++k) {
+            const T send = up ? x[k] : x[k + h];
+            const T keep = up ? x[k + h] : x[k];
+            x[k] = keep + __shfl_xor_sync(FULL, send, o);
+        }
+    }
+#pragma unroll
+    for (int o = 16 >> L; o >= 1; o >>= 1) x[0] += __shfl_xor_sync(FULL, x[0], o);
+}
+
+// Rotation of one pair from its Gram entries: the reference's rotation
+// (primitives.py:334-347) in an algebraically equal form with one square
+// root and one division.  With d = aqq - app, tau = d / (2|apq|) and
+//   t = sign(tau) / (|tau| + hypot(tau, 1)) = sign(d) 2|apq| / (|d| + sqrt(d^2 + 4 apq^2)),
+// c = 1/sqrt(1 + t^2), s = t c sign(apq); t = 1 when d = 0, as in the
+// reference.  The active test ratio = |apq| / sqrt(app aqq) > tol is taken
+// on squares.  Inputs are scaled (max |a| < 1), so d^2 + 4 apq^2 cannot
+// overflow, and active pairs keep apq^2 far above the underflow range.
+// Returns bit 0: active; bit 1: ratio > sqrt(tol) / 2 (the confirmation
+// heuristic of rb_sweeps).  Inactive pairs get c = 1, s = 0.
+__device__ __forceinline__ float rcp_sqrt(float x) { return 1.0f / sqrtf(x); }
+__device__ __forceinline__ double rcp_sqrt(double x) { return rsqrt(x); }
+
+template <typename T>
+__device__ __forceinline__ int rot_params(T app, T aqq, T apq, T tol2, T big2, T floor_, T &c, T &s) {
+    c = T(1);
+    s = T(0);
+    const T apq2 = apq * apq;
+    const T prod = app * aqq;
+    const bool active = apq2 > tol2 * prod && fmin(app, aqq) > floor_;
+    if (!active) return 0;
+    const T d = aqq - app;
+    const T t = copysign(T(2) * dabs(apq), d) / (dabs(d) + dsqrt(dfma(d, d, T(4) * apq2)));
+    c = rcp_sqrt(dfma(t, t, T(1)));
+    s = t * c;
+    if (apq < T(0)) s = -s;
+    return 1 | (apq2 > big2 * prod ? 2 : 0);
+}
+
+// Register column of the first / second member of pair i in a step.
+// CROSS steps pair x_i with y_i; INTRA steps pair positions (k, B-1-k) of
+// each held block.
+template <bool INTRA, int B>
+__device__ __forceinline__ constexpr int pair_p(int i) {
+    return INTRA ? (i < B / 2 ? i : B + (i - B / 2)) : i;
+}
+template <bool INTRA, int B>
+__device__ __forceinline__ constexpr int pair_q(int i) {
+    return INTRA ? (i < B / 2 ? B - 1 - i : 2 * B - 1 - (i - B / 2)) : B + i;
+}
+
+// One step: B disjoint pairs; ORs the pairs' rot_params flags into fl.
+template <bool INTRA, typename T, int B, int R, int RV>
+__device__ __forceinline__ void step(Tile<T, B, R, RV> &t, T tol2, T big2, T floor_, int &fl, bool rotate, int lane,
+                                     int nr, int nv) {
+    constexpr int LB = Log2<B>::value;
+    T pa[B], pb[B], pc[B];
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        const int p = pair_p<INTRA, B>(i), q = pair_q<INTRA, B>(i);
+        T a = 0, b = 0, c = 0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (r < nr) {
+                const T x = t.w[p][r], y = t.w[q][r];
+                a = dfma(x, x, a);
+                b = dfma(y, y, b);
+                c = dfma(x, y, c);
+            }
+        }
+        pa[i] = a; pb[i] = b; pc[i] = c;
+    }
+    reduce_scatter<T, B>(pa, lane);
+    reduce_scatter<T, B>(pb, lane);
+    reduce_scatter<T, B>(pc, lane);
+    T c, s;
+    const int f = rot_params(pa[0], pb[0], pc[0], tol2, big2, floor_, c, s);
+    fl |= f;
+    if (!rotate || !__any_sync(FULL, f != 0)) return;
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        const int src = i << (5 - LB);
+        const T ci = __shfl_sync(FULL, c, src), si = __shfl_sync(FULL, s, src);
+        const int p = pair_p<INTRA, B>(i), q = pair_q<INTRA, B>(i);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (r < nr) {
+                const T x = t.w[p][r], y = t.w[q][r];
+                t.w[p][r] = dfma(ci, x, -si * y);
+                t.w[q][r] = dfma(si, x, ci * y);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RV; ++r) {
+            if (r < nv) {
+                const T x = t.v[p][r], y = t.v[q][r];
+                t.v[p][r] = dfma(ci, x, -si * y);
+                t.v[q][r] = dfma(si, x, ci * y);
+            }
+        }
+    }
+}
+
+// y_i <- y_(i+1) (cyclic): the next CROSS step pairs x_i with the old y_(i+1).
+template <typename T, int B, int R, int RV>
+__device__ __forceinline__ void shift_y(Tile<T, B, R, RV> &t) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const T f = t.w[B][r];
+#pragma unroll
+        for (int i = 0; i < B - 1; ++i) t.w[B + i][r] = t.w[B + i + 1][r];
+        t.w[2 * B - 1][r] = f;
+    }
+#pragma unroll
+    for (int r = 0; r < RV; ++r) {
+        const T f = t.v[B][r];
+#pragma unroll
+        for (int i = 0; i < B - 1; ++i) t.v[B + i][r] = t.v[B + i + 1][r];
+        t.v[2 * B - 1][r] = f;
+    }
+}
+
+// Circle rotation inside both blocks: positions 1..B-1 move one step right.
+template <typename T, int B, int R, int RV>
+__device__ __forceinline__ void circle_shift(Tile<T, B, R, RV> &t) {
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        const int o = half * B;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const T last = t.w[o + B - 1][r];
+#pragma unroll
+            for (int i = B - 1; i >= 2; --i) t.w[o + i][r] = t.w[o + i - 1][r];
+            t.w[o + 1][r] = last;
+        }
+#pragma unroll
+        for (int r = 0; r < RV; ++r) {
+            const T last = t.v[o + B - 1][r];
+#pragma unroll
+            for (int i = B - 1; i >= 2; --i) t.v[o + i][r] = t.v[o + i - 1][r];
+            t.v[o + 1][r] = last;
+        }
+    }
+}
+
+template <typename T, int B, int R, int RV>
+__device__ __forceinline__ void tile_io(Tile<T, B, R, RV> &t, T *W, int ldw, T *V, int ldv, int X, int Y, int lane,
+                                        bool store, int nr, int nv) {
+#pragma unroll
+    for (int c = 0; c < 2 * B; ++c) {
+        const int col = (c < B ? X * B + c : Y * B + (c - B));
+        T *w = W + (size_t)col * ldw + lane;
+        T *v = V + (size_t)col * ldv + lane;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (r < nr) {
+                if (store) w[32 * r] = t.w[c][r];
+                else t.w[c][r] = w[32 * r];
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < RV; ++r) {
+            if (r < nv) {
+                if (store) v[32 * r] = t.v[c][r];
+                else t.v[c][r] = v[32 * r];
+            }
+        }
+    }
+}
+
+// Sweeps over W/V in shared memory until off <= tol or max_sweeps.  nb blocks
+// (even), of which the first `live` hold real columns; blocks >= live are
+// zero and their pairs are skipped.  All threads of the CTA call this; warps
+// >= nb/2 only take part in the barriers.  `red` needs 2*32 doubles.
+// confirm: after a rotating sweep whose off is already below sqrt(tol)/2,
+// run the next sweep without rotations; when it confirms off <= tol the
+// reference would have rotated nothing in that sweep either.
+// nr = ldw / 32 and nv = ldv / 32 are the rows per lane actually used
+// (<= R, RV): one instantiation serves every matrix up to 32R x 32RV.
+template <typename T, int B, int R, int RV>
+__device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, int max_sweeps, bool confirm,
+                         double *red, bool &converged) {
+    const int nr = ldw >> 5, nv = ldv >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nw = nwarps();
+    const bool act = warp < nb / 2;
+    Tile<T, B, R, RV> t;
+    int rr = 0;
+    int X = act ? circ(warp, 0, nb) : 0, Y = act ? circ(nb - 1 - warp, 0, nb) : 0;
+    if (act) tile_io(t, W, ldw, V, ldv, X, Y, lane, false, nr, nv);
+    bool measure = false, measure_allowed = confirm;
+    const T tol2 = tol * tol, big2 = tol / T(4);  // ratio > tol, ratio > sqrt(tol)/2
+    converged = false;
+    int sweep = 0;
+    for (sweep = 1; sweep <= max_sweeps; ++sweep) {
+        // Null-column floor from the column norms at the sweep start.
+        T nmax = 0;
+        if (act) {
+            T nrm[2 * B];
+#pragma unroll
+            for (int c = 0; c < 2 * B; ++c) {
+                T a = 0;
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    if (r < nr) a = dfma(t.w[c][r], t.w[c][r], a);
+                nrm[c] = a;
+            }
+            reduce_scatter<T, 2 * B>(nrm, lane);
+            nmax = warp_max(nrm[0]);
+        }
+        if (lane == 0) red[warp] = (double)nmax;
+        __syncthreads();
+        double gm = red[0];
+        for (int w = 1; w < nw; ++w) gm = fmax(gm, red[w]);
+        const T floor_ = Lim<T>::eps() * Lim<T>::eps() * (T)gm;
+        const bool rotate = !measure;
+        int fl = 0;
+        if (act && (X < live || Y < live)) {
+            for (int j = 0; j < B - 1; ++j) {
+                step<true>(t, tol2, big2, floor_, fl, rotate, lane, nr, nv);
+                circle_shift(t);
+            }
+        }
+        for (int br = 0; br < nb - 1; ++br) {
+            if (br > 0 || sweep > 1) {
+                if (act) tile_io(t, W, ldw, V, ldv, X, Y, lane, true, nr, nv);
+                __syncthreads();
+                rr = rr + 1 == nb - 1 ? 0 : rr + 1;
+                if (act) {
+                    X = circ(warp, rr, nb);
+                    Y = circ(nb - 1 - warp, rr, nb);
+                    tile_io(t, W, ldw, V, ldv, X, Y, lane, false, nr, nv);
+                }
+            }
+            if (act && X < live && Y < live) {
+                for (int j = 0; j < B; ++j) {
+                    step<false>(t, tol2, big2, floor_, fl, rotate, lane, nr, nv);
+                    shift_y(t);
+                }
+            }
+        }
+        // off <= tol  <=>  no active pair in the sweep (primitives.py:352).
+        const int any_active = __syncthreads_or(fl & 1);
+        const int any_big = __syncthreads_or(fl & 2);
+        if (!any_active) { converged = true; break; }
+        if (measure) {
+            measure = false;
+            measure_allowed = false;  // a failed confirmation: rotate from now on
+        } else if (measure_allowed && !any_big) {
+            measure = true;
+        }
+    }
+    if (act) tile_io(t, W, ldw, V, ldv, X, Y, lane, true, nr, nv);
+    __syncthreads();
+    return converged ? sweep : max_sweeps;
+}
+
+}  // namespace jb

@@ -15,7 +15,7 @@ from .build import library_path
 # Return codes and per-matrix status words (include/jacobi_b200.h).
 JB_OK, JB_EINVAL, JB_ETOOBIG, JB_EWORKSPACE, JB_ECUDA = 0, 1, 2, 3, 4
 ST_OK, ST_NOT_CONVERGED, ST_NONFINITE_IN, ST_NULL_FAILED, ST_NONFINITE_OUT, ST_BAD_DESC = 0, 1, 2, 3, 4, 5
-FULL_MATRICES, VALUES_ONLY = 1, 2
+FULL_MATRICES, VALUES_ONLY, ROUND_ROBIN = 1, 2, 4
 PREC_NATIVE, PREC_MIXED = 0, 1
 
 RC_NAMES = {JB_EINVAL: "invalid argument", JB_ETOOBIG: "shape too large for this entry point",
@@ -30,10 +30,10 @@ class MatrixDesc(ctypes.Structure):
     """jb_matrix_desc: one matrix of an uneven batch (offsets in elements)."""
     _fields_ = [("m", ctypes.c_int32), ("n", ctypes.c_int32), ("rank", ctypes.c_int32),
                 ("flags", ctypes.c_int32), ("a_off", ctypes.c_int64), ("u_off", ctypes.c_int64),
-                ("s_off", ctypes.c_int64), ("v_off", ctypes.c_int64)]
+                ("s_off", ctypes.c_int64), ("v_off", ctypes.c_int64), ("x_off", ctypes.c_int64)]
 
 
-DESC_BYTES = ctypes.sizeof(MatrixDesc)  # 48
+DESC_BYTES = ctypes.sizeof(MatrixDesc)  # 56
 
 _lock = threading.Lock()
 _lib = None

@@ -18,6 +18,10 @@ Differences, by design:
     FP32 arithmetic alone does not; ``'fp32'`` is the plain FP32 Jacobi of the
     reference.  float64 input always runs in FP64.
   * Scaling by a power of two (exact) instead of max|a| (solvers.py:294-295).
+  * ``ordering`` option: ``'block'`` (default) sweeps in a register-blocked
+    cyclic order (every pair once per sweep, like the reference);
+    ``'round_robin'`` uses the reference's own pair order
+    (primitives.py:309-313) for sweep-for-sweep comparisons.
 """
 from __future__ import annotations
 
@@ -32,6 +36,7 @@ REFERENCE_ALGORITHMS = (
 )  # svdbench/standalone/solvers.py:7-11
 ALGORITHMS = ('jacobi',)
 PRECISIONS = ('mixed', 'fp32')
+ORDERINGS = ('block', 'round_robin')
 
 
 class Unsupported(RuntimeError):
@@ -66,6 +71,8 @@ def _validate(a, algorithm, full_matrices, opts):
     precision = opts.get('precision', 'mixed')
     if precision not in PRECISIONS:
         raise ValueError(f'precision must be one of {PRECISIONS}')
+    if opts.get('ordering', 'block') not in ORDERINGS:
+        raise ValueError(f'ordering must be one of {ORDERINGS}')
     return rank, precision
 
 
@@ -128,9 +135,9 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
 
     Same contract as svdbench.standalone.svd (solvers.py:264-310) for
     algorithm='jacobi'; options ``tol``, ``max_sweeps`` (default 60,
-    solvers.py:24-27), ``rank`` and ``precision``; other options are accepted
-    and ignored, as the reference's Jacobi ignores them.  Input is never
-    overwritten."""
+    solvers.py:24-27), ``rank``, ``precision`` and ``ordering``; other
+    options are accepted and ignored, as the reference's Jacobi ignores them.
+    Input is never overwritten."""
     rank, precision = _validate(a, algorithm, full_matrices, opts)
     max_sweeps = opts.get('max_sweeps', 60)
     tol = opts.get('tol')
@@ -142,6 +149,8 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
         x = a.detach().reshape(-1, m, n).contiguous()
         b = x.shape[0]
         flags = (N.FULL_MATRICES if full_matrices else 0) | (N.VALUES_ONLY if values_only else 0)
+        if opts.get('ordering', 'block') == 'round_robin':
+            flags |= N.ROUND_ROBIN
         ucols = m if full_matrices else rank
         vrows = n if full_matrices else rank
         u = None if values_only else torch.empty(b, m, ucols, dtype=a.dtype, device=dev)

@@ -41,15 +41,17 @@ def test_library_is_sm100a_and_torch_free(pkg):
 def test_workspace_query_is_host_only(pkg):
     lib = pkg.native.load()
     assert lib.jb_version() >= 100
-    small = lib.jb_workspace_bytes(128, 64, 8192, 4, 1, 0)
+    small = lib.jb_workspace_bytes(128, 64, 8192, 4, 0, 0)
     assert 0 < small < 1 << 20
+    mixed = lib.jb_workspace_bytes(128, 64, 8192, 4, 1, 0)
+    assert mixed >= small + 8192 * 64 * 64 * 4  # FP32-phase V of every matrix
     assert lib.jb_workspace_bytes(0, 4, 1, 4, 0, 0) == 0
     assert lib.jb_workspace_bytes(4, 4, 1, 3, 0, 0) == 0
 
 
 def test_descriptor_layout_matches_header(pkg):
     B = __import__("importlib").import_module("pavel-s_svd_b200.batch")
-    assert pkg.native.DESC_BYTES == 48 == B.DESC_DTYPE.itemsize
+    assert pkg.native.DESC_BYTES == 56 == B.DESC_DTYPE.itemsize
     assert pkg.native.MatrixDesc.a_off.offset == 16
 
 
