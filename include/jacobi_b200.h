@@ -127,6 +127,33 @@ JB_API int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh,
                       int32_t *sweeps, int32_t *status,
                       void *workspace, size_t workspace_bytes, void *stream);
 
+/* Size of the fixed device scratch array of jb_svd_batched_f32_noalloc. */
+#define JB_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* jb_svd_batched_f32 without a workspace argument: allocates nothing.
+ * No counterpart in the reference (its Python solver always allocates); this
+ * is for callers that cannot allocate device memory when they solve, e.g.
+ * code running while a CUDA graph is being captured (cudaMalloc is illegal
+ * then) or plug-ins whose host framework owns all device allocations.
+ *   - Scratch is one file-scope __device__ array of JB_NOALLOC_SCRATCH_BYTES
+ *     (16 MiB) that every GPU loading the library keeps until process exit.
+ *   - Requests whose scratch would exceed it return JB_ETOOBIG: equal shapes
+ *     need about 256 bytes plus, with JB_PREC_MIXED, 4*batch*min(m,n)^2
+ *     bytes (e.g. at most 1023 matrices of 64 columns); shapes above 128 x 64
+ *     (tall view) run only if their work area fits in shared memory.
+ *   - The first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) and caches it; make that first call before any
+ *     stream capture.
+ *   - All calls share the array: calls that overlap on the GPU (other
+ *     streams, other host threads) race and corrupt each other's results;
+ *     serialise them.  Work tickets are cleared on the stream by each call.
+ * Other arguments and results: as jb_svd_batched_f32. */
+JB_API int jb_svd_batched_f32_noalloc(const float *A, float *U, float *S, float *Vh,
+                                      int64_t batch, int32_t m, int32_t n, int32_t rank,
+                                      int32_t flags, double tol, int32_t max_sweeps,
+                                      int32_t precision, int32_t *sweeps, int32_t *status,
+                                      void *stream);
+
 #ifdef __cplusplus
 }
 #endif

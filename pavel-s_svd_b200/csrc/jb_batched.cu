@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
+#include <mutex>
 #include "jacobi_b200.h"
 #include "jb_device.cuh"
 #include "jb_regblock.cuh"
@@ -744,6 +745,40 @@ static size_t uniform_workspace(int32_t m, int32_t n, int64_t count, int32_t ele
     return bytes;
 }
 
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of jb_svd_batched_f32.
+//
+// Some callers cannot allocate device memory at the moment they need an SVD:
+// code running while another library captures the stream into a CUDA graph
+// (cudaMalloc is not allowed during capture), plug-ins whose host framework
+// owns every device allocation, or real-time paths that must not touch the
+// allocator.  This entry point takes only inputs and outputs; its scratch
+// (the kernels' work tickets and, in mixed precision, the FP32-phase V of
+// every matrix) is the fixed array below, which every GPU that loads this
+// library holds until the process exits.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[JB_NOALLOC_SCRATCH_BYTES];
+
+static std::mutex g_noalloc_mutex;
+static void *g_noalloc_ptr[64];
+
+// Device address of g_noalloc_scratch on the current device.  In host code
+// the array's name is only a host-side stand-in, so the address is looked up
+// once per device (with that device current) and cached.
+static int noalloc_scratch(void **out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return JB_ECUDA;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void *ptr = nullptr;
+        if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) return JB_ECUDA;
+        g_noalloc_ptr[dev] = ptr;
+    }
+    *out = g_noalloc_ptr[dev];
+    return JB_OK;
+}
+
 }  // namespace jb
 
 using namespace jb;
@@ -817,6 +852,21 @@ int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh, const jb_ma
     p.tol = tol; p.max_sweeps = max_sweeps; p.tol32 = tol; p.max_sweeps32 = max_sweeps;
     p.sweeps = sweeps; p.status = status;
     return launch_any(p, pl, 4, precision, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int jb_svd_batched_f32_noalloc(const float *A, float *U, float *S, float *Vh, int64_t batch, int32_t m, int32_t n,
+                               int32_t rank, int32_t flags, double tol, int32_t max_sweeps, int32_t precision,
+                               int32_t *sweeps, int32_t *status, void *stream) {
+    int rc = check_common(batch, m, n, rank, flags, max_sweeps);
+    if (rc) return rc;
+    if (!A || !S || (!(flags & JB_VALUES_ONLY) && (!U || !Vh))) return JB_EINVAL;
+    if (precision != JB_PREC_NATIVE && precision != JB_PREC_MIXED) return JB_EINVAL;
+    if (batch == 0) return JB_OK;
+    if (uniform_workspace(m, n, batch, 4, precision, flags) > (size_t)JB_NOALLOC_SCRATCH_BYTES) return JB_ETOOBIG;
+    void *scratch = nullptr;
+    if ((rc = noalloc_scratch(&scratch))) return rc;
+    return jb_svd_batched_f32(A, U, S, Vh, batch, m, n, rank, flags, tol, max_sweeps, precision, sweeps, status,
+                              scratch, (size_t)JB_NOALLOC_SCRATCH_BYTES, stream);
 }
 
 }  // extern "C"

@@ -23,7 +23,8 @@ RC_NAMES = {JB_EINVAL: "invalid argument", JB_ETOOBIG: "shape too large for this
 
 # Exported symbols, in declaration order of include/jacobi_b200.h.
 SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_batched_f32",
-           "jb_svd_batched_f64", "jb_svd_uneven_f32")
+           "jb_svd_batched_f64", "jb_svd_uneven_f32", "jb_svd_batched_f32_noalloc")
+NOALLOC_SCRATCH_BYTES = 16 << 20  # JB_NOALLOC_SCRATCH_BYTES
 
 
 class MatrixDesc(ctypes.Structure):
@@ -54,6 +55,8 @@ def _declare(l):
     l.jb_svd_batched_f64.argtypes = [P, P, P, P, I64, I32, I32, I32, I32, F64, I32, P, P, P, SZ, P]
     l.jb_svd_uneven_f32.restype = ctypes.c_int
     l.jb_svd_uneven_f32.argtypes = [P, P, P, P, P, P, I64, I32, I32, F64, I32, I32, P, P, P, SZ, P]
+    l.jb_svd_batched_f32_noalloc.restype = ctypes.c_int
+    l.jb_svd_batched_f32_noalloc.argtypes = [P, P, P, P, I64, I32, I32, I32, I32, F64, I32, I32, P, P, P]
     return l
 
 
