@@ -127,6 +127,31 @@ JB_API int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh,
                       int32_t *sweeps, int32_t *status,
                       void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---- tensor-core building blocks (tcgen05, sm_100a) --------------------- */
+#define JB_GEMM_PLAIN   0   /* C = alpha A0 B0^T (+ C)                              */
+#define JB_GEMM_SPLIT3  1   /* C = alpha (A0 B0^T + A0 B1^T + A1 B0^T) (+ C): the
+                               compensated 3xBF16 product of X = A0 + A1 and
+                               Y = B0 + B1 (hi and lo BF16 parts)               */
+
+/* Batched BF16 GEMM on the 5th-generation tensor cores with an FP32
+ * accumulator in tensor memory.  A_i: batch x M x K, B_i: batch x N x K, both
+ * row-major BF16 (leading dimensions lda, ldb, multiples of 8; 16-byte
+ * aligned; batch strides in elements).  C: batch x M x N row-major FP32.
+ * beta 0 overwrites C, beta 1 adds to it.  split_k > 1 splits K over CTAs
+ * and accumulates atomically (C is zeroed first when beta is 0).
+ * error_flag (device int, may be NULL) is set to 1 if a pipeline wait timed
+ * out.  No counterpart in the reference, whose products are torch matmuls
+ * (svdbench/standalone/solvers.py:49-50, 52). */
+JB_API int jb_gemm_bf16(const void *A0, const void *A1, const void *B0, const void *B1,
+                        int32_t mode, float *C, int64_t M, int64_t N, int64_t K,
+                        int64_t lda, int64_t ldb, int64_t ldc, int64_t batch,
+                        int64_t strideA, int64_t strideB, int64_t strideC,
+                        float alpha, float beta, int32_t split_k, int32_t *error_flag,
+                        void *stream);
+
+/* hi = bf16(X), lo = bf16(X - hi) for n floats (lo may be NULL). */
+JB_API int jb_split_bf16(const float *X, void *hi, void *lo, int64_t n, void *stream);
+
 /* Size of the fixed device scratch array of jb_svd_batched_f32_noalloc. */
 #define JB_NOALLOC_SCRATCH_BYTES (16u << 20)
 

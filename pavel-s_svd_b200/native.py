@@ -23,7 +23,9 @@ RC_NAMES = {JB_EINVAL: "invalid argument", JB_ETOOBIG: "shape too large for this
 
 # Exported symbols, in declaration order of include/jacobi_b200.h.
 SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_batched_f32",
-           "jb_svd_batched_f64", "jb_svd_uneven_f32", "jb_svd_batched_f32_noalloc")
+           "jb_svd_batched_f64", "jb_svd_uneven_f32", "jb_gemm_bf16", "jb_split_bf16",
+           "jb_svd_batched_f32_noalloc")
+GEMM_PLAIN, GEMM_SPLIT3 = 0, 1
 NOALLOC_SCRATCH_BYTES = 16 << 20  # JB_NOALLOC_SCRATCH_BYTES
 
 
@@ -55,6 +57,11 @@ def _declare(l):
     l.jb_svd_batched_f64.argtypes = [P, P, P, P, I64, I32, I32, I32, I32, F64, I32, P, P, P, SZ, P]
     l.jb_svd_uneven_f32.restype = ctypes.c_int
     l.jb_svd_uneven_f32.argtypes = [P, P, P, P, P, P, I64, I32, I32, F64, I32, I32, P, P, P, SZ, P]
+    l.jb_gemm_bf16.restype = ctypes.c_int
+    l.jb_gemm_bf16.argtypes = [P, P, P, P, I32, P, I64, I64, I64, I64, I64, I64, I64, I64, I64, I64,
+                               ctypes.c_float, ctypes.c_float, I32, P, P]
+    l.jb_split_bf16.restype = ctypes.c_int
+    l.jb_split_bf16.argtypes = [P, P, P, I64, P]
     l.jb_svd_batched_f32_noalloc.restype = ctypes.c_int
     l.jb_svd_batched_f32_noalloc.argtypes = [P, P, P, P, I64, I32, I32, I32, I32, F64, I32, I32, P, P, P]
     return l

@@ -1,0 +1,58 @@
+"""tcgen05 GEMM (jb_gemm_bf16) against a PyTorch FP32 reference of the same op.
+
+Tolerances: the plain BF16 product is compared with torch's FP32 matmul of
+the same BF16 inputs (FP32 accumulation on both sides): rel. Frobenius error
+<= 1e-5.  The 3xBF16 product of FP32 inputs is compared with an FP64 matmul:
+rel. Frobenius error <= 5e-5 (about 2^-16 per product term)."""
+import importlib
+
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def T():
+    return importlib.import_module("pavel-s_svd_b200.tensor")
+
+
+def rel(a, b):
+    return float((a.double() - b.double()).norm() / b.double().norm())
+
+
+@pytest.mark.parametrize("M,N,K,batch,split", [(128, 128, 64, 1, 1), (300, 200, 520, 1, 1), (64, 64, 4096, 3, 4),
+                                                 (1000, 256, 2080, 1, 1), (128, 1024, 1024, 2, 1), (77, 33, 8, 1, 1)])
+def test_plain_bf16_gemm(T, M, N, K, batch, split):
+    g = torch.Generator(device="cuda").manual_seed(M * N + K)
+    a = torch.randn(batch, M, K, device="cuda", generator=g).bfloat16()
+    b = torch.randn(batch, N, K, device="cuda", generator=g).bfloat16()
+    flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+    c = T.gemm(a, b, split_k=split, error_flag=flag)
+    ref = a.float() @ b.float().transpose(-1, -2)
+    torch.cuda.synchronize()
+    assert int(flag) == 0
+    assert rel(c, ref) <= 1e-5
+
+
+def test_accumulate_and_alpha(T):
+    a = torch.randn(256, 192, device="cuda").bfloat16()
+    b = torch.randn(160, 192, device="cuda").bfloat16()
+    c0 = torch.randn(256, 160, device="cuda")
+    c = c0.clone()
+    T.gemm(a, b, c, alpha=-0.5, beta=1.0)
+    ref = c0 - 0.5 * (a.float() @ b.float().T)
+    assert rel(c, ref) <= 1e-5
+
+
+def test_split3_product_accuracy(T):
+    g = torch.Generator(device="cuda").manual_seed(5)
+    x = torch.randn(4, 4096, 64, device="cuda", generator=g)
+    y = torch.randn(4, 4096, 64, device="cuda", generator=g)
+    xh, xl = T.split_bf16(x.transpose(-1, -2).contiguous())   # (4, 64, 4096)
+    yh, yl = T.split_bf16(y.transpose(-1, -2).contiguous())
+    c = T.gemm(xh, yh, a_lo=xl, b_lo=yl, split_k=8)
+    ref = x.double().transpose(-1, -2) @ y.double()
+    e3 = rel(c, ref)
+    c1 = T.gemm(xh, yh)
+    assert e3 <= 5e-5 and e3 < rel(c1, ref) / 20
