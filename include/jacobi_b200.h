@@ -152,6 +152,54 @@ JB_API int jb_gemm_bf16(const void *A0, const void *A1, const void *B0, const vo
 /* hi = bf16(X), lo = bf16(X - hi) for n floats (lo may be NULL). */
 JB_API int jb_split_bf16(const float *X, void *hi, void *lo, int64_t n, void *stream);
 
+/* ---- learned warm start --------------------------------------------------
+ * No counterpart in the reference: its Jacobi always starts from V = I
+ * (svdbench/standalone/primitives.py:324). */
+
+/* Warm-start preparation for `batch` tall float32 matrices (m >= n, n a
+ * multiple of 4): V0 (batch x n x n, row-major, columns = start vectors, e.g.
+ * a network's prediction) is orthonormalised by Householder QR (the
+ * primitives.py:41-89 convention, column signs kept); the result is kept as
+ * start when it lowers the Gram off-norm ||offdiag(W^T W)||_F / ||W^T W||_F
+ * of W = A Q below that of A, else the start is the identity.  Writes
+ * Vstart (batch x n x n, column c contiguous), used[z] (1 = warm start kept)
+ * and the two off-norms (may be NULL). */
+JB_API int jb_warm_prep_f32(const float *A, const float *V0, float *Vstart, int32_t *used,
+                            float *off0, float *off1, int64_t batch, int32_t m, int32_t n,
+                            void *stream);
+
+/* jb_svd_batched_f32 starting the sweeps from V = Vstart, W = A Vstart
+ * instead of V = I (tall matrices up to 128 x 64). */
+JB_API int jb_svd_warm_f32(const float *A, const float *Vstart, float *U, float *S, float *Vh,
+                           int64_t batch, int32_t m, int32_t n, int32_t rank, int32_t flags,
+                           double tol, int32_t max_sweeps, int32_t precision,
+                           int32_t *sweeps, int32_t *status,
+                           void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- element-wise kernels of the warm-start network (jb_mlp.cu) --------- */
+/* dst[z] (cols x rows, bf16) = transpose of src[z] (rows x cols, f32 or bf16). */
+JB_API int jb_transpose_bf16(const void *src, int32_t src_is_f32, void *dst, int64_t rows,
+                             int64_t cols, int64_t batch, void *stream);
+/* out = act(Z + bias[col]) (ReLU when relu != 0), stored bf16 or f32. */
+JB_API int jb_bias_act(const float *Z, const float *bias, void *out, int64_t rows, int64_t cols,
+                       int32_t relu, int32_t out_bf16, void *stream);
+/* G = dH where H > 0 else 0 (H bf16), stored bf16 or f32. */
+JB_API int jb_relu_backward(const float *dH, const void *H, void *G, int32_t out_bf16, int64_t n,
+                            void *stream);
+/* out[c] = sum over rows of X[r][c]. */
+JB_API int jb_col_sum(const float *X, float *out, int64_t rows, int64_t cols, void *stream);
+/* dY = scale (Y - T); *loss += sum (Y - T)^2. */
+JB_API int jb_mse_grad(const float *Y, const float *T, float *dY, float *loss, int64_t n,
+                       float scale, void *stream);
+/* Adam step on a rows x cols parameter; refreshes its bf16 copy and (when
+ * wT_bf16 is given) its bf16 transpose. */
+JB_API int jb_adam(float *w, const float *g, float *m, float *v, void *w_bf16, void *wT_bf16,
+                   int64_t rows, int64_t cols, float lr, float beta1, float beta2, float eps,
+                   int32_t step, void *stream);
+/* X[z] = upper triangle (i <= j, row-major) of A^T A / ||A||_F^2 as bf16, for
+ * batch row-major m x n float32 matrices (the network's input sketch). */
+JB_API int jb_gram_sketch(const float *A, void *X, int64_t batch, int32_t m, int32_t n, void *stream);
+
 /* Size of the fixed device scratch array of jb_svd_batched_f32_noalloc. */
 #define JB_NOALLOC_SCRATCH_BYTES (16u << 20)
 

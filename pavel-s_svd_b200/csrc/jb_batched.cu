@@ -91,6 +91,7 @@ struct Params {
     unsigned char *gws;           // NULL: work area in shared memory
     size_t gws_stride;
     Dims maxd;                    // sizing of aux / region (largest matrix)
+    const float *vstart;          // warm start: nt x nt start V per matrix (x_off), or NULL
     float *x32;                   // mixed scratch (V of the FP32 phase)
     int64_t x_cap;                // floats available at x32
     size_t region_cap;            // bytes of the shared-memory work area
@@ -286,7 +287,8 @@ __device__ inline bool rdesc_fits(const jb_matrix_desc &d, int B, int elem, cons
     if ((d.flags & JB_FULL_MATRICES) && d.rank != nt) return false;
     const RGeo r = rgeo(mt, nt, B, d.flags);
     if (r.R > kMaxR || r.RV > kMaxRV) return false;
-    const size_t need = (mixed_scratch && elem == 8) ? rregion_mixed64(r, nt) : rregion_bytes(r, elem);
+    size_t need = (mixed_scratch && elem == 8) ? rregion_mixed64(r, nt) : rregion_bytes(r, elem);
+    if (elem == 4 && p.vstart) need += align16((size_t)r.ldw * nt * 4);
     if (need > p.region_cap) return false;
     if (r.ldw > p.maxd.mt || r.npb > p.maxd.np || r.ncp > p.maxd.ncp) return false;
     if (mixed_scratch && (d.x_off < 0 || d.x_off + (int64_t)nt * nt > p.x_cap)) return false;
@@ -309,6 +311,17 @@ __device__ void load_padded(const TI *A, const Geo &g, const RGeo &r, int e, T *
         W[(size_t)j * r.ldw + i] = dscale((T)A[idx], -e);
     }
     for (int j = threadIdx.x; j < r.npb; j += blockDim.x) V[(size_t)j * r.ldv + j] = T(1);
+}
+
+// A_t (tall view of A, float, rows < mt) into As (ld x nt, zero-filled).
+template <typename TI>
+__device__ void load_stage(const TI *A, const Geo &g, int ld, float *As) {
+    const int total = g.m * g.n;
+    for (int k = threadIdx.x; k < total; k += blockDim.x) {
+        const int row = k / g.n, col = k - row * g.n;
+        const int i = g.wide ? col : row, j = g.wide ? row : col;
+        As[(size_t)j * ld + i] = (float)A[k];
+    }
 }
 
 template <typename T, int B>
@@ -334,94 +347,30 @@ __device__ inline bool next_ticket(int *counter, int &s_idx, int64_t &idx) {
     return true;
 }
 
-// K1: FP32 sweeps.  MIXED: store the FP32 V (nt x nt) in the scratch for K2;
-// else run the epilogue and write U, S, Vh.
-template <bool MIXED>
-__global__ void __launch_bounds__(kT32) rb32_kernel(Params p) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_idx;
-    Aux ax = carve_aux(smem, p.maxd);
-    unsigned char *region = smem + aux_bytes(p.maxd);
-    for (;;) {
-        int64_t idx;
-        next_ticket(p.counter, s_idx, idx);
-        if (idx >= p.count) break;
-        const int64_t mat = p.order ? (int64_t)p.order[idx] : idx;
-        const jb_matrix_desc d = desc_of(p, mat);
-        if (threadIdx.x < 4) ax.flag[threadIdx.x] = 0;
-        __syncthreads();
-        int ns = 0, st = JB_ST_OK;
-        if (!rdesc_fits(d, kB32, 4, p, MIXED)) {
-            st = JB_ST_BAD_DESC;
-        } else {
-            const RGeo r = rgeo(d.m > d.n ? d.m : d.n, d.m > d.n ? d.n : d.m, kB32, d.flags);
-            const Geo g = reg_geo(d, r);
-            const float *A = (const float *)p.A + d.a_off;
-            float *W = (float *)region;
-            float *V = (float *)(region + align16((size_t)r.ldw * r.ncp * 4));
-            bool bad;
-            const int e = scan_input(A, g.m * g.n, ax, bad);
-            if (bad) {
-                st = JB_ST_NONFINITE_IN;
-            } else {
-                zero_fill(W, (size_t)r.ldw * r.ncp);
-                zero_fill(V, (size_t)r.ldv * r.npb);
-                __syncthreads();
-                load_padded(A, g, r, e, W, V);
-                __syncthreads();
-                const float tol = MIXED ? (p.tol32 > 0 ? (float)p.tol32 : 10.0f * Lim<float>::eps())
-                                        : (p.tol > 0 ? (float)p.tol : 10.0f * Lim<float>::eps());
-                bool conv;
-                ns = rb_dispatch<float, kB32>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true, ax.red, conv);
-                if (MIXED) {
-                    float *x = p.x32 + d.x_off;
-                    const int nt = g.nt;
-                    for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) {
-                        const int c = k / nt, i = k - c * nt;
-                        x[k] = V[(size_t)c * r.ldv + i];
-                    }
-                } else if (!conv) {
-                    st = JB_ST_NOT_CONVERGED;
-                } else {
-                    float *U = p.U ? (float *)p.U + d.u_off : nullptr;
-                    float *Vh = p.Vh ? (float *)p.Vh + d.v_off : nullptr;
-                    st = epilogue<float, float>(W, V, g, e, U, (float *)p.S + d.s_off, Vh, ax);
-                }
-            }
-        }
-        if (threadIdx.x == 0) {
-            if (p.status) p.status[mat] = st;
-            if (p.sweeps) p.sweeps[mat] = ns;
-        }
-        __syncthreads();
-    }
-}
-
-
 // C (M x N) = alpha * A (M x K) * B (K x N), column-major, in shared memory;
 // M and N multiples of 4.  Each thread owns 4 x 4 tiles of C, consecutive
 // lanes take consecutive row tiles (contiguous A loads, B loads broadcast).
-template <typename TA>
-__device__ void gemm_nn(double *C, int ldc, const TA *A, int lda, const double *B, int ldb, int M, int N, int K,
-                        double alpha) {
+template <typename TA, typename TC = double, typename TB = double>
+__device__ void gemm_nn(TC *C, int ldc, const TA *A, int lda, const TB *B, int ldb, int M, int N, int K,
+                        TC alpha) {
     const int tm = M >> 2, tn = N >> 2;
     for (int t = threadIdx.x; t < tm * tn; t += blockDim.x) {
         const int i0 = (t % tm) << 2, j0 = (t / tm) << 2;
-        double acc[4][4];
+        TC acc[4][4];
 #pragma unroll
         for (int r = 0; r < 4; ++r)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+            for (int c = 0; c < 4; ++c) acc[r][c] = TC(0);
         for (int k = 0; k < K; ++k) {
-            double a[4], b[4];
+            TC a[4], b[4];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) a[r] = (double)A[(size_t)k * lda + i0 + r];
+            for (int r = 0; r < 4; ++r) a[r] = (TC)A[(size_t)k * lda + i0 + r];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) b[c] = B[(size_t)(j0 + c) * ldb + k];
+            for (int c = 0; c < 4; ++c) b[c] = (TC)B[(size_t)(j0 + c) * ldb + k];
 #pragma unroll
             for (int r = 0; r < 4; ++r)
 #pragma unroll
-                for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+                for (int c = 0; c < 4; ++c) acc[r][c] = dfma(a[r], b[c], acc[r][c]);
         }
 #pragma unroll
         for (int r = 0; r < 4; ++r)
@@ -459,6 +408,88 @@ __device__ double polar_step(double *V, int n, int ld, double *VT, double *H, do
     __syncthreads();
     return err;
 }
+
+// K1: FP32 sweeps.  MIXED: store the FP32 V (nt x nt) in the scratch for K2;
+// else run the epilogue and write U, S, Vh.
+template <bool MIXED>
+__global__ void __launch_bounds__(kT32) rb32_kernel(Params p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_idx;
+    Aux ax = carve_aux(smem, p.maxd);
+    unsigned char *region = smem + aux_bytes(p.maxd);
+    for (;;) {
+        int64_t idx;
+        next_ticket(p.counter, s_idx, idx);
+        if (idx >= p.count) break;
+        const int64_t mat = p.order ? (int64_t)p.order[idx] : idx;
+        const jb_matrix_desc d = desc_of(p, mat);
+        if (threadIdx.x < 4) ax.flag[threadIdx.x] = 0;
+        __syncthreads();
+        int ns = 0, st = JB_ST_OK;
+        if (!rdesc_fits(d, kB32, 4, p, MIXED)) {
+            st = JB_ST_BAD_DESC;
+        } else {
+            const RGeo r = rgeo(d.m > d.n ? d.m : d.n, d.m > d.n ? d.n : d.m, kB32, d.flags);
+            const Geo g = reg_geo(d, r);
+            const float *A = (const float *)p.A + d.a_off;
+            float *W = (float *)region;
+            float *V = (float *)(region + align16((size_t)r.ldw * r.ncp * 4));
+            bool bad;
+            const int e = scan_input(A, g.m * g.n, ax, bad);
+            if (bad) {
+                st = JB_ST_NONFINITE_IN;
+            } else {
+                zero_fill(W, (size_t)r.ldw * r.ncp);
+                zero_fill(V, (size_t)r.ldv * r.npb);
+                __syncthreads();
+                if (!p.vstart) {
+                    load_padded(A, g, r, e, W, V);
+                } else {
+                    // Warm start: V = given start (identity on the padding),
+                    // W = A_t V with A_t staged after the work area.
+                    float *As = (float *)(region + rregion_bytes(r, 4));
+                    const int nt = g.nt;
+                    zero_fill(As, (size_t)r.ldw * nt);
+                    __syncthreads();
+                    load_stage(A, g, r.ldw, As);
+                    const float *vs = p.vstart + d.x_off;
+                    for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) {
+                        const int c = k / nt, i = k - c * nt;
+                        V[(size_t)c * r.ldv + i] = vs[k];
+                    }
+                    for (int j = nt + threadIdx.x; j < r.npb; j += blockDim.x) V[(size_t)j * r.ldv + j] = 1.0f;
+                    __syncthreads();
+                    gemm_nn<float, float, float>(W, r.ldw, As, r.ldw, V, r.ldv, r.ldw, r.npb, nt, ldexpf(1.0f, -e));
+                }
+                __syncthreads();
+                const float tol = MIXED ? (p.tol32 > 0 ? (float)p.tol32 : 10.0f * Lim<float>::eps())
+                                        : (p.tol > 0 ? (float)p.tol : 10.0f * Lim<float>::eps());
+                bool conv;
+                ns = rb_dispatch<float, kB32>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true, ax.red, conv);
+                if (MIXED) {
+                    float *x = p.x32 + d.x_off;
+                    const int nt = g.nt;
+                    for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) {
+                        const int c = k / nt, i = k - c * nt;
+                        x[k] = V[(size_t)c * r.ldv + i];
+                    }
+                } else if (!conv) {
+                    st = JB_ST_NOT_CONVERGED;
+                } else {
+                    float *U = p.U ? (float *)p.U + d.u_off : nullptr;
+                    float *Vh = p.Vh ? (float *)p.Vh + d.v_off : nullptr;
+                    st = epilogue<float, float>(W, V, g, e, U, (float *)p.S + d.s_off, Vh, ax);
+                }
+            }
+        }
+        if (threadIdx.x == 0) {
+            if (p.status) p.status[mat] = st;
+            if (p.sweeps) p.sweeps[mat] = ns;
+        }
+        __syncthreads();
+    }
+}
+
 
 // K2: FP64 sweeps.  MIXED (TI = float): start from the FP32 V of K1, made
 // orthogonal to FP64 accuracy by Newton-Schulz polar steps (it is orthogonal
@@ -529,12 +560,7 @@ __global__ void __launch_bounds__(kT64) rb64_kernel(Params p) {
                     float *As = (float *)X2;
                     zero_fill(As, (size_t)r.ldw * nt);
                     __syncthreads();
-                    const int total = g.m * g.n;
-                    for (int k = threadIdx.x; k < total; k += blockDim.x) {
-                        const int row = k / g.n, col = k - row * g.n;
-                        const int i = g.wide ? col : row, j = g.wide ? row : col;
-                        As[(size_t)j * r.ldw + i] = (float)A[k];
-                    }
+                    load_stage(A, g, r.ldw, As);
                     __syncthreads();
                     gemm_nn<float>(W, r.ldw, As, r.ldw, V, r.ldv, r.ldw, r.npb, nt, ldexp(1.0, -e));
                     for (int j = r.npb; j < r.ncp; ++j)
@@ -557,6 +583,82 @@ __global__ void __launch_bounds__(kT64) rb64_kernel(Params p) {
         if (threadIdx.x == 0) {
             if (p.status) p.status[mat] = st;
             if (p.sweeps) p.sweeps[mat] = ns;
+        }
+        __syncthreads();
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// Warm start preparation (one CTA per matrix): V0 (the network's guess,
+// row-major n x n, columns = start vectors) -> Householder QR, column signs
+// kept (householder_orthonormalize) -> Q.  The start is kept when it lowers
+// the Gram off-norm ||offdiag(W^T W)||_F / ||W^T W||_F of W = A Q below that
+// of A itself; otherwise the start is the identity (the plain solver).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) warm_prep_kernel(const float *A, const float *V0, float *Vs, int32_t *used,
+                                                        float *off0, float *off1, int64_t batch, int m, int n) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int ldm = (m + 3) & ~3;
+    float *Arow = (float *)smem;                                   // m x n row-major
+    float *Acol = Arow + (size_t)m * n;                            // ldm x n column-major
+    double *G = (double *)(smem + align16(((size_t)m * n + (size_t)ldm * n) * 4));  // n x n
+    double *Q = G + (size_t)n * n;
+    double *T = Q + (size_t)n * n;
+    Aux ax;
+    ax.red = T + (size_t)n * n;
+    ax.tau = ax.red + 64;
+    ax.sig = ax.tau + n;
+    for (int64_t z = blockIdx.x; z < batch; z += gridDim.x) {
+        const float *a = A + z * (int64_t)m * n;
+        for (int k = threadIdx.x; k < ldm * n; k += blockDim.x) Acol[k] = 0.f;
+        __syncthreads();
+        for (int k = threadIdx.x; k < m * n; k += blockDim.x) {
+            const int i = k / n, j = k - i * n;
+            const float x = a[k];
+            Arow[k] = x;
+            Acol[(size_t)j * ldm + i] = x;
+        }
+        __syncthreads();
+        // G = A^T A (A^T column-major is A row-major).
+        gemm_nn<float, double, float>(G, n, Arow, n, Acol, ldm, n, n, m, 1.0);
+        __syncthreads();
+        double on = 0.0, dg = 0.0;
+        for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+            const int c = k / n, i = k - c * n;
+            const double g2 = G[k] * G[k];
+            if (i == c) dg += g2; else on += g2;
+        }
+        const double off_a = sqrt(block_sum(on, ax.red) / fmax(block_sum(on + dg, ax.red), 1e-300));
+        const float *v0 = V0 + z * (int64_t)n * n;
+        for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+            const int i = k / n, j = k - i * n;
+            Q[(size_t)j * n + i] = (double)v0[k];
+        }
+        __syncthreads();
+        householder_orthonormalize(Q, n, n, T, n, ax);
+        // G1 = Q^T (G Q): T = G Q, then G1_ij = q_i . T_j.
+        gemm_nn<double, double, double>(T, n, G, n, Q, n, n, n, n, 1.0);
+        __syncthreads();
+        on = 0.0;
+        dg = 0.0;
+        for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+            const int j = k / n, i = k - j * n;
+            double acc = 0.0;
+            for (int t = 0; t < n; ++t) acc = fma(Q[(size_t)i * n + t], T[(size_t)j * n + t], acc);
+            if (i == j) dg += acc * acc; else on += acc * acc;
+        }
+        const double off_q = sqrt(block_sum(on, ax.red) / fmax(block_sum(on + dg, ax.red), 1e-300));
+        const bool keep = off_q < off_a;
+        float *vs = Vs + z * (int64_t)n * n;
+        for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+            const int c = k / n, i = k - c * n;
+            vs[k] = keep ? (float)Q[(size_t)c * n + i] : (i == c ? 1.f : 0.f);
+        }
+        if (threadIdx.x == 0) {
+            if (used) used[z] = keep;
+            if (off0) off0[z] = (float)off_a;
+            if (off1) off1[z] = (float)off_q;
         }
         __syncthreads();
     }
@@ -852,6 +954,54 @@ int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh, const jb_ma
     p.tol = tol; p.max_sweeps = max_sweeps; p.tol32 = tol; p.max_sweeps32 = max_sweeps;
     p.sweeps = sweeps; p.status = status;
     return launch_any(p, pl, 4, precision, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+
+int jb_warm_prep_f32(const float *A, const float *V0, float *Vstart, int32_t *used, float *off0, float *off1,
+                     int64_t batch, int32_t m, int32_t n, void *stream) {
+    if (!A || !V0 || !Vstart || batch < 0 || m < n || n < 1 || n % 4) return JB_EINVAL;
+    if (batch == 0) return JB_OK;
+    const int ldm = (m + 3) & ~3;
+    const size_t smem = align16(((size_t)m * n + (size_t)ldm * n) * 4) + ((size_t)3 * n * n + 64 + 2 * n) * 8;
+    if (smem > kSmemLimit) return JB_ETOOBIG;
+    if (cudaFuncSetAttribute(warm_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return JB_ECUDA;
+    const int sms = sm_count();
+    if (sms <= 0) return JB_ECUDA;
+    int64_t grid = (int64_t)sms * 4;
+    if (grid > batch) grid = batch;
+    warm_prep_kernel<<<(unsigned)grid, 256, smem, (cudaStream_t)stream>>>(A, V0, Vstart, used, off0, off1, batch,
+                                                                          m, n);
+    return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+}
+
+int jb_svd_warm_f32(const float *A, const float *Vstart, float *U, float *S, float *Vh, int64_t batch, int32_t m,
+                    int32_t n, int32_t rank, int32_t flags, double tol, int32_t max_sweeps, int32_t precision,
+                    int32_t *sweeps, int32_t *status, void *workspace, size_t workspace_bytes, void *stream) {
+    int rc = check_common(batch, m, n, rank, flags, max_sweeps);
+    if (rc) return rc;
+    if (!A || !Vstart || !S || m < n || (!(flags & JB_VALUES_ONLY) && (!U || !Vh))) return JB_EINVAL;
+    if (precision != JB_PREC_NATIVE && precision != JB_PREC_MIXED) return JB_EINVAL;
+    if (batch == 0) return JB_OK;
+    Plan pl = make_plan(m, n, 4, precision, flags);
+    if (!pl.reg) return JB_ETOOBIG;
+    const size_t stage = align16((size_t)32 * ((m + 31) / 32) * n * 4);
+    pl.reg32 += stage;
+    pl.smem32 += stage;
+    if (pl.smem32 > kSmemLimit) return JB_ETOOBIG;
+    if (workspace_bytes < uniform_workspace(m, n, batch, 4, precision, flags)) return JB_EWORKSPACE;
+    Params p;
+    memset(&p, 0, sizeof(p));
+    p.A = A;
+    p.U = (flags & JB_VALUES_ONLY) ? nullptr : U;
+    p.S = S;
+    p.Vh = (flags & JB_VALUES_ONLY) ? nullptr : Vh;
+    p.count = batch; p.um = m; p.un = n; p.urank = rank; p.uflags = flags & ~JB_ROUND_ROBIN;
+    p.tol = tol; p.max_sweeps = max_sweeps; p.tol32 = tol; p.max_sweeps32 = max_sweeps;
+    p.sweeps = sweeps; p.status = status;
+    p.vstart = Vstart;
+    return launch_reg(p, pl, 4, precision, (unsigned char *)workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
 int jb_svd_batched_f32_noalloc(const float *A, float *U, float *S, float *Vh, int64_t batch, int32_t m, int32_t n,

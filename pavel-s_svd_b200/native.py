@@ -24,7 +24,8 @@ RC_NAMES = {JB_EINVAL: "invalid argument", JB_ETOOBIG: "shape too large for this
 # Exported symbols, in declaration order of include/jacobi_b200.h.
 SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_batched_f32",
            "jb_svd_batched_f64", "jb_svd_uneven_f32", "jb_gemm_bf16", "jb_split_bf16",
-           "jb_svd_batched_f32_noalloc")
+           "jb_warm_prep_f32", "jb_svd_warm_f32", "jb_transpose_bf16", "jb_bias_act", "jb_relu_backward",
+           "jb_col_sum", "jb_mse_grad", "jb_adam", "jb_gram_sketch", "jb_svd_batched_f32_noalloc")
 GEMM_PLAIN, GEMM_SPLIT3 = 0, 1
 NOALLOC_SCRATCH_BYTES = 16 << 20  # JB_NOALLOC_SCRATCH_BYTES
 
@@ -62,6 +63,19 @@ def _declare(l):
                                ctypes.c_float, ctypes.c_float, I32, P, P]
     l.jb_split_bf16.restype = ctypes.c_int
     l.jb_split_bf16.argtypes = [P, P, P, I64, P]
+    FL = ctypes.c_float
+    for name, args in (("jb_warm_prep_f32", [P, P, P, P, P, P, I64, I32, I32, P]),
+                       ("jb_svd_warm_f32", [P, P, P, P, P, I64, I32, I32, I32, I32, F64, I32, I32, P, P, P, SZ, P]),
+                       ("jb_transpose_bf16", [P, I32, P, I64, I64, I64, P]),
+                       ("jb_bias_act", [P, P, P, I64, I64, I32, I32, P]),
+                       ("jb_relu_backward", [P, P, P, I32, I64, P]),
+                       ("jb_col_sum", [P, P, I64, I64, P]),
+                       ("jb_mse_grad", [P, P, P, P, I64, FL, P]),
+                       ("jb_adam", [P, P, P, P, P, P, I64, I64, FL, FL, FL, FL, I32, P]),
+                       ("jb_gram_sketch", [P, P, I64, I32, I32, P])):
+        f = getattr(l, name)
+        f.restype = ctypes.c_int
+        f.argtypes = args
     l.jb_svd_batched_f32_noalloc.restype = ctypes.c_int
     l.jb_svd_batched_f32_noalloc.argtypes = [P, P, P, P, I64, I32, I32, I32, I32, F64, I32, I32, P, P, P]
     return l

@@ -100,23 +100,43 @@ def _expm_skew(k):
     return np.real((q * e[..., None, :]) @ np.conj(np.swapaxes(q, -1, -2)))
 
 
+def family_v(theta, seed=4, n=64, dims=16, strength=0.3, device=None):
+    """The generator's V(theta) = expm(strength * sum_i theta_i K_i) for given
+    theta (count, dims): the smooth frame of the warm-start family."""
+    _, basis = skew_basis(seed, n, dims)
+    k = strength * np.einsum("bd,dij->bij", np.asarray(theta), basis)
+    if device is None:
+        return _expm_skew(k)
+    import torch
+    return torch.linalg.matrix_exp(torch.from_numpy(k).to(device)).float()
+
+
 def warm_family(count=65536, seed=4, m=128, n=64, dims=16, strength=0.3, decades=3.0,
-                chunk=4096):
+                chunk=4096, device=None):
     """A = U diag(s) V^T with U = qr(G m x n).Q, log10 s ~ U[-decades, 0] (unsorted),
     V = expm(strength * sum_i theta_i K_i), theta ~ N(0, I_dims).
 
     Returns (A float32 (count, m, n), theta float64 (count, dims)).  Draw order:
     the skew basis, then all theta, then per chunk the U Gaussians and the
-    spectra."""
+    spectra.  With `device` (a CUDA torch device) the QR and exp steps run
+    in float64 on that device (same draws; results equal to rounding)."""
     rng, basis = skew_basis(seed, n, dims)
     theta = rng.standard_normal((count, dims))
     out = np.empty((count, m, n), np.float32)
     for lo in range(0, count, chunk):
         hi = min(lo + chunk, count)
         g = rng.standard_normal((hi - lo, m, n))
-        u, _ = np.linalg.qr(g, mode="reduced")
         s = 10.0 ** (-decades * rng.random((hi - lo, n)))
         k = strength * np.einsum("bd,dij->bij", theta[lo:hi], basis)
-        v = _expm_skew(k)
-        out[lo:hi] = ((u * s[:, None, :]) @ np.swapaxes(v, -1, -2)).astype(np.float32)
+        if device is None:
+            u, _ = np.linalg.qr(g, mode="reduced")
+            v = _expm_skew(k)
+            out[lo:hi] = ((u * s[:, None, :]) @ np.swapaxes(v, -1, -2)).astype(np.float32)
+        else:
+            import torch
+            gt = torch.from_numpy(g).to(device)
+            u = torch.linalg.qr(gt, mode="reduced")[0]
+            v = torch.linalg.matrix_exp(torch.from_numpy(k).to(device))
+            a = (u * torch.from_numpy(s).to(device)[:, None, :]) @ v.transpose(-1, -2)
+            out[lo:hi] = a.float().cpu().numpy()
     return out, theta
