@@ -132,6 +132,12 @@ JB_API int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh,
 #define JB_GEMM_SPLIT3  1   /* C = alpha (A0 B0^T + A0 B1^T + A1 B0^T) (+ C): the
                                compensated 3xBF16 product of X = A0 + A1 and
                                Y = B0 + B1 (hi and lo BF16 parts)               */
+#define JB_GEMM_SPLIT6  2   /* three-part split X = A0 + A1 + A2 (hi, mid, lo),
+                               six products (every pair of parts two or fewer
+                               splits below the leading one): ~FP32 accuracy
+                               (jb_gemm_bf16x only)                            */
+#define JB_GEMM_B_MN    4   /* flag: B_i is stored K x N row-major (N
+                               contiguous, leading dimension ldb >= N)         */
 
 /* Batched BF16 GEMM on the 5th-generation tensor cores with an FP32
  * accumulator in tensor memory.  A_i: batch x M x K, B_i: batch x N x K, both
@@ -149,8 +155,20 @@ JB_API int jb_gemm_bf16(const void *A0, const void *A1, const void *B0, const vo
                         float alpha, float beta, int32_t split_k, int32_t *error_flag,
                         void *stream);
 
+/* jb_gemm_bf16 with the split parts as arrays: A[0..s), B[0..s) where s is
+ * 1 (PLAIN), 2 (SPLIT3) or 3 (SPLIT6). */
+JB_API int jb_gemm_bf16x(const void *const *A, const void *const *B, int32_t mode, float *C,
+                         int64_t M, int64_t N, int64_t K, int64_t lda, int64_t ldb, int64_t ldc,
+                         int64_t batch, int64_t strideA, int64_t strideB, int64_t strideC,
+                         float alpha, float beta, int32_t split_k, int32_t *error_flag,
+                         void *stream);
+
 /* hi = bf16(X), lo = bf16(X - hi) for n floats (lo may be NULL). */
 JB_API int jb_split_bf16(const float *X, void *hi, void *lo, int64_t n, void *stream);
+
+/* Three-part split: hi = bf16(X), mid = bf16(X - hi), lo = bf16(X - hi - mid)
+ * (lo may be NULL, then as jb_split_bf16). */
+JB_API int jb_split3_bf16(const float *X, void *hi, void *mid, void *lo, int64_t n, void *stream);
 
 /* ---- learned warm start --------------------------------------------------
  * No counterpart in the reference: its Jacobi always starts from V = I
@@ -199,6 +217,47 @@ JB_API int jb_adam(float *w, const float *g, float *m, float *v, void *w_bf16, v
 /* X[z] = upper triangle (i <= j, row-major) of A^T A / ||A||_F^2 as bf16, for
  * batch row-major m x n float32 matrices (the network's input sketch). */
 JB_API int jb_gram_sketch(const float *A, void *X, int64_t batch, int32_t m, int32_t n, void *stream);
+
+/* ---- blocked one-sided Jacobi (large matrices) ---------------------------
+ * Building blocks of block_jacobi (svdbench/standalone/solvers.py:30-68) on
+ * the tensor cores: block-pair Grams and rotations run on jb_gemm_bf16x, the
+ * rest on these kernels (jb_block.cu). */
+
+/* FP64 eigen-solve of `pairs` symmetric n x n FP32 Grams G[k] (n even): the
+ * one-sided Jacobi rotations of the slot's columns applied to its Gram
+ * (G <- J^T G J, round-robin pairs, relative threshold tol, at most
+ * max_sweeps sweeps).  Writes vv^T (rows = eigenvectors, eigenvalues
+ * descending: the inner solve's V of solvers.py:48) as hi/lo BF16 (and a
+ * third part when Qt_lo2 is given), the
+ * largest pair ratio |g_pq| / sqrt(g_pp g_qq) of the first sweep (off) and
+ * the sweeps used. */
+JB_API int jb_block_eig_f64(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off,
+                            int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps, double tol,
+                            void *stream);
+
+/* Row r of src (rows x L, FP32) -> row map[r] (identity when NULL) of the
+ * BF16 parts hi, lo, lo2 (a two- or three-part split; any may be NULL)
+ * and/or an FP32 destination. */
+JB_API int jb_rows_scatter(const float *src, const int32_t *map, void *hi, void *lo, void *lo2,
+                           float *f32, int64_t rows, int64_t L, void *stream);
+
+/* Row r of hi (+ lo (+ lo2)) BF16 -> row map[r] of dst (FP32). */
+JB_API int jb_rows_combine(const void *hi, const void *lo, const void *lo2, const int32_t *map,
+                           float *dst, int64_t rows, int64_t L, void *stream);
+
+/* C (M x N, f32) = A (M x K) B (N x K)^T, FP32 inputs (row-major, K
+ * contiguous) with FP64 accumulation on the CUDA cores: recomputes W = A V
+ * from the exact input at the end of the blocked solve. */
+JB_API int jb_gemm_f64acc(const float *A, const float *B, float *C, int64_t M, int64_t N, int64_t K,
+                          int64_t lda, int64_t ldb, int64_t ldc, void *stream);
+
+/* Final step: sigma_j = ||Wt row j|| (FP64), stable descending order perm,
+ * S[r] = sigma * 2^e or 0 below eps32 * cut_width * sigma_1, U (m x rank,
+ * row-major) = W[:, perm] / sigma, Vh (rank x n) = Vt[perm, :].  sig (n
+ * doubles) and perm (n ints) are device scratch. */
+JB_API int jb_block_finish(const float *Wt, const float *Vt, float *U, float *S, float *Vh, double *sig,
+                           int32_t *perm, int64_t m, int64_t n, int32_t rank, int32_t e,
+                           int32_t cut_width, void *stream);
 
 /* Size of the fixed device scratch array of jb_svd_batched_f32_noalloc. */
 #define JB_NOALLOC_SCRATCH_BYTES (16u << 20)

@@ -1,0 +1,238 @@
+"""Blocked one-sided Jacobi SVD of one large matrix on the tensor cores.
+
+Counterpart of block_jacobi (svdbench/standalone/solvers.py:30-68): column
+blocks of width b, a round-robin tournament over blocks, and per block pair
+the rotation vv of the pair's own SVD applied to W and V.  B200 form:
+
+phase 1 (tensor cores, FP64 eigen-solves), per round, all block pairs at once
+(two-part 3xBF16 operands while the off value is above 5e-2, then three-part
+6xBF16 operands, ~FP32, until it is <= tol_phase1):
+    G_k  = X_k^T X_k               jb_gemm_bf16x SPLIT3, split-K (<= 128-long
+                                   accumulation chains), X_k = the pair's 2b
+                                   columns (a "slot" of W^T rows)
+    vv_k = eig(G_k), descending     jb_block_eig_f64 (FP64)
+    W_k  <- W_k vv_k, V_k <- V_k vv_k   jb_gemm_bf16x SPLIT3 (B N-contiguous),
+                                   scattered into the next round's slots
+  until the largest pair ratio |g_pq| / sqrt(g_pp g_qq) of a sweep (FP64) is
+  <= tol_phase1.  Carrying W in 16-bit parts would cost a small column
+  ~2^-16 sigma_1 / sigma_j of its own accuracy per rotation; the three-part
+  sweeps bring that to the FP32 level before V is taken.
+phase 2 (accuracy): V <- V (3I - V^T V) / 2 (Newton-Schulz, SPLIT6 products,
+  ~FP32 accurate), W = A V recomputed from the exact input with FP64
+  accumulation (jb_gemm_f64acc), sigma = column norms of W in FP64.  With V
+  orthogonal to ~1e-6 (a multiplicative perturbation of every sigma) and
+  W's columns orthogonal to ~tol_phase1 (an error ~tol_phase1^2 relative),
+  every sigma above the cut keeps a relative error of a few 1e-6.
+Outputs follow the reference: sigma sorted descending, values below
+eps32 * max(m, n) * sigma_1 reported as 0 (solvers.py:18-21).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from . import native as N
+from .tensor import gemm_parts, split3_bf16, split_bf16
+
+CHAIN = 128  # longest tensor-memory accumulation chain (K) per CTA
+
+
+def _st(dev):
+    return torch.cuda.current_stream(dev).cuda_stream
+
+
+def circ(pos, r, n):
+    return 0 if pos == 0 else 1 + (pos - 1 - r) % (n - 1)
+
+
+def schedule(nb):
+    """slot[r][k] = (i, j), i < j: the blocks of pair slot k in round r
+    (circle method, primitives.py:309-313)."""
+    out = []
+    for r in range(nb - 1):
+        row = []
+        for k in range(nb // 2):
+            a, b = circ(k, r, nb), circ(nb - 1 - k, r, nb)
+            row.append((min(a, b), max(a, b)))
+        out.append(row)
+    return out
+
+
+def _split_k(K):
+    return max(1, min(64, math.ceil(K / CHAIN)))
+
+
+class BlockJacobi:
+    """Plan + buffers for one m x n (m >= n) float32 matrix, block width b."""
+
+    def __init__(self, m, n, block_size, device="cuda"):
+        self.m, self.n, self.b = int(m), int(n), int(block_size)
+        if self.m < self.n:
+            raise ValueError("BlockJacobi takes tall matrices (m >= n)")
+        b = self.b
+        if b < 8 or b % 8 or 2 * b > 128:
+            raise ValueError("block_size must be a multiple of 8 in [8, 64]")
+        nb = -(-self.n // b)
+        nb += nb % 2
+        self.nb, self.npad, self.P = nb, nb * b, nb // 2
+        self.mpad = -(-self.m // 8) * 8
+        dev = torch.device(device)
+        if dev.type == "cuda" and dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        self.sched = schedule(nb)
+        R = nb - 1
+        # slot position of every block in every round: pos[r][blk] = (k, h)
+        pos = np.zeros((R, nb, 2), np.int64)
+        for r, row in enumerate(self.sched):
+            for k, (i, j) in enumerate(row):
+                pos[r, i] = (k, 0)
+                pos[r, j] = (k, 1)
+        self.pos = pos
+        # update output row (k, t) of round r -> row in round r+1's layout
+        maps = np.zeros((R, self.P * 2 * b), np.int32)
+        for r in range(R):
+            nr = (r + 1) % R
+            for k, (i, j) in enumerate(self.sched[r]):
+                for t in range(2 * b):
+                    blk = i if t < b else j
+                    k2, h2 = pos[nr, blk]
+                    maps[r, k * 2 * b + t] = k2 * 2 * b + h2 * b + (t % b)
+        self.maps = torch.from_numpy(maps).to(dev)
+        # column c -> row of round 0's layout; and the inverse for every round
+        init = np.zeros(self.npad, np.int32)
+        for c in range(self.npad):
+            k, h = pos[0, c // b]
+            init[c] = k * 2 * b + h * b + c % b
+        self.init_map = torch.from_numpy(init).to(dev)
+        back = np.zeros((R, self.npad), np.int32)
+        for r in range(R):
+            for c in range(self.npad):
+                k, h = pos[r, c // b]
+                back[r, k * 2 * b + h * b + c % b] = c
+        self.back_maps = torch.from_numpy(back).to(dev)
+        bf = dict(dtype=torch.bfloat16, device=dev)
+        rows = self.P * 2 * b
+        # [buffer][part]: hi, mid (lo of the two-part split), lo (three-part split)
+        self.W = [[torch.zeros(rows, self.mpad, **bf) for _ in range(3)] for _ in range(2)]
+        self.V = [[torch.zeros(rows, self.npad, **bf) for _ in range(3)] for _ in range(2)]
+        f32 = dict(dtype=torch.float32, device=dev)
+        self.G = torch.empty(self.P, 2 * b, 2 * b, **f32)
+        self.Qt = [torch.empty(self.P, 2 * b, 2 * b, **bf) for _ in range(3)]
+        self.off = torch.zeros(R, self.P, **f32)
+        self.isweeps = torch.zeros(self.P, dtype=torch.int32, device=dev)
+        self.CW = torch.empty(self.P, 2 * b, self.mpad, **f32)
+        self.CV = torch.empty(self.P, 2 * b, self.npad, **f32)
+
+    def _combine_v(self, cur):
+        """V^T (npad x npad, FP32) from the slots of buffer `cur` (round 0 layout)."""
+        vt = torch.empty(self.npad, self.npad, dtype=torch.float32, device=self.device)
+        N.check(N.lib().jb_rows_combine(self.V[cur][0].data_ptr(), self.V[cur][1].data_ptr(),
+                                        self.V[cur][2].data_ptr(), self.back_maps[0].data_ptr(), vt.data_ptr(),
+                                        self.P * 2 * self.b, self.npad, _st(self.device)), "combine V")
+        return vt
+
+    def _polar(self, vt, steps):
+        """Newton-Schulz: V <- V (3I - V^T V) / 2 on V^T rows (G = Vt Vt^T,
+        Vt <- H Vt), SPLIT6 products with 128-long accumulation chains."""
+        eye = torch.eye(self.npad, dtype=torch.float32, device=self.device)
+        sk = _split_k(self.npad)
+        for _ in range(steps):
+            vp = split3_bf16(vt)
+            g = gemm_parts(vp, vp, split_k=sk)[0]
+            h = (3.0 * eye - g) * 0.5
+            vt = gemm_parts(split3_bf16(h), vp, b_mn=True, split_k=sk)[0]
+        return vt
+
+    def _w_from_v(self, vt, ap):
+        """W^T = V^T A^T with FP64 accumulation of exact float products."""
+        wt = torch.empty(self.npad, self.mpad, dtype=torch.float32, device=self.device)
+        N.check(N.lib().jb_gemm_f64acc(vt.data_ptr(), ap.data_ptr(), wt.data_ptr(), self.npad, self.mpad, self.npad,
+                                       self.npad, self.npad, self.mpad, _st(self.device)), "jb_gemm_f64acc")
+        return wt
+
+    def solve(self, a: torch.Tensor, *, tol_phase1=5e-6, switch=5e-2, max_sweeps=30, inner_sweeps=2,
+              inner_tol=1e-7, polar_steps=2):
+        """SVD of a (m x n float32, CUDA).  Returns U (m x n), S (n), Vh (n x n),
+        info dict.  Sweeps run with two-part (3xBF16) operands while the
+        sweep's off value is above `switch`, then with three-part (6xBF16,
+        ~FP32) operands until it is <= tol_phase1."""
+        lib = N.lib()
+        dev, st = self.device, _st(self.device)
+        m, n, b, P, R = self.m, self.n, self.b, self.P, self.nb - 1
+        if tuple(a.shape) != (m, n) or a.dtype != torch.float32 or a.device != dev:
+            raise ValueError("input must be a float32 (m, n) tensor on the plan's device")
+        if not bool(torch.isfinite(a).all()):
+            raise ValueError("input contains NaN or infinity")
+        amax = float(a.abs().max())
+        e = math.frexp(amax)[1] if amax > 0 else 0
+        # A padded (mpad x npad), scaled by 2^-e (exact); W^T rows = columns of A.
+        ap = torch.zeros(self.mpad, self.npad, dtype=torch.float32, device=dev)
+        ap[:m, :n] = a * (2.0 ** -e)
+        at = ap.t().contiguous()                                   # npad x mpad
+        eye = torch.eye(self.npad, dtype=torch.float32, device=dev)
+        for buf, src, L in ((self.W[0], at, self.mpad), (self.V[0], eye, self.npad)):
+            buf[2].zero_()
+            N.check(lib.jb_rows_scatter(src.data_ptr(), self.init_map.data_ptr(), buf[0].data_ptr(), buf[1].data_ptr(),
+                                        None, None, self.npad, L, st), "scatter")
+        cur = 0
+        sweeps = 0
+        off_hist = []
+        parts = 2
+        skW = _split_k(self.mpad)
+        rows = P * 2 * b
+        for sweeps in range(1, max_sweeps + 1):
+            for r in range(R):
+                Wp = [x.view(P, 2 * b, self.mpad) for x in self.W[cur][:parts]]
+                Vp = [x.view(P, 2 * b, self.npad) for x in self.V[cur][:parts]]
+                # Grams of every slot: G_k = X_k X_k^T with X_k = 2b rows of W^T.
+                gemm_parts(Wp, Wp, self.G, split_k=skW)
+                N.check(lib.jb_block_eig_f64(self.G.data_ptr(), self.Qt[0].data_ptr(), self.Qt[1].data_ptr(),
+                                             self.Qt[2].data_ptr() if parts == 3 else None, self.off[r].data_ptr(),
+                                             self.isweeps.data_ptr(), P, 2 * b, inner_sweeps, inner_tol, st),
+                        "jb_block_eig_f64")
+                # X_k <- vv^T X_k (rows of W^T), same for V.
+                gemm_parts(self.Qt[:parts], Wp, self.CW, b_mn=True)
+                gemm_parts(self.Qt[:parts], Vp, self.CV, b_mn=True)
+                nxt = 1 - cur
+                mp = self.maps[r].data_ptr()
+                for buf, src, L in ((self.W[nxt], self.CW, self.mpad), (self.V[nxt], self.CV, self.npad)):
+                    N.check(lib.jb_rows_scatter(src.data_ptr(), mp, buf[0].data_ptr(), buf[1].data_ptr(),
+                                                buf[2].data_ptr() if parts == 3 else None, None, rows, L, st),
+                            "scatter")
+                cur = nxt
+            off = float(self.off.max())
+            off_hist.append((off, parts))
+            if parts == 3 and off <= tol_phase1:
+                break
+            if parts == 2 and off <= switch:
+                # Re-synchronise before the accurate sweeps: V made orthogonal,
+                # W = A V recomputed from the exact input (the 16-bit sweeps
+                # left W's small columns off by ~2^-16 sigma_1 / sigma_j).
+                parts = 3
+                vt = self._combine_v(cur)
+                vt = self._polar(vt, polar_steps)
+                wt = self._w_from_v(vt, ap)
+                for buf, src, L in ((self.W[cur], wt, self.mpad), (self.V[cur], vt, self.npad)):
+                    N.check(lib.jb_rows_scatter(src.data_ptr(), self.init_map.data_ptr(), buf[0].data_ptr(),
+                                                buf[1].data_ptr(), buf[2].data_ptr(), None, self.npad, L, st),
+                            "scatter")
+        else:
+            raise RuntimeError("block Jacobi did not converge")
+        # The data now sits in round 0's layout of the next sweep.
+        vt = self._polar(self._combine_v(cur), polar_steps)
+        wt = self._w_from_v(vt, ap)                                       # npad x mpad
+        U = torch.empty(self.mpad, n, dtype=torch.float32, device=dev)
+        S = torch.empty(n, dtype=torch.float32, device=dev)
+        Vh = torch.empty(n, self.npad, dtype=torch.float32, device=dev)
+        sig = torch.empty(self.npad, dtype=torch.float64, device=dev)
+        perm = torch.empty(self.npad, dtype=torch.int32, device=dev)
+        N.check(lib.jb_block_finish(wt.data_ptr(), vt.data_ptr(), U.data_ptr(), S.data_ptr(), Vh.data_ptr(),
+                                    sig.data_ptr(), perm.data_ptr(), self.mpad, self.npad, n, e, max(m, n), st),
+                "jb_block_finish")
+        info = {"algorithm": "block_jacobi", "block_sweeps": sweeps, "off_per_sweep": off_hist,
+                "precision": "tensor-core sweeps (3xBF16 then 6xBF16) with FP64 block eigen-solves; "
+                             "6xBF16 Newton-Schulz V, FP64-accumulated W = A V"}
+        return U[:m], S, Vh[:, :n].contiguous(), info

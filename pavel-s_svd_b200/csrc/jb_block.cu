@@ -1,0 +1,370 @@
+// jb_block.cu - the non-GEMM kernels of the blocked one-sided Jacobi SVD
+// (svdbench/standalone/solvers.py:30-68, block_jacobi).
+//
+// Block pairs live in "slots": slot k of a round holds the 2b columns of its
+// pair (block i, then block j, i < j) as 2b rows of length L (columns of W
+// are rows of W^T), in hi/lo BF16 parts that feed the tensor-core products.
+//   jb_block_eig_f64   FP64 eigen-solve of every slot's Gram (2b x 2b):
+//                      the rotation vv of the reference's inner Jacobi
+//                      (solvers.py:48), written as vv^T in hi/lo BF16.
+//   jb_rows_scatter    FP32 rows -> hi/lo BF16 rows at mapped positions
+//                      (moves rotated blocks into the next round's slots).
+//   jb_rows_combine    hi + lo BF16 rows -> FP32 rows at mapped positions.
+//   jb_block_finish    sigma = column norms (FP64), descending order, cut,
+//                      U = W / sigma, Vh (solvers.py:61-66 with
+//                      _finish_columns :18-21).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+#include "jacobi_b200.h"
+
+namespace jb {
+namespace blk {
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int circ(int pos, int r, int n) {
+    if (pos == 0) return 0;
+    int x = (pos - 1 - r) % (n - 1);
+    if (x < 0) x += n - 1;
+    return 1 + x;
+}
+
+// One CTA per slot.  G (n x n, FP64, symmetric) is rotated as G <- J^T G J
+// with the one-sided Jacobi rotation of columns p, q of the slot (app = g_pp,
+// aqq = g_qq, apq = g_pq; primitives.py:334-347), the pairs of a round in
+// parallel (round-robin order), Q <- Q J accumulated (FP32), until no pair is
+// active or `sweeps` sweeps.  The off value of the slot is the largest
+// |g_pq| / sqrt(g_pp g_qq) over its active pairs in the first sweep.
+__global__ void __launch_bounds__(256) eig_kernel(const float *Gin, __nv_bfloat16 *Qt_hi, __nv_bfloat16 *Qt_lo,
+                                                  __nv_bfloat16 *Qt_lo2, float *off_out, int *sweeps_out, int n,
+                                                  int max_sweeps, double tol) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    double *G = (double *)smem;                       // n x n
+    float *Q = (float *)(G + (size_t)n * n);           // n x n (column-major)
+    double *cs = (double *)(Q + (size_t)n * n + (n & 1)); // c[n/2], s[n/2]
+    double *red = cs + n;                              // 32 + n
+    int *perm = (int *)(red + 32 + n);
+    __shared__ int s_any;
+    const int k = blockIdx.x;
+    const float *g_in = Gin + (size_t)k * n * n;
+    for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
+        G[i] = (double)g_in[i];
+        const int c = i / n, r = i - c * n;
+        Q[i] = (r == c) ? 1.f : 0.f;
+    }
+    __syncthreads();
+    // symmetrise (the tensor-core Gram is symmetric up to rounding)
+    for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
+        const int c = i / n, r = i - c * n;
+        if (r < c) {
+            const double v = 0.5 * (G[i] + G[(size_t)r * n + c]);
+            G[i] = v;
+            G[(size_t)r * n + c] = v;
+        }
+    }
+    __syncthreads();
+    double dmax = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dmax = fmax(dmax, G[(size_t)i * n + i]);
+    for (int o = 16; o; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dmax;
+    __syncthreads();
+    double gmax = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) gmax = fmax(gmax, red[w]);
+    __syncthreads();
+    const double floor_ = 2.220446049250313e-16 * 2.220446049250313e-16 * gmax;
+    const int half = n / 2;
+    double first_off = 0.0;
+    int sweep = 0;
+    for (sweep = 1; sweep <= max_sweeps; ++sweep) {
+        if (threadIdx.x == 0) s_any = 0;
+        double off = 0.0;
+        for (int r = 0; r < n - 1; ++r) {
+            __syncthreads();
+            for (int t = threadIdx.x; t < half; t += blockDim.x) {
+                int p = circ(t, r, n), q = circ(n - 1 - t, r, n);
+                if (p > q) { const int x = p; p = q; q = x; }
+                const double app = G[(size_t)p * n + p], aqq = G[(size_t)q * n + q], apq = G[(size_t)q * n + p];
+                double c = 1.0, s = 0.0;
+                const double den = sqrt(app) * sqrt(aqq);
+                const double ratio = fabs(apq) / fmax(den, 1e-300);
+                if (ratio > tol && fmin(app, aqq) > floor_) {
+                    off = fmax(off, ratio);
+                    const double d = aqq - app;
+                    const double tt = copysign(2.0 * fabs(apq), d) / (fabs(d) + sqrt(d * d + 4.0 * apq * apq));
+                    c = 1.0 / sqrt(1.0 + tt * tt);
+                    s = tt * c;
+                    if (apq < 0.0) s = -s;
+                    s_any = 1;
+                }
+                cs[t] = c;
+                cs[half + t] = s;
+            }
+            __syncthreads();
+            // G <- J^T G J, one 2 x 2 block (pair a rows, pair b columns) per item.
+            for (int t = threadIdx.x; t < half * half; t += blockDim.x) {
+                const int a = t / half, b = t - a * half;
+                int p = circ(a, r, n), q = circ(n - 1 - a, r, n);
+                if (p > q) { const int x = p; p = q; q = x; }
+                int u = circ(b, r, n), v = circ(n - 1 - b, r, n);
+                if (u > v) { const int x = u; u = v; v = x; }
+                const double ca = cs[a], sa = cs[half + a], cb = cs[b], sb = cs[half + b];
+                const double gpu = G[(size_t)u * n + p], gqu = G[(size_t)u * n + q];
+                const double gpv = G[(size_t)v * n + p], gqv = G[(size_t)v * n + q];
+                // rows: [p; q] <- J_a^T [p; q] with J = [[c, s], [-s, c]] acting on columns (p, q)
+                const double rpu = ca * gpu - sa * gqu, rqu = sa * gpu + ca * gqu;
+                const double rpv = ca * gpv - sa * gqv, rqv = sa * gpv + ca * gqv;
+                // columns: [u, v] <- [u, v] J_b
+                G[(size_t)u * n + p] = cb * rpu - sb * rpv;
+                G[(size_t)v * n + p] = sb * rpu + cb * rpv;
+                G[(size_t)u * n + q] = cb * rqu - sb * rqv;
+                G[(size_t)v * n + q] = sb * rqu + cb * rqv;
+            }
+            for (int t = threadIdx.x; t < half * n; t += blockDim.x) {
+                const int b = t / n, i = t - b * n;
+                int u = circ(b, r, n), v = circ(n - 1 - b, r, n);
+                if (u > v) { const int x = u; u = v; v = x; }
+                const float cb = (float)cs[b], sb = (float)cs[half + b];
+                const float xu = Q[(size_t)u * n + i], xv = Q[(size_t)v * n + i];
+                Q[(size_t)u * n + i] = cb * xu - sb * xv;
+                Q[(size_t)v * n + i] = sb * xu + cb * xv;
+            }
+        }
+        __syncthreads();
+        for (int o = 16; o; o >>= 1) off = fmax(off, __shfl_xor_sync(0xffffffffu, off, o));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = off;
+        __syncthreads();
+        double om = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) om = fmax(om, red[w]);
+        if (sweep == 1) first_off = om;
+        const int any = s_any;
+        __syncthreads();
+        if (!any) break;
+    }
+    // Eigenvalues descending (stable), Q^T rows in that order.
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const double dj = G[(size_t)j * n + j];
+        int rk = 0;
+        for (int i = 0; i < n; ++i) {
+            const double di = G[(size_t)i * n + i];
+            rk += (di > dj) || (di == dj && i < j);
+        }
+        perm[rk] = j;
+    }
+    __syncthreads();
+    __nv_bfloat16 *qh = Qt_hi + (size_t)k * n * n, *ql = Qt_lo + (size_t)k * n * n;
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+        const int rrow = t / n, i = t - rrow * n;       // Q^T row rrow = column perm[rrow] of Q
+        const float x = Q[(size_t)perm[rrow] * n + i];
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        qh[t] = h;
+        const float rem = x - __bfloat162float(h);
+        const __nv_bfloat16 l = __float2bfloat16_rn(rem);
+        ql[t] = l;
+        if (Qt_lo2) Qt_lo2[(size_t)k * n * n + t] = __float2bfloat16_rn(rem - __bfloat162float(l));
+    }
+    if (threadIdx.x == 0) {
+        if (off_out) off_out[k] = (float)first_off;
+        if (sweeps_out) sweeps_out[k] = sweep > max_sweeps ? max_sweeps : sweep;
+    }
+}
+
+// dst row map[r] <- src row r (length L), split into hi / lo BF16.
+__global__ void scatter_kernel(const float *src, const int *map, __nv_bfloat16 *hi, __nv_bfloat16 *lo,
+                               __nv_bfloat16 *lo2, float *f32, int64_t rows, int64_t L) {
+    for (int64_t r = blockIdx.y; r < rows; r += gridDim.y) {
+        const int64_t d = map ? map[r] : r;
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L; i += (int64_t)gridDim.x * blockDim.x) {
+            const float v = src[r * L + i];
+            const __nv_bfloat16 h = __float2bfloat16_rn(v);
+            if (hi) hi[d * L + i] = h;
+            const float rem = v - __bfloat162float(h);
+            const __nv_bfloat16 l = __float2bfloat16_rn(rem);
+            if (lo) lo[d * L + i] = l;
+            if (lo2) lo2[d * L + i] = __float2bfloat16_rn(rem - __bfloat162float(l));
+            if (f32) f32[d * L + i] = v;
+        }
+    }
+}
+
+__global__ void combine_kernel(const __nv_bfloat16 *hi, const __nv_bfloat16 *lo, const __nv_bfloat16 *lo2,
+                               const int *map, float *dst, int64_t rows, int64_t L) {
+    for (int64_t r = blockIdx.y; r < rows; r += gridDim.y) {
+        const int64_t d = map ? map[r] : r;
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < L; i += (int64_t)gridDim.x * blockDim.x)
+            dst[d * L + i] = __bfloat162float(hi[r * L + i]) + (lo ? __bfloat162float(lo[r * L + i]) : 0.f) +
+                             (lo2 ? __bfloat162float(lo2[r * L + i]) : 0.f);
+    }
+}
+
+// sigma_j = ||Wt row j|| * 2^e (FP64 sums), one warp per row.
+__global__ void norms_kernel(const float *Wt, double *sig, int64_t n, int64_t m) {
+    const int64_t row = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (row >= n) return;
+    double acc = 0.0;
+    for (int64_t i = lane; i < m; i += 32) {
+        const double x = Wt[row * m + i];
+        acc = fma(x, x, acc);
+    }
+    acc = warp_sum_d(acc);
+    if (lane == 0) sig[row] = sqrt(acc);
+}
+
+// Stable descending rank of every sigma (n^2 comparisons, n <= a few 1000).
+__global__ void rank_kernel(const double *sig, int *perm, int n) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const double sj = sig[j];
+    int rk = 0;
+    for (int i = 0; i < n; ++i) {
+        const double si = sig[i];
+        rk += (si > sj) || (si == sj && i < j);
+    }
+    perm[rk] = j;
+}
+
+// Outputs: S[r] (cut below eps32 max(m, n_even) sigma_1), U[:, r] = W_perm[r] /
+// sigma (kept columns; cut columns of nonzero norm are normalised the same
+// way), Vh[r, :] = Vt[perm[r], :].
+__global__ void finish_kernel(const float *Wt, const float *Vt, const double *sig, const int *perm, float *U,
+                              float *S, float *Vh, int64_t m, int64_t n, int rank, int e, int cutw) {
+    const double smax = sig[perm[0]];
+    const double cut = 1.1920928955078125e-07 * (double)cutw * smax;
+    const int64_t total_u = m * rank, total_v = (int64_t)rank * n;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < total_u + total_v + rank;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        if (t < total_u) {
+            const int64_t i = t / rank, r = t - i * rank;
+            const int j = perm[r];
+            const double sj = sig[j];
+            U[t] = U ? (float)(sj > 0.0 ? Wt[(int64_t)j * m + i] / sj : 0.0) : 0.f;
+        } else if (t < total_u + total_v) {
+            const int64_t q = t - total_u, r = q / n, c = q - r * n;
+            Vh[q] = Vt[(int64_t)perm[r] * n + c];
+        } else {
+            const int r = (int)(t - total_u - total_v);
+            const double sj = sig[perm[r]];
+            S[r] = (float)(sj > cut ? ldexp(sj, e) : 0.0);
+        }
+    }
+}
+
+
+// C (M x N, f32) = A (M x K) * B (N x K)^T with FP32 inputs (row-major, K
+// contiguous) and FP64 accumulation: every product of two floats is exact in
+// FP64, so C carries FP64 accuracy until its final rounding.  128 x 128
+// tiles, K steps of 8, 256 threads with 8 x 8 outputs each.
+__global__ void __launch_bounds__(256) gemm_f64acc_kernel(const float *A, const float *B, float *C, int64_t M,
+                                                          int64_t N, int64_t K, int64_t lda, int64_t ldb,
+                                                          int64_t ldc) {
+    __shared__ double As[8][128];
+    __shared__ double Bs[8][128];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int64_t m0 = (int64_t)blockIdx.y * 128, n0 = (int64_t)blockIdx.x * 128;
+    double acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    const int lr = threadIdx.x >> 1, lk = (threadIdx.x & 1) * 4;
+    for (int64_t k0 = 0; k0 < K; k0 += 8) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int64_t ka = k0 + lk + q;
+            const int64_t ra = m0 + lr, rb = n0 + lr;
+            As[lk + q][lr] = (ra < M && ka < K) ? (double)A[ra * lda + ka] : 0.0;
+            Bs[lk + q][lr] = (rb < N && ka < K) ? (double)B[rb * ldb + ka] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            double a[8], b[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) a[i] = As[k][ty + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) b[j] = Bs[k][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int64_t r = m0 + ty + 16 * i;
+        if (r >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int64_t c = n0 + tx + 16 * j;
+            if (c < N) C[r * ldc + c] = (float)acc[i][j];
+        }
+    }
+}
+
+}  // namespace blk
+}  // namespace jb
+
+using namespace jb::blk;
+
+extern "C" {
+
+int jb_block_eig_f64(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, int32_t *sweeps,
+                     int64_t pairs, int32_t n, int32_t max_sweeps, double tol, void *stream) {
+    if (!G || !Qt_hi || !Qt_lo || pairs < 1 || n < 2 || (n & 1) || max_sweeps < 1) return JB_EINVAL;
+    const size_t smem = (size_t)n * n * 8 + (size_t)n * n * 4 + 8 + ((size_t)n + 32 + n) * 8 + (size_t)n * 4 + 16;
+    if (smem > 227 * 1024) return JB_ETOOBIG;
+    if (cudaFuncSetAttribute(eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return JB_ECUDA;
+    eig_kernel<<<(unsigned)pairs, 256, smem, (cudaStream_t)stream>>>(G, (__nv_bfloat16 *)Qt_hi, (__nv_bfloat16 *)Qt_lo,
+                                                                     (__nv_bfloat16 *)Qt_lo2, off, sweeps, n,
+                                                                     max_sweeps, tol);
+    return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+}
+
+int jb_rows_scatter(const float *src, const int32_t *map, void *hi, void *lo, void *lo2, float *f32, int64_t rows,
+                    int64_t L, void *stream) {
+    if (!src || rows < 1 || L < 1 || (!hi && !f32)) return JB_EINVAL;
+    dim3 grid((unsigned)((L + 255) / 256 > 64 ? 64 : (L + 255) / 256), (unsigned)(rows > 65535 ? 65535 : rows));
+    scatter_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(src, map, (__nv_bfloat16 *)hi, (__nv_bfloat16 *)lo,
+                                                           (__nv_bfloat16 *)lo2, f32, rows, L);
+    return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+}
+
+int jb_rows_combine(const void *hi, const void *lo, const void *lo2, const int32_t *map, float *dst, int64_t rows,
+                    int64_t L, void *stream) {
+    if (!hi || !dst || rows < 1 || L < 1) return JB_EINVAL;
+    dim3 grid((unsigned)((L + 255) / 256 > 64 ? 64 : (L + 255) / 256), (unsigned)(rows > 65535 ? 65535 : rows));
+    combine_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)hi, (const __nv_bfloat16 *)lo,
+                                                           (const __nv_bfloat16 *)lo2, map, dst, rows, L);
+    return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+}
+
+int jb_block_finish(const float *Wt, const float *Vt, float *U, float *S, float *Vh, double *sig, int32_t *perm,
+                    int64_t m, int64_t n, int32_t rank, int32_t e, int32_t cut_width, void *stream) {
+    if (!Wt || !Vt || !S || !Vh || !U || !sig || !perm || m < 1 || n < 1 || rank < 1 || rank > n) return JB_EINVAL;
+    cudaStream_t st = (cudaStream_t)stream;
+    norms_kernel<<<(unsigned)((n + 7) / 8), 256, 0, st>>>(Wt, sig, n, m);
+    rank_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(sig, perm, (int)n);
+    const int64_t total = m * rank + (int64_t)rank * n + rank;
+    int64_t blocks = (total + 255) / 256;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    finish_kernel<<<(unsigned)blocks, 256, 0, st>>>(Wt, Vt, sig, perm, U, S, Vh, m, n, rank, e, cut_width);
+    return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+}
+
+int jb_gemm_f64acc(const float *A, const float *B, float *C, int64_t M, int64_t N, int64_t K, int64_t lda,
+                   int64_t ldb, int64_t ldc, void *stream) {
+    if (!A || !B || !C || M < 1 || N < 1 || K < 1 || lda < K || ldb < K || ldc < N) return JB_EINVAL;
+    if ((M + 127) / 128 > 65535) return JB_ETOOBIG;
+    dim3 grid((unsigned)((N + 127) / 128), (unsigned)((M + 127) / 128));
+    gemm_f64acc_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(A, B, C, M, N, K, lda, ldb, ldc);
+    return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+}
+
+}  // extern "C"

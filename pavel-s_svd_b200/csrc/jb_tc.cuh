@@ -30,7 +30,7 @@ constexpr uint32_t A_TILE = BM * BK * 2;  // 16 KiB
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
 
 struct TcParams {
-    CUtensorMap ta[2], tb[2];
+    CUtensorMap ta[3], tb[3];
     float *C;
     long long ldc, sC;
     int M, N, K;
@@ -38,8 +38,9 @@ struct TcParams {
     int splits;        // blockIdx.z = batch * splits + split
     int stages;        // shared-memory ring depth
     int nterm;
-    int term_a[3], term_b[3];
+    int term_a[6], term_b[6];
     int na, nb;        // operand variants actually loaded
+    int b_mn;          // B stored K x N (N contiguous) instead of N x K
     float alpha, beta; // beta: 0 overwrite, 1 accumulate (atomic when splits > 1)
     int *error_flag;
 };
@@ -101,9 +102,25 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(const void *tile) {
     return d;
 }
 
-// Instruction descriptor, kind::f16: D fp32, A and B bf16, both K-major.
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+// MN-major tile (N contiguous), 128-byte swizzle: rows of 64 N-elements per
+// k, 8-row K groups 1024 bytes apart (SBO), 64-element N chunks (one TMA box
+// of 64 x 64) 8192 bytes apart (LBO).
+__device__ __forceinline__ uint64_t smem_desc_mn_sw128(const void *tile) {
+    const uint64_t addr = smem_u32(tile);
+    uint64_t d = 0;
+    d |= (addr >> 4) & 0x3FFFull;
+    d |= (uint64_t)(8192 >> 4) << 16;        // leading byte offset: next N chunk
+    d |= (uint64_t)(1024 >> 4) << 32;        // stride byte offset: next 8-row K group
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
+// Instruction descriptor, kind::f16: D fp32, A and B bf16, A K-major, B
+// K-major or (b_mn) MN-major.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, int b_mn = 0) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(b_mn ? 1 : 0) << 16) | ((uint32_t)(N >> 3) << 17) |
+           ((uint32_t)(M >> 4) << 24);
 }
 
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -188,8 +205,14 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
             unsigned char *st = smem + s * stage_bytes;
             const int kx = kbeg + kb * BK;
             for (int a = 0; a < p.na; ++a) tma_load_3d(st + a * A_TILE, &p.ta[a], kx, m0, batch, &full[s]);
-            for (int b = 0; b < p.nb; ++b)
-                tma_load_3d(st + p.na * A_TILE + b * B_TILE, &p.tb[b], kx, n0, batch, &full[s]);
+            for (int b = 0; b < p.nb; ++b) {
+                unsigned char *bt = st + p.na * A_TILE + b * B_TILE;
+                if (!p.b_mn) {
+                    tma_load_3d(bt, &p.tb[b], kx, n0, batch, &full[s]);
+                } else {
+                    for (int g = 0; g < BN / 64; ++g) tma_load_3d(bt + g * 8192, &p.tb[b], n0 + 64 * g, kx, batch, &full[s]);
+                }
+            }
             issued = kb + 1;
         }
         // Drain: the last stages' copies must land before the CTA can exit.
@@ -197,7 +220,8 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
             mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1, nullptr);
     } else if (warp == 1 && lane == 0) {
         // MMA issuer.
-        const uint32_t idesc = idesc_bf16(BM, BN);
+        const uint32_t idesc = idesc_bf16(BM, BN, p.b_mn);
+        const uint32_t bstep = p.b_mn ? (2048 >> 4) : 2;  // +16 K rows (MN-major) or +32 bytes (K-major)
         bool ok = true;
         for (int kb = 0; kb < nk && ok; ++kb) {
             const int s = kb % STAGES;
@@ -207,10 +231,11 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
             unsigned char *st = smem + s * stage_bytes;
             for (int t = 0; t < p.nterm; ++t) {
                 const uint64_t ad = smem_desc_sw128(st + p.term_a[t] * A_TILE);
-                const uint64_t bd = smem_desc_sw128(st + p.na * A_TILE + p.term_b[t] * B_TILE);
+                const unsigned char *bt = st + p.na * A_TILE + p.term_b[t] * B_TILE;
+                const uint64_t bd = p.b_mn ? smem_desc_mn_sw128(bt) : smem_desc_sw128(bt);
 #pragma unroll
                 for (int k = 0; k < BK / 16; ++k)  // +32 bytes per K=16 step inside the swizzled row
-                    mma_bf16(tmem, ad + 2 * k, bd + 2 * k, idesc, (kb | t | k) != 0);
+                    mma_bf16(tmem, ad + 2 * k, bd + bstep * k, idesc, (kb | t | k) != 0);
             }
             mma_commit(&empty[s]);
         }

@@ -30,7 +30,8 @@ static PFN_cuTensorMapEncodeTiled_v12000 encoder() {
     return g_encode;
 }
 
-// 3-D map over a row-major BF16 array: x = K (contiguous), y = rows, z = batch.
+// 3-D map over a row-major BF16 array: x = inner (contiguous), y = rows, z =
+// batch; boxes of 64 inner elements (one 128-byte swizzle row) x box_rows.
 static bool make_map(CUtensorMap *map, const void *ptr, int64_t K, int64_t rows, int64_t ld, int64_t batch,
                      int64_t bstride, int box_rows) {
     auto enc = encoder();
@@ -65,12 +66,17 @@ static int launch(TcParams &p, int64_t batch, cudaStream_t st) {
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
 }
 
-__global__ void split_kernel(const float *x, __nv_bfloat16 *hi, __nv_bfloat16 *lo, int64_t n) {
+__global__ void split_kernel(const float *x, __nv_bfloat16 *hi, __nv_bfloat16 *lo, __nv_bfloat16 *lo2, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const float v = x[i];
         const __nv_bfloat16 h = __float2bfloat16_rn(v);
         hi[i] = h;
-        if (lo) lo[i] = __float2bfloat16_rn(v - __bfloat162float(h));
+        if (lo) {
+            const float r = v - __bfloat162float(h);
+            const __nv_bfloat16 l = __float2bfloat16_rn(r);
+            lo[i] = l;
+            if (lo2) lo2[i] = __float2bfloat16_rn(r - __bfloat162float(l));
+        }
     }
 }
 
@@ -85,38 +91,49 @@ int jb_gemm_bf16(const void *A0, const void *A1, const void *B0, const void *B1,
                  int64_t N, int64_t K, int64_t lda, int64_t ldb, int64_t ldc, int64_t batch, int64_t strideA,
                  int64_t strideB, int64_t strideC, float alpha, float beta, int32_t split_k, int32_t *error_flag,
                  void *stream) {
-    if (!A0 || !B0 || !C || M < 1 || N < 1 || K < 1 || batch < 1 || split_k < 1) return JB_EINVAL;
-    if (mode != JB_GEMM_PLAIN && mode != JB_GEMM_SPLIT3) return JB_EINVAL;
-    if (mode == JB_GEMM_SPLIT3 && (!A1 || !B1)) return JB_EINVAL;
-    if (lda % 8 || ldb % 8 || lda < K || ldb < K || ldc < N) return JB_EINVAL;
+    const void *A[3] = {A0, A1, nullptr}, *B[3] = {B0, B1, nullptr};
+    return jb_gemm_bf16x(A, B, mode, C, M, N, K, lda, ldb, ldc, batch, strideA, strideB, strideC, alpha, beta,
+                         split_k, error_flag, stream);
+}
+
+int jb_gemm_bf16x(const void *const *A, const void *const *B, int32_t mode, float *C, int64_t M, int64_t N, int64_t K,
+                  int64_t lda, int64_t ldb, int64_t ldc, int64_t batch, int64_t strideA, int64_t strideB,
+                  int64_t strideC, float alpha, float beta, int32_t split_k, int32_t *error_flag, void *stream) {
+    if (!A || !B || !A[0] || !B[0] || !C || M < 1 || N < 1 || K < 1 || batch < 1 || split_k < 1) return JB_EINVAL;
+    const int kind = mode & 3;
+    const int b_mn = (mode & JB_GEMM_B_MN) ? 1 : 0;
+    if (kind == 3 || (mode & ~(3 | JB_GEMM_B_MN))) return JB_EINVAL;
+    const int nsplit = kind == JB_GEMM_PLAIN ? 1 : (kind == JB_GEMM_SPLIT3 ? 2 : 3);
+    for (int i = 0; i < nsplit; ++i)
+        if (!A[i] || !B[i] || ((uintptr_t)A[i] & 15) || ((uintptr_t)B[i] & 15)) return JB_EINVAL;
+    if (lda % 8 || ldb % 8 || lda < K || ldc < N) return JB_EINVAL;
+    if (b_mn ? ldb < N : ldb < K) return JB_EINVAL;
     if (batch > 1 && (strideA % 8 || strideB % 8)) return JB_EINVAL;
-    const void *ptrs[4] = {A0, A1, B0, B1};
-    for (const void *q : ptrs)
-        if (q && ((uintptr_t)q & 15)) return JB_EINVAL;
     if (M > (1 << 30) || N > (1 << 30) || batch * split_k > 65535) return JB_ETOOBIG;
     tc::TcParams p;
     memset(&p, 0, sizeof(p));
-    const int bn = N <= 64 ? 64 : (N <= 128 ? 128 : 256);
-    p.na = mode == JB_GEMM_SPLIT3 ? 2 : 1;
-    p.nb = p.na;
-    for (int a = 0; a < p.na; ++a)
-        if (!tc::make_map(&p.ta[a], a ? A1 : A0, K, M, lda, batch, strideA, tc::BM)) return JB_ECUDA;
-    for (int b = 0; b < p.nb; ++b)
-        if (!tc::make_map(&p.tb[b], b ? B1 : B0, K, N, ldb, batch, strideB, bn)) return JB_ECUDA;
+    const int bn = N <= 64 ? 64 : (N <= 128 || nsplit == 3 ? 128 : 256);
+    p.na = p.nb = nsplit;
+    p.b_mn = b_mn;
+    for (int a = 0; a < nsplit; ++a)
+        if (!tc::make_map(&p.ta[a], A[a], K, M, lda, batch, strideA, tc::BM)) return JB_ECUDA;
+    for (int b = 0; b < nsplit; ++b) {
+        const bool ok = b_mn ? tc::make_map(&p.tb[b], B[b], N, K, ldb, batch, strideB, tc::BK)
+                             : tc::make_map(&p.tb[b], B[b], K, N, ldb, batch, strideB, bn);
+        if (!ok) return JB_ECUDA;
+    }
     p.C = C; p.ldc = ldc; p.sC = strideC;
     p.M = (int)M; p.N = (int)N; p.K = (int)K;
     int64_t chunk = (K + split_k - 1) / split_k;
     chunk = (chunk + tc::BK - 1) / tc::BK * tc::BK;
     p.kchunk = (int)chunk;
     p.splits = (int)((K + chunk - 1) / chunk);
-    if (mode == JB_GEMM_SPLIT3) {
-        p.nterm = 3;
-        p.term_a[0] = 0; p.term_b[0] = 0;   // hi * hi
-        p.term_a[1] = 0; p.term_b[1] = 1;   // hi * lo
-        p.term_a[2] = 1; p.term_b[2] = 0;   // lo * hi
-    } else {
-        p.nterm = 1;
-    }
+    // Products of the split parts kept: hi*hi, hi*mid, mid*hi (3 terms), plus
+    // hi*lo, mid*mid, lo*hi (6 terms): every pair whose exponents sum to at
+    // most two splits below the leading term.
+    static const int ta6[6] = {0, 0, 1, 0, 1, 2}, tb6[6] = {0, 1, 0, 2, 1, 0};
+    p.nterm = nsplit == 1 ? 1 : (nsplit == 2 ? 3 : 6);
+    for (int t = 0; t < p.nterm; ++t) { p.term_a[t] = ta6[t]; p.term_b[t] = tb6[t]; }
     p.alpha = alpha;
     p.beta = (p.splits > 1) ? 1.f : beta;
     p.error_flag = error_flag;
@@ -139,11 +156,16 @@ int jb_gemm_bf16(const void *A0, const void *A1, const void *B0, const void *B1,
 }
 
 int jb_split_bf16(const float *X, void *hi, void *lo, int64_t n, void *stream) {
-    if (!X || !hi || n < 0) return JB_EINVAL;
+    return jb_split3_bf16(X, hi, lo, nullptr, n, stream);
+}
+
+int jb_split3_bf16(const float *X, void *hi, void *mid, void *lo, int64_t n, void *stream) {
+    if (!X || !hi || n < 0 || (lo && !mid)) return JB_EINVAL;
     if (n == 0) return JB_OK;
     int blocks = (int)((n + 255) / 256);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    tc::split_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(X, (__nv_bfloat16 *)hi, (__nv_bfloat16 *)lo, n);
+    tc::split_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(X, (__nv_bfloat16 *)hi, (__nv_bfloat16 *)mid,
+                                                               (__nv_bfloat16 *)lo, n);
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
 }
 

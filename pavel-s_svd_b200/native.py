@@ -23,10 +23,12 @@ RC_NAMES = {JB_EINVAL: "invalid argument", JB_ETOOBIG: "shape too large for this
 
 # Exported symbols, in declaration order of include/jacobi_b200.h.
 SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_batched_f32",
-           "jb_svd_batched_f64", "jb_svd_uneven_f32", "jb_gemm_bf16", "jb_split_bf16",
+           "jb_svd_batched_f64", "jb_svd_uneven_f32", "jb_gemm_bf16", "jb_gemm_bf16x", "jb_split_bf16",
+           "jb_split3_bf16",
            "jb_warm_prep_f32", "jb_svd_warm_f32", "jb_transpose_bf16", "jb_bias_act", "jb_relu_backward",
-           "jb_col_sum", "jb_mse_grad", "jb_adam", "jb_gram_sketch", "jb_svd_batched_f32_noalloc")
-GEMM_PLAIN, GEMM_SPLIT3 = 0, 1
+           "jb_col_sum", "jb_mse_grad", "jb_adam", "jb_gram_sketch", "jb_block_eig_f64", "jb_rows_scatter",
+           "jb_rows_combine", "jb_gemm_f64acc", "jb_block_finish", "jb_svd_batched_f32_noalloc")
+GEMM_PLAIN, GEMM_SPLIT3, GEMM_SPLIT6, GEMM_B_MN = 0, 1, 2, 4
 NOALLOC_SCRATCH_BYTES = 16 << 20  # JB_NOALLOC_SCRATCH_BYTES
 
 
@@ -63,6 +65,11 @@ def _declare(l):
                                ctypes.c_float, ctypes.c_float, I32, P, P]
     l.jb_split_bf16.restype = ctypes.c_int
     l.jb_split_bf16.argtypes = [P, P, P, I64, P]
+    l.jb_split3_bf16.restype = ctypes.c_int
+    l.jb_split3_bf16.argtypes = [P, P, P, P, I64, P]
+    l.jb_gemm_bf16x.restype = ctypes.c_int
+    l.jb_gemm_bf16x.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p), I32, P, I64, I64,
+                                I64, I64, I64, I64, I64, I64, I64, I64, ctypes.c_float, ctypes.c_float, I32, P, P]
     FL = ctypes.c_float
     for name, args in (("jb_warm_prep_f32", [P, P, P, P, P, P, I64, I32, I32, P]),
                        ("jb_svd_warm_f32", [P, P, P, P, P, I64, I32, I32, I32, I32, F64, I32, I32, P, P, P, SZ, P]),
@@ -72,7 +79,12 @@ def _declare(l):
                        ("jb_col_sum", [P, P, I64, I64, P]),
                        ("jb_mse_grad", [P, P, P, P, I64, FL, P]),
                        ("jb_adam", [P, P, P, P, P, P, I64, I64, FL, FL, FL, FL, I32, P]),
-                       ("jb_gram_sketch", [P, P, I64, I32, I32, P])):
+                       ("jb_gram_sketch", [P, P, I64, I32, I32, P]),
+                       ("jb_block_eig_f64", [P, P, P, P, P, P, I64, I32, I32, F64, P]),
+                       ("jb_rows_scatter", [P, P, P, P, P, P, I64, I64, P]),
+                       ("jb_rows_combine", [P, P, P, P, P, I64, I64, P]),
+                       ("jb_gemm_f64acc", [P, P, P, I64, I64, I64, I64, I64, I64, P]),
+                       ("jb_block_finish", [P, P, P, P, P, P, P, I64, I64, I32, I32, I32, P])):
         f = getattr(l, name)
         f.restype = ctypes.c_int
         f.argtypes = args

@@ -22,6 +22,45 @@ def split_bf16(x: torch.Tensor):
     return hi, lo
 
 
+def split3_bf16(x: torch.Tensor):
+    """(hi, mid, lo) BF16 parts of a float32 tensor (x ~ hi + mid + lo)."""
+    x = x.contiguous()
+    parts = [torch.empty(x.shape, dtype=torch.bfloat16, device=x.device) for _ in range(3)]
+    N.check(N.lib().jb_split3_bf16(x.data_ptr(), parts[0].data_ptr(), parts[1].data_ptr(), parts[2].data_ptr(),
+                                   x.numel(), torch.cuda.current_stream(x.device).cuda_stream), "jb_split3_bf16")
+    return tuple(parts)
+
+
+def gemm_parts(a_parts, b_parts, c=None, *, b_mn=False, alpha=1.0, beta=0.0, split_k=1, error_flag=None,
+               M=None, N_=None, K=None, lda=None, ldb=None, ldc=None, batch=None, sA=None, sB=None, sC=None):
+    """General entry over split parts (1, 2 or 3 of them): C = alpha A B^T (+ beta C).
+
+    a parts: (batch, M, K) bf16; b parts: (batch, N, K) bf16, or with b_mn
+    (batch, K, N) bf16 (N contiguous).  Returns C (batch, M, N) float32."""
+    a0, b0 = a_parts[0], b_parts[0]
+    if a0.dim() == 2:
+        a_parts = [x[None] for x in a_parts]
+    if b0.dim() == 2:
+        b_parts = [x[None] for x in b_parts]
+    a0, b0 = a_parts[0], b_parts[0]
+    bsz, M, K = a0.shape
+    Nn = b0.shape[-1] if b_mn else b0.shape[-2]
+    if c is None:
+        c = torch.empty(bsz, M, Nn, dtype=torch.float32, device=a0.device)
+        beta = 0.0
+    c3 = c if c.dim() == 3 else c[None]
+    ns = len(a_parts)
+    mode = {1: N.GEMM_PLAIN, 2: N.GEMM_SPLIT3, 3: N.GEMM_SPLIT6}[ns] | (N.GEMM_B_MN if b_mn else 0)
+    import ctypes
+    A = (ctypes.c_void_p * 3)(*[x.data_ptr() for x in a_parts] + [None] * (3 - ns))
+    B = (ctypes.c_void_p * 3)(*[x.data_ptr() for x in b_parts] + [None] * (3 - ns))
+    rc = N.lib().jb_gemm_bf16x(A, B, mode, c3.data_ptr(), M, Nn, K, a0.stride(1), b0.stride(1), c3.stride(1),
+                               bsz, a0.stride(0), b0.stride(0), c3.stride(0), float(alpha), float(beta), int(split_k),
+                               _ptr(error_flag), torch.cuda.current_stream(a0.device).cuda_stream)
+    N.check(rc, "jb_gemm_bf16x")
+    return c
+
+
 def gemm(a, b, c=None, *, a_lo=None, b_lo=None, alpha=1.0, beta=0.0, split_k=1, error_flag=None):
     """C = alpha * A @ B^T (+ beta C) on the tensor cores.
 

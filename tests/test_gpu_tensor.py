@@ -56,3 +56,34 @@ def test_split3_product_accuracy(T):
     e3 = rel(c, ref)
     c1 = T.gemm(xh, yh)
     assert e3 <= 5e-5 and e3 < rel(c1, ref) / 20
+
+
+@pytest.mark.parametrize("M,N,K,batch", [(128, 256, 64, 1), (64, 1000, 128, 5), (200, 304, 72, 2)])
+def test_mn_major_b(T, M, N, K, batch):
+    """B given as K x N (N contiguous): C = A B (the update products of the
+    blocked Jacobi)."""
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    a = torch.randn(batch, M, K, device="cuda", generator=g)
+    bt = torch.randn(batch, K, N, device="cuda", generator=g)
+    ah, al = T.split_bf16(a)
+    bh, bl = T.split_bf16(bt)
+    c1 = T.gemm_parts([ah], [bh], b_mn=True)
+    assert rel(c1, ah.float() @ bh.float()) <= 1e-5
+    c3 = T.gemm_parts([ah, al], [bh, bl], b_mn=True)
+    assert rel(c3, a.double() @ bt.double()) <= 5e-5
+
+
+def test_split6_reaches_fp32_accuracy(T):
+    """The tensor-memory accumulator loses accuracy over long K chains, so the
+    accurate modes bound the chain with split-K (128 K per chain here)."""
+    g = torch.Generator(device="cuda").manual_seed(9)
+    x = torch.randn(2, 300, 2048, device="cuda", generator=g)
+    y = torch.randn(2, 260, 2048, device="cuda", generator=g)
+    c6 = T.gemm_parts(T.split3_bf16(x), T.split3_bf16(y), split_k=16)
+    ref = x.double() @ y.double().transpose(-1, -2)
+    e6 = rel(c6, ref)
+    e3 = rel(T.gemm_parts(T.split_bf16(x), T.split_bf16(y), split_k=16), ref)
+    assert e6 <= 2e-6 and e6 < e3 / 2.5
+    bt = torch.randn(2, 2048, 304, device="cuda", generator=g)
+    c6m = T.gemm_parts(T.split3_bf16(x), T.split3_bf16(bt), b_mn=True, split_k=16)
+    assert rel(c6m, x.double() @ bt.double()) <= 2e-6
