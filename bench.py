@@ -11,6 +11,13 @@ Metric: matrices/s (whole job).  Each step is timed with CUDA events on the
 launching stream; a 256 MiB buffer is written between steps (outside the
 events) so every step starts with a cold L2.
 
+--workload selects one of the other configurations (one JSON line each):
+  plain_single     256x128 f32, s_i = 10^(-4i/127), tol 1e-6, <= 30 sweeps
+  clustered_large  4096x1024 f32, 64 clusters x 16, blocked Jacobi b = 32
+  tall_lowrank     8192x2048 f32 rank 64 + noise, blocked Jacobi b = 64
+  warm_family      65536 x 128x64 f32 family: network trained on 60000,
+                   warm vs plain timed on 4096 held-out matrices
+
 --impl reference: the reference algorithm's CPU implementation, timed on the
 host cores of this machine (the C restatement in oracle/, all threads; the
 reference itself is Python/PyTorch and is not present here), on a bounded
@@ -318,12 +325,176 @@ def run_ours(args, rank, world, local_rank):
     del graph
 
 
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def lapack_check(a, U, S, Vh, cut_width):
+    """Accuracy against FP64 LAPACK of the same float32 input; 'resolved'
+    values are those above twice the reference cut eps32 * cut_width * sigma_1."""
+    import scipy.linalg
+    a64 = a.astype(np.float64)
+    sr = scipy.linalg.svd(a64, compute_uv=False, lapack_driver="gesdd")
+    s = S.cpu().numpy().astype(np.float64)
+    k = len(s)
+    cut = np.finfo(np.float32).eps * cut_width * sr[0]
+    res = sr[:k] > 2 * cut
+    big = sr[:k] >= 0.1 * sr[0]
+    out = {"spectrum_error_over_sigma1": float(np.abs(s - sr[:k]).max() / sr[0]),
+           "resolved_spectrum_max_relative_error": float(np.max(np.abs(s[res] - sr[:k][res]) / sr[:k][res])),
+           "max_relative_error_sigma_ge_0.1_sigma1": float(np.max(np.abs(s[big] - sr[:k][big]) / sr[:k][big])),
+           "resolved_values": int(res.sum())}
+    if U is not None:
+        u = U.cpu().numpy().astype(np.float64)
+        vh = Vh.cpu().numpy().astype(np.float64)
+        keep = s > 0
+        out["orthogonality_u_max"] = float(np.abs(u[:, keep].T @ u[:, keep] - np.eye(keep.sum())).max())
+        out["orthogonality_v_max"] = float(np.abs(vh @ vh.T - np.eye(vh.shape[0])).max())
+        out["reconstruction_relative_fro"] = float(np.linalg.norm(a64 - (u[:, keep] * s[keep]) @ vh[keep]) /
+                                                   np.linalg.norm(a64))
+    return out
+
+
+def run_plain_single(args):
+    import torch
+    S_ = importlib.import_module("pavel-s_svd_b200.solvers")
+    wl = importlib.import_module("pavel-s_svd_b200.workloads")
+    a_np = wl.plain_single()
+    a = torch.from_numpy(a_np).cuda()
+    res = {}
+    for prec in ("fp32", "mixed"):
+        x = a[None].contiguous()
+        out = (torch.empty(1, 256, 128, device="cuda"), torch.empty(1, 128, device="cuda"),
+               torch.empty(1, 128, 128, device="cuda"))
+        info = torch.empty(2, 1, dtype=torch.int32, device="cuda")
+        ws = S_.Workspace()
+        run = lambda: S_.launch_batched(x, 128, 0, 1e-6, 30, prec, out, info, ws)
+        for _ in range(args.warmup):
+            run()
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(args.steps):
+            run()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        acc = lapack_check(a_np, out[0][0], out[1][0], out[2][0], 256)
+        res[prec] = {"ms": ms, "matrices_per_s": 1e3 / ms, "sweeps": int(info[0, 0]), **acc}
+    from oracle import c_oracle
+    t = time.perf_counter()
+    _, so, _, swo, _ = c_oracle.svd_batched(a_np[None], tol=1e-6, max_sweeps=30, threads=1)
+    cpu_ms = (time.perf_counter() - t) * 1e3
+    line = {"metric": "Jacobi SVD matrices/s (single 256x128 matrix)", "value": res["mixed"]["matrices_per_s"],
+            "unit": "matrices/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res["mixed"]["ms"], "higher_is_better": True, "scaling": "none (single matrix)",
+            "vs_baseline": None, "dtype": "f32 in/out", "data": "synthetic (seeded, BASELINE config 1)",
+            "config": {"workload": "plain_single_256x128", "tol": 1e-6, "max_sweeps": 30},
+            "variants": res, "cpu_baseline": {"value": 1e3 / cpu_ms, "unit": "matrices/s", "cores": 1,
+                                              "kind": "port", "sample": "the one matrix, C oracle (fp32)",
+                                              "sweeps": int(swo[0])}}
+    print(json.dumps(line), flush=True)
+
+
+def run_blocked(args, name):
+    import torch
+    wl = importlib.import_module("pavel-s_svd_b200.workloads")
+    BJ = importlib.import_module("pavel-s_svd_b200.blocked")
+    if name == "clustered_large":
+        a_np, b = wl.clustered_large(), 32
+    else:
+        a_np, b = wl.tall_lowrank(), 64
+    m, n = a_np.shape
+    a = torch.from_numpy(a_np).cuda()
+    plan = BJ.BlockJacobi(m, n, b)
+    U, S, Vh, info = plan.solve(a)                     # warm-up (and the result checked)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        e0, e1 = _events()
+        e0.record()
+        U, S, Vh, info = plan.solve(a)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = float(np.median(times))
+    R, P, mp, npd = plan.nb - 1, plan.P, plan.mpad, plan.npad
+    per_round = P * (2 * mp * (2 * b) ** 2 * 2 + 2 * npd * (2 * b) ** 2)       # Gram + W and V updates
+    terms = [3 if p == 2 else 6 for _, p in info["off_per_sweep"]]
+    tensor_flop = sum(R * per_round * t for t in terms)
+    acc = lapack_check(a_np, U, S, Vh, max(m, n))
+    line = {"metric": f"blocked Jacobi SVD matrices/s ({m}x{n}, b={b})", "value": 1e3 / ms, "unit": "matrices/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": 1, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "none (single matrix)", "vs_baseline": None,
+            "dtype": "f32 in/out; bf16x3/bf16x6 tensor; f64 eig", "config": {"workload": name, "m": m, "n": n,
+                                                                              "block_size": b},
+            "data": f"synthetic (seeded, BASELINE config {'3' if name == 'clustered_large' else '4'})",
+            "block_sweeps": info["block_sweeps"], "off_per_sweep": info["off_per_sweep"],
+            "converged": info["converged"], "reached_tol": info["reached_tol"],
+            "tensor_flop_per_solve": tensor_flop, "tensor_tflops_whole_solve": tensor_flop / (ms / 1e3) / 1e12,
+            "accuracy": acc}
+    print(json.dumps(line), flush=True)
+
+
+def run_warm(args):
+    import torch
+    W = importlib.import_module("pavel-s_svd_b200.warmstart")
+    wl = importlib.import_module("pavel-s_svd_b200.workloads")
+    a_np, theta = wl.warm_family(count=65536, device="cuda")
+    a = torch.from_numpy(a_np).cuda()
+    tr, te = a[:60000].contiguous(), a[60000:64096].contiguous()
+    frame = wl.family_v(theta[:60000], device="cuda")
+    e0, e1 = _events()
+    e0.record()
+    v_tr, _ = W.plain_v(tr)
+    net = W.WarmStartMLP(seed=0)
+    hist = W.train(net, tr, v_tr, epochs=15, batch=512, lr=1e-3, order="frame", frame=frame)
+    e1.record()
+    torch.cuda.synchronize()
+    train_ms = e0.elapsed_time(e1)
+    solver = W.WarmSolver(net, m=128, n=64, batch=4096)
+    eye = torch.eye(64, device="cuda").expand(4096, 64, 64).contiguous()
+    ideal = wl.family_v(theta[60000:64096], device="cuda").contiguous()
+    res = {}
+    for label, v0 in (("plain", eye), ("warm", None), ("ideal_start", ideal)):
+        for _ in range(args.warmup):
+            solver.launch(te, v0=v0)
+        torch.cuda.synchronize()
+        e0, e1 = _events()
+        e0.record()
+        for _ in range(args.steps):
+            solver.launch(te, v0=v0)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        sweeps, used = solver.check()
+        worst = 0.0
+        S = solver.S.cpu().numpy()
+        for i in range(0, 4096, 64):
+            sr = np.linalg.svd(te[i].cpu().numpy().astype(np.float64), compute_uv=False)
+            worst = max(worst, float(np.max(np.abs(S[i] - sr) / sr)))
+        res[label] = {"ms": ms, "matrices_per_s": 4096 / (ms / 1e3), "sweeps_mean": float(sweeps.mean()),
+                      "kept": float(used.mean()), "max_rel_sigma_err_vs_fp64_sample": worst}
+    line = {"metric": "Jacobi SVD matrices/s, learned warm start vs plain (128x64 family, 4096 held-out)",
+            "value": res["warm"]["matrices_per_s"], "unit": "matrices/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["warm"]["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 in/out; f32+f64 sweeps; bf16 network",
+            "data": "synthetic (seeded, BASELINE config 5)", "config": {"workload": "warm_family", "train": 60000,
+                                                                         "held_out": 4096, "epochs": 15},
+            "train_ms": train_ms, "loss_first_last": [hist[0], hist[-1]], "variants": res,
+            "note": "ideal_start = the generator's own V(theta): what a perfect network would give"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", choices=("uneven_batch", "plain_single", "clustered_large", "tall_lowrank",
+                                           "warm_family"), default="uneven_batch")
     ap.add_argument("--precision", choices=("mixed", "fp32"), default="mixed")
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -338,6 +509,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload != "uneven_batch":
+        {"plain_single": run_plain_single, "warm_family": run_warm}.get(
+            args.workload, lambda a: run_blocked(a, args.workload))(args)
         return
     if world > 1:
         import datetime

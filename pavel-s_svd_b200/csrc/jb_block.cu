@@ -39,10 +39,12 @@ __device__ __forceinline__ int circ(int pos, int r, int n) {
 // aqq = g_qq, apq = g_pq; primitives.py:334-347), the pairs of a round in
 // parallel (round-robin order), Q <- Q J accumulated (FP32), until no pair is
 // active or `sweeps` sweeps.  The off value of the slot is the largest
-// |g_pq| / sqrt(g_pp g_qq) over its active pairs in the first sweep.
+// |g_pq| / sqrt(g_pp g_qq) over its active pairs of live columns (g_pp and
+// g_qq above live_floor) in the first sweep; dmax is the slot's largest g_pp.
 __global__ void __launch_bounds__(256) eig_kernel(const float *Gin, __nv_bfloat16 *Qt_hi, __nv_bfloat16 *Qt_lo,
-                                                  __nv_bfloat16 *Qt_lo2, float *off_out, int *sweeps_out, int n,
-                                                  int max_sweeps, double tol) {
+                                                  __nv_bfloat16 *Qt_lo2, float *off_out, float *dmax_out,
+                                                  int *sweeps_out, int n, int max_sweeps, double tol,
+                                                  double live_floor) {
     extern __shared__ __align__(16) unsigned char smem[];
     double *G = (double *)smem;                       // n x n
     float *Q = (float *)(G + (size_t)n * n);           // n x n (column-major)
@@ -93,7 +95,9 @@ __global__ void __launch_bounds__(256) eig_kernel(const float *Gin, __nv_bfloat1
                 const double den = sqrt(app) * sqrt(aqq);
                 const double ratio = fabs(apq) / fmax(den, 1e-300);
                 if (ratio > tol && fmin(app, aqq) > floor_) {
-                    off = fmax(off, ratio);
+                    // off over live columns only (norm^2 above live_floor),
+                    // like the reference's convergence check (solvers.py:55-57)
+                    if (fmin(app, aqq) > live_floor) off = fmax(off, ratio);
                     const double d = aqq - app;
                     const double tt = copysign(2.0 * fabs(apq), d) / (fabs(d) + sqrt(d * d + 4.0 * apq * apq));
                     c = 1.0 / sqrt(1.0 + tt * tt);
@@ -169,6 +173,7 @@ __global__ void __launch_bounds__(256) eig_kernel(const float *Gin, __nv_bfloat1
     }
     if (threadIdx.x == 0) {
         if (off_out) off_out[k] = (float)first_off;
+        if (dmax_out) dmax_out[k] = (float)gmax;
         if (sweeps_out) sweeps_out[k] = sweep > max_sweeps ? max_sweeps : sweep;
     }
 }
@@ -314,16 +319,17 @@ using namespace jb::blk;
 
 extern "C" {
 
-int jb_block_eig_f64(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, int32_t *sweeps,
-                     int64_t pairs, int32_t n, int32_t max_sweeps, double tol, void *stream) {
+int jb_block_eig_f64(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
+                     int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps, double tol, double live_floor,
+                     void *stream) {
     if (!G || !Qt_hi || !Qt_lo || pairs < 1 || n < 2 || (n & 1) || max_sweeps < 1) return JB_EINVAL;
     const size_t smem = (size_t)n * n * 8 + (size_t)n * n * 4 + 8 + ((size_t)n + 32 + n) * 8 + (size_t)n * 4 + 16;
     if (smem > 227 * 1024) return JB_ETOOBIG;
     if (cudaFuncSetAttribute(eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return JB_ECUDA;
     eig_kernel<<<(unsigned)pairs, 256, smem, (cudaStream_t)stream>>>(G, (__nv_bfloat16 *)Qt_hi, (__nv_bfloat16 *)Qt_lo,
-                                                                     (__nv_bfloat16 *)Qt_lo2, off, sweeps, n,
-                                                                     max_sweeps, tol);
+                                                                     (__nv_bfloat16 *)Qt_lo2, off, dmax, sweeps,
+                                                                     n, max_sweeps, tol, live_floor);
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
 }
 
