@@ -138,6 +138,13 @@ JB_API int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh,
                                (jb_gemm_bf16x only)                            */
 #define JB_GEMM_B_MN    4   /* flag: B_i is stored K x N row-major (N
                                contiguous, leading dimension ldb >= N)         */
+#define JB_GEMM_CHAIN128 8  /* flag: accumulate along K in chains of at most
+                               128 per tensor-memory accumulator (several per
+                               CTA, summed in FP32 registers); split_k is then
+                               a lower bound on the CTAs along K               */
+#define JB_GEMM_SYRK    16  /* flag: B is A (C = A A^T, M == N): B and ldb /
+                               strideB are ignored and the A tiles are read
+                               once as both operands                           */
 
 /* Batched BF16 GEMM on the 5th-generation tensor cores with an FP32
  * accumulator in tensor memory.  A_i: batch x M x K, B_i: batch x N x K, both
@@ -162,6 +169,19 @@ JB_API int jb_gemm_bf16x(const void *const *A, const void *const *B, int32_t mod
                          int64_t batch, int64_t strideA, int64_t strideB, int64_t strideC,
                          float alpha, float beta, int32_t split_k, int32_t *error_flag,
                          void *stream);
+
+/* jb_gemm_bf16x (split_k 1, no beta) whose result is written as BF16 split
+ * parts into mapped rows instead of FP32 C: row r of batch z goes to row
+ * row_map[z * M + r] (z * M + r when row_map is NULL) of out[0..nparts),
+ * each output row ld_out elements long (a multiple of 8); nparts 1..3 gives
+ * hi, hi + mid, hi + mid + lo as jb_split3_bf16 would.  This fuses the
+ * rotation update of the blocked Jacobi with the move of each rotated block
+ * into its next-round slot. */
+JB_API int jb_gemm_bf16x_rows(const void *const *A, const void *const *B, int32_t mode,
+                              void *const *out, int32_t nparts, const int32_t *row_map,
+                              int64_t ld_out, int64_t M, int64_t N, int64_t K, int64_t lda,
+                              int64_t ldb, int64_t batch, int64_t strideA, int64_t strideB,
+                              float alpha, int32_t *error_flag, void *stream);
 
 /* hi = bf16(X), lo = bf16(X - hi) for n floats (lo may be NULL). */
 JB_API int jb_split_bf16(const float *X, void *hi, void *lo, int64_t n, void *stream);

@@ -1,30 +1,35 @@
 """Blocked one-sided Jacobi SVD of one large matrix on the tensor cores.
 
 Counterpart of block_jacobi (svdbench/standalone/solvers.py:30-68): column
-blocks of width b, a round-robin tournament over blocks, and per block pair
-the rotation vv of the pair's own SVD applied to W and V.  B200 form:
+blocks of width b, a round-robin tournament over blocks (primitives.py:309-313),
+and per block pair the rotation vv of the pair's own SVD applied to W and V.
+B200 form, per round, all block pairs ("slots") at once:
 
-phase 1 (tensor cores, FP64 eigen-solves), per round, all block pairs at once
-(two-part 3xBF16 operands while the off value is above 5e-2, then three-part
-6xBF16 operands, ~FP32, until it is <= tol_phase1):
-    G_k  = X_k^T X_k               jb_gemm_bf16x SPLIT3, split-K (<= 128-long
-                                   accumulation chains), X_k = the pair's 2b
-                                   columns (a "slot" of W^T rows)
-    vv_k = eig(G_k), descending     jb_block_eig_f64 (FP64)
-    W_k  <- W_k vv_k, V_k <- V_k vv_k   jb_gemm_bf16x SPLIT3 (B N-contiguous),
-                                   scattered into the next round's slots
-  until the largest pair ratio |g_pq| / sqrt(g_pp g_qq) of a sweep (FP64) is
-  <= tol_phase1.  Carrying W in 16-bit parts would cost a small column
-  ~2^-16 sigma_1 / sigma_j of its own accuracy per rotation; the three-part
-  sweeps bring that to the FP32 level before V is taken.
-phase 2 (accuracy): V <- V (3I - V^T V) / 2 (Newton-Schulz, SPLIT6 products,
-  ~FP32 accurate), W = A V recomputed from the exact input with FP64
-  accumulation (jb_gemm_f64acc), sigma = column norms of W in FP64.  With V
-  orthogonal to ~1e-6 (a multiplicative perturbation of every sigma) and
-  W's columns orthogonal to ~tol_phase1 (an error ~tol_phase1^2 relative),
-  every sigma above the cut keeps a relative error of a few 1e-6.
-Outputs follow the reference: sigma sorted descending, values below
-eps32 * max(m, n) * sigma_1 reported as 0 (solvers.py:18-21).
+    G_k  = X_k X_k^T        jb_gemm_bf16x, SYRK + CHAIN128: one TMA stream of
+                            the slot's 2b rows of W^T read as both operands,
+                            accumulation chains of <= 128 along K in separate
+                            tensor-memory accumulators summed in FP32
+    vv_k = eig(G_k)         jb_block_eig_f64: FP64 Jacobi on the 2b x 2b Gram,
+                            eigenvectors sorted by descending eigenvalue (the
+                            reference's inner SVD sorts, primitives.py:357-358)
+    X_k <- vv_k^T X_k       jb_gemm_bf16x_rows: the update for W^T and V^T,
+                            each rotated row written as BF16 parts straight
+                            into its slot of the next round
+
+Precision stages.  The first sweeps run on two-part operands (compensated
+3xBF16 products, FP32 accumulation): their off value counts only columns of
+norm >= 1e-2 sigma_1, for which the ~2^-16 sigma_1 storage error of a part
+pair is harmless, and they end when it is <= `switch`.  Then V is made
+orthogonal (Newton-Schulz, 6xBF16 products), W = A V is recomputed from the
+exact input with FP64 accumulation (jb_gemm_f64acc), and the sweeps continue
+on three-part operands (6xBF16, ~FP32) over the reference's live set until
+off <= tol_phase1 (the reference's 40 eps32, solvers.py:41,55-57).
+
+Finish: V orthogonalised again, W = A V with FP64 accumulation, sigma =
+column norms in FP64, sorted descending, values below eps32 * max(m, n) *
+sigma_1 reported as 0 (solvers.py:18-21, 61-66).  With V orthogonal to ~1e-6
+and W's columns orthogonal to ~tol_phase1, every sigma above the cut keeps a
+relative error of a few 1e-6.
 """
 from __future__ import annotations
 
@@ -34,9 +39,7 @@ import numpy as np
 import torch
 
 from . import native as N
-from .tensor import gemm_parts, split3_bf16, split_bf16
-
-CHAIN = 128  # longest tensor-memory accumulation chain (K) per CTA
+from .tensor import gemm_parts, gemm_parts_rows, split3_bf16
 
 
 def _st(dev):
@@ -58,10 +61,6 @@ def schedule(nb):
             row.append((min(a, b), max(a, b)))
         out.append(row)
     return out
-
-
-def _split_k(K):
-    return max(1, min(64, math.ceil(K / CHAIN)))
 
 
 class BlockJacobi:
@@ -124,8 +123,6 @@ class BlockJacobi:
         self.off = torch.zeros(R, self.P, **f32)
         self.dmax = torch.zeros(R, self.P, **f32)
         self.isweeps = torch.zeros(self.P, dtype=torch.int32, device=dev)
-        self.CW = torch.empty(self.P, 2 * b, self.mpad, **f32)
-        self.CV = torch.empty(self.P, 2 * b, self.npad, **f32)
 
     def _combine_v(self, cur):
         """V^T (npad x npad, FP32) from the slots of buffer `cur` (round 0 layout)."""
@@ -139,12 +136,11 @@ class BlockJacobi:
         """Newton-Schulz: V <- V (3I - V^T V) / 2 on V^T rows (G = Vt Vt^T,
         Vt <- H Vt), SPLIT6 products with 128-long accumulation chains."""
         eye = torch.eye(self.npad, dtype=torch.float32, device=self.device)
-        sk = _split_k(self.npad)
         for _ in range(steps):
             vp = split3_bf16(vt)
-            g = gemm_parts(vp, vp, split_k=sk)[0]
+            g = gemm_parts(vp, vp, chain128=True)[0]
             h = (3.0 * eye - g) * 0.5
-            vt = gemm_parts(split3_bf16(h), vp, b_mn=True, split_k=sk)[0]
+            vt = gemm_parts(split3_bf16(h), vp, b_mn=True, chain128=True)[0]
         return vt
 
     def _w_from_v(self, vt, ap):
@@ -194,8 +190,6 @@ class BlockJacobi:
         sweeps = 0
         off_hist = []
         parts = 2
-        skW = _split_k(self.mpad)
-        rows = P * 2 * b
         live_rel = (np.finfo(np.float32).eps * max(m, n)) ** 2
         dmax = float((at * at).sum(1).max())
         best, stall, converged, stage_sweeps = float("inf"), 0, False, 0
@@ -206,20 +200,16 @@ class BlockJacobi:
                 Wp = [x.view(P, 2 * b, self.mpad) for x in self.W[cur][:parts]]
                 Vp = [x.view(P, 2 * b, self.npad) for x in self.V[cur][:parts]]
                 # Grams of every slot: G_k = X_k X_k^T with X_k = 2b rows of W^T.
-                gemm_parts(Wp, Wp, self.G, split_k=skW)
+                gemm_parts(Wp, None, self.G, syrk=True, chain128=True)
                 N.check(lib.jb_block_eig_f64(self.G.data_ptr(), self.Qt[0].data_ptr(), self.Qt[1].data_ptr(),
                                              self.Qt[2].data_ptr() if parts == 3 else None, self.off[r].data_ptr(),
                                              self.dmax[r].data_ptr(), self.isweeps.data_ptr(), P, 2 * b,
                                              inner_sweeps, inner_tol, live_floor, st), "jb_block_eig_f64")
-                # X_k <- vv^T X_k (rows of W^T), same for V.
-                gemm_parts(self.Qt[:parts], Wp, self.CW, b_mn=True)
-                gemm_parts(self.Qt[:parts], Vp, self.CV, b_mn=True)
+                # X_k <- vv^T X_k (rows of W^T), same for V, each rotated row
+                # written (as BF16 parts) straight into its next-round slot.
                 nxt = 1 - cur
-                mp = self.maps[r].data_ptr()
-                for buf, src, L in ((self.W[nxt], self.CW, self.mpad), (self.V[nxt], self.CV, self.npad)):
-                    N.check(lib.jb_rows_scatter(src.data_ptr(), mp, buf[0].data_ptr(), buf[1].data_ptr(),
-                                                buf[2].data_ptr() if parts == 3 else None, None, rows, L, st),
-                            "scatter")
+                gemm_parts_rows(self.Qt[:parts], Wp, self.W[nxt][:parts], self.maps[r], b_mn=True)
+                gemm_parts_rows(self.Qt[:parts], Vp, self.V[nxt][:parts], self.maps[r], b_mn=True)
                 cur = nxt
             off = float(self.off.max())
             dmax = max(dmax, float(self.dmax.max()))

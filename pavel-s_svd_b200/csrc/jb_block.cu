@@ -34,40 +34,57 @@ __device__ __forceinline__ int circ(int pos, int r, int n) {
     return 1 + x;
 }
 
-// One CTA per slot.  G (n x n, FP64, symmetric) is rotated as G <- J^T G J
-// with the one-sided Jacobi rotation of columns p, q of the slot (app = g_pp,
-// aqq = g_qq, apq = g_pq; primitives.py:334-347), the pairs of a round in
-// parallel (round-robin order), Q <- Q J accumulated (FP32), until no pair is
-// active or `sweeps` sweeps.  The off value of the slot is the largest
-// |g_pq| / sqrt(g_pp g_qq) over its active pairs of live columns (g_pp and
-// g_qq above live_floor) in the first sweep; dmax is the slot's largest g_pp.
-__global__ void __launch_bounds__(256) eig_kernel(const float *Gin, __nv_bfloat16 *Qt_hi, __nv_bfloat16 *Qt_lo,
-                                                  __nv_bfloat16 *Qt_lo2, float *off_out, float *dmax_out,
-                                                  int *sweeps_out, int n, int max_sweeps, double tol,
-                                                  double live_floor) {
+constexpr int kEigThreads = 512;
+
+// Shared-memory bytes of eig_kernel for a 2b = n slot.
+__host__ __device__ inline size_t eig_smem_bytes(int n) {
+    return (size_t)n * n * 8            // G, FP64
+           + (size_t)n * n * 4          // Q, FP32
+           + (size_t)n * 8 + 32 * 8     // c/s of a round, warp partials
+           + (size_t)n * 4              // permutation
+           + (size_t)(n - 1) * n + n    // round-robin table, pairs of a round
+           + 16;
+}
+
+// One CTA per slot.  G (n x n, FP64, symmetric, column-major) is rotated as
+// G <- J^T G J with the one-sided Jacobi rotation of columns p, q of the slot
+// (app = g_pp, aqq = g_qq, apq = g_pq; primitives.py:334-347), the pairs of a
+// round in parallel (round-robin order, primitives.py:309-313), Q <- Q J
+// accumulated (FP32), until no pair is active or `sweeps` sweeps.  The off
+// value of the slot is the largest |g_pq| / sqrt(g_pp g_qq) over its active
+// pairs of live columns (g_pp and g_qq above live_floor) in the first sweep;
+// dmax is the slot's largest g_pp.
+//
+// Per round: the pair parameters (half the threads of one or two warps), one
+// barrier, then the G blocks and the Q columns of all pairs, one barrier.
+// The player table of every round is built once; G items are laid out with
+// the row pair fastest so that a warp reads one column at 32 distinct rows.
+__global__ void __launch_bounds__(kEigThreads) eig_kernel(const float *Gin, __nv_bfloat16 *Qt_hi,
+                                                          __nv_bfloat16 *Qt_lo, __nv_bfloat16 *Qt_lo2,
+                                                          float *off_out, float *dmax_out, int *sweeps_out, int n,
+                                                          int max_sweeps, double tol, double live_floor) {
     extern __shared__ __align__(16) unsigned char smem[];
-    double *G = (double *)smem;                       // n x n
-    float *Q = (float *)(G + (size_t)n * n);           // n x n (column-major)
-    double *cs = (double *)(Q + (size_t)n * n + (n & 1)); // c[n/2], s[n/2]
-    double *red = cs + n;                              // 32 + n
-    int *perm = (int *)(red + 32 + n);
+    double *G = (double *)smem;                         // n x n, G[col * n + row]
+    float *Q = (float *)(G + (size_t)n * n);             // n x n, Q[col * n + row]
+    double *cs = (double *)(Q + (size_t)n * n);          // c[half], s[half] (n even: 8-byte aligned)
+    double *red = cs + n;                                // 32 warp partials
+    int *perm = (int *)(red + 32);                       // n
+    unsigned char *sched = (unsigned char *)(perm + n);  // (n - 1) x n players
+    unsigned char *pq = sched + (size_t)(n - 1) * n;     // p[half], q[half] of the round
     __shared__ int s_any;
     const int k = blockIdx.x;
+    const int half = n / 2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     const float *g_in = Gin + (size_t)k * n * n;
     for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
-        G[i] = (double)g_in[i];
         const int c = i / n, r = i - c * n;
+        // symmetrise (the tensor-core Gram is symmetric up to rounding)
+        G[i] = 0.5 * ((double)g_in[i] + (double)g_in[(size_t)r * n + c]);
         Q[i] = (r == c) ? 1.f : 0.f;
     }
-    __syncthreads();
-    // symmetrise (the tensor-core Gram is symmetric up to rounding)
-    for (int i = threadIdx.x; i < n * n; i += blockDim.x) {
-        const int c = i / n, r = i - c * n;
-        if (r < c) {
-            const double v = 0.5 * (G[i] + G[(size_t)r * n + c]);
-            G[i] = v;
-            G[(size_t)r * n + c] = v;
-        }
+    for (int i = threadIdx.x; i < (n - 1) * n; i += blockDim.x) {
+        const int r = i / n, pos = i - r * n;
+        sched[i] = (unsigned char)circ(pos, r, n);
     }
     __syncthreads();
     double dmax = 0.0;
@@ -77,78 +94,79 @@ __global__ void __launch_bounds__(256) eig_kernel(const float *Gin, __nv_bfloat1
     __syncthreads();
     double gmax = 0.0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) gmax = fmax(gmax, red[w]);
-    __syncthreads();
     const double floor_ = 2.220446049250313e-16 * 2.220446049250313e-16 * gmax;
-    const int half = n / 2;
+    const double tol2 = tol * tol;
     double first_off = 0.0;
     int sweep = 0;
     for (sweep = 1; sweep <= max_sweeps; ++sweep) {
+        __syncthreads();                                 // red / s_any readers of the last sweep are done
         if (threadIdx.x == 0) s_any = 0;
-        double off = 0.0;
+        double off2 = 0.0;
         for (int r = 0; r < n - 1; ++r) {
-            __syncthreads();
-            for (int t = threadIdx.x; t < half; t += blockDim.x) {
-                int p = circ(t, r, n), q = circ(n - 1 - t, r, n);
+            __syncthreads();                             // G, Q of the previous round complete
+            if (threadIdx.x < half) {
+                const int t = threadIdx.x;
+                int p = sched[r * n + t], q = sched[r * n + n - 1 - t];
                 if (p > q) { const int x = p; p = q; q = x; }
                 const double app = G[(size_t)p * n + p], aqq = G[(size_t)q * n + q], apq = G[(size_t)q * n + p];
                 double c = 1.0, s = 0.0;
-                const double den = sqrt(app) * sqrt(aqq);
-                const double ratio = fabs(apq) / fmax(den, 1e-300);
-                if (ratio > tol && fmin(app, aqq) > floor_) {
+                const double prod = app * aqq, apq2 = apq * apq;
+                if (apq2 > tol2 * prod && fmin(app, aqq) > floor_) {
                     // off over live columns only (norm^2 above live_floor),
                     // like the reference's convergence check (solvers.py:55-57)
-                    if (fmin(app, aqq) > live_floor) off = fmax(off, ratio);
+                    if (fmin(app, aqq) > live_floor) off2 = fmax(off2, apq2 / prod);
                     const double d = aqq - app;
-                    const double tt = copysign(2.0 * fabs(apq), d) / (fabs(d) + sqrt(d * d + 4.0 * apq * apq));
-                    c = 1.0 / sqrt(1.0 + tt * tt);
+                    const double tt = copysign(2.0 * fabs(apq), d) / (fabs(d) + sqrt(d * d + 4.0 * apq2));
+                    c = rsqrt(1.0 + tt * tt);
                     s = tt * c;
                     if (apq < 0.0) s = -s;
                     s_any = 1;
                 }
                 cs[t] = c;
                 cs[half + t] = s;
+                pq[t] = (unsigned char)p;
+                pq[half + t] = (unsigned char)q;
             }
             __syncthreads();
-            // G <- J^T G J, one 2 x 2 block (pair a rows, pair b columns) per item.
-            for (int t = threadIdx.x; t < half * half; t += blockDim.x) {
-                const int a = t / half, b = t - a * half;
-                int p = circ(a, r, n), q = circ(n - 1 - a, r, n);
-                if (p > q) { const int x = p; p = q; q = x; }
-                int u = circ(b, r, n), v = circ(n - 1 - b, r, n);
-                if (u > v) { const int x = u; u = v; v = x; }
-                const double ca = cs[a], sa = cs[half + a], cb = cs[b], sb = cs[half + b];
-                const double gpu = G[(size_t)u * n + p], gqu = G[(size_t)u * n + q];
-                const double gpv = G[(size_t)v * n + p], gqv = G[(size_t)v * n + q];
-                // rows: [p; q] <- J_a^T [p; q] with J = [[c, s], [-s, c]] acting on columns (p, q)
-                const double rpu = ca * gpu - sa * gqu, rqu = sa * gpu + ca * gqu;
-                const double rpv = ca * gpv - sa * gqv, rqv = sa * gpv + ca * gqv;
-                // columns: [u, v] <- [u, v] J_b
-                G[(size_t)u * n + p] = cb * rpu - sb * rpv;
-                G[(size_t)v * n + p] = sb * rpu + cb * rpv;
-                G[(size_t)u * n + q] = cb * rqu - sb * rqv;
-                G[(size_t)v * n + q] = sb * rqu + cb * rqv;
-            }
-            for (int t = threadIdx.x; t < half * n; t += blockDim.x) {
-                const int b = t / n, i = t - b * n;
-                int u = circ(b, r, n), v = circ(n - 1 - b, r, n);
-                if (u > v) { const int x = u; u = v; v = x; }
-                const float cb = (float)cs[b], sb = (float)cs[half + b];
-                const float xu = Q[(size_t)u * n + i], xv = Q[(size_t)v * n + i];
-                Q[(size_t)u * n + i] = cb * xu - sb * xv;
-                Q[(size_t)v * n + i] = sb * xu + cb * xv;
+            // G <- J^T G J: warp w takes column pairs b = w, w + nwarps, ...,
+            // its lanes the row pairs a (one 2 x 2 block per (a, b)); then the
+            // same column pairs of Q, lanes over rows.
+            for (int b = warp; b < half; b += nwarps) {
+                const int u = pq[b], v = pq[half + b];
+                const double cb = cs[b], sb = cs[half + b];
+                double *cu = G + u * n, *cv = G + v * n;
+                for (int a = lane; a < half; a += 32) {
+                    const int p = pq[a], q = pq[half + a];
+                    const double ca = cs[a], sa = cs[half + a];
+                    const double gpu = cu[p], gqu = cu[q], gpv = cv[p], gqv = cv[q];
+                    // rows: [p; q] <- J_a^T [p; q] with J = [[c, s], [-s, c]] acting on columns (p, q)
+                    const double rpu = ca * gpu - sa * gqu, rqu = sa * gpu + ca * gqu;
+                    const double rpv = ca * gpv - sa * gqv, rqv = sa * gpv + ca * gqv;
+                    // columns: [u, v] <- [u, v] J_b
+                    cu[p] = cb * rpu - sb * rpv;
+                    cv[p] = sb * rpu + cb * rpv;
+                    cu[q] = cb * rqu - sb * rqv;
+                    cv[q] = sb * rqu + cb * rqv;
+                }
+                const float fc = (float)cb, fs = (float)sb;
+                float *qu = Q + u * n, *qv = Q + v * n;
+                for (int i = lane; i < n; i += 32) {
+                    const float xu = qu[i], xv = qv[i];
+                    qu[i] = fc * xu - fs * xv;
+                    qv[i] = fs * xu + fc * xv;
+                }
             }
         }
         __syncthreads();
-        for (int o = 16; o; o >>= 1) off = fmax(off, __shfl_xor_sync(0xffffffffu, off, o));
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = off;
+        for (int o = 16; o; o >>= 1) off2 = fmax(off2, __shfl_xor_sync(0xffffffffu, off2, o));
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = off2;
         __syncthreads();
         double om = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) om = fmax(om, red[w]);
-        if (sweep == 1) first_off = om;
-        const int any = s_any;
-        __syncthreads();
-        if (!any) break;
+        if (sweep == 1) first_off = sqrt(om);
+        if (!s_any) break;
     }
+    __syncthreads();
     // Eigenvalues descending (stable), Q^T rows in that order.
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
         const double dj = G[(size_t)j * n + j];
@@ -323,11 +341,12 @@ int jb_block_eig_f64(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, flo
                      int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps, double tol, double live_floor,
                      void *stream) {
     if (!G || !Qt_hi || !Qt_lo || pairs < 1 || n < 2 || (n & 1) || max_sweeps < 1) return JB_EINVAL;
-    const size_t smem = (size_t)n * n * 8 + (size_t)n * n * 4 + 8 + ((size_t)n + 32 + n) * 8 + (size_t)n * 4 + 16;
+    if (n > 256) return JB_ETOOBIG;                  // players are stored as bytes
+    const size_t smem = eig_smem_bytes(n);
     if (smem > 227 * 1024) return JB_ETOOBIG;
     if (cudaFuncSetAttribute(eig_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return JB_ECUDA;
-    eig_kernel<<<(unsigned)pairs, 256, smem, (cudaStream_t)stream>>>(G, (__nv_bfloat16 *)Qt_hi, (__nv_bfloat16 *)Qt_lo,
+    eig_kernel<<<(unsigned)pairs, kEigThreads, smem, (cudaStream_t)stream>>>(G, (__nv_bfloat16 *)Qt_hi, (__nv_bfloat16 *)Qt_lo,
                                                                      (__nv_bfloat16 *)Qt_lo2, off, dmax, sweeps,
                                                                      n, max_sweeps, tol, live_floor);
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;

@@ -18,6 +18,7 @@
 // *error_flag, drains what it issued, frees its TMEM and returns.
 #pragma once
 #include <cuda.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -43,6 +44,18 @@ struct TcParams {
     int b_mn;          // B stored K x N (N contiguous) instead of N x K
     float alpha, beta; // beta: 0 overwrite, 1 accumulate (atomic when splits > 1)
     int *error_flag;
+    // Accumulation chains: k-blocks (of BK) per TMEM accumulator and the
+    // number of accumulators (BN * nacc <= 512 columns); the epilogue sums
+    // them in FP32 registers.
+    int acc_kb, nacc;
+    int a_as_b;        // B = A (a Gram X X^T): the B operand is read from the A tiles
+    // Row-mapped BF16-part output instead of C: row r of batch z goes to row
+    // out_map[z * M + r] (or z * M + r) of out_part[0..out_nparts), each row
+    // out_ld elements long, as hi / mid / lo splits of alpha * (A B^T).
+    __nv_bfloat16 *out_part[3];
+    int out_nparts;
+    const int *out_map;
+    long long out_ld;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -152,15 +165,56 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Stores 32 consecutive values of one output row as hi / mid / lo BF16
+// parts (16-byte stores when the row segment is 16-byte aligned and whole).
+__device__ __forceinline__ void store_parts32(const TcParams &p, long long base, int col0, const float (&v)[32]) {
+    const bool vec = col0 + 32 <= p.N && ((base + col0) & 7) == 0;
+    if (vec) {
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+            uint32_t wh[4], wm[4], wl[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                wh[i] = wm[i] = wl[i] = 0u;
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const float x = p.alpha * v[g * 8 + i * 2 + e];
+                    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+                    const float r1 = x - __bfloat162float(h);
+                    const __nv_bfloat16 m = __float2bfloat16_rn(r1);
+                    const __nv_bfloat16 l = __float2bfloat16_rn(r1 - __bfloat162float(m));
+                    wh[i] |= (uint32_t)__bfloat16_as_ushort(h) << (16 * e);
+                    wm[i] |= (uint32_t)__bfloat16_as_ushort(m) << (16 * e);
+                    wl[i] |= (uint32_t)__bfloat16_as_ushort(l) << (16 * e);
+                }
+            }
+            const long long o = base + col0 + g * 8;
+            *(uint4 *)(p.out_part[0] + o) = make_uint4(wh[0], wh[1], wh[2], wh[3]);
+            if (p.out_nparts > 1) *(uint4 *)(p.out_part[1] + o) = make_uint4(wm[0], wm[1], wm[2], wm[3]);
+            if (p.out_nparts > 2) *(uint4 *)(p.out_part[2] + o) = make_uint4(wl[0], wl[1], wl[2], wl[3]);
+        }
+    } else {
+        for (int i = 0; i < 32 && col0 + i < p.N; ++i) {
+            const float x = p.alpha * v[i];
+            const __nv_bfloat16 h = __float2bfloat16_rn(x);
+            const float r1 = x - __bfloat162float(h);
+            const __nv_bfloat16 m = __float2bfloat16_rn(r1);
+            p.out_part[0][base + col0 + i] = h;
+            if (p.out_nparts > 1) p.out_part[1][base + col0 + i] = m;
+            if (p.out_nparts > 2) p.out_part[2][base + col0 + i] = __float2bfloat16_rn(r1 - __bfloat162float(m));
+        }
+    }
+}
+
 template <int BN>
 __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__ TcParams p) {
     const int STAGES = p.stages;
     constexpr uint32_t B_TILE = BN * BK * 2;
-    constexpr uint32_t TMEM_COLS = BN < 32 ? 32 : BN;
+    const uint32_t tmem_cols = (uint32_t)(BN * p.nacc) < 32 ? 32u : (uint32_t)(BN * p.nacc);
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1024-byte alignment for the swizzled tiles.
     unsigned char *smem = (unsigned char *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    const uint32_t stage_bytes = p.na * A_TILE + p.nb * B_TILE;
+    const uint32_t stage_bytes = p.na * A_TILE + (p.a_as_b ? 0u : p.nb * B_TILE);
     uint64_t *full = (uint64_t *)(smem + STAGES * stage_bytes);
     uint64_t *empty = full + STAGES;
     uint64_t *done = empty + STAGES;
@@ -173,6 +227,8 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
     const int kbeg = split * p.kchunk;
     const int kend = min(p.K, kbeg + p.kchunk);
     const int nk = kend > kbeg ? (kend - kbeg + BK - 1) / BK : 0;
+    // accumulators that receive at least one chain
+    const int nacc_used = min(p.nacc, (nk + p.acc_kb - 1) / p.acc_kb);
 
     if (threadIdx.x == 0) {
         s_err = 0;
@@ -185,7 +241,7 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(TMEM_COLS));
+                     "r"(tmem_cols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -205,12 +261,15 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
             unsigned char *st = smem + s * stage_bytes;
             const int kx = kbeg + kb * BK;
             for (int a = 0; a < p.na; ++a) tma_load_3d(st + a * A_TILE, &p.ta[a], kx, m0, batch, &full[s]);
-            for (int b = 0; b < p.nb; ++b) {
-                unsigned char *bt = st + p.na * A_TILE + b * B_TILE;
-                if (!p.b_mn) {
-                    tma_load_3d(bt, &p.tb[b], kx, n0, batch, &full[s]);
-                } else {
-                    for (int g = 0; g < BN / 64; ++g) tma_load_3d(bt + g * 8192, &p.tb[b], n0 + 64 * g, kx, batch, &full[s]);
+            if (!p.a_as_b) {
+                for (int b = 0; b < p.nb; ++b) {
+                    unsigned char *bt = st + p.na * A_TILE + b * B_TILE;
+                    if (!p.b_mn) {
+                        tma_load_3d(bt, &p.tb[b], kx, n0, batch, &full[s]);
+                    } else {
+                        for (int g = 0; g < BN / 64; ++g)
+                            tma_load_3d(bt + g * 8192, &p.tb[b], n0 + 64 * g, kx, batch, &full[s]);
+                    }
                 }
             }
             issued = kb + 1;
@@ -229,13 +288,17 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
             if (!mbar_wait(&full[s], ph, p.error_flag)) { s_err = 1; ok = false; break; }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             unsigned char *st = smem + s * stage_bytes;
+            const int chain = kb / p.acc_kb;
+            const uint32_t acc = tmem + (uint32_t)((chain % p.nacc) * BN);
+            const bool fresh = (kb % p.acc_kb) == 0 && chain < p.nacc;
             for (int t = 0; t < p.nterm; ++t) {
                 const uint64_t ad = smem_desc_sw128(st + p.term_a[t] * A_TILE);
-                const unsigned char *bt = st + p.na * A_TILE + p.term_b[t] * B_TILE;
+                const unsigned char *bt = p.a_as_b ? st + p.term_b[t] * A_TILE
+                                                   : st + p.na * A_TILE + p.term_b[t] * B_TILE;
                 const uint64_t bd = p.b_mn ? smem_desc_mn_sw128(bt) : smem_desc_sw128(bt);
 #pragma unroll
                 for (int k = 0; k < BK / 16; ++k)  // +32 bytes per K=16 step inside the swizzled row
-                    mma_bf16(tmem, ad + 2 * k, bd + bstep * k, idesc, (kb | t | k) != 0);
+                    mma_bf16(acc, ad + 2 * k, bd + bstep * k, idesc, (fresh && t == 0 && k == 0) ? 0u : 1u);
             }
             mma_commit(&empty[s]);
         }
@@ -246,14 +309,39 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
     const bool have = nk > 0 && mbar_wait(done, 0, p.error_flag);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int row = m0 + warp * 32 + lane;
-    float *crow = p.C + (long long)batch * p.sC + (long long)row * p.ldc;
     // tcgen05.ld is warp-collective: decide per warp.
     if (__all_sync(0xffffffffu, have && !s_err)) {
+        const long long obase = p.out_nparts
+            ? (long long)(p.out_map && row < p.M ? p.out_map[(long long)batch * p.M + row]
+                                                 : (long long)batch * p.M + row) * p.out_ld
+            : 0;
+        float *crow = p.C ? p.C + (long long)batch * p.sC + (long long)row * p.ldc : nullptr;
 #pragma unroll 1
         for (int c0 = 0; c0 < BN; c0 += 32) {
             float v[32];
             tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + c0, v);
-            if (row < p.M) {
+            for (int a = 1; a < nacc_used; ++a) {
+                float w[32];
+                tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(a * BN) + c0, w);
+#pragma unroll
+                for (int i = 0; i < 32; ++i) v[i] += w[i];
+            }
+            if (row >= p.M || n0 + c0 >= p.N) continue;
+            if (p.out_nparts) {
+                store_parts32(p, obase, n0 + c0, v);
+            } else if (p.splits == 1 && n0 + c0 + 32 <= p.N && (((uintptr_t)(crow + n0 + c0)) & 15) == 0) {
+#pragma unroll
+                for (int g = 0; g < 8; ++g) {
+                    float4 *dst = (float4 *)(crow + n0 + c0 + 4 * g);
+                    float4 x = make_float4(p.alpha * v[4 * g], p.alpha * v[4 * g + 1], p.alpha * v[4 * g + 2],
+                                           p.alpha * v[4 * g + 3]);
+                    if (p.beta != 0.f) {
+                        const float4 o = *dst;
+                        x.x += o.x; x.y += o.y; x.z += o.z; x.w += o.w;
+                    }
+                    *dst = x;
+                }
+            } else {
 #pragma unroll
                 for (int i = 0; i < 32; ++i) {
                     const int col = n0 + c0 + i;
@@ -270,7 +358,7 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
     __syncthreads();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tmem_cols));
     }
 }
 

@@ -52,12 +52,12 @@ static size_t smem_bytes(int stages, int na, int nb, int bn) {
 
 template <int BN>
 static int launch(TcParams &p, int64_t batch, cudaStream_t st) {
-    const size_t per_stage = p.na * A_TILE + p.nb * (size_t)BN * BK * 2;
+    const size_t per_stage = p.na * A_TILE + (p.a_as_b ? 0 : p.nb * (size_t)BN * BK * 2);
     int stages = (int)((227 * 1024 - 1024 - 64) / per_stage);
     if (stages > 6) stages = 6;
     if (stages < 2) return JB_ETOOBIG;
     p.stages = stages;
-    const size_t smem = smem_bytes(stages, p.na, p.nb, BN);
+    const size_t smem = smem_bytes(stages, p.na, p.a_as_b ? 0 : p.nb, BN);
     auto kern = tc_gemm_kernel<BN>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return JB_ECUDA;
@@ -96,38 +96,69 @@ int jb_gemm_bf16(const void *A0, const void *A1, const void *B0, const void *B1,
                          split_k, error_flag, stream);
 }
 
-int jb_gemm_bf16x(const void *const *A, const void *const *B, int32_t mode, float *C, int64_t M, int64_t N, int64_t K,
-                  int64_t lda, int64_t ldb, int64_t ldc, int64_t batch, int64_t strideA, int64_t strideB,
-                  int64_t strideC, float alpha, float beta, int32_t split_k, int32_t *error_flag, void *stream) {
-    if (!A || !B || !A[0] || !B[0] || !C || M < 1 || N < 1 || K < 1 || batch < 1 || split_k < 1) return JB_EINVAL;
+}  // extern "C"
+
+namespace jb {
+namespace tc {
+
+// Validates the operands, builds the tensor maps and the K split.  Returns
+// JB_OK and the tile width in *bn_out.
+static int setup(const void *const *A, const void *const *B, int32_t mode, int64_t M, int64_t N, int64_t K,
+                 int64_t lda, int64_t ldb, int64_t batch, int64_t strideA, int64_t strideB, int32_t split_k,
+                 float alpha, int32_t *error_flag, TcParams &p, int &bn_out) {
+    if (!A || !A[0] || M < 1 || N < 1 || K < 1 || batch < 1 || split_k < 1) return JB_EINVAL;
     const int kind = mode & 3;
     const int b_mn = (mode & JB_GEMM_B_MN) ? 1 : 0;
-    if (kind == 3 || (mode & ~(3 | JB_GEMM_B_MN))) return JB_EINVAL;
+    const int chain128 = (mode & JB_GEMM_CHAIN128) ? 1 : 0;
+    const int syrk = (mode & JB_GEMM_SYRK) ? 1 : 0;
+    if (kind == 3 || (mode & ~(3 | JB_GEMM_B_MN | JB_GEMM_CHAIN128 | JB_GEMM_SYRK))) return JB_EINVAL;
+    if (syrk && (b_mn || M != N || N > BM)) return JB_EINVAL;
+    if (!syrk && (!B || !B[0])) return JB_EINVAL;
     const int nsplit = kind == JB_GEMM_PLAIN ? 1 : (kind == JB_GEMM_SPLIT3 ? 2 : 3);
     for (int i = 0; i < nsplit; ++i)
-        if (!A[i] || !B[i] || ((uintptr_t)A[i] & 15) || ((uintptr_t)B[i] & 15)) return JB_EINVAL;
-    if (lda % 8 || ldb % 8 || lda < K || ldc < N) return JB_EINVAL;
-    if (b_mn ? ldb < N : ldb < K) return JB_EINVAL;
-    if (batch > 1 && (strideA % 8 || strideB % 8)) return JB_EINVAL;
-    if (M > (1 << 30) || N > (1 << 30) || batch * split_k > 65535) return JB_ETOOBIG;
-    tc::TcParams p;
+        if (!A[i] || ((uintptr_t)A[i] & 15) || (!syrk && (!B[i] || ((uintptr_t)B[i] & 15)))) return JB_EINVAL;
+    if (lda % 8 || lda < K) return JB_EINVAL;
+    if (!syrk && (ldb % 8 || (b_mn ? ldb < N : ldb < K))) return JB_EINVAL;
+    if (batch > 1 && (strideA % 8 || (!syrk && strideB % 8))) return JB_EINVAL;
+    if (M > (1 << 30) || N > (1 << 30)) return JB_ETOOBIG;
     memset(&p, 0, sizeof(p));
-    const int bn = N <= 64 ? 64 : (N <= 128 || nsplit == 3 ? 128 : 256);
+    int bn = N <= 64 ? 64 : (N <= 128 || nsplit == 3 ? 128 : 256);
+    if (syrk && bn > BM) return JB_EINVAL;
     p.na = p.nb = nsplit;
     p.b_mn = b_mn;
+    p.a_as_b = syrk;
     for (int a = 0; a < nsplit; ++a)
-        if (!tc::make_map(&p.ta[a], A[a], K, M, lda, batch, strideA, tc::BM)) return JB_ECUDA;
-    for (int b = 0; b < nsplit; ++b) {
-        const bool ok = b_mn ? tc::make_map(&p.tb[b], B[b], N, K, ldb, batch, strideB, tc::BK)
-                             : tc::make_map(&p.tb[b], B[b], K, N, ldb, batch, strideB, bn);
-        if (!ok) return JB_ECUDA;
+        if (!make_map(&p.ta[a], A[a], K, M, lda, batch, strideA, BM)) return JB_ECUDA;
+    if (!syrk) {
+        for (int b = 0; b < nsplit; ++b) {
+            const bool ok = b_mn ? make_map(&p.tb[b], B[b], N, K, ldb, batch, strideB, BK)
+                                 : make_map(&p.tb[b], B[b], K, N, ldb, batch, strideB, bn);
+            if (!ok) return JB_ECUDA;
+        }
     }
-    p.C = C; p.ldc = ldc; p.sC = strideC;
     p.M = (int)M; p.N = (int)N; p.K = (int)K;
-    int64_t chunk = (K + split_k - 1) / split_k;
-    chunk = (chunk + tc::BK - 1) / tc::BK * tc::BK;
+    int64_t splits = split_k;
+    if (chain128) {
+        // up to 512 / bn accumulators of 128 along K per CTA
+        const int64_t per_cta = (int64_t)(512 / bn) * 128;
+        const int64_t need = (K + per_cta - 1) / per_cta;
+        if (splits < need) splits = need;
+    }
+    int64_t chunk = (K + splits - 1) / splits;
+    chunk = (chunk + BK - 1) / BK * BK;
     p.kchunk = (int)chunk;
     p.splits = (int)((K + chunk - 1) / chunk);
+    if (batch * p.splits > 65535) return JB_ETOOBIG;
+    if (chain128) {
+        p.acc_kb = 128 / BK;
+        const int chains = (int)((chunk + 127) / 128);
+        int nacc = 1;
+        while (nacc < chains) nacc *= 2;       // TMEM allocations are powers of two
+        p.nacc = nacc;
+    } else {
+        p.acc_kb = (int)(chunk / BK);
+        p.nacc = 1;
+    }
     // Products of the split parts kept: hi*hi, hi*mid, mid*hi (3 terms), plus
     // hi*lo, mid*mid, lo*hi (6 terms): every pair whose exponents sum to at
     // most two splits below the leading term.
@@ -135,8 +166,35 @@ int jb_gemm_bf16x(const void *const *A, const void *const *B, int32_t mode, floa
     p.nterm = nsplit == 1 ? 1 : (nsplit == 2 ? 3 : 6);
     for (int t = 0; t < p.nterm; ++t) { p.term_a[t] = ta6[t]; p.term_b[t] = tb6[t]; }
     p.alpha = alpha;
-    p.beta = (p.splits > 1) ? 1.f : beta;
     p.error_flag = error_flag;
+    bn_out = bn;
+    return JB_OK;
+}
+
+static int dispatch(TcParams &p, int bn, int64_t batch, cudaStream_t st) {
+    switch (bn) {
+        case 64: return launch<64>(p, batch, st);
+        case 128: return launch<128>(p, batch, st);
+        default: return launch<256>(p, batch, st);
+    }
+}
+
+}  // namespace tc
+}  // namespace jb
+
+extern "C" {
+
+int jb_gemm_bf16x(const void *const *A, const void *const *B, int32_t mode, float *C, int64_t M, int64_t N, int64_t K,
+                  int64_t lda, int64_t ldb, int64_t ldc, int64_t batch, int64_t strideA, int64_t strideB,
+                  int64_t strideC, float alpha, float beta, int32_t split_k, int32_t *error_flag, void *stream) {
+    if (!C || ldc < N) return JB_EINVAL;
+    tc::TcParams p;
+    int bn = 0;
+    const int rc = tc::setup(A, B, mode, M, N, K, lda, ldb, batch, strideA, strideB, split_k, alpha, error_flag, p,
+                             bn);
+    if (rc != JB_OK) return rc;
+    p.C = C; p.ldc = ldc; p.sC = strideC;
+    p.beta = (p.splits > 1) ? 1.f : beta;
     cudaStream_t st = (cudaStream_t)stream;
     if (p.splits > 1 && beta == 0.f) {
         if (ldc == N && (batch == 1 || strideC == M * N)) {
@@ -148,11 +206,26 @@ int jb_gemm_bf16x(const void *const *A, const void *const *B, int32_t mode, floa
                     return JB_ECUDA;
         }
     }
-    switch (bn) {
-        case 64: return tc::launch<64>(p, batch, st);
-        case 128: return tc::launch<128>(p, batch, st);
-        default: return tc::launch<256>(p, batch, st);
-    }
+    return tc::dispatch(p, bn, batch, st);
+}
+
+int jb_gemm_bf16x_rows(const void *const *A, const void *const *B, int32_t mode, void *const *out, int32_t nparts,
+                       const int32_t *row_map, int64_t ld_out, int64_t M, int64_t N, int64_t K, int64_t lda,
+                       int64_t ldb, int64_t batch, int64_t strideA, int64_t strideB, float alpha,
+                       int32_t *error_flag, void *stream) {
+    if (!out || nparts < 1 || nparts > 3 || ld_out < N || ld_out % 8) return JB_EINVAL;
+    for (int i = 0; i < nparts; ++i)
+        if (!out[i] || ((uintptr_t)out[i] & 15)) return JB_EINVAL;
+    tc::TcParams p;
+    int bn = 0;
+    const int rc = tc::setup(A, B, mode, M, N, K, lda, ldb, batch, strideA, strideB, 1, alpha, error_flag, p, bn);
+    if (rc != JB_OK) return rc;
+    if (p.splits != 1) return JB_ETOOBIG;            // one CTA along K (the TMEM accumulators hold it)
+    for (int i = 0; i < nparts; ++i) p.out_part[i] = (__nv_bfloat16 *)out[i];
+    p.out_nparts = nparts;
+    p.out_map = row_map;
+    p.out_ld = ld_out;
+    return tc::dispatch(p, bn, batch, (cudaStream_t)stream);
 }
 
 int jb_split_bf16(const float *X, void *hi, void *lo, int64_t n, void *stream) {

@@ -23,12 +23,13 @@ RC_NAMES = {JB_EINVAL: "invalid argument", JB_ETOOBIG: "shape too large for this
 
 # Exported symbols, in declaration order of include/jacobi_b200.h.
 SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_batched_f32",
-           "jb_svd_batched_f64", "jb_svd_uneven_f32", "jb_gemm_bf16", "jb_gemm_bf16x", "jb_split_bf16",
+           "jb_svd_batched_f64", "jb_svd_uneven_f32", "jb_gemm_bf16", "jb_gemm_bf16x", "jb_gemm_bf16x_rows",
+           "jb_split_bf16",
            "jb_split3_bf16",
            "jb_warm_prep_f32", "jb_svd_warm_f32", "jb_transpose_bf16", "jb_bias_act", "jb_relu_backward",
            "jb_col_sum", "jb_mse_grad", "jb_adam", "jb_gram_sketch", "jb_block_eig_f64", "jb_rows_scatter",
            "jb_rows_combine", "jb_gemm_f64acc", "jb_block_finish", "jb_svd_batched_f32_noalloc")
-GEMM_PLAIN, GEMM_SPLIT3, GEMM_SPLIT6, GEMM_B_MN = 0, 1, 2, 4
+GEMM_PLAIN, GEMM_SPLIT3, GEMM_SPLIT6, GEMM_B_MN, GEMM_CHAIN128, GEMM_SYRK = 0, 1, 2, 4, 8, 16
 NOALLOC_SCRATCH_BYTES = 16 << 20  # JB_NOALLOC_SCRATCH_BYTES
 
 
@@ -70,6 +71,10 @@ def _declare(l):
     l.jb_gemm_bf16x.restype = ctypes.c_int
     l.jb_gemm_bf16x.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p), I32, P, I64, I64,
                                 I64, I64, I64, I64, I64, I64, I64, I64, ctypes.c_float, ctypes.c_float, I32, P, P]
+    l.jb_gemm_bf16x_rows.restype = ctypes.c_int
+    l.jb_gemm_bf16x_rows.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p), I32,
+                                     ctypes.POINTER(ctypes.c_void_p), I32, P, I64, I64, I64, I64, I64, I64, I64,
+                                     I64, I64, ctypes.c_float, P, P]
     FL = ctypes.c_float
     for name, args in (("jb_warm_prep_f32", [P, P, P, P, P, P, I64, I32, I32, P]),
                        ("jb_svd_warm_f32", [P, P, P, P, P, I64, I32, I32, I32, I32, F64, I32, I32, P, P, P, SZ, P]),

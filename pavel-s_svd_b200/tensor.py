@@ -3,6 +3,8 @@ jb_split_bf16).  Buffers are torch tensors on the current device; the work is
 enqueued on the current stream."""
 from __future__ import annotations
 
+import ctypes
+
 import torch
 
 from . import native as N
@@ -31,12 +33,22 @@ def split3_bf16(x: torch.Tensor):
     return tuple(parts)
 
 
+def _mode(ns, b_mn, chain128, syrk):
+    return ({1: N.GEMM_PLAIN, 2: N.GEMM_SPLIT3, 3: N.GEMM_SPLIT6}[ns] | (N.GEMM_B_MN if b_mn else 0) |
+            (N.GEMM_CHAIN128 if chain128 else 0) | (N.GEMM_SYRK if syrk else 0))
+
+
 def gemm_parts(a_parts, b_parts, c=None, *, b_mn=False, alpha=1.0, beta=0.0, split_k=1, error_flag=None,
-               M=None, N_=None, K=None, lda=None, ldb=None, ldc=None, batch=None, sA=None, sB=None, sC=None):
+               chain128=False, syrk=False):
     """General entry over split parts (1, 2 or 3 of them): C = alpha A B^T (+ beta C).
 
     a parts: (batch, M, K) bf16; b parts: (batch, N, K) bf16, or with b_mn
-    (batch, K, N) bf16 (N contiguous).  Returns C (batch, M, N) float32."""
+    (batch, K, N) bf16 (N contiguous).  With syrk, B is A (C = A A^T) and
+    b_parts is ignored.  chain128 keeps every accumulation chain <= 128 long
+    (several tensor-memory accumulators per CTA).  Returns C (batch, M, N)
+    float32."""
+    if syrk:
+        b_parts = a_parts
     a0, b0 = a_parts[0], b_parts[0]
     if a0.dim() == 2:
         a_parts = [x[None] for x in a_parts]
@@ -50,8 +62,7 @@ def gemm_parts(a_parts, b_parts, c=None, *, b_mn=False, alpha=1.0, beta=0.0, spl
         beta = 0.0
     c3 = c if c.dim() == 3 else c[None]
     ns = len(a_parts)
-    mode = {1: N.GEMM_PLAIN, 2: N.GEMM_SPLIT3, 3: N.GEMM_SPLIT6}[ns] | (N.GEMM_B_MN if b_mn else 0)
-    import ctypes
+    mode = _mode(ns, b_mn, chain128, syrk)
     A = (ctypes.c_void_p * 3)(*[x.data_ptr() for x in a_parts] + [None] * (3 - ns))
     B = (ctypes.c_void_p * 3)(*[x.data_ptr() for x in b_parts] + [None] * (3 - ns))
     rc = N.lib().jb_gemm_bf16x(A, B, mode, c3.data_ptr(), M, Nn, K, a0.stride(1), b0.stride(1), c3.stride(1),
@@ -59,6 +70,25 @@ def gemm_parts(a_parts, b_parts, c=None, *, b_mn=False, alpha=1.0, beta=0.0, spl
                                _ptr(error_flag), torch.cuda.current_stream(a0.device).cuda_stream)
     N.check(rc, "jb_gemm_bf16x")
     return c
+
+
+def gemm_parts_rows(a_parts, b_parts, out_parts, row_map=None, *, b_mn=False, alpha=1.0, chain128=True,
+                    error_flag=None):
+    """alpha A B^T written as BF16 split parts into mapped rows:
+    row r of batch z -> row row_map[z * M + r] of every out part (2-D,
+    rows x L, L >= N).  len(out_parts) parts (1..3) are written."""
+    a0, b0 = a_parts[0], b_parts[0]
+    bsz, M, K = a0.shape
+    Nn = b0.shape[-1] if b_mn else b0.shape[-2]
+    ns = len(a_parts)
+    A = (ctypes.c_void_p * 3)(*[x.data_ptr() for x in a_parts] + [None] * (3 - ns))
+    B = (ctypes.c_void_p * 3)(*[x.data_ptr() for x in b_parts] + [None] * (3 - ns))
+    O = (ctypes.c_void_p * 3)(*[x.data_ptr() for x in out_parts] + [None] * (3 - len(out_parts)))
+    rc = N.lib().jb_gemm_bf16x_rows(A, B, _mode(ns, b_mn, chain128, False), O, len(out_parts), _ptr(row_map),
+                                    out_parts[0].shape[-1], M, Nn, K, a0.stride(1), b0.stride(1), bsz,
+                                    a0.stride(0), b0.stride(0), float(alpha), _ptr(error_flag),
+                                    torch.cuda.current_stream(a0.device).cuda_stream)
+    N.check(rc, "jb_gemm_bf16x_rows")
 
 
 def gemm(a, b, c=None, *, a_lo=None, b_lo=None, alpha=1.0, beta=0.0, split_k=1, error_flag=None):

@@ -87,3 +87,66 @@ def test_split6_reaches_fp32_accuracy(T):
     bt = torch.randn(2, 2048, 304, device="cuda", generator=g)
     c6m = T.gemm_parts(T.split3_bf16(x), T.split3_bf16(bt), b_mn=True, split_k=16)
     assert rel(c6m, x.double() @ bt.double()) <= 2e-6
+
+
+@pytest.mark.parametrize("M,N,K,batch", [(300, 260, 2048, 2), (64, 64, 4096, 16), (128, 128, 8192, 4),
+                                         (96, 200, 1000, 3)])
+def test_chain128_accumulators(T, M, N, K, batch):
+    """CHAIN128: chains of <= 128 along K in separate tensor-memory
+    accumulators summed in FP32 -- the accuracy of split-K 128 without its
+    atomics (and with far fewer CTAs along K)."""
+    g = torch.Generator(device="cuda").manual_seed(M + N + K + batch)
+    x = torch.randn(batch, M, K, device="cuda", generator=g)
+    y = torch.randn(batch, N, K, device="cuda", generator=g)
+    ref = x.double() @ y.double().transpose(-1, -2)
+    flag = torch.zeros(1, dtype=torch.int32, device="cuda")
+    c6 = T.gemm_parts(T.split3_bf16(x), T.split3_bf16(y), chain128=True, error_flag=flag)
+    torch.cuda.synchronize()
+    assert int(flag) == 0
+    assert rel(c6, ref) <= 2e-6
+    c3 = T.gemm_parts(T.split_bf16(x), T.split_bf16(y), chain128=True)
+    assert rel(c3, ref) <= 5e-5
+
+
+@pytest.mark.parametrize("M,K,batch,parts", [(64, 4096, 16, 3), (128, 8192, 16, 2), (40, 1000, 5, 3)])
+def test_syrk_gram(T, M, K, batch, parts):
+    """SYRK (B = A, one TMA stream for both operands): the block-pair Gram."""
+    g = torch.Generator(device="cuda").manual_seed(M + K)
+    x = torch.randn(batch, M, K, device="cuda", generator=g) * torch.logspace(0, -3, M, device="cuda")[:, None]
+    sp = (T.split3_bf16 if parts == 3 else T.split_bf16)(x)
+    c = T.gemm_parts(list(sp), None, syrk=True, chain128=True)
+    ref = x.double() @ x.double().transpose(-1, -2)
+    assert rel(c, ref) <= (2e-6 if parts == 3 else 5e-5)
+    # entry-wise: relative to the column norms (what the Jacobi ratio needs)
+    d = ref.diagonal(dim1=-2, dim2=-1).sqrt()
+    scaled = (c.double() - ref).abs() / (d[..., :, None] * d[..., None, :])
+    # FP32 accumulation over K: ~1e-6 relative per entry for the 6-term product
+    assert float(scaled.max()) <= (5e-6 if parts == 3 else 5e-5)
+    assert torch.equal(c, c.transpose(-1, -2)) or float((c - c.transpose(-1, -2)).abs().max()) <= 1e-6 * float(c.abs().max())
+
+
+@pytest.mark.parametrize("parts", [1, 2, 3])
+def test_rows_output_parts_and_map(T, parts):
+    """jb_gemm_bf16x_rows: alpha A B (B N-contiguous) written as BF16 parts
+    into mapped rows equals the FP32 product, split and scattered."""
+    g = torch.Generator(device="cuda").manual_seed(parts)
+    batch, M, K, L = 8, 64, 64, 1000
+    a = torch.randn(batch, M, K, device="cuda", generator=g)
+    bt = torch.randn(batch, K, L, device="cuda", generator=g)
+    sa = T.split3_bf16(a)[:max(parts, 1)] if parts > 1 else (T.split_bf16(a)[0],)
+    sb = T.split3_bf16(bt)[:max(parts, 1)] if parts > 1 else (T.split_bf16(bt)[0],)
+    rows = batch * M
+    perm = torch.randperm(rows, generator=torch.Generator().manual_seed(5)).to(torch.int32).cuda()
+    out = [torch.full((rows, 1008), 7.0, dtype=torch.bfloat16, device="cuda") for _ in range(parts)]
+    T.gemm_parts_rows(list(sa), list(sb), out, perm, b_mn=True, alpha=0.5)
+    c = 0.5 * T.gemm_parts(list(sa), list(sb), b_mn=True).reshape(rows, L)
+    got = torch.zeros(rows, L, dtype=torch.float32, device="cuda")
+    for o in out:
+        got += o[:, :L].float()
+    expect = torch.empty_like(got)
+    expect[perm.long()] = c
+    # the parts carry 8, 16 or 24 significant bits of the FP32 result
+    tol = {1: 2 ** -8, 2: 2 ** -16, 3: 2 ** -23}[parts]
+    assert float(((got - expect).abs() / expect.abs().clamp_min(1e-30)).max()) <= tol
+    for o in out:  # the padding past N is untouched
+        assert bool((o[:, L:] == 7.0).all())
