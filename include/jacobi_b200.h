@@ -245,16 +245,19 @@ JB_API int jb_gram_sketch(const float *A, void *X, int64_t batch, int32_t m, int
 
 /* FP64 eigen-solve of `pairs` symmetric n x n FP32 Grams G[k] (n even): the
  * one-sided Jacobi rotations of the slot's columns applied to its Gram
- * (G <- J^T G J, round-robin pairs, relative threshold tol, at most
- * max_sweeps sweeps).  Writes vv^T (rows = eigenvectors, eigenvalues
- * descending: the inner solve's V of solvers.py:48) as hi/lo BF16 (and a
- * third part when Qt_lo2 is given), the largest pair ratio
+ * (G <- J^T G J, relative threshold tol, at most max_sweeps sweeps; slots
+ * of n = 64 and 128 use the odd-even pair order with registers-resident G,
+ * others the round-robin order).  Writes vv^T (rows = eigenvectors,
+ * eigenvalues descending: the inner solve's V of solvers.py:48) as hi/lo
+ * BF16 (and a third part when Qt_lo2 is given), the largest pair ratio
  * |g_pq| / sqrt(g_pp g_qq) of the first sweep over live columns (g_pp, g_qq
- * > live_floor: the reference checks only those, solvers.py:55-57) (off),
- * the slot's largest diagonal entry (dmax) and the sweeps used. */
+ * > *live_floor, a device double, 0 when NULL: the reference checks only
+ * those, solvers.py:55-57) (off), the slot's largest diagonal entry (dmax)
+ * and the sweeps used.  The floor is read on the device so that a captured
+ * CUDA graph of a whole sweep can be replayed with a new floor. */
 JB_API int jb_block_eig_f64(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off,
                             float *dmax, int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps,
-                            double tol, double live_floor, void *stream);
+                            double tol, const double *live_floor, void *stream);
 
 /* Row r of src (rows x L, FP32) -> row map[r] (identity when NULL) of the
  * BF16 parts hi, lo, lo2 (a two- or three-part split; any may be NULL)

@@ -123,6 +123,8 @@ class BlockJacobi:
         self.off = torch.zeros(R, self.P, **f32)
         self.dmax = torch.zeros(R, self.P, **f32)
         self.isweeps = torch.zeros(self.P, dtype=torch.int32, device=dev)
+        self.live = torch.zeros(1, dtype=torch.float64, device=dev)   # live-column floor of the sweep
+        self._graphs, self._seen = {}, set()
 
     def _combine_v(self, cur):
         """V^T (npad x npad, FP32) from the slots of buffer `cur` (round 0 layout)."""
@@ -150,8 +152,50 @@ class BlockJacobi:
                                        self.npad, self.npad, self.mpad, _st(self.device)), "jb_gemm_f64acc")
         return wt
 
+    def _sweep(self, cur, parts, inner_sweeps, inner_tol):
+        """Enqueue one sweep (nb - 1 rounds) on the current stream; returns the
+        buffer index holding the result (the rounds alternate buffers and
+        their count is odd)."""
+        lib = N.lib()
+        st = _st(self.device)
+        P, b = self.P, self.b
+        for r in range(self.nb - 1):
+            Wp = [x.view(P, 2 * b, self.mpad) for x in self.W[cur][:parts]]
+            Vp = [x.view(P, 2 * b, self.npad) for x in self.V[cur][:parts]]
+            # Grams of every slot: G_k = X_k X_k^T with X_k = 2b rows of W^T.
+            gemm_parts(Wp, None, self.G, syrk=True, chain128=True)
+            N.check(lib.jb_block_eig_f64(self.G.data_ptr(), self.Qt[0].data_ptr(), self.Qt[1].data_ptr(),
+                                         self.Qt[2].data_ptr() if parts == 3 else None, self.off[r].data_ptr(),
+                                         self.dmax[r].data_ptr(), self.isweeps.data_ptr(), P, 2 * b,
+                                         inner_sweeps, inner_tol, self.live.data_ptr(), st), "jb_block_eig_f64")
+            # X_k <- vv^T X_k (rows of W^T), same for V, each rotated row
+            # written (as BF16 parts) straight into its next-round slot.
+            nxt = 1 - cur
+            gemm_parts_rows(self.Qt[:parts], Wp, self.W[nxt][:parts], self.maps[r], b_mn=True)
+            gemm_parts_rows(self.Qt[:parts], Vp, self.V[nxt][:parts], self.maps[r], b_mn=True)
+            cur = nxt
+        return cur
+
+    def _run_sweep(self, cur, parts, inner_sweeps, inner_tol, use_graphs):
+        """One sweep, replayed from a CUDA graph after its first (eager) run:
+        the ~4 (nb - 1) launches of a sweep then cost one host call.  The
+        graphs hold only this plan's buffers; the live floor is read on the
+        device (self.live)."""
+        key = (cur, parts, inner_sweeps, inner_tol)
+        if not use_graphs or key not in self._seen:
+            self._seen.add(key)
+            return self._sweep(cur, parts, inner_sweeps, inner_tol)
+        g = self._graphs.get(key)
+        if g is None:
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._sweep(cur, parts, inner_sweeps, inner_tol)
+            self._graphs[key] = g
+        g.replay()
+        return 1 - cur
+
     def solve(self, a: torch.Tensor, *, tol_phase1=5e-6, switch=5e-2, max_sweeps=30, max_two_part=12,
-              inner_sweeps=2, inner_tol=1e-7, polar_steps=2, require_convergence=True):
+              inner_sweeps=1, inner_tol=1e-7, polar_steps=2, require_convergence=True, use_graphs=True):
         """SVD of a (m x n float32, CUDA).  Returns U (m x n), S (n), Vh (n x n),
         info dict.
 
@@ -194,23 +238,9 @@ class BlockJacobi:
         dmax = float((at * at).sum(1).max())
         best, stall, converged, stage_sweeps = float("inf"), 0, False, 0
         for sweeps in range(1, max_sweeps + 1):
-            live_floor = (live_rel if parts == 3 else 1e-4) * dmax
+            self.live.fill_((live_rel if parts == 3 else 1e-4) * dmax)
             stage_sweeps += 1
-            for r in range(R):
-                Wp = [x.view(P, 2 * b, self.mpad) for x in self.W[cur][:parts]]
-                Vp = [x.view(P, 2 * b, self.npad) for x in self.V[cur][:parts]]
-                # Grams of every slot: G_k = X_k X_k^T with X_k = 2b rows of W^T.
-                gemm_parts(Wp, None, self.G, syrk=True, chain128=True)
-                N.check(lib.jb_block_eig_f64(self.G.data_ptr(), self.Qt[0].data_ptr(), self.Qt[1].data_ptr(),
-                                             self.Qt[2].data_ptr() if parts == 3 else None, self.off[r].data_ptr(),
-                                             self.dmax[r].data_ptr(), self.isweeps.data_ptr(), P, 2 * b,
-                                             inner_sweeps, inner_tol, live_floor, st), "jb_block_eig_f64")
-                # X_k <- vv^T X_k (rows of W^T), same for V, each rotated row
-                # written (as BF16 parts) straight into its next-round slot.
-                nxt = 1 - cur
-                gemm_parts_rows(self.Qt[:parts], Wp, self.W[nxt][:parts], self.maps[r], b_mn=True)
-                gemm_parts_rows(self.Qt[:parts], Vp, self.V[nxt][:parts], self.maps[r], b_mn=True)
-                cur = nxt
+            cur = self._run_sweep(cur, parts, inner_sweeps, inner_tol, use_graphs)
             off = float(self.off.max())
             dmax = max(dmax, float(self.dmax.max()))
             off_hist.append((off, parts))

@@ -40,10 +40,26 @@ constexpr int kEigThreads = 512;
 __host__ __device__ inline size_t eig_smem_bytes(int n) {
     return (size_t)n * n * 8            // G, FP64
            + (size_t)n * n * 4          // Q, FP32
-           + (size_t)n * 8 + 32 * 8     // c/s of a round, warp partials
+           + (size_t)2 * n * 8          // c/s of two rounds
            + (size_t)n * 4              // permutation
-           + (size_t)(n - 1) * n + n    // round-robin table, pairs of a round
+           + (size_t)(n - 1) * n        // round-robin table
+           + (size_t)2 * n              // pairs of two rounds
            + 16;
+}
+
+// Q columns u, v <- [u, v] J for the column pairs b = b0, b0 + bstep, ...
+__device__ __forceinline__ void rotate_q(float *Q, const unsigned char *pq, const double *cs, int n, int half, int b0,
+                                         int bstep, int lane) {
+    for (int b = b0; b < half; b += bstep) {
+        const int u = pq[b], v = pq[half + b];
+        const float fc = (float)cs[b], fs = (float)cs[half + b];
+        float *qu = Q + u * n, *qv = Q + v * n;
+        for (int i = lane; i < n; i += 32) {
+            const float xu = qu[i], xv = qv[i];
+            qu[i] = fc * xu - fs * xv;
+            qv[i] = fs * xu + fc * xv;
+        }
+    }
 }
 
 // One CTA per slot.  G (n x n, FP64, symmetric, column-major) is rotated as
@@ -55,24 +71,29 @@ __host__ __device__ inline size_t eig_smem_bytes(int n) {
 // pairs of live columns (g_pp and g_qq above live_floor) in the first sweep;
 // dmax is the slot's largest g_pp.
 //
-// Per round: the pair parameters (half the threads of one or two warps), one
-// barrier, then the G blocks and the Q columns of all pairs, one barrier.
-// The player table of every round is built once; G items are laid out with
-// the row pair fastest so that a warp reads one column at 32 distinct rows.
+// Per round r: warp 0 computes the rotations of round r while the other
+// warps apply round r - 1's rotations to Q (c/s and pairs double-buffered);
+// one barrier; all warps rotate G with round r; one barrier.  The angle
+// t = tan(theta) is formed in FP32 from exponent-scaled FP64 inputs (an
+// angle error of ~1e-7 leaves |g_pq| 1e-7 of itself, which the next sweep
+// removes); c = 1 / sqrt(1 + t^2) and s = t c are FP64, so every applied J
+// is orthogonal to FP64 accuracy.
 __global__ void __launch_bounds__(kEigThreads) eig_kernel(const float *Gin, __nv_bfloat16 *Qt_hi,
                                                           __nv_bfloat16 *Qt_lo, __nv_bfloat16 *Qt_lo2,
                                                           float *off_out, float *dmax_out, int *sweeps_out, int n,
-                                                          int max_sweeps, double tol, double live_floor) {
+                                                          int max_sweeps, double tol, const double *live_floor_ptr) {
     extern __shared__ __align__(16) unsigned char smem[];
     double *G = (double *)smem;                         // n x n, G[col * n + row]
     float *Q = (float *)(G + (size_t)n * n);             // n x n, Q[col * n + row]
-    double *cs = (double *)(Q + (size_t)n * n);          // c[half], s[half] (n even: 8-byte aligned)
-    double *red = cs + n;                                // 32 warp partials
-    int *perm = (int *)(red + 32);                       // n
+    double *csb = (double *)(Q + (size_t)n * n);         // [2][c[half], s[half]] (n even: 8-byte aligned)
+    int *perm = (int *)(csb + 2 * n);                    // n
     unsigned char *sched = (unsigned char *)(perm + n);  // (n - 1) x n players
-    unsigned char *pq = sched + (size_t)(n - 1) * n;     // p[half], q[half] of the round
+    unsigned char *pqb = sched + (size_t)(n - 1) * n;    // [2][p[half], q[half]]
     __shared__ int s_any;
+    __shared__ double s_red[32];
+    __shared__ double s_first_off;
     const int k = blockIdx.x;
+    const double live_floor = live_floor_ptr ? *live_floor_ptr : 0.0;
     const int half = n / 2;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
     const float *g_in = Gin + (size_t)k * n * n;
@@ -86,51 +107,62 @@ __global__ void __launch_bounds__(kEigThreads) eig_kernel(const float *Gin, __nv
         const int r = i / n, pos = i - r * n;
         sched[i] = (unsigned char)circ(pos, r, n);
     }
+    if (threadIdx.x == 0) s_first_off = 0.0;
     __syncthreads();
     double dmax = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) dmax = fmax(dmax, G[(size_t)i * n + i]);
     for (int o = 16; o; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dmax;
+    if (lane == 0) s_red[warp] = dmax;
     __syncthreads();
     double gmax = 0.0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) gmax = fmax(gmax, red[w]);
+    for (int w = 0; w < nwarps; ++w) gmax = fmax(gmax, s_red[w]);
     const double floor_ = 2.220446049250313e-16 * 2.220446049250313e-16 * gmax;
     const double tol2 = tol * tol;
-    double first_off = 0.0;
     int sweep = 0;
     for (sweep = 1; sweep <= max_sweeps; ++sweep) {
-        __syncthreads();                                 // red / s_any readers of the last sweep are done
+        __syncthreads();                                 // s_any readers of the last sweep are done
         if (threadIdx.x == 0) s_any = 0;
-        double off2 = 0.0;
+        // largest ratio^2 of the sweep as num / den (one division at the end)
+        double offn = 0.0, offd = 1.0;
         for (int r = 0; r < n - 1; ++r) {
-            __syncthreads();                             // G, Q of the previous round complete
-            if (threadIdx.x < half) {
-                const int t = threadIdx.x;
-                int p = sched[r * n + t], q = sched[r * n + n - 1 - t];
-                if (p > q) { const int x = p; p = q; q = x; }
-                const double app = G[(size_t)p * n + p], aqq = G[(size_t)q * n + q], apq = G[(size_t)q * n + p];
-                double c = 1.0, s = 0.0;
-                const double prod = app * aqq, apq2 = apq * apq;
-                if (apq2 > tol2 * prod && fmin(app, aqq) > floor_) {
-                    // off over live columns only (norm^2 above live_floor),
-                    // like the reference's convergence check (solvers.py:55-57)
-                    if (fmin(app, aqq) > live_floor) off2 = fmax(off2, apq2 / prod);
-                    const double d = aqq - app;
-                    const double tt = copysign(2.0 * fabs(apq), d) / (fabs(d) + sqrt(d * d + 4.0 * apq2));
-                    c = rsqrt(1.0 + tt * tt);
-                    s = tt * c;
-                    if (apq < 0.0) s = -s;
-                    s_any = 1;
+            const int buf = r & 1;
+            double *cs = csb + buf * n;
+            unsigned char *pq = pqb + buf * n;
+            __syncthreads();                             // G of round r - 1 complete
+            if (warp == 0) {
+                for (int t = lane; t < half; t += 32) {
+                    int p = sched[r * n + t], q = sched[r * n + n - 1 - t];
+                    if (p > q) { const int x = p; p = q; q = x; }
+                    const double app = G[p * n + p], aqq = G[q * n + q], apq = G[q * n + p];
+                    double c = 1.0, sn = 0.0;
+                    const double prod = app * aqq, apq2 = apq * apq;
+                    if (apq2 > tol2 * prod && fmin(app, aqq) > floor_) {
+                        // off over live columns only (norm^2 above live_floor),
+                        // like the reference's convergence check (solvers.py:55-57)
+                        if (fmin(app, aqq) > live_floor && apq2 * offd > offn * prod) { offn = apq2; offd = prod; }
+                        const double d = aqq - app, a2 = 2.0 * fabs(apq);
+                        // exact power-of-two scaling of (d, 2|apq|) into [1, 2) for the FP32 angle
+                        const int ex = (__double2hiint(fmax(fabs(d), a2)) >> 20) & 0x7ff;
+                        const double sc = __hiloint2double((2046 - ex) << 20, 0);
+                        const float df = fabsf((float)(d * sc)), af = (float)(a2 * sc);
+                        const float tf = __fdividef(af, df + sqrtf(df * df + af * af));
+                        const double tt = d < 0.0 ? -(double)tf : (double)tf;
+                        c = rsqrt(1.0 + tt * tt);
+                        sn = tt * c;
+                        if (apq < 0.0) sn = -sn;
+                        s_any = 1;
+                    }
+                    cs[t] = c;
+                    cs[half + t] = sn;
+                    pq[t] = (unsigned char)p;
+                    pq[half + t] = (unsigned char)q;
                 }
-                cs[t] = c;
-                cs[half + t] = s;
-                pq[t] = (unsigned char)p;
-                pq[half + t] = (unsigned char)q;
+            } else if (r > 0) {
+                rotate_q(Q, pqb + (buf ^ 1) * n, csb + (buf ^ 1) * n, n, half, warp - 1, nwarps - 1, lane);
             }
             __syncthreads();
             // G <- J^T G J: warp w takes column pairs b = w, w + nwarps, ...,
-            // its lanes the row pairs a (one 2 x 2 block per (a, b)); then the
-            // same column pairs of Q, lanes over rows.
+            // its lanes the row pairs a (one 2 x 2 block per (a, b)).
             for (int b = warp; b < half; b += nwarps) {
                 const int u = pq[b], v = pq[half + b];
                 const double cb = cs[b], sb = cs[half + b];
@@ -148,22 +180,18 @@ __global__ void __launch_bounds__(kEigThreads) eig_kernel(const float *Gin, __nv
                     cu[q] = cb * rqu - sb * rqv;
                     cv[q] = sb * rqu + cb * rqv;
                 }
-                const float fc = (float)cb, fs = (float)sb;
-                float *qu = Q + u * n, *qv = Q + v * n;
-                for (int i = lane; i < n; i += 32) {
-                    const float xu = qu[i], xv = qv[i];
-                    qu[i] = fc * xu - fs * xv;
-                    qv[i] = fs * xu + fc * xv;
-                }
             }
         }
+        // the last round's Q rotation, all warps
+        rotate_q(Q, pqb + ((n - 2) & 1) * n, csb + ((n - 2) & 1) * n, n, half, warp, nwarps, lane);
+        if (sweep == 1 && warp == 0) {
+            for (int o = 16; o; o >>= 1) {
+                const double on = __shfl_xor_sync(0xffffffffu, offn, o), od = __shfl_xor_sync(0xffffffffu, offd, o);
+                if (on * offd > offn * od) { offn = on; offd = od; }
+            }
+            if (lane == 0) s_first_off = sqrt(offn / offd);
+        }
         __syncthreads();
-        for (int o = 16; o; o >>= 1) off2 = fmax(off2, __shfl_xor_sync(0xffffffffu, off2, o));
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = off2;
-        __syncthreads();
-        double om = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) om = fmax(om, red[w]);
-        if (sweep == 1) first_off = sqrt(om);
         if (!s_any) break;
     }
     __syncthreads();
@@ -190,10 +218,278 @@ __global__ void __launch_bounds__(kEigThreads) eig_kernel(const float *Gin, __nv
         if (Qt_lo2) Qt_lo2[(size_t)k * n * n + t] = __float2bfloat16_rn(rem - __bfloat162float(l));
     }
     if (threadIdx.x == 0) {
-        if (off_out) off_out[k] = (float)first_off;
+        if (off_out) off_out[k] = (float)s_first_off;
         if (dmax_out) dmax_out[k] = (float)gmax;
         if (sweeps_out) sweeps_out[k] = sweep > max_sweeps ? max_sweeps : sweep;
     }
+}
+
+// Register-resident variant of eig_kernel for n = 32 * RPT (64 or 128), the
+// slot widths of b = 32 and b = 64.  Same rotations and outputs; the pairs of
+// a sweep follow the odd-even ordering instead of the round robin: round r
+// pairs adjacent positions (2t + r % 2, 2t + r % 2 + 1) and every rotation
+// also swaps its two positions (J P), so after n rounds each pair of columns
+// has met exactly once (the swaps reverse the order).  With positions fixed,
+// G and Q stay in registers: lane l holds rows RPT l .. RPT l + RPT - 1 and
+// warp w columns 8 w .. 8 w + 7.  Row pairs that straddle two lanes use warp
+// shuffles, column pairs that straddle two warps (odd rounds) one exchange
+// through shared memory.  Per round: warp 0 forms the angles from the
+// diagonal d and superdiagonal e (published in shared memory by their
+// owners), one barrier, rotations, (odd rounds: boundary exchange, one
+// barrier), new d / e, one barrier.
+template <int RPT>
+__global__ void __launch_bounds__(RPT * 128) eig_reg_kernel(const float *Gin, __nv_bfloat16 *Qt_hi,
+                                                            __nv_bfloat16 *Qt_lo, __nv_bfloat16 *Qt_lo2,
+                                                            float *off_out, float *dmax_out, int *sweeps_out,
+                                                            int max_sweeps, double tol, const double *live_floor_ptr) {
+    constexpr int n = 32 * RPT;
+    constexpr int CB = 8;                      // columns per warp
+    constexpr int NW = n / CB;                 // warps
+    extern __shared__ __align__(16) unsigned char smem[];
+    double *sd = (double *)smem;               // d[x] = G[x][x]
+    double *se = sd + n;                       // e[x] = G[x][x + 1]
+    double *sc = se + n;                       // c of the pair starting at position p
+    double *ss = sc + n;                       // s of the pair starting at position p
+    double *bg = ss + n;                       // [NW][2][n] boundary columns of G (first, last)
+    float *bq = (float *)(bg + (size_t)NW * 2 * n);  // [NW][2][n] boundary columns of Q
+    float *Qs = bq + (size_t)NW * 2 * n;       // n x n, Q[col * n + row] (write-out)
+    int *perm = (int *)(Qs + (size_t)n * n);   // n
+    __shared__ int s_any;
+    __shared__ double s_first_off;
+    __shared__ double s_red[NW];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int r0 = lane * RPT, c0 = warp * CB;
+    const int k = blockIdx.x;
+    const double live_floor = live_floor_ptr ? *live_floor_ptr : 0.0;
+    const float *g_in = Gin + (size_t)k * n * n;
+
+    double g[RPT][CB];
+    float q[RPT][CB];
+#pragma unroll
+    for (int i = 0; i < RPT; ++i)
+#pragma unroll
+        for (int j = 0; j < CB; ++j) {
+            const int r = r0 + i, c = c0 + j;
+            // symmetrise (the tensor-core Gram is symmetric up to rounding)
+            g[i][j] = 0.5 * ((double)g_in[(size_t)r * n + c] + (double)g_in[(size_t)c * n + r]);
+            q[i][j] = (r == c) ? 1.f : 0.f;
+        }
+    auto publish_de = [&]() {
+#pragma unroll
+        for (int i = 0; i < RPT; ++i) {
+            const int x = r0 + i;
+#pragma unroll
+            for (int j = 0; j < CB; ++j) {
+                if (c0 + j == x) sd[x] = g[i][j];
+                if (c0 + j == x + 1) se[x] = g[i][j];
+            }
+        }
+    };
+    publish_de();
+    if (threadIdx.x == 0) s_first_off = 0.0;
+    __syncthreads();
+    double dm = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dm = fmax(dm, sd[i]);
+    for (int o = 16; o; o >>= 1) dm = fmax(dm, __shfl_xor_sync(0xffffffffu, dm, o));
+    if (lane == 0) s_red[warp] = dm;
+    __syncthreads();
+    double gmax = 0.0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) gmax = fmax(gmax, s_red[w]);
+    const double floor_ = 2.220446049250313e-16 * 2.220446049250313e-16 * gmax;
+    const double tol2 = tol * tol;
+    int sweep = 0;
+    for (sweep = 1; sweep <= max_sweeps; ++sweep) {
+        if (threadIdx.x == 0) s_any = 0;
+        double offn = 0.0, offd = 1.0;
+        for (int r = 0; r < n; ++r) {
+            const int par = r & 1;
+            __syncthreads();                   // d / e of the previous round published; s_any reset
+            if (warp < RPT / 2) {                 // one pair per lane
+                {
+                    const int t = warp * 32 + lane;
+                    if (t >= n / 2 - par) goto angles_done;
+                    const int p = 2 * t + par;
+                    const double app = sd[p], aqq = sd[p + 1], apq = se[p];
+                    double c = 1.0, sn = 0.0;
+                    const double prod = app * aqq, apq2 = apq * apq;
+                    if (apq2 > tol2 * prod && fmin(app, aqq) > floor_) {
+                        // off over live columns only (solvers.py:55-57)
+                        if (fmin(app, aqq) > live_floor && apq2 * offd > offn * prod) { offn = apq2; offd = prod; }
+                        const double d = aqq - app, a2 = 2.0 * fabs(apq);
+                        const int ex = (__double2hiint(fmax(fabs(d), a2)) >> 20) & 0x7ff;
+                        const double scl = __hiloint2double((2046 - ex) << 20, 0);
+                        const float df = fabsf((float)(d * scl)), af = (float)(a2 * scl);
+                        const float tf = __fdividef(af, df + sqrtf(df * df + af * af));
+                        const double tt = d < 0.0 ? -(double)tf : (double)tf;
+                        // c = 1 / sqrt(1 + t^2): FP32 estimate and one Newton step in FP64
+                        const double x = 1.0 + tt * tt;
+                        const double c0 = (double)rsqrtf(1.f + tf * tf);
+                        c = c0 * (1.5 - 0.5 * x * c0 * c0);
+                        sn = tt * c;
+                        if (apq < 0.0) sn = -sn;
+                        s_any = 1;
+                    }
+                    sc[p] = c;
+                    ss[p] = sn;
+                }
+            angles_done:;
+            }
+            __syncthreads();
+            // Rows (J^T from the left, then the swap): (x_p, x_q) <- (s x_p + c x_q, c x_p - s x_q).
+            if (par == 0) {
+#pragma unroll
+                for (int i = 0; i < RPT; i += 2) {
+                    const double c = sc[r0 + i], sn = ss[r0 + i];
+#pragma unroll
+                    for (int j = 0; j < CB; ++j) {
+                        const double x = g[i][j], y = g[i + 1][j];
+                        g[i][j] = sn * x + c * y;
+                        g[i + 1][j] = c * x - sn * y;
+                    }
+                }
+            } else {
+                const bool has_up = lane > 0, has_down = lane < 31;
+                const double cu = has_up ? sc[r0 - 1] : 1.0, su = has_up ? ss[r0 - 1] : 0.0;
+                const double cd = has_down ? sc[r0 + RPT - 1] : 1.0, sdn = has_down ? ss[r0 + RPT - 1] : 0.0;
+#pragma unroll
+                for (int j = 0; j < CB; ++j) {
+                    const double up = __shfl_up_sync(0xffffffffu, g[RPT - 1][j], 1);   // row r0 - 1
+                    const double dn = __shfl_down_sync(0xffffffffu, g[0][j], 1);       // row r0 + RPT
+                    const double first = g[0][j], last = g[RPT - 1][j];
+                    if (has_up) g[0][j] = cu * up - su * first;                         // second of pair (r0 - 1, r0)
+                    if (has_down) g[RPT - 1][j] = sdn * last + cd * dn;                 // first of pair (r0 + RPT - 1, r0 + RPT)
+                }
+#pragma unroll
+                for (int i = 1; i + 1 < RPT; i += 2) {
+                    const double c = sc[r0 + i], sn = ss[r0 + i];
+#pragma unroll
+                    for (int j = 0; j < CB; ++j) {
+                        const double x = g[i][j], y = g[i + 1][j];
+                        g[i][j] = sn * x + c * y;
+                        g[i + 1][j] = c * x - sn * y;
+                    }
+                }
+            }
+            // Columns (J from the right, then the swap), G and Q alike.
+            if (par == 0) {
+#pragma unroll
+                for (int j = 0; j < CB; j += 2) {
+                    const double c = sc[c0 + j], sn = ss[c0 + j];
+                    const float fc = (float)c, fs = (float)sn;
+#pragma unroll
+                    for (int i = 0; i < RPT; ++i) {
+                        const double x = g[i][j], y = g[i][j + 1];
+                        g[i][j] = sn * x + c * y;
+                        g[i][j + 1] = c * x - sn * y;
+                        const float u = q[i][j], v = q[i][j + 1];
+                        q[i][j] = fs * u + fc * v;
+                        q[i][j + 1] = fc * u - fs * v;
+                    }
+                }
+            } else {
+                // publish this warp's first and last columns (after the row rotation)
+#pragma unroll
+                for (int i = 0; i < RPT; ++i) {
+                    bg[((size_t)warp * 2 + 0) * n + r0 + i] = g[i][0];
+                    bg[((size_t)warp * 2 + 1) * n + r0 + i] = g[i][CB - 1];
+                    bq[((size_t)warp * 2 + 0) * n + r0 + i] = q[i][0];
+                    bq[((size_t)warp * 2 + 1) * n + r0 + i] = q[i][CB - 1];
+                }
+                __syncthreads();
+                const bool has_left = warp > 0, has_right = warp < NW - 1;
+                const double cl = has_left ? sc[c0 - 1] : 1.0, sl = has_left ? ss[c0 - 1] : 0.0;
+                const double cr = has_right ? sc[c0 + CB - 1] : 1.0, sr = has_right ? ss[c0 + CB - 1] : 0.0;
+#pragma unroll
+                for (int i = 0; i < RPT; ++i) {
+                    const int row = r0 + i;
+                    if (has_left) {                // pair (c0 - 1, c0): this warp holds the second
+                        const double x = bg[((size_t)(warp - 1) * 2 + 1) * n + row];
+                        const float u = bq[((size_t)(warp - 1) * 2 + 1) * n + row];
+                        g[i][0] = cl * x - sl * g[i][0];
+                        q[i][0] = (float)cl * u - (float)sl * q[i][0];
+                    }
+                    if (has_right) {               // pair (c0 + CB - 1, c0 + CB): this warp holds the first
+                        const double y = bg[((size_t)(warp + 1) * 2 + 0) * n + row];
+                        const float v = bq[((size_t)(warp + 1) * 2 + 0) * n + row];
+                        g[i][CB - 1] = sr * g[i][CB - 1] + cr * y;
+                        q[i][CB - 1] = (float)sr * q[i][CB - 1] + (float)cr * v;
+                    }
+                }
+#pragma unroll
+                for (int j = 1; j + 1 < CB; j += 2) {
+                    const double c = sc[c0 + j], sn = ss[c0 + j];
+                    const float fc = (float)c, fs = (float)sn;
+#pragma unroll
+                    for (int i = 0; i < RPT; ++i) {
+                        const double x = g[i][j], y = g[i][j + 1];
+                        g[i][j] = sn * x + c * y;
+                        g[i][j + 1] = c * x - sn * y;
+                        const float u = q[i][j], v = q[i][j + 1];
+                        q[i][j] = fs * u + fc * v;
+                        q[i][j + 1] = fc * u - fs * v;
+                    }
+                }
+            }
+            publish_de();
+        }
+        if (sweep == 1 && warp < RPT / 2) {
+            for (int o = 16; o; o >>= 1) {
+                const double on = __shfl_xor_sync(0xffffffffu, offn, o), od = __shfl_xor_sync(0xffffffffu, offd, o);
+                if (on * offd > offn * od) { offn = on; offd = od; }
+            }
+            if (lane == 0) s_red[warp] = sqrt(offn / offd);
+        }
+        __syncthreads();
+        if (sweep == 1 && threadIdx.x == 0) {
+            double o = 0.0;
+#pragma unroll
+            for (int w = 0; w < RPT / 2; ++w) o = fmax(o, s_red[w]);
+            s_first_off = o;
+        }
+        const int any = s_any;
+        __syncthreads();                       // everyone has read s_any before it is reset
+        if (!any) break;
+    }
+    // Q to shared memory (column-major) for the sorted write-out.
+#pragma unroll
+    for (int i = 0; i < RPT; ++i)
+#pragma unroll
+        for (int j = 0; j < CB; ++j) Qs[(size_t)(c0 + j) * n + r0 + i] = q[i][j];
+    __syncthreads();
+    // Eigenvalues descending (stable), Q^T rows in that order.
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        const double dj = sd[j];
+        int rk = 0;
+        for (int i = 0; i < n; ++i) {
+            const double di = sd[i];
+            rk += (di > dj) || (di == dj && i < j);
+        }
+        perm[rk] = j;
+    }
+    __syncthreads();
+    __nv_bfloat16 *qh = Qt_hi + (size_t)k * n * n, *ql = Qt_lo + (size_t)k * n * n;
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+        const int rrow = t / n, i = t - rrow * n;       // Q^T row rrow = column perm[rrow] of Q
+        const float x = Qs[(size_t)perm[rrow] * n + i];
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        qh[t] = h;
+        const float rem = x - __bfloat162float(h);
+        const __nv_bfloat16 l = __float2bfloat16_rn(rem);
+        ql[t] = l;
+        if (Qt_lo2) Qt_lo2[(size_t)k * n * n + t] = __float2bfloat16_rn(rem - __bfloat162float(l));
+    }
+    if (threadIdx.x == 0) {
+        if (off_out) off_out[k] = (float)s_first_off;
+        if (dmax_out) dmax_out[k] = (float)gmax;
+        if (sweeps_out) sweeps_out[k] = sweep > max_sweeps ? max_sweeps : sweep;
+    }
+}
+
+__host__ inline size_t eig_reg_smem_bytes(int n) {
+    const int nw = n / 8;
+    return (size_t)4 * n * 8 + (size_t)nw * 2 * n * 8 + (size_t)nw * 2 * n * 4 + (size_t)n * n * 4 + (size_t)n * 4 +
+           16;
 }
 
 // dst row map[r] <- src row r (length L), split into hi / lo BF16.
@@ -338,9 +634,28 @@ using namespace jb::blk;
 extern "C" {
 
 int jb_block_eig_f64(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
-                     int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps, double tol, double live_floor,
+                     int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps, double tol, const double *live_floor,
                      void *stream) {
     if (!G || !Qt_hi || !Qt_lo || pairs < 1 || n < 2 || (n & 1) || max_sweeps < 1) return JB_EINVAL;
+    if (n == 64 || n == 128) {
+        const size_t smem = eig_reg_smem_bytes(n);
+        if (n == 64) {
+            if (cudaFuncSetAttribute(eig_reg_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+                cudaSuccess)
+                return JB_ECUDA;
+            eig_reg_kernel<2><<<(unsigned)pairs, 256, smem, (cudaStream_t)stream>>>(
+                G, (__nv_bfloat16 *)Qt_hi, (__nv_bfloat16 *)Qt_lo, (__nv_bfloat16 *)Qt_lo2, off, dmax, sweeps,
+                max_sweeps, tol, live_floor);
+        } else {
+            if (cudaFuncSetAttribute(eig_reg_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+                cudaSuccess)
+                return JB_ECUDA;
+            eig_reg_kernel<4><<<(unsigned)pairs, 512, smem, (cudaStream_t)stream>>>(
+                G, (__nv_bfloat16 *)Qt_hi, (__nv_bfloat16 *)Qt_lo, (__nv_bfloat16 *)Qt_lo2, off, dmax, sweeps,
+                max_sweeps, tol, live_floor);
+        }
+        return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+    }
     if (n > 256) return JB_ETOOBIG;                  // players are stored as bytes
     const size_t smem = eig_smem_bytes(n);
     if (smem > 227 * 1024) return JB_ETOOBIG;

@@ -85,7 +85,7 @@ def _declare(l):
                        ("jb_mse_grad", [P, P, P, P, I64, FL, P]),
                        ("jb_adam", [P, P, P, P, P, P, I64, I64, FL, FL, FL, FL, I32, P]),
                        ("jb_gram_sketch", [P, P, I64, I32, I32, P]),
-                       ("jb_block_eig_f64", [P, P, P, P, P, P, P, I64, I32, I32, F64, F64, P]),
+                       ("jb_block_eig_f64", [P, P, P, P, P, P, P, I64, I32, I32, F64, P, P]),
                        ("jb_rows_scatter", [P, P, P, P, P, P, I64, I64, P]),
                        ("jb_rows_combine", [P, P, P, P, P, I64, I64, P]),
                        ("jb_gemm_f64acc", [P, P, P, I64, I64, I64, I64, I64, I64, P]),

@@ -34,7 +34,7 @@ REFERENCE_ALGORITHMS = (
     'gram_jacobi', 'gram_dc', 'polar_qdwh', 'polar_newton_schulz',
     'polar_halley', 'polar_polynomial', 'randomized', 'subspace', 'block_krylov', 'lanczos',
 )  # svdbench/standalone/solvers.py:7-11
-ALGORITHMS = ('jacobi',)
+ALGORITHMS = ('jacobi', 'block_jacobi')
 PRECISIONS = ('mixed', 'fp32')
 ORDERINGS = ('block', 'round_robin')
 
@@ -137,8 +137,12 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
     algorithm='jacobi'; options ``tol``, ``max_sweeps`` (default 60,
     solvers.py:24-27), ``rank``, ``precision`` and ``ordering``; other
     options are accepted and ignored, as the reference's Jacobi ignores them.
+    algorithm='block_jacobi' (solvers.py:30-68) runs the tensor-core blocked
+    solver on each matrix of the batch (see _block_svd).
     Input is never overwritten."""
     rank, precision = _validate(a, algorithm, full_matrices, opts)
+    if algorithm == 'block_jacobi':
+        return _block_svd(a, full_matrices, values_only, return_info, rank, opts)
     max_sweeps = opts.get('max_sweeps', 60)
     tol = opts.get('tol')
     shape = a.shape[:-2]
@@ -173,6 +177,66 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
         result = (None if values_only else u.reshape(*shape, *u.shape[-2:]),
                   s.reshape(*shape, rank),
                   None if values_only else vh.reshape(*shape, *vh.shape[-2:]))
+    return (*result, stats) if return_info else result
+
+
+_block_plans = {}
+
+
+def _block_svd(a, full_matrices, values_only, return_info, rank, opts):
+    """block_jacobi (solvers.py:30-68) on the tensor cores, one matrix at a
+    time (blocked.BlockJacobi).  Like the reference: block_size defaults to 4
+    and must be positive (:32-34); a matrix whose tall view has a single block
+    is solved by the plain Jacobi (:36-37); tol defaults to 40 eps (:41);
+    max_sweeps (default 30) bounds the block sweeps and exhausting it raises
+    RuntimeError('block Jacobi did not converge') (:59-60); wide matrices are
+    solved transposed (:225-227).  The block width only shapes the schedule:
+    widths the tensor-core kernels do not take (not a multiple of 8 in
+    [8, 64]) run with width 32, reported as info['block_size_used'].  float32
+    only (the products are 3xBF16 / 6xBF16); float64 input and
+    full_matrices raise Unsupported."""
+    from .blocked import BlockJacobi
+    width = opts.get('block_size', 4)
+    if width < 1:
+        raise ValueError('block_size must be positive')
+    m, n = a.shape[-2:]
+    if -(-min(m, n) // width) == 1:
+        rest = {k: v for k, v in opts.items() if k != 'block_size'}
+        return svd(a, 'jacobi', full_matrices=full_matrices, values_only=values_only, return_info=return_info,
+                   **rest)
+    if a.dtype != torch.float32:
+        raise Unsupported('block_jacobi runs float32 on the tensor cores; use jacobi for float64')
+    if full_matrices:
+        raise Unsupported('block_jacobi does not complete full bases on the B200 solver; use jacobi')
+    used = width if (width % 8 == 0 and 8 <= width <= 64) else 32
+    tol = opts.get('tol') or 40 * 1.1920928955078125e-07
+    max_sweeps = opts.get('max_sweeps', 30)
+    mt, nt = max(m, n), min(m, n)
+    shape = a.shape[:-2]
+    dev = a.device
+    with torch.no_grad(), torch.cuda.device(dev):
+        x = a.detach().reshape(-1, m, n)
+        key = (mt, nt, used, dev)
+        plan = _block_plans.get(key)
+        if plan is None:
+            plan = _block_plans[key] = BlockJacobi(mt, nt, used, device=dev)
+        us, ss, vs, sweeps = [], [], [], 0
+        for z in range(x.shape[0]):
+            xt = x[z] if m >= n else x[z].t()
+            u, s_, vh, info = plan.solve(xt.contiguous(), tol_phase1=tol, max_sweeps=max_sweeps)
+            if m < n:
+                u, vh = vh.t(), u.t()
+            us.append(u[:, :rank]); ss.append(s_[:rank]); vs.append(vh[:rank])
+            sweeps = max(sweeps, info['block_sweeps'])
+        s = torch.stack(ss).reshape(*shape, rank)
+        u = None if values_only else torch.stack(us).reshape(*shape, m, rank).contiguous()
+        vh = None if values_only else torch.stack(vs).reshape(*shape, rank, n).contiguous()
+        if not all(bool(torch.isfinite(t).all()) for t in (s,) + (() if values_only else (u, vh))):
+            raise RuntimeError('standalone solver produced nonfinite output')
+    stats = {'algorithm': 'block_jacobi', 'vendor_factorizations': 0, 'converged': True, 'block_sweeps': sweeps,
+             'block_size_used': used, 'precision': 'tensor-core 3xBF16/6xBF16 sweeps, FP64 block eigen-solves',
+             'implementation': 'B200 sm_100a blocked one-sided Jacobi (tcgen05 + FP64 eigen-blocks)'}
+    result = (u, s, vh)
     return (*result, stats) if return_info else result
 
 

@@ -49,3 +49,72 @@ def test_blocked_matches_lapack(BJ, m, n, b, cond):
     err1, relbig, rec, ou, ov = check(a, U, S, Vh)
     print(m, n, b, info["block_sweeps"], ["%.1e/%d" % x for x in info["off_per_sweep"]], err1, relbig, rec, ou, ov)
     assert err1 <= 5e-6 and relbig <= 1e-5 and rec <= 2e-5 and ou <= max(2e-5, 2e-7 * cond) and ov <= 2e-5
+
+
+@pytest.mark.parametrize("n", [64, 128, 48])
+def test_block_eig_f64(n):
+    """jb_block_eig_f64 alone: Qt (hi + lo + lo2) orthogonal, Qt G Qt^T
+    diagonal with a descending diagonal, for slot widths served by the
+    register-resident odd-even kernel (64, 128) and by the shared-memory
+    round-robin kernel (48)."""
+    N = importlib.import_module("pavel-s_svd_b200.native")
+    g = torch.Generator(device="cuda").manual_seed(n)
+    P = 5
+    x = torch.randn(P, n, 3 * n, device="cuda", generator=g, dtype=torch.float64)
+    x = x * torch.logspace(0, -3, n, device="cuda", dtype=torch.float64)[:, None]
+    G64 = x @ x.transpose(1, 2)
+    G = G64.float().contiguous()
+    qt = [torch.empty(P, n, n, dtype=torch.bfloat16, device="cuda") for _ in range(3)]
+    off = torch.zeros(P, device="cuda")
+    dmax = torch.zeros(P, device="cuda")
+    sweeps = torch.zeros(P, dtype=torch.int32, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    N.check(N.lib().jb_block_eig_f64(G.data_ptr(), qt[0].data_ptr(), qt[1].data_ptr(), qt[2].data_ptr(),
+                                     off.data_ptr(), dmax.data_ptr(), sweeps.data_ptr(), P, n, 12, 1e-12, None, st),
+            "jb_block_eig_f64")
+    torch.cuda.synchronize()
+    Q = (qt[0].double() + qt[1].double() + qt[2].double())
+    eye = torch.eye(n, device="cuda", dtype=torch.float64)
+    # Q accumulates its rotations in FP32: ~eps32 * sqrt(rotations per column)
+    assert float((Q @ Q.transpose(1, 2) - eye).abs().max()) <= 1e-5
+    D = Q @ G.double() @ Q.transpose(1, 2)
+    diag = D.diagonal(dim1=1, dim2=2)
+    offd = (D - torch.diag_embed(diag)).abs() / (diag.abs().sqrt()[:, :, None] * diag.abs().sqrt()[:, None, :])
+    assert float(offd.max()) <= 1e-5
+    assert bool((diag[:, :-1] >= diag[:, 1:] * (1 - 1e-6)).all())
+    ref = torch.linalg.eigvalsh(G.double()).flip(-1)
+    # eigenvalues to ~2x the FP32 non-orthogonality of Q, relative to the largest
+    assert float(((diag - ref).abs() / ref.abs().max(dim=1, keepdim=True).values).max()) <= 1e-5
+    assert float(dmax.max()) > 0 and int(sweeps.min()) >= 2
+    assert 0.0 < float(off.min())
+
+
+def test_block_jacobi_drop_in():
+    """svd(a, 'block_jacobi', ...) through the drop-in API: tall and wide
+    inputs, the reference's defaults (block_size 4 -> width 32 here), the
+    one-block case routed to the plain Jacobi, values_only and rank."""
+    pkg = importlib.import_module("pavel-s_svd_b200")
+    rng = np.random.default_rng(11)
+    for m, n, bs in ((512, 256, 32), (256, 384, 4)):
+        a = rng.standard_normal((m, n)).astype(np.float32)
+        x = torch.from_numpy(a).cuda()
+        u, s, vh, info = pkg.svd(x, 'block_jacobi', block_size=bs, return_info=True)
+        assert info['block_size_used'] == 32 and info['block_sweeps'] >= 2
+        assert torch.equal(x, torch.from_numpy(a).cuda())          # input untouched
+        sr = np.linalg.svd(a.astype(np.float64), compute_uv=False)
+        k = min(m, n)
+        assert u.shape == (m, k) and s.shape == (k,) and vh.shape == (k, n)
+        assert float(np.abs(s.cpu().numpy() - sr).max() / sr[0]) <= 5e-6
+        rec = (u.double() * s.double()) @ vh.double()
+        assert float((rec - x.double()).norm() / x.double().norm()) <= 2e-5
+    u, s, vh = pkg.svd(x, 'block_jacobi', block_size=32, values_only=True)
+    assert u is None and vh is None and s.shape == (256,)
+    u, s, vh = pkg.svd(x, 'block_jacobi', block_size=32, rank=10)
+    assert u.shape == (256, 10) and vh.shape == (10, 384)
+    small = torch.randn(3, 40, 24, device="cuda")
+    u, s, vh, info = pkg.svd(small, 'block_jacobi', block_size=32, return_info=True)
+    assert info['algorithm'] == 'jacobi' and s.shape == (3, 24)
+    with pytest.raises(ValueError):
+        pkg.svd(x, 'block_jacobi', block_size=0)
+    with pytest.raises(pkg.Unsupported):
+        pkg.svd(x.double(), 'block_jacobi', block_size=32)
