@@ -237,6 +237,11 @@ __global__ void __launch_bounds__(1024, 1) batched_kernel(Params p) {
 // Register-tile path (matrices up to 128 x 64 in their tall view).
 // ---------------------------------------------------------------------------
 constexpr int kB32 = 4;   // block width of the FP32 sweeps (8 warps for 64 columns)
+// Mixed precision: the FP32 phase ends after the first sweep whose largest
+// pair ratio is <= this (its rotations leave ~1e-6, the FP32 floor); the FP64
+// phase then converges to the requested tolerance in one rotating sweep and
+// one confirming sweep.
+constexpr float kMixedExitRatio = 1e-3f;
 constexpr int kB64 = 2;   // block width of the FP64 sweeps (16 warps for 64 columns)
 constexpr int kT32 = 256, kT64 = 512;  // threads of the two kernels
 constexpr int kMaxR = 4;  // rows per lane: mt <= 128
@@ -326,8 +331,9 @@ __device__ void load_stage(const TI *A, const Geo &g, int ld, float *As) {
 
 template <typename T, int B>
 __device__ int rb_dispatch(const RGeo &r, T *W, T *V, T tol, int max_sweeps, bool confirm, double *red,
-                           bool &conv) {
-    return rb_sweeps<T, B, kMaxR, kMaxRV>(W, r.ldw, V, r.ldv, r.nb, r.live, tol, max_sweeps, confirm, red, conv);
+                           bool &conv, T exit_ratio = T(0)) {
+    return rb_sweeps<T, B, kMaxR, kMaxRV>(W, r.ldw, V, r.ldv, r.nb, r.live, tol, max_sweeps, confirm, red, conv,
+                                          exit_ratio);
 }
 
 __device__ inline Geo reg_geo(const jb_matrix_desc &d, const RGeo &r) {
@@ -465,7 +471,8 @@ __global__ void __launch_bounds__(kT32) rb32_kernel(Params p) {
                 const float tol = MIXED ? (p.tol32 > 0 ? (float)p.tol32 : 10.0f * Lim<float>::eps())
                                         : (p.tol > 0 ? (float)p.tol : 10.0f * Lim<float>::eps());
                 bool conv;
-                ns = rb_dispatch<float, kB32>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true, ax.red, conv);
+                ns = rb_dispatch<float, kB32>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true, ax.red, conv,
+                                              MIXED ? kMixedExitRatio : 0.0f);
                 if (MIXED) {
                     float *x = p.x32 + d.x_off;
                     const int nt = g.nt;

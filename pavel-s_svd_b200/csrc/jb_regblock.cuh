@@ -71,12 +71,13 @@ __device__ __forceinline__ void reduce_scatter(T (&x)[NV], int lane) {
 // on squares.  Inputs are scaled (max |a| < 1), so d^2 + 4 apq^2 cannot
 // overflow, and active pairs keep apq^2 far above the underflow range.
 // Returns bit 0: active; bit 1: ratio > sqrt(tol) / 2 (the confirmation
-// heuristic of rb_sweeps).  Inactive pairs get c = 1, s = 0.
+// heuristic of rb_sweeps); bit 2: ratio > the phase exit ratio (ex2 its
+// square).  Inactive pairs get c = 1, s = 0.
 __device__ __forceinline__ float rcp_sqrt(float x) { return 1.0f / sqrtf(x); }
 __device__ __forceinline__ double rcp_sqrt(double x) { return rsqrt(x); }
 
 template <typename T>
-__device__ __forceinline__ int rot_params(T app, T aqq, T apq, T tol2, T big2, T floor_, T &c, T &s) {
+__device__ __forceinline__ int rot_params(T app, T aqq, T apq, T tol2, T big2, T ex2, T floor_, T &c, T &s) {
     c = T(1);
     s = T(0);
     const T apq2 = apq * apq;
@@ -88,7 +89,7 @@ __device__ __forceinline__ int rot_params(T app, T aqq, T apq, T tol2, T big2, T
     c = rcp_sqrt(dfma(t, t, T(1)));
     s = t * c;
     if (apq < T(0)) s = -s;
-    return 1 | (apq2 > big2 * prod ? 2 : 0);
+    return 1 | (apq2 > big2 * prod ? 2 : 0) | (apq2 > ex2 * prod ? 4 : 0);
 }
 
 // Register column of the first / second member of pair i in a step.
@@ -105,8 +106,8 @@ __device__ __forceinline__ constexpr int pair_q(int i) {
 
 // One step: B disjoint pairs; ORs the pairs' rot_params flags into fl.
 template <bool INTRA, typename T, int B, int R, int RV>
-__device__ __forceinline__ void step(Tile<T, B, R, RV> &t, T tol2, T big2, T floor_, int &fl, bool rotate, int lane,
-                                     int nr, int nv) {
+__device__ __forceinline__ void step(Tile<T, B, R, RV> &t, T tol2, T big2, T ex2, T floor_, int &fl, bool rotate,
+                                     int lane, int nr, int nv) {
     constexpr int LB = Log2<B>::value;
     T pa[B], pb[B], pc[B];
 #pragma unroll
@@ -128,7 +129,7 @@ __device__ __forceinline__ void step(Tile<T, B, R, RV> &t, T tol2, T big2, T flo
     reduce_scatter<T, B>(pb, lane);
     reduce_scatter<T, B>(pc, lane);
     T c, s;
-    const int f = rot_params(pa[0], pb[0], pc[0], tol2, big2, floor_, c, s);
+    const int f = rot_params(pa[0], pb[0], pc[0], tol2, big2, ex2, floor_, c, s);
     fl |= f;
     if (!rotate || !__any_sync(FULL, f != 0)) return;
 #pragma unroll
@@ -231,9 +232,13 @@ __device__ __forceinline__ void tile_io(Tile<T, B, R, RV> &t, T *W, int ldw, T *
 // reference would have rotated nothing in that sweep either.
 // nr = ldw / 32 and nv = ldv / 32 are the rows per lane actually used
 // (<= R, RV): one instantiation serves every matrix up to 32R x 32RV.
+// exit_ratio > 0 (the first phase of the mixed solve): also stop after the
+// first sweep whose largest ratio is <= exit_ratio -- the rotations of that
+// sweep leave ~exit_ratio^2, below what FP32 sweeps resolve, and the FP64
+// phase that follows takes it from there (converged is then set).
 template <typename T, int B, int R, int RV>
 __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, int max_sweeps, bool confirm,
-                         double *red, bool &converged) {
+                         double *red, bool &converged, T exit_ratio = T(0)) {
     const int nr = ldw >> 5, nv = ldv >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nw = nwarps();
@@ -244,6 +249,7 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
     if (act) tile_io(t, W, ldw, V, ldv, X, Y, lane, false, nr, nv);
     bool measure = false, measure_allowed = confirm;
     const T tol2 = tol * tol, big2 = tol / T(4);  // ratio > tol, ratio > sqrt(tol)/2
+    const T ex2 = exit_ratio * exit_ratio;
     converged = false;
     int sweep = 0;
     for (sweep = 1; sweep <= max_sweeps; ++sweep) {
@@ -271,7 +277,7 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
         int fl = 0;
         if (act && (X < live || Y < live)) {
             for (int j = 0; j < B - 1; ++j) {
-                step<true>(t, tol2, big2, floor_, fl, rotate, lane, nr, nv);
+                step<true>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
                 circle_shift(t);
             }
         }
@@ -288,7 +294,7 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
             }
             if (act && X < live && Y < live) {
                 for (int j = 0; j < B; ++j) {
-                    step<false>(t, tol2, big2, floor_, fl, rotate, lane, nr, nv);
+                    step<false>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
                     shift_y(t);
                 }
             }
@@ -296,7 +302,9 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
         // off <= tol  <=>  no active pair in the sweep (primitives.py:352).
         const int any_active = __syncthreads_or(fl & 1);
         const int any_big = __syncthreads_or(fl & 2);
+        const int any_above_exit = __syncthreads_or(fl & 4);
         if (!any_active) { converged = true; break; }
+        if (exit_ratio > T(0) && rotate && !any_above_exit) { converged = true; break; }
         if (measure) {
             measure = false;
             measure_allowed = false;  // a failed confirmation: rotate from now on
