@@ -59,6 +59,17 @@ def load_matrices(rank):
     return wl.uneven_batch(COUNT, seed=1 if rank == 0 else 1 + 1000 * rank)
 
 
+def reduce_max(x, device):
+    """Max of x over the ranks of the default process group (x itself
+    without one): every multi-GPU time is the slowest rank's."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def algorithmic(m, n):
     """Compulsory HBM bytes and FP work of one solve of the batch.
     bytes: read A, write U (m x k), S (k), Vh (k x n), descriptors (48 B) and
@@ -242,11 +253,7 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
     step_ms = [a.elapsed_time(b) for a, b in times]
-    total_ms = sum(step_ms)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = reduce_max(sum(step_ms), dev)
     ms_per_step = total_ms / args.steps
     value = COUNT * world / (ms_per_step / 1e3)
 
@@ -283,11 +290,8 @@ def run_ours(args, rank, world, local_rank):
         e1.record(stream)
         e2e_ev.append((e0, e1))
     torch.cuda.synchronize(dev)
-    e2e_ms = sum(a.elapsed_time(b) for a, b in e2e_ev)
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = COUNT * world / (float(t.item()) / args.steps / 1e3)
+    e2e_ms = reduce_max(sum(a.elapsed_time(b) for a, b in e2e_ev), dev)
+    e2e_value = COUNT * world / (e2e_ms / args.steps / 1e3)
 
     if rank != 0:
         return

@@ -124,6 +124,8 @@ class BlockJacobi:
         self.dmax = torch.zeros(R, self.P, **f32)
         self.isweeps = torch.zeros(self.P, dtype=torch.int32, device=dev)
         self.live = torch.zeros(1, dtype=torch.float64, device=dev)   # live-column floor of the sweep
+        # CTAs along K of the Gram products: about one wave over the SMs
+        self.gram_split = max(1, torch.cuda.get_device_properties(dev).multi_processor_count // self.P)
         self._graphs, self._seen = {}, set()
 
     def _combine_v(self, cur):
@@ -163,7 +165,7 @@ class BlockJacobi:
             Wp = [x.view(P, 2 * b, self.mpad) for x in self.W[cur][:parts]]
             Vp = [x.view(P, 2 * b, self.npad) for x in self.V[cur][:parts]]
             # Grams of every slot: G_k = X_k X_k^T with X_k = 2b rows of W^T.
-            gemm_parts(Wp, None, self.G, syrk=True, chain128=True)
+            gemm_parts(Wp, None, self.G, syrk=True, chain128=True, split_k=self.gram_split)
             N.check(lib.jb_block_eig_f64(self.G.data_ptr(), self.Qt[0].data_ptr(), self.Qt[1].data_ptr(),
                                          self.Qt[2].data_ptr() if parts == 3 else None, self.off[r].data_ptr(),
                                          self.dmax[r].data_ptr(), self.isweeps.data_ptr(), P, 2 * b,

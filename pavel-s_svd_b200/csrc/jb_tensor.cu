@@ -55,7 +55,11 @@ static int launch(TcParams &p, int64_t batch, cudaStream_t st) {
     const size_t per_stage = p.na * A_TILE + (p.a_as_b ? 0 : p.nb * (size_t)BN * BK * 2);
     int stages = (int)((227 * 1024 - 1024 - 64) / per_stage);
     if (stages > 6) stages = 6;
-    if (stages < 2) return JB_ETOOBIG;
+    // No more stages than k-blocks per CTA: short-K products (the rotation
+    // updates, K = 2b) then leave room for several CTAs per SM.
+    const int nk = (p.kchunk + BK - 1) / BK;
+    if (stages > nk) stages = nk;
+    if (stages < 1) return JB_ETOOBIG;
     p.stages = stages;
     const size_t smem = smem_bytes(stages, p.na, p.a_as_b ? 0 : p.nb, BN);
     auto kern = tc_gemm_kernel<BN>;
