@@ -44,6 +44,10 @@ sys.path.insert(0, str(ROOT))
 METRIC = "Jacobi SVD matrices/s at sigma-rel-err<=1e-5 vs FP64 (uneven batch)"
 WORKLOAD = "uneven_batch_8192"
 COUNT = 8192
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one solve of
+# this workload, rb32_kernel + rb64_kernel, from one ncu --set full capture
+# of `bench.py --steps 1 --warmup 3 --no-cpu-baseline`.
+MEASURED_TRAFFIC_PER_SOLVE = 318.05e6
 
 
 def workload_config(n_gpus):
@@ -312,7 +316,8 @@ def run_ours(args, rank, world, local_rank):
                          "sweeps_mean": float(sweeps.mean()), "sweeps_max": int(sweeps.max())},
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved_gbs / hbm_peak, "peak_kind": peak_kind,
-                         "traffic": args.traffic_bytes,
+                         "traffic": args.traffic_bytes if args.traffic_bytes is not None else
+                         MEASURED_TRAFFIC_PER_SOLVE,
                          "algorithmic_bytes_per_launch": nbytes,
                          "note": "compulsory bytes only; the path is bound by the FP32/FP64 pipes, see fp_pipe"},
             "fp_pipe": {"achieved_tflops": fp_tflops, "flop_per_launch": flop,

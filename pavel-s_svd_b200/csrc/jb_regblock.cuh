@@ -73,23 +73,80 @@ __device__ __forceinline__ void reduce_scatter(T (&x)[NV], int lane) {
 // Returns bit 0: active; bit 1: ratio > sqrt(tol) / 2 (the confirmation
 // heuristic of rb_sweeps); bit 2: ratio > the phase exit ratio (ex2 its
 // square).  Inactive pairs get c = 1, s = 0.
-__device__ __forceinline__ float rcp_sqrt(float x) { return 1.0f / sqrtf(x); }
-__device__ __forceinline__ double rcp_sqrt(double x) { return rsqrt(x); }
-
 template <typename T>
-__device__ __forceinline__ int rot_params(T app, T aqq, T apq, T tol2, T big2, T ex2, T floor_, T &c, T &s) {
-    c = T(1);
-    s = T(0);
-    const T apq2 = apq * apq;
-    const T prod = app * aqq;
+__device__ __forceinline__ int rot_params(T app, T aqq, T apq, T tol2, T big2, T ex2, T floor_, T &c, T &s);
+
+// FP32: t from approximate reciprocal / reciprocal square root (an error of
+// a few ulp in t only leaves |apq| a few ulp of itself), c = 1/sqrt(1+t^2)
+// refined by one Newton step so that c^2 + s^2 = 1 to ~1 ulp: every applied
+// rotation stays orthogonal at FP32 precision.
+template <>
+__device__ __forceinline__ int rot_params<float>(float app, float aqq, float apq, float tol2, float big2, float ex2,
+                                                 float floor_, float &c, float &s) {
+    c = 1.f;
+    s = 0.f;
+    const float apq2 = apq * apq;
+    const float prod = app * aqq;
+    const bool active = apq2 > tol2 * prod && fminf(app, aqq) > floor_;
+    if (!active) return 0;
+    const float d = aqq - app;
+    const float h = fmaf(d, d, 4.f * apq2);
+    const float sq = h * rsqrtf(h);                       // sqrt(h), h > 0 for an active pair
+    const float t = copysignf(__fdividef(2.f * fabsf(apq), fabsf(d) + sq), d);
+    const float x = fmaf(t, t, 1.f);
+    const float c0 = rsqrtf(x);
+    c = c0 * fmaf(-0.5f * x, c0 * c0, 1.5f);
+    s = t * c;
+    if (apq < 0.f) s = -s;
+    return 1 | (apq2 > big2 * prod ? 2 : 0) | (apq2 > ex2 * prod ? 4 : 0);
+}
+
+// FP64: the angle in FP32 from exponent-scaled (d, 2|apq|) -- exact power of
+// two scaling into [1, 2), so no FP32 overflow or underflow -- and
+// c = 1/sqrt(1+t^2), s = t c in FP64 (FP32 estimate + one Newton step), so
+// every applied rotation is orthogonal to FP64 precision.
+template <>
+__device__ __forceinline__ int rot_params<double>(double app, double aqq, double apq, double tol2, double big2,
+                                                  double ex2, double floor_, double &c, double &s) {
+    c = 1.0;
+    s = 0.0;
+    const double apq2 = apq * apq;
+    const double prod = app * aqq;
     const bool active = apq2 > tol2 * prod && fmin(app, aqq) > floor_;
     if (!active) return 0;
-    const T d = aqq - app;
-    const T t = copysign(T(2) * dabs(apq), d) / (dabs(d) + dsqrt(dfma(d, d, T(4) * apq2)));
-    c = rcp_sqrt(dfma(t, t, T(1)));
+    const double d = aqq - app, a2 = 2.0 * fabs(apq);
+    const int ex = (__double2hiint(fmax(fabs(d), a2)) >> 20) & 0x7ff;
+    const double scl = __hiloint2double((2046 - ex) << 20, 0);
+    const float df = fabsf((float)(d * scl)), af = (float)(a2 * scl);
+    const float hf = fmaf(df, df, af * af);
+    const float tf = __fdividef(af, df + hf * rsqrtf(hf));
+    const double t = d < 0.0 ? -(double)tf : (double)tf;
+    const double x = fma(t, t, 1.0);
+    const double c0 = (double)rsqrtf((float)x);
+    c = c0 * fma(-0.5 * x, c0 * c0, 1.5);
     s = t * c;
-    if (apq < T(0)) s = -s;
+    if (apq < 0.0) s = -s;
     return 1 | (apq2 > big2 * prod ? 2 : 0) | (apq2 > ex2 * prod ? 4 : 0);
+}
+
+// Packed FP32 (two rows per instruction): a += x * y for (a0, a1), and the
+// rotation pair (x, y) <- (c x - s y, s x + c y) for two rows at once.
+__device__ __forceinline__ void fma2(float &a0, float &a1, float x0, float x1, float y0, float y1) {
+    asm("{\n\t.reg .b64 ra, rx, ry;\n\t"
+        "mov.b64 ra, {%0, %1};\n\tmov.b64 rx, {%2, %3};\n\tmov.b64 ry, {%4, %5};\n\t"
+        "fma.rn.f32x2 ra, rx, ry, ra;\n\tmov.b64 {%0, %1}, ra;\n\t}"
+        : "+f"(a0), "+f"(a1) : "f"(x0), "f"(x1), "f"(y0), "f"(y1));
+}
+__device__ __forceinline__ void rot2(float &x0, float &x1, float &y0, float &y1, float c, float s) {
+    asm("{\n\t.reg .b64 rx, ry, rc, rs, rn, t1, t2;\n\t"
+        "mov.b64 rx, {%0, %1};\n\tmov.b64 ry, {%2, %3};\n\t"
+        "mov.b64 rc, {%4, %4};\n\tmov.b64 rs, {%5, %5};\n\tmov.b64 rn, {%6, %6};\n\t"
+        "mul.rn.f32x2 t1, rn, ry;\n\t"          // -s y
+        "fma.rn.f32x2 t1, rc, rx, t1;\n\t"      // c x - s y
+        "mul.rn.f32x2 t2, rc, ry;\n\t"          // c y
+        "fma.rn.f32x2 t2, rs, rx, t2;\n\t"      // s x + c y
+        "mov.b64 {%0, %1}, t1;\n\tmov.b64 {%2, %3}, t2;\n\t}"
+        : "+f"(x0), "+f"(x1), "+f"(y0), "+f"(y1) : "f"(c), "f"(s), "f"(-s));
 }
 
 // Register column of the first / second member of pair i in a step.
@@ -105,31 +162,49 @@ __device__ __forceinline__ constexpr int pair_q(int i) {
 }
 
 // One step: B disjoint pairs; ORs the pairs' rot_params flags into fl.
+// FP32 tiles work on row pairs with packed instructions; rows >= nr of a
+// lane are zero in the tile (tile_io), so a pair past nr adds nothing and
+// stays zero.
 template <bool INTRA, typename T, int B, int R, int RV>
 __device__ __forceinline__ void step(Tile<T, B, R, RV> &t, T tol2, T big2, T ex2, T floor_, int &fl, bool rotate,
                                      int lane, int nr, int nv) {
     constexpr int LB = Log2<B>::value;
+    constexpr bool PACK = sizeof(T) == 4 && R % 2 == 0 && RV % 2 == 0;
     T pa[B], pb[B], pc[B];
 #pragma unroll
     for (int i = 0; i < B; ++i) {
         const int p = pair_p<INTRA, B>(i), q = pair_q<INTRA, B>(i);
-        T a = 0, b = 0, c = 0;
+        if constexpr (PACK) {
+            float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f, c0 = 0.f, c1 = 0.f;
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            if (r < nr) {
-                const T x = t.w[p][r], y = t.w[q][r];
-                a = dfma(x, x, a);
-                b = dfma(y, y, b);
-                c = dfma(x, y, c);
+            for (int r = 0; r < R; r += 2) {
+                if (r < nr) {
+                    const float x0 = t.w[p][r], x1 = t.w[p][r + 1], y0 = t.w[q][r], y1 = t.w[q][r + 1];
+                    fma2(a0, a1, x0, x1, x0, x1);
+                    fma2(b0, b1, y0, y1, y0, y1);
+                    fma2(c0, c1, x0, x1, y0, y1);
+                }
             }
+            pa[i] = a0 + a1; pb[i] = b0 + b1; pc[i] = c0 + c1;
+        } else {
+            T a = 0, b = 0, c = 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (r < nr) {
+                    const T x = t.w[p][r], y = t.w[q][r];
+                    a = dfma(x, x, a);
+                    b = dfma(y, y, b);
+                    c = dfma(x, y, c);
+                }
+            }
+            pa[i] = a; pb[i] = b; pc[i] = c;
         }
-        pa[i] = a; pb[i] = b; pc[i] = c;
     }
     reduce_scatter<T, B>(pa, lane);
     reduce_scatter<T, B>(pb, lane);
     reduce_scatter<T, B>(pc, lane);
     T c, s;
-    const int f = rot_params(pa[0], pb[0], pc[0], tol2, big2, ex2, floor_, c, s);
+    const int f = rot_params<T>(pa[0], pb[0], pc[0], tol2, big2, ex2, floor_, c, s);
     fl |= f;
     if (!rotate || !__any_sync(FULL, f != 0)) return;
 #pragma unroll
@@ -137,20 +212,29 @@ __device__ __forceinline__ void step(Tile<T, B, R, RV> &t, T tol2, T big2, T ex2
         const int src = i << (5 - LB);
         const T ci = __shfl_sync(FULL, c, src), si = __shfl_sync(FULL, s, src);
         const int p = pair_p<INTRA, B>(i), q = pair_q<INTRA, B>(i);
+        if constexpr (PACK) {
 #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            if (r < nr) {
-                const T x = t.w[p][r], y = t.w[q][r];
-                t.w[p][r] = dfma(ci, x, -si * y);
-                t.w[q][r] = dfma(si, x, ci * y);
+            for (int r = 0; r < R; r += 2)
+                if (r < nr) rot2(t.w[p][r], t.w[p][r + 1], t.w[q][r], t.w[q][r + 1], ci, si);
+#pragma unroll
+            for (int r = 0; r < RV; r += 2)
+                if (r < nv) rot2(t.v[p][r], t.v[p][r + 1], t.v[q][r], t.v[q][r + 1], ci, si);
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (r < nr) {
+                    const T x = t.w[p][r], y = t.w[q][r];
+                    t.w[p][r] = dfma(ci, x, -si * y);
+                    t.w[q][r] = dfma(si, x, ci * y);
+                }
             }
-        }
 #pragma unroll
-        for (int r = 0; r < RV; ++r) {
-            if (r < nv) {
-                const T x = t.v[p][r], y = t.v[q][r];
-                t.v[p][r] = dfma(ci, x, -si * y);
-                t.v[q][r] = dfma(si, x, ci * y);
+            for (int r = 0; r < RV; ++r) {
+                if (r < nv) {
+                    const T x = t.v[p][r], y = t.v[q][r];
+                    t.v[p][r] = dfma(ci, x, -si * y);
+                    t.v[q][r] = dfma(si, x, ci * y);
+                }
             }
         }
     }
@@ -211,6 +295,8 @@ __device__ __forceinline__ void tile_io(Tile<T, B, R, RV> &t, T *W, int ldw, T *
             if (r < nr) {
                 if (store) w[32 * r] = t.w[c][r];
                 else t.w[c][r] = w[32 * r];
+            } else if (!store) {
+                t.w[c][r] = T(0);
             }
         }
 #pragma unroll
@@ -218,6 +304,8 @@ __device__ __forceinline__ void tile_io(Tile<T, B, R, RV> &t, T *W, int ldw, T *
             if (r < nv) {
                 if (store) v[32 * r] = t.v[c][r];
                 else t.v[c][r] = v[32 * r];
+            } else if (!store) {
+                t.v[c][r] = T(0);
             }
         }
     }
