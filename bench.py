@@ -53,7 +53,8 @@ MEASURED_TRAFFIC_PER_SOLVE = 318.05e6
 def workload_config(n_gpus):
     return {"workload": WORKLOAD, "matrices_per_gpu": COUNT, "n_range": [8, 64], "m_range": "[n, 2n]",
             "dtype": "float32", "seed": 1, "tol": "10*eps32 (reference default)", "max_sweeps": 60,
-            "precision": "mixed (FP32 sweeps, then FP64 sweeps from Householder-QR V)",
+            "precision": "mixed (FP32 sweeps, then FP64 sweeps from the Newton-Schulz orthogonalised V, "
+                         "W = A V recomputed in FP64)",
             "parallelism": f"dp{n_gpus} (independent matrices per GPU, no collective)",
             "l2": "256 MiB write between steps, outside the timed events"}
 
@@ -463,10 +464,12 @@ def run_warm(args):
     torch.cuda.synchronize()
     train_ms = e0.elapsed_time(e1)
     solver = W.WarmSolver(net, m=128, n=64, batch=4096)
+    solver32 = W.WarmSolver(net, m=128, n=64, batch=4096, precision="fp32")
     eye = torch.eye(64, device="cuda").expand(4096, 64, 64).contiguous()
     ideal = wl.family_v(theta[60000:64096], device="cuda").contiguous()
     res = {}
-    for label, v0 in (("plain", eye), ("warm", None), ("ideal_start", ideal)):
+    for label, v0 in (("plain_fp32", eye), ("plain", eye), ("warm", None), ("ideal_start", ideal)):
+        solver = solver32 if label == "plain_fp32" else W.WarmSolver(net, m=128, n=64, batch=4096)
         for _ in range(args.warmup):
             solver.launch(te, v0=v0)
         torch.cuda.synchronize()
@@ -492,7 +495,9 @@ def run_warm(args):
             "data": "synthetic (seeded, BASELINE config 5)", "config": {"workload": "warm_family", "train": 60000,
                                                                          "held_out": 4096, "epochs": 15},
             "train_ms": train_ms, "loss_first_last": [hist[0], hist[-1]], "variants": res,
-            "note": "ideal_start = the generator's own V(theta): what a perfect network would give"}
+            "note": "plain_fp32 = the plain FP32 Jacobi from V = I; plain = the mixed-precision solver from V = I; "
+                    "warm = the network's V0 (QR-orthonormalised, identity fallback); ideal_start = the "
+                    "generator's own V(theta): what a perfect network would give"}
     print(json.dumps(line), flush=True)
 
 
