@@ -115,11 +115,15 @@ JB_API int jb_svd_batched_f64(const double *A, double *U, double *S, double *Vh,
  * device descriptors; order: optional device permutation of [0, count)
  * giving the processing order (largest cost first balances the persistent
  * grid), or NULL.  max_m/max_n bound every descriptor (either orientation).
- * Workspace: jb_workspace_bytes(max_m, max_n, count, 4, precision, 0) bytes,
- * followed (JB_PREC_MIXED) by the scratch floats the descriptors' x_off
- * address; a descriptor whose scratch does not fit gets JB_ST_BAD_DESC.
+ * Workspace: jb_uneven_workspace_bytes(max_m, max_n, count, precision,
+ * scratch_floats) bytes, where scratch_floats (JB_PREC_MIXED) covers every
+ * descriptor's x_off + nt^2 (the FP32 V handed from the FP32 to the FP64
+ * phase); a descriptor whose scratch does not fit gets JB_ST_BAD_DESC.
  * Replaces a harness loop of svd(x, 'jacobi') over matrices of different
  * shapes. */
+JB_API size_t jb_uneven_workspace_bytes(int32_t max_m, int32_t max_n, int64_t count,
+                                        int32_t precision, int64_t scratch_floats);
+
 JB_API int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh,
                       const jb_matrix_desc *descs, const int32_t *order,
                       int64_t count, int32_t max_m, int32_t max_n,

@@ -98,10 +98,10 @@ class UnevenBatch:
         self.Vh = None if values_only else torch.zeros(max(vt, 1), dtype=torch.float32, device=dev)
         self.info = torch.zeros(2, max(self.count, 1), dtype=torch.int32, device=dev)
         lib = N.lib()
-        # Workspace: the base area (ticket counters) followed, in mixed
-        # precision, by the scratch floats the descriptors' x_off address.
-        base = lib.jb_workspace_bytes(self.max_m, self.max_n, self.count, 4, N.PREC_NATIVE, 0)
-        ws = base + (4 * xt if self.precision == N.PREC_MIXED else 0)
+        # Workspace: the base area (ticket counters, per-CTA areas of the
+        # round-robin kernels) followed, in mixed precision, by the scratch
+        # floats the descriptors' x_off address.
+        ws = lib.jb_uneven_workspace_bytes(self.max_m, self.max_n, self.count, self.precision, int(xt))
         self.workspace = torch.empty(max(int(ws), 256), dtype=torch.uint8, device=dev)
         # memset of the work tickets + one persistent kernel per precision phase
         self.kernels_per_solve = 2 if self.precision == N.PREC_MIXED else 1

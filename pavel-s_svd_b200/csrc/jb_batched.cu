@@ -16,6 +16,7 @@
 #include "jacobi_b200.h"
 #include "jb_device.cuh"
 #include "jb_regblock.cuh"
+#include "jb_gram64.cuh"
 
 namespace jb {
 
@@ -88,6 +89,7 @@ struct Params {
     int32_t *sweeps, *status;
     int *counter;                 // NULL: static grid-stride schedule
     int *counter2;                // ticket of the second (FP64) kernel
+    int from_x32;                 // mixed round-robin solve: start from the FP32 V in x32 (large-tile K1)
     unsigned char *gws;           // NULL: work area in shared memory
     size_t gws_stride;
     Dims maxd;                    // sizing of aux / region (largest matrix)
@@ -151,6 +153,7 @@ __device__ int solve_native(const Params &p, const jb_matrix_desc &d, unsigned c
 // V in FP64, W = A V in FP64, FP64 sweeps to the same tolerance.
 __device__ int solve_mixed(const Params &p, const jb_matrix_desc &d, unsigned char *region, Aux &ax,
                            int &nsweeps) {
+    const int k1_sweeps = nsweeps;  // FP32 sweeps of the large-tile kernel (from_x32)
     const Geo g = make_geo(d.m, d.n, d.rank, d.flags);
     const float *A = (const float *)p.A + d.a_off;
     double *V64 = (double *)region;
@@ -161,17 +164,29 @@ __device__ int solve_mixed(const Params &p, const jb_matrix_desc &d, unsigned ch
     const int e = scan_input(A, g.m * g.n, ax, bad);
     nsweeps = 0;
     if (bad) return JB_ST_NONFINITE_IN;
-    Geo g32 = g;
-    g32.ncp = g.np;
-    load_tall(A, g32, e, W32);
-    set_identity(V32, g.np, g.ldv);
-    __syncthreads();
-    const float tol32 = p.tol32 > 0 ? (float)p.tol32 : 10.0f * Lim<float>::eps();
-    bool conv32;
-    const int s1 = sweeps<float>(W32, V32, g32, tol32, p.max_sweeps32, ax, conv32);
-    for (int idx = threadIdx.x; idx < g.np * g.np; idx += blockDim.x) {
-        int c = idx / g.np, i = idx - c * g.np;
-        V64[(size_t)c * g.ldv + i] = (double)V32[(size_t)c * g.ldv + i];
+    int s1 = 0;
+    if (p.from_x32) {
+        // the FP32 sweeps ran in the large-tile kernel: V (nt x nt,
+        // column-major) in x32, identity on the padding column
+        s1 = k1_sweeps;
+        const float *x = p.x32 + d.x_off;
+        for (int idx = threadIdx.x; idx < g.np * g.np; idx += blockDim.x) {
+            const int c = idx / g.np, i = idx - c * g.np;
+            V64[(size_t)c * g.ldv + i] = (c < g.nt && i < g.nt) ? (double)x[(size_t)c * g.nt + i] : (c == i ? 1.0 : 0.0);
+        }
+    } else {
+        Geo g32 = g;
+        g32.ncp = g.np;
+        load_tall(A, g32, e, W32);
+        set_identity(V32, g.np, g.ldv);
+        __syncthreads();
+        const float tol32 = p.tol32 > 0 ? (float)p.tol32 : 10.0f * Lim<float>::eps();
+        bool conv32;
+        s1 = sweeps<float>(W32, V32, g32, tol32, p.max_sweeps32, ax, conv32);
+        for (int idx = threadIdx.x; idx < g.np * g.np; idx += blockDim.x) {
+            int c = idx / g.np, i = idx - c * g.np;
+            V64[(size_t)c * g.ldv + i] = (double)V32[(size_t)c * g.ldv + i];
+        }
     }
     __syncthreads();
     householder_orthonormalize(V64, g.np, g.ldv, W64, g.ldv, ax);
@@ -220,7 +235,19 @@ __global__ void __launch_bounds__(1024, 1) batched_kernel(Params p) {
         if (threadIdx.x < 4) ax.flag[threadIdx.x] = 0;
         __syncthreads();
         int ns = 0, st;
-        if (!desc_fits(d, p.maxd)) st = JB_ST_BAD_DESC;
+        int prev = JB_ST_OK;
+        if (PREC == JB_PREC_MIXED && p.from_x32) {
+            // K1 (large-tile FP32 sweeps) left its status and sweep count
+            if (threadIdx.x == 0) { ax.flag[3] = p.status[mat]; ax.flag[2] = p.sweeps[mat]; }
+            __syncthreads();
+            prev = ax.flag[3];
+            ns = ax.flag[2];
+            __syncthreads();
+            if (threadIdx.x == 0) ax.flag[2] = 0;
+            __syncthreads();
+        }
+        if (prev != JB_ST_OK) st = prev;
+        else if (!desc_fits(d, p.maxd)) st = JB_ST_BAD_DESC;
         else if (PREC == JB_PREC_MIXED) st = solve_mixed(p, d, region, ax, ns);
         else st = solve_native<T>(p, d, region, ax, ns);
         if (threadIdx.x == 0) {
@@ -246,6 +273,8 @@ constexpr int kB64 = 2;   // block width of the FP64 sweeps (16 warps for 64 col
 constexpr int kT32 = 256, kT64 = 512;  // threads of the two kernels
 constexpr int kMaxR = 4;  // rows per lane: mt <= 128
 constexpr int kMaxRV = 2; // V rows per lane: padded width <= 64
+// Large-tile FP32 kernel (one matrix up to 256 x 128 per CTA, 16 warps).
+constexpr int kT32L = 512, kMaxRL = 8, kMaxRVL = 4;
 
 struct RGeo {
     int R, RV, nb, npb, live, ldw, ldv, ncp;
@@ -285,13 +314,14 @@ __host__ __device__ inline Dims raux_dims(const RGeo &r) {
     return d;
 }
 
-__device__ inline bool rdesc_fits(const jb_matrix_desc &d, int B, int elem, const Params &p, bool mixed_scratch) {
+__device__ inline bool rdesc_fits(const jb_matrix_desc &d, int B, int elem, const Params &p, bool mixed_scratch,
+                                  int max_r = kMaxR, int max_rv = kMaxRV) {
     if (d.m < 1 || d.n < 1) return false;
     const int mt = d.m > d.n ? d.m : d.n, nt = d.m > d.n ? d.n : d.m;
     if (d.rank < 1 || d.rank > nt) return false;
     if ((d.flags & JB_FULL_MATRICES) && d.rank != nt) return false;
     const RGeo r = rgeo(mt, nt, B, d.flags);
-    if (r.R > kMaxR || r.RV > kMaxRV) return false;
+    if (r.R > max_r || r.RV > max_rv) return false;
     size_t need = (mixed_scratch && elem == 8) ? rregion_mixed64(r, nt) : rregion_bytes(r, elem);
     if (elem == 4 && p.vstart) need += align16((size_t)r.ldw * nt * 4);
     if (need > p.region_cap) return false;
@@ -329,11 +359,11 @@ __device__ void load_stage(const TI *A, const Geo &g, int ld, float *As) {
     }
 }
 
-template <typename T, int B>
+template <typename T, int B, int MR = kMaxR, int MRV = kMaxRV>
 __device__ int rb_dispatch(const RGeo &r, T *W, T *V, T tol, int max_sweeps, bool confirm, double *red,
                            bool &conv, T exit_ratio = T(0)) {
-    return rb_sweeps<T, B, kMaxR, kMaxRV>(W, r.ldw, V, r.ldv, r.nb, r.live, tol, max_sweeps, confirm, red, conv,
-                                          exit_ratio);
+    return rb_sweeps<T, B, MR, MRV>(W, r.ldw, V, r.ldv, r.nb, r.live, tol, max_sweeps, confirm, red, conv,
+                                    exit_ratio);
 }
 
 __device__ inline Geo reg_geo(const jb_matrix_desc &d, const RGeo &r) {
@@ -416,9 +446,12 @@ __device__ double polar_step(double *V, int n, int ld, double *VT, double *H, do
 }
 
 // K1: FP32 sweeps.  MIXED: store the FP32 V (nt x nt) in the scratch for K2;
-// else run the epilogue and write U, S, Vh.
-template <bool MIXED>
-__global__ void __launch_bounds__(kT32) rb32_kernel(Params p) {
+// else run the epilogue and write U, S, Vh.  THREADS / MR / MRV: the CTA size
+// and the register tile (rows per lane of W and V); rb32_kernel is the
+// 256-thread form for matrices up to 128 x 64, rb32_large_kernel the
+// 512-thread form for one matrix up to 256 x 128 per CTA.
+template <bool MIXED, int THREADS, int MR, int MRV>
+__global__ void __launch_bounds__(THREADS) rb32_kernel_t(Params p) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_idx;
     Aux ax = carve_aux(smem, p.maxd);
@@ -432,7 +465,7 @@ __global__ void __launch_bounds__(kT32) rb32_kernel(Params p) {
         if (threadIdx.x < 4) ax.flag[threadIdx.x] = 0;
         __syncthreads();
         int ns = 0, st = JB_ST_OK;
-        if (!rdesc_fits(d, kB32, 4, p, MIXED)) {
+        if (!rdesc_fits(d, kB32, 4, p, MIXED, MR, MRV)) {
             st = JB_ST_BAD_DESC;
         } else {
             const RGeo r = rgeo(d.m > d.n ? d.m : d.n, d.m > d.n ? d.n : d.m, kB32, d.flags);
@@ -471,8 +504,8 @@ __global__ void __launch_bounds__(kT32) rb32_kernel(Params p) {
                 const float tol = MIXED ? (p.tol32 > 0 ? (float)p.tol32 : 10.0f * Lim<float>::eps())
                                         : (p.tol > 0 ? (float)p.tol : 10.0f * Lim<float>::eps());
                 bool conv;
-                ns = rb_dispatch<float, kB32>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true, ax.red, conv,
-                                              MIXED ? kMixedExitRatio : 0.0f);
+                ns = rb_dispatch<float, kB32, MR, MRV>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true,
+                                                       ax.red, conv, MIXED ? kMixedExitRatio : 0.0f);
                 if (MIXED) {
                     float *x = p.x32 + d.x_off;
                     const int nt = g.nt;
@@ -596,6 +629,136 @@ __global__ void __launch_bounds__(kT64) rb64_kernel(Params p) {
 }
 
 
+// K2 of the mixed solve for large tiles (after rb32_kernel_t<true, kT32L>):
+// the FP64 phase on the Gram of W (jb_gram64.cuh).  Work arrays in the
+// per-CTA global area: V64 (ldv x np) | W64 (ldw x ncp) | X, Ad (ldx x ncp
+// each, ldx = max(ldw, ldv): they also hold the temporaries), FP64; G, D and
+// the round bookkeeping in shared memory.
+__host__ __device__ inline size_t gram64_region(const Dims &d) {
+    const size_t ldx = d.ldw > d.ldv ? d.ldw : d.ldv;
+    return align16((size_t)d.ldv * d.np * 8) + align16((size_t)d.ldw * d.ncp * 8) + 2 * align16(ldx * d.ncp * 8);
+}
+
+__global__ void __launch_bounds__(kTG, 1) gram64_kernel(Params p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_idx, s_any;
+    Aux ax = carve_aux(smem, p.maxd);
+    const int npmax = p.maxd.np;
+    size_t gsz, dd;
+    gram64_regions(npmax, p.maxd.mt, gsz, dd);
+    double *G = (double *)(smem + aux_bytes(p.maxd));
+    float *D = (float *)((unsigned char *)G + gsz);
+    double *cs = (double *)((unsigned char *)D + dd);
+    unsigned char *pq = (unsigned char *)(cs + npmax);
+    unsigned char *sched = pq + npmax;
+    unsigned char *area = p.gws + (size_t)blockIdx.x * p.gws_stride;
+    for (;;) {
+        int64_t idx;
+        next_ticket(p.counter, s_idx, idx);
+        if (idx >= p.count) break;
+        const int64_t mat = p.order ? (int64_t)p.order[idx] : idx;
+        const jb_matrix_desc d = desc_of(p, mat);
+        if (threadIdx.x < 4) ax.flag[threadIdx.x] = 0;
+        __syncthreads();
+        if (threadIdx.x == 0) { ax.flag[3] = p.status[mat]; ax.flag[2] = p.sweeps[mat]; }
+        __syncthreads();
+        const int prev = ax.flag[3], s1 = ax.flag[2];
+        __syncthreads();
+        if (threadIdx.x == 0) ax.flag[2] = 0;
+        __syncthreads();
+        if (prev != JB_ST_OK) continue;  // K1 already reported this matrix
+        int ns = s1, st = JB_ST_OK;
+        if (!desc_fits(d, p.maxd) || d.x_off < 0) {
+            st = JB_ST_BAD_DESC;
+        } else {
+            const Geo g = make_geo(d.m, d.n, d.rank, d.flags);
+            const float *A = (const float *)p.A + d.a_off;
+            const int np = g.np, nt = g.nt, mt = g.mt, ldv = g.ldv, ldw = g.ldw;
+            const int ldx = ldw > ldv ? ldw : ldv;
+            double *V64 = (double *)area;
+            double *W64 = (double *)((unsigned char *)V64 + align16((size_t)ldv * np * 8));
+            double *X = (double *)((unsigned char *)W64 + align16((size_t)ldw * g.ncp * 8));
+            double *Ad = (double *)((unsigned char *)X + align16((size_t)ldx * g.ncp * 8));
+            bool bad;
+            const int e = scan_input(A, g.m * g.n, ax, bad);
+            if (bad) {
+                st = JB_ST_NONFINITE_IN;
+            } else {
+                // V from the FP32 phase (nt x nt, column-major), identity on the padding
+                const float *x = p.x32 + d.x_off;
+                for (int k = threadIdx.x; k < ldv * np; k += blockDim.x) {
+                    const int c = k / ldv, i = k - c * ldv;
+                    V64[k] = (c < nt && i < nt) ? (double)x[(size_t)c * nt + i] : ((i == c && i < np) ? 1.0 : 0.0);
+                }
+                __syncthreads();
+                double *stage = (double *)D;
+                // Newton-Schulz: X = V^T V, V <- 1.5 V - 0.5 V X (once; twice if V was far from
+                // orthogonal); the product V X is staged in Ad (ldx x ncp), free until A_t goes there
+                for (int it = 0; it < 2; ++it) {
+                    gemm64<true, double>(V64, ldv, V64, ldv, X, ldx, np, np, np, 1.0, 0.0, stage);
+                    double dev = 0.0;
+                    for (int k = threadIdx.x; k < np * np; k += blockDim.x) {
+                        const int c = k / np, i = k - c * np;
+                        dev = fmax(dev, fabs(X[(size_t)c * ldx + i] - (i == c ? 1.0 : 0.0)));
+                    }
+                    dev = block_max(dev, ax.red);
+                    if (it == 1 && dev < 1e-10) break;
+                    gemm64<false, double>(V64, ldv, X, ldx, Ad, ldx, np, np, np, -0.5, 0.0, stage);
+                    for (int k = threadIdx.x; k < np * np; k += blockDim.x) {
+                        const int c = k / np, i = k - c * np;
+                        V64[(size_t)c * ldv + i] = fma(1.5, V64[(size_t)c * ldv + i], Ad[(size_t)c * ldx + i]);
+                    }
+                    __syncthreads();
+                    if (dev < 1e-5) break;   // one step took it to ~dev^2
+                }
+                // A_t, scaled by 2^-e (exact), zero padding column (ld ldx)
+                for (int k = threadIdx.x; k < ldx * np; k += blockDim.x) {
+                    const int c = k / ldx, i = k - c * ldx;
+                    double a = 0.0;
+                    if (c < nt && i < mt) a = ldexp((double)(g.wide ? A[(size_t)c * g.n + i] : A[(size_t)i * g.n + c]), -e);
+                    Ad[k] = a;
+                }
+                __syncthreads();
+                // W = A_t V (FP64); extra full-basis columns zero
+                gemm64<false, double>(Ad, ldx, V64, ldv, W64, ldw, mt, np, np, 1.0, 0.0, stage);
+                for (int k = threadIdx.x; k < ldw * (g.ncp - np); k += blockDim.x) W64[(size_t)np * ldw + k] = 0.0;
+                // G = W^T W in shared memory
+                gemm64<true, double>(W64, ldw, W64, ldw, G, np, np, np, mt, 1.0, 0.0, stage);
+                const double tol = p.tol > 0 ? (double)(float)p.tol : (double)(10.0f * Lim<float>::eps());
+                const int s2 = gram_sweeps(G, D, np, tol, p.max_sweeps, sched, pq, cs, &s_any);
+                if (s2 > p.max_sweeps) {
+                    ns += p.max_sweeps;
+                    st = JB_ST_NOT_CONVERGED;
+                } else {
+                    ns += s2;
+                    // W <- W + W D, V <- V + V D (staging in G, no longer needed)
+                    stage = G;
+                    gemm64<false, float>(W64, ldw, D, np, Ad, ldx, mt, np, np, 1.0, 0.0, stage);
+                    for (int k = threadIdx.x; k < mt * np; k += blockDim.x) {
+                        const int c = k / mt, i = k - c * mt;
+                        W64[(size_t)c * ldw + i] += Ad[(size_t)c * ldx + i];
+                    }
+                    gemm64<false, float>(V64, ldv, D, np, X, ldx, np, np, np, 1.0, 0.0, stage);
+                    for (int k = threadIdx.x; k < np * np; k += blockDim.x) {
+                        const int c = k / np, i = k - c * np;
+                        V64[(size_t)c * ldv + i] += X[(size_t)c * ldx + i];
+                    }
+                    __syncthreads();
+                    float *U = p.U ? (float *)p.U + d.u_off : nullptr;
+                    float *Vh = p.Vh ? (float *)p.Vh + d.v_off : nullptr;
+                    st = epilogue<double, float>(W64, V64, g, e, U, (float *)p.S + d.s_off, Vh, ax);
+                }
+            }
+        }
+        if (threadIdx.x == 0) {
+            if (p.status) p.status[mat] = st;
+            if (p.sweeps) p.sweeps[mat] = ns;
+        }
+        __syncthreads();
+    }
+}
+
+
 // ---------------------------------------------------------------------------
 // Warm start preparation (one CTA per matrix): V0 (the network's guess,
 // row-major n x n, columns = start vectors) -> Householder QR, column signs
@@ -698,6 +861,9 @@ static int sm_count() {
 // Launch plan for one batch (sized by its largest tall shape).
 struct Plan {
     bool reg;             // register-tile path
+    bool big;             // large-tile FP32 kernel (+ round-robin FP64 phase when mixed)
+    size_t gram_stride;   // big + mixed: per-CTA area of the Gram FP64 kernel (0: round-robin FP64 phase)
+    size_t gram_smem;
     // round-robin path
     Dims d;
     size_t aux, region, smem;
@@ -732,6 +898,17 @@ static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags
         pl.smem64 = aux_bytes(pl.d64) + pl.reg64;
         if (pl.smem64 > kSmemLimit || pl.smem32 > kSmemLimit) pl.reg = false;
     }
+    if (!pl.reg && elem == 4 && !(flags & JB_ROUND_ROBIN) && r32.R <= kMaxRL && r32.RV <= kMaxRVL &&
+        r32.nb / 2 <= kT32L / 32) {
+        pl.d32 = raux_dims(r32);
+        pl.reg32 = rregion_bytes(r32, 4);
+        pl.smem32 = aux_bytes(pl.d32) + pl.reg32;
+        pl.big = pl.smem32 <= kSmemLimit;
+        if (pl.big && precision == JB_PREC_MIXED) {
+            pl.gram_smem = aux_bytes(pl.d) + gram64_smem(pl.d.np, pl.d.mt);
+            if (pl.gram_smem <= kSmemLimit && pl.d.np <= 256) pl.gram_stride = gram64_region(pl.d) + 256;
+        }
+    }
     return pl;
 }
 
@@ -739,7 +916,12 @@ static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags
 // round-robin path, per-CTA global work areas.
 static size_t base_bytes(const Plan &pl, int64_t count) {
     size_t bytes = kCounterBytes;
-    if (!pl.reg && pl.global_region) {
+    if (pl.gram_stride) {
+        const int sms = sm_count();
+        int64_t grid = sms > 0 ? sms : 148;
+        if (grid > count) grid = count;
+        bytes += (size_t)grid * pl.gram_stride;
+    } else if (!pl.reg && pl.global_region) {
         const int sms = sm_count();
         int64_t grid = sms > 0 ? sms : 148;
         if (grid > count) grid = count;
@@ -803,7 +985,7 @@ static int launch_reg(Params &p, const Plan &pl, int elem, int precision, unsign
     int64_t grid;
     int rc;
     if (elem == 4) {
-        auto k1 = mixed ? rb32_kernel<true> : rb32_kernel<false>;
+        auto k1 = mixed ? rb32_kernel_t<true, kT32, kMaxR, kMaxRV> : rb32_kernel_t<false, kT32, kMaxR, kMaxRV>;
         if ((rc = occupancy_grid(k1, kT32, pl.smem32, p.count, grid))) return rc;
         p.maxd = pl.d32;
         p.region_cap = pl.reg32;
@@ -825,11 +1007,57 @@ static int launch_reg(Params &p, const Plan &pl, int elem, int precision, unsign
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
 }
 
+// Large tiles (FP32 input): the 512-thread register kernel for the FP32
+// sweeps; with mixed precision the round-robin kernel then runs the FP64
+// phase from the FP32 V it left in x32.
+static int launch_big(Params &p, const Plan &pl, int precision, unsigned char *ws, size_t ws_bytes,
+                      cudaStream_t st) {
+    const bool mixed = precision == JB_PREC_MIXED;
+    p.counter = (int *)ws;
+    if (mixed) {
+        const size_t base = base_bytes(pl, p.count);
+        if (ws_bytes < base) return JB_EWORKSPACE;
+        p.x32 = (float *)(ws + base);
+        p.x_cap = (int64_t)((ws_bytes - base) / 4);
+    }
+    if (cudaMemsetAsync(ws, 0, sizeof(int), st) != cudaSuccess) return JB_ECUDA;
+    auto k1 = mixed ? rb32_kernel_t<true, kT32L, kMaxRL, kMaxRVL> : rb32_kernel_t<false, kT32L, kMaxRL, kMaxRVL>;
+    int64_t grid;
+    int rc;
+    if ((rc = occupancy_grid(k1, kT32L, pl.smem32, p.count, grid))) return rc;
+    p.maxd = pl.d32;
+    p.region_cap = pl.reg32;
+    k1<<<(unsigned)grid, kT32L, pl.smem32, st>>>(p);
+    if (cudaGetLastError() != cudaSuccess) return JB_ECUDA;
+    if (!mixed) return JB_OK;
+    if (!pl.gram_stride) {
+        p.from_x32 = 1;
+        return launch_rr<float, JB_PREC_MIXED>(p, pl, ws, ws_bytes, st);
+    }
+    // FP64 phase on the Gram of W, one CTA per SM, per-CTA global areas
+    if (cudaFuncSetAttribute(gram64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.gram_smem) !=
+        cudaSuccess)
+        return JB_ECUDA;
+    const int sms = sm_count();
+    if (sms <= 0) return JB_ECUDA;
+    int64_t g2 = sms < p.count ? sms : p.count;
+    const int64_t fit = (int64_t)((ws_bytes - kCounterBytes) / pl.gram_stride);
+    if (g2 > fit) g2 = fit;
+    if (g2 < 1) return JB_EWORKSPACE;
+    p.maxd = pl.d;
+    p.gws = ws + kCounterBytes;
+    p.gws_stride = pl.gram_stride;
+    if (cudaMemsetAsync(p.counter, 0, sizeof(int), st) != cudaSuccess) return JB_ECUDA;
+    gram64_kernel<<<(unsigned)g2, kTG, pl.gram_smem, st>>>(p);
+    return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+}
+
 static int launch_any(Params &p, const Plan &pl, int elem, int precision, void *workspace, size_t ws_bytes,
                       cudaStream_t st) {
     unsigned char *ws = (unsigned char *)workspace;
     if (!ws || ws_bytes < kCounterBytes) return JB_EWORKSPACE;
     if (pl.reg) return launch_reg(p, pl, elem, precision, ws, ws_bytes, st);
+    if (pl.big && elem == 4) return launch_big(p, pl, precision, ws, ws_bytes, st);
     if (elem == 8) return launch_rr<double, JB_PREC_NATIVE>(p, pl, ws, ws_bytes, st);
     return precision == JB_PREC_MIXED ? launch_rr<float, JB_PREC_MIXED>(p, pl, ws, ws_bytes, st)
                                       : launch_rr<float, JB_PREC_NATIVE>(p, pl, ws, ws_bytes, st);
@@ -850,7 +1078,7 @@ static size_t uniform_workspace(int32_t m, int32_t n, int64_t count, int32_t ele
     const int prec = elem == 4 ? precision : JB_PREC_NATIVE;
     const Plan pl = make_plan(mt, nt, elem, prec, flags);
     size_t bytes = base_bytes(pl, count);
-    if (pl.reg && prec == JB_PREC_MIXED) bytes += (size_t)count * nt * nt * 4;
+    if ((pl.reg || pl.big) && prec == JB_PREC_MIXED) bytes += (size_t)count * nt * nt * 4;
     return bytes;
 }
 
@@ -941,6 +1169,17 @@ int jb_svd_batched_f64(const double *A, double *U, double *S, double *Vh, int64_
                        int32_t *status, void *workspace, size_t workspace_bytes, void *stream) {
     return batched_common(A, U, S, Vh, batch, m, n, rank, flags, tol, max_sweeps, JB_PREC_NATIVE, sweeps, status,
                           workspace, workspace_bytes, stream, 8);
+}
+
+size_t jb_uneven_workspace_bytes(int32_t max_m, int32_t max_n, int64_t count, int32_t precision,
+                                 int64_t scratch_floats) {
+    if (max_m < 1 || max_n < 1 || count < 0 || scratch_floats < 0) return 0;
+    if (precision != JB_PREC_NATIVE && precision != JB_PREC_MIXED) return 0;
+    const int mt = max_m > max_n ? max_m : max_n, nt = max_m > max_n ? max_n : max_m;
+    const Plan pl = make_plan(mt, nt, 4, precision, 0);
+    size_t bytes = base_bytes(pl, count);
+    if (precision == JB_PREC_MIXED) bytes += (size_t)scratch_floats * 4;
+    return bytes;
 }
 
 int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh, const jb_matrix_desc *descs,

@@ -23,7 +23,7 @@ RC_NAMES = {JB_EINVAL: "invalid argument", JB_ETOOBIG: "shape too large for this
 
 # Exported symbols, in declaration order of include/jacobi_b200.h.
 SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_batched_f32",
-           "jb_svd_batched_f64", "jb_svd_uneven_f32", "jb_gemm_bf16", "jb_gemm_bf16x", "jb_gemm_bf16x_rows",
+           "jb_svd_batched_f64", "jb_uneven_workspace_bytes", "jb_svd_uneven_f32", "jb_gemm_bf16", "jb_gemm_bf16x", "jb_gemm_bf16x_rows",
            "jb_split_bf16",
            "jb_split3_bf16",
            "jb_warm_prep_f32", "jb_svd_warm_f32", "jb_transpose_bf16", "jb_bias_act", "jb_relu_backward",
@@ -55,6 +55,8 @@ def _declare(l):
     l.jb_device_sm_count.argtypes = []
     l.jb_workspace_bytes.restype = SZ
     l.jb_workspace_bytes.argtypes = [I32, I32, I64, I32, I32, I32]
+    l.jb_uneven_workspace_bytes.restype = SZ
+    l.jb_uneven_workspace_bytes.argtypes = [I32, I32, I64, I32, I64]
     l.jb_svd_batched_f32.restype = ctypes.c_int
     l.jb_svd_batched_f32.argtypes = [P, P, P, P, I64, I32, I32, I32, I32, F64, I32, I32, P, P, P, SZ, P]
     l.jb_svd_batched_f64.restype = ctypes.c_int
