@@ -969,6 +969,8 @@ static int launch_rr(Params &p, const Plan &pl, unsigned char *ws, size_t ws_byt
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
 }
 
+static int launch_gram(Params &p, const Plan &pl, unsigned char *ws, size_t ws_bytes, cudaStream_t st);
+
 // elem: 4 (f32 input) or 8 (f64 input).
 static int launch_reg(Params &p, const Plan &pl, int elem, int precision, unsigned char *ws, size_t ws_bytes,
                       cudaStream_t st) {
@@ -1034,7 +1036,12 @@ static int launch_big(Params &p, const Plan &pl, int precision, unsigned char *w
         p.from_x32 = 1;
         return launch_rr<float, JB_PREC_MIXED>(p, pl, ws, ws_bytes, st);
     }
-    // FP64 phase on the Gram of W, one CTA per SM, per-CTA global areas
+    return launch_gram(p, pl, ws, ws_bytes, st);
+}
+
+// FP64 phase on the Gram of W (gram64_kernel), one CTA per SM, per-CTA
+// global areas after the ticket counters.
+static int launch_gram(Params &p, const Plan &pl, unsigned char *ws, size_t ws_bytes, cudaStream_t st) {
     if (cudaFuncSetAttribute(gram64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.gram_smem) !=
         cudaSuccess)
         return JB_ECUDA;
