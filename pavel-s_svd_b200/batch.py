@@ -148,6 +148,104 @@ class UnevenBatch:
         return u, s, vh
 
 
+class StreamedUneven:
+    """Host-to-host solve of an uneven batch with the transfers overlapped
+    with the compute.
+
+    The matrices (in ``pack`` order) are split into ``chunks`` contiguous
+    groups of about equal cost, each with its own UnevenBatch.  Per chunk:
+    the host->device copy of its inputs on one copy stream, its solve on the
+    compute stream once that copy has landed, the device->host copy of its
+    U, S, Vh and status on another copy stream once the solve is done.
+    Chunk i+1's input copy and chunk i-1's output copy overlap chunk i's
+    solve, so a step costs about the compute plus one chunk's transfers
+    instead of compute + all transfers.  Host buffers are the flat ``pack``
+    layouts of the whole batch (pinned for asynchronous copies)."""
+
+    def __init__(self, m, n, device, *, chunks=4, tol=None, max_sweeps=60, precision="mixed"):
+        m = np.asarray(m, np.int64)
+        n = np.asarray(n, np.int64)
+        count = len(m)
+        dev = torch.device(device)
+        if dev.type == "cuda" and dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device, self.count, self.max_sweeps = dev, count, int(max_sweeps)
+        k = np.minimum(m, n)
+        self.a_off, self.a_total = _aligned_offsets(m * n)
+        self.u_off, self.u_total = _aligned_offsets(m * k)
+        self.s_off, self.s_total = _aligned_offsets(k)
+        self.v_off, self.v_total = _aligned_offsets(k * n)
+        mt, nt = np.maximum(m, n), np.minimum(m, n)
+        cost = np.cumsum(nt.astype(np.float64) ** 2 * (7 * mt + 4 * nt))
+        chunks = max(1, min(int(chunks), count))
+        cuts = [0] + [int(np.searchsorted(cost, cost[-1] * c / chunks)) + 1 for c in range(1, chunks)] + [count]
+        cuts = sorted(set(min(max(x, 0), count) for x in cuts))
+        self.ranges = [(lo, hi) for lo, hi in zip(cuts[:-1], cuts[1:]) if hi > lo]
+
+        def span(off, total, lo, hi):
+            return int(off[lo]), int(off[hi]) if hi < count else total
+
+        self.plans, self.dev_in, self.spans = [], [], []
+        for lo, hi in self.ranges:
+            plan = UnevenBatch(m[lo:hi], n[lo:hi], dev, tol=tol, max_sweeps=max_sweeps, precision=precision)
+            a0, a1 = span(self.a_off, self.a_total, lo, hi)
+            self.plans.append(plan)
+            self.dev_in.append(torch.empty(max(a1 - a0, 1), dtype=torch.float32, device=dev))
+            self.spans.append((span(self.a_off, self.a_total, lo, hi), span(self.u_off, self.u_total, lo, hi),
+                               span(self.s_off, self.s_total, lo, hi), span(self.v_off, self.v_total, lo, hi)))
+        self.s_in = torch.cuda.Stream(dev)
+        self.s_comp = torch.cuda.Stream(dev)
+        self.s_out = torch.cuda.Stream(dev)
+        self.host_info = [torch.empty(2, max(hi - lo, 1), dtype=torch.int32).pin_memory() for lo, hi in self.ranges]
+
+    def host_buffers(self):
+        """Pinned host buffers of the whole batch: (input, U, S, Vh)."""
+        mk = lambda size: torch.empty(max(size, 1), dtype=torch.float32).pin_memory()
+        return mk(self.a_total), mk(self.u_total), mk(self.s_total), mk(self.v_total)
+
+    def run(self, host_in, host_u, host_s, host_vh):
+        """Enqueue the overlapped copy-in / solve / copy-out of every chunk;
+        the caller's current stream waits for all of it.  Call check() to
+        synchronise and raise the reference's errors."""
+        main = torch.cuda.current_stream(self.device)
+        for s in (self.s_in, self.s_comp, self.s_out):
+            s.wait_stream(main)
+        landed, solved = [], []
+        for (a, _, _, _), d in zip(self.spans, self.dev_in):
+            with torch.cuda.stream(self.s_in):
+                d[:a[1] - a[0]].copy_(host_in[a[0]:a[1]], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(self.s_in)
+            landed.append(ev)
+        for plan, d, ev in zip(self.plans, self.dev_in, landed):
+            self.s_comp.wait_event(ev)
+            plan.launch(d, stream=self.s_comp)
+            done = torch.cuda.Event()
+            done.record(self.s_comp)
+            solved.append(done)
+        for plan, (_, u, s_, v), ev, info in zip(self.plans, self.spans, solved, self.host_info):
+            self.s_out.wait_event(ev)
+            with torch.cuda.stream(self.s_out):
+                host_u[u[0]:u[1]].copy_(plan.U[:u[1] - u[0]], non_blocking=True)
+                host_s[s_[0]:s_[1]].copy_(plan.S[:s_[1] - s_[0]], non_blocking=True)
+                host_vh[v[0]:v[1]].copy_(plan.Vh[:v[1] - v[0]], non_blocking=True)
+                info[:, :plan.count].copy_(plan.info[:, :plan.count], non_blocking=True)
+        main.wait_stream(self.s_out)
+
+    def check(self):
+        """Synchronise; raise for any failed matrix; return the sweep counts."""
+        self.s_out.synchronize()
+        sweeps = []
+        for plan, info in zip(self.plans, self.host_info):
+            raise_for_status(info[1, :plan.count], self.max_sweeps)
+            sweeps.append(info[0, :plan.count].numpy().copy())
+        return np.concatenate(sweeps) if sweeps else np.zeros(0, np.int32)
+
+    def device_bytes_per_run(self):
+        """Bytes copied host->device and device->host by one run."""
+        return 4 * self.a_total, 4 * (self.u_total + self.s_total + self.v_total) + 8 * self.count
+
+
 def svd_uneven(mats, *, tol=None, max_sweeps=60, precision="mixed", values_only=False):
     """Solve a list of float32 CUDA matrices of different shapes in one launch.
     Returns a list of (U, s, Vh) like svd() of each matrix would."""
