@@ -361,9 +361,9 @@ __device__ void load_stage(const TI *A, const Geo &g, int ld, float *As) {
 
 template <typename T, int B, int MR = kMaxR, int MRV = kMaxRV>
 __device__ int rb_dispatch(const RGeo &r, T *W, T *V, T tol, int max_sweeps, bool confirm, double *red,
-                           bool &conv, T exit_ratio = T(0)) {
+                           bool &conv, T exit_ratio = T(0), double *colnorm = nullptr) {
     return rb_sweeps<T, B, MR, MRV>(W, r.ldw, V, r.ldv, r.nb, r.live, tol, max_sweeps, confirm, red, conv,
-                                    exit_ratio);
+                                    exit_ratio, colnorm);
 }
 
 __device__ inline Geo reg_geo(const jb_matrix_desc &d, const RGeo &r) {
@@ -505,7 +505,7 @@ __global__ void __launch_bounds__(THREADS) rb32_kernel_t(Params p) {
                                         : (p.tol > 0 ? (float)p.tol : 10.0f * Lim<float>::eps());
                 bool conv;
                 ns = rb_dispatch<float, kB32, MR, MRV>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true,
-                                                       ax.red, conv, MIXED ? kMixedExitRatio : 0.0f);
+                                                       ax.red, conv, MIXED ? kMixedExitRatio : 0.0f, ax.sig);
                 if (MIXED) {
                     float *x = p.x32 + d.x_off;
                     const int nt = g.nt;
@@ -610,7 +610,7 @@ __global__ void __launch_bounds__(kT64) rb64_kernel(Params p) {
                 const double tol = MIXED ? (p.tol > 0 ? (double)(float)p.tol : (double)(10.0f * Lim<float>::eps()))
                                          : (p.tol > 0 ? p.tol : 10.0 * Lim<double>::eps());
                 bool conv;
-                ns += rb_dispatch<double, kB64>(r, W, V, tol, p.max_sweeps, true, ax.red, conv);
+                ns += rb_dispatch<double, kB64>(r, W, V, tol, p.max_sweeps, true, ax.red, conv, 0.0, ax.sig);
                 if (!conv) {
                     st = JB_ST_NOT_CONVERGED;
                 } else {

@@ -311,6 +311,58 @@ __device__ __forceinline__ void tile_io(Tile<T, B, R, RV> &t, T *W, int ldw, T *
     }
 }
 
+// The measuring sweep as one Gram pass: every pair ratio |w_p^T w_q| /
+// (||w_p|| ||w_q||) of the current W (shared memory, column-major, ldw = 32 nr
+// rows per lane) tested as rot_params tests it, without rotating.  A sweep
+// with no rotation measures exactly these ratios (primitives.py:334-339), so
+// "no active pair" here is the reference's convergence test (:352-353) at a
+// fraction of a sweep's latency: 4 x 4 tiles of W^T W per warp, lanes over
+// rows, one warp reduce-scatter per tile.  colnorm: npb doubles of shared
+// memory.  All threads of the CTA call it; returns nonzero if a pair is active.
+template <typename T>
+__device__ int gram_check(const T *W, int ldw, int npb, int nr, T tol2, T floor_, double *colnorm) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = nwarps();
+    for (int c = warp; c < npb; c += nw) {
+        const T *w = W + (size_t)c * ldw + lane;
+        T a = 0;
+        for (int r = 0; r < nr; ++r) a = dfma(w[32 * r], w[32 * r], a);
+        a = warp_sum(a);
+        if (lane == 0) colnorm[c] = (double)a;
+    }
+    __syncthreads();
+    const int nbk = npb >> 2;                      // 4-column blocks
+    const int ntile = nbk * (nbk + 1) / 2;         // blocks bp <= bq
+    int active = 0;
+    for (int t = warp; t < ntile; t += nw) {
+        int bp = 0, rem = t;                       // t -> (bp, bq), row-major upper triangle
+        while (rem >= nbk - bp) { rem -= nbk - bp; ++bp; }
+        const int bq = bp + rem;
+        T acc[16];
+#pragma unroll
+        for (int v = 0; v < 16; ++v) acc[v] = 0;
+        for (int r = 0; r < nr; ++r) {
+            T x[4], y[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                x[k] = W[(size_t)(4 * bp + k) * ldw + lane + 32 * r];
+                y[k] = W[(size_t)(4 * bq + k) * ldw + lane + 32 * r];
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) acc[4 * a + b] = dfma(x[a], y[b], acc[4 * a + b]);
+        }
+        reduce_scatter<T, 16>(acc, lane);
+        const int v = lane >> 1, a = v >> 2, b = v & 3;
+        const int p = 4 * bp + a, q = 4 * bq + b;
+        if (p < q) {
+            const T app = (T)colnorm[p], aqq = (T)colnorm[q], apq = acc[0];
+            if (apq * apq > tol2 * app * aqq && fmin(app, aqq) > floor_) active = 1;
+        }
+    }
+    return __syncthreads_or(active);
+}
+
 // Sweeps over W/V in shared memory until off <= tol or max_sweeps.  nb blocks
 // (even), of which the first `live` hold real columns; blocks >= live are
 // zero and their pairs are skipped.  All threads of the CTA call this; warps
@@ -324,9 +376,11 @@ __device__ __forceinline__ void tile_io(Tile<T, B, R, RV> &t, T *W, int ldw, T *
 // first sweep whose largest ratio is <= exit_ratio -- the rotations of that
 // sweep leave ~exit_ratio^2, below what FP32 sweeps resolve, and the FP64
 // phase that follows takes it from there (converged is then set).
+// colnorm (npb doubles of shared memory, or NULL): when given, a measuring
+// sweep is replaced by gram_check.
 template <typename T, int B, int R, int RV>
 __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, int max_sweeps, bool confirm,
-                         double *red, bool &converged, T exit_ratio = T(0)) {
+                         double *red, bool &converged, T exit_ratio = T(0), double *colnorm = nullptr) {
     const int nr = ldw >> 5, nv = ldv >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nw = nwarps();
@@ -361,6 +415,15 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
         double gm = red[0];
         for (int w = 1; w < nw; ++w) gm = fmax(gm, red[w]);
         const T floor_ = Lim<T>::eps() * Lim<T>::eps() * (T)gm;
+        if (measure && colnorm) {
+            // the measuring sweep as one Gram pass over the current W
+            if (act) tile_io(t, W, ldw, V, ldv, X, Y, lane, true, nr, nv);
+            __syncthreads();
+            if (!gram_check<T>(W, ldw, nb * B, nr, tol2, floor_, colnorm)) { converged = true; break; }
+            measure = false;
+            measure_allowed = false;  // a failed confirmation: rotate from now on
+            continue;
+        }
         const bool rotate = !measure;
         int fl = 0;
         if (act && (X < live || Y < live)) {
