@@ -264,6 +264,7 @@ __global__ void __launch_bounds__(1024, 1) batched_kernel(Params p) {
 // Register-tile path (matrices up to 128 x 64 in their tall view).
 // ---------------------------------------------------------------------------
 constexpr int kB32 = 4;   // block width of the FP32 sweeps (8 warps for 64 columns)
+constexpr int kB32L = 4;  // block width of the large-tile FP32 kernel (16 warps for 128 columns)
 // Mixed precision: the FP32 phase ends after the first sweep whose largest
 // pair ratio is <= this (quadratic convergence leaves ~1e-4 after it); the
 // FP64 phase then converges to the requested tolerance in one rotating sweep
@@ -450,7 +451,7 @@ __device__ double polar_step(double *V, int n, int ld, double *VT, double *H, do
 // and the register tile (rows per lane of W and V); rb32_kernel is the
 // 256-thread form for matrices up to 128 x 64, rb32_large_kernel the
 // 512-thread form for one matrix up to 256 x 128 per CTA.
-template <bool MIXED, int THREADS, int MR, int MRV>
+template <bool MIXED, int THREADS, int BW, int MR, int MRV>
 __global__ void __launch_bounds__(THREADS) rb32_kernel_t(Params p) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_idx;
@@ -465,10 +466,10 @@ __global__ void __launch_bounds__(THREADS) rb32_kernel_t(Params p) {
         if (threadIdx.x < 4) ax.flag[threadIdx.x] = 0;
         __syncthreads();
         int ns = 0, st = JB_ST_OK;
-        if (!rdesc_fits(d, kB32, 4, p, MIXED, MR, MRV)) {
+        if (!rdesc_fits(d, BW, 4, p, MIXED, MR, MRV)) {
             st = JB_ST_BAD_DESC;
         } else {
-            const RGeo r = rgeo(d.m > d.n ? d.m : d.n, d.m > d.n ? d.n : d.m, kB32, d.flags);
+            const RGeo r = rgeo(d.m > d.n ? d.m : d.n, d.m > d.n ? d.n : d.m, BW, d.flags);
             const Geo g = reg_geo(d, r);
             const float *A = (const float *)p.A + d.a_off;
             float *W = (float *)region;
@@ -504,7 +505,7 @@ __global__ void __launch_bounds__(THREADS) rb32_kernel_t(Params p) {
                 const float tol = MIXED ? (p.tol32 > 0 ? (float)p.tol32 : 10.0f * Lim<float>::eps())
                                         : (p.tol > 0 ? (float)p.tol : 10.0f * Lim<float>::eps());
                 bool conv;
-                ns = rb_dispatch<float, kB32, MR, MRV>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true,
+                ns = rb_dispatch<float, BW, MR, MRV>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true,
                                                        ax.red, conv, MIXED ? kMixedExitRatio : 0.0f, ax.sig);
                 if (MIXED) {
                     float *x = p.x32 + d.x_off;
@@ -898,10 +899,11 @@ static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags
         pl.smem64 = aux_bytes(pl.d64) + pl.reg64;
         if (pl.smem64 > kSmemLimit || pl.smem32 > kSmemLimit) pl.reg = false;
     }
-    if (!pl.reg && elem == 4 && !(flags & JB_ROUND_ROBIN) && r32.R <= kMaxRL && r32.RV <= kMaxRVL &&
-        r32.nb / 2 <= kT32L / 32) {
-        pl.d32 = raux_dims(r32);
-        pl.reg32 = rregion_bytes(r32, 4);
+    const RGeo r32l = rgeo(max_mt, max_nt, kB32L, flags);
+    if (!pl.reg && elem == 4 && !(flags & JB_ROUND_ROBIN) && r32l.R <= kMaxRL && r32l.RV <= kMaxRVL &&
+        r32l.nb / 2 <= kT32L / 32) {
+        pl.d32 = raux_dims(r32l);
+        pl.reg32 = rregion_bytes(r32l, 4);
         pl.smem32 = aux_bytes(pl.d32) + pl.reg32;
         pl.big = pl.smem32 <= kSmemLimit;
         if (pl.big && precision == JB_PREC_MIXED) {
@@ -987,7 +989,7 @@ static int launch_reg(Params &p, const Plan &pl, int elem, int precision, unsign
     int64_t grid;
     int rc;
     if (elem == 4) {
-        auto k1 = mixed ? rb32_kernel_t<true, kT32, kMaxR, kMaxRV> : rb32_kernel_t<false, kT32, kMaxR, kMaxRV>;
+        auto k1 = mixed ? rb32_kernel_t<true, kT32, kB32, kMaxR, kMaxRV> : rb32_kernel_t<false, kT32, kB32, kMaxR, kMaxRV>;
         if ((rc = occupancy_grid(k1, kT32, pl.smem32, p.count, grid))) return rc;
         p.maxd = pl.d32;
         p.region_cap = pl.reg32;
@@ -1023,7 +1025,8 @@ static int launch_big(Params &p, const Plan &pl, int precision, unsigned char *w
         p.x_cap = (int64_t)((ws_bytes - base) / 4);
     }
     if (cudaMemsetAsync(ws, 0, sizeof(int), st) != cudaSuccess) return JB_ECUDA;
-    auto k1 = mixed ? rb32_kernel_t<true, kT32L, kMaxRL, kMaxRVL> : rb32_kernel_t<false, kT32L, kMaxRL, kMaxRVL>;
+    auto k1 = mixed ? rb32_kernel_t<true, kT32L, kB32L, kMaxRL, kMaxRVL>
+                    : rb32_kernel_t<false, kT32L, kB32L, kMaxRL, kMaxRVL>;
     int64_t grid;
     int rc;
     if ((rc = occupancy_grid(k1, kT32L, pl.smem32, p.count, grid))) return rc;
