@@ -47,7 +47,7 @@ COUNT = 8192
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one solve of
 # this workload, rb32_kernel + rb64_kernel, from one ncu --set full capture
 # of `bench.py --steps 1 --warmup 3 --no-cpu-baseline`.
-MEASURED_TRAFFIC_PER_SOLVE = 318.05e6
+MEASURED_TRAFFIC_PER_SOLVE = 313.8e6
 
 
 def workload_config(n_gpus):
