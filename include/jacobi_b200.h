@@ -287,6 +287,25 @@ JB_API int jb_block_finish(const float *Wt, const float *Vt, float *U, float *S,
                            int32_t *perm, int64_t m, int64_t n, int32_t rank, int32_t e,
                            int32_t cut_width, void *stream);
 
+/* ---- symmetric eigen-solver ----------------------------------------------
+ * Batched two-sided cyclic Jacobi for real symmetric n x n matrices (n <=
+ * 255): svdbench/standalone/primitives.py:370-427 (jacobi_eigh, the syevj
+ * structure) for real dtypes.  H: batch x n x n row-major (symmetrised as
+ * (H + H^T) / 2).  W: batch x n eigenvalues ascending; V: batch x n x n
+ * row-major, column j the eigenvector of W[j].  tol <= 0 selects 10 eps
+ * of the dtype; a pair is active when |g_pq| > tol max|G|.  sweeps/status
+ * (device int32, batch each; status JB_ST_OK or JB_ST_NOT_CONVERGED).
+ * Computed in FP64 for both dtypes.  Workspace: jb_eigh_workspace_bytes
+ * (0 when G and V fit in shared memory, n <= 118; above that V, and beyond
+ * n = 166 also G, live in the workspace). */
+JB_API size_t jb_eigh_workspace_bytes(int32_t n, int64_t batch);
+JB_API int jb_eigh_f32(const float *H, float *W, float *V, int32_t *sweeps, int32_t *status,
+                       int64_t batch, int32_t n, double tol, int32_t max_sweeps,
+                       void *workspace, size_t workspace_bytes, void *stream);
+JB_API int jb_eigh_f64(const double *H, double *W, double *V, int32_t *sweeps, int32_t *status,
+                       int64_t batch, int32_t n, double tol, int32_t max_sweeps,
+                       void *workspace, size_t workspace_bytes, void *stream);
+
 /* Size of the fixed device scratch array of jb_svd_batched_f32_noalloc. */
 #define JB_NOALLOC_SCRATCH_BYTES (16u << 20)
 

@@ -11,6 +11,7 @@ exactly like the PyTorch original:
 
   round_robin            svdbench/standalone/primitives.py:309-313
   jacobi_svd             svdbench/standalone/primitives.py:316-367
+  jacobi_eigh            svdbench/standalone/primitives.py:370-427 (real dtypes)
   complete_null_columns  svdbench/standalone/primitives.py:430-455
   complete_basis         svdbench/standalone/primitives.py:458-467
   svd                    svdbench/standalone/solvers.py:264-310 ('jacobi' only)
@@ -24,7 +25,7 @@ from __future__ import annotations
 
 import numpy as np
 
-__all__ = ["round_robin", "jacobi_svd", "complete_null_columns", "complete_basis",
+__all__ = ["round_robin", "jacobi_svd", "jacobi_eigh", "complete_null_columns", "complete_basis",
            "svd", "raw", "reference", "validate", "eps"]
 
 
@@ -267,3 +268,61 @@ def validate(a, result, refs):
         values = [r[key] for r in rows if r[key] is not None]
         worst[key] = (all(values) if isinstance(values[0], bool) else max(values)) if values else None
     return {"worst": worst, "per_matrix": rows}
+
+
+def jacobi_eigh(H, tol=None, max_sweeps=30):
+    """Two-sided cyclic Jacobi of real symmetric H (b, n, n): w ascending, V,
+    sweeps.  Restates primitives.py:370-427 for real input, in the input's
+    dtype, batched in lock-step: zero-padding to even n (:384-386), tol =
+    10 eps (:388), per round the scale max|G| (:395), active pairs
+    |g_pq| > tol scale (:396), off = max |g_pq| / scale (:397), the rotation
+    (:398-405), G <- G J then G <- J^T G (:407-414), V <- V J (:410-411),
+    convergence after the sweep when off <= tol (:415-416)."""
+    H = np.asarray(H)
+    b, n, _ = H.shape
+    padded = n % 2 == 1
+    G = H.copy()
+    if padded:
+        Z = np.zeros((b, n + 1, n + 1), H.dtype)
+        Z[:, :n, :n] = G
+        G = Z
+        n += 1
+    V = np.broadcast_to(np.eye(n, dtype=G.dtype), (b, n, n)).copy()
+    tol = tol or 10 * eps(H.dtype)
+    bi = np.arange(b)[:, None]
+    sched = [(np.array([p for p, _ in prs]), np.array([q for _, q in prs])) for prs in round_robin(n)]
+    off = np.inf
+    sweeps = 0
+    for sweeps in range(1, max_sweeps + 1):
+        off = 0.0
+        for P, Q in sched:
+            gpp, gqq, gpq = G[bi, P, P], G[bi, Q, Q], G[bi, P, Q]
+            a = np.abs(gpq)
+            scale = np.broadcast_to(np.abs(G).max(axis=(-2, -1))[:, None], a.shape)
+            active = a > tol * scale
+            off = max(off, float((a / np.maximum(scale, np.finfo(scale.dtype).tiny)).max()))
+            a_safe = np.where(active, a, 1)
+            tau = (gqq - gpp) / (2 * a_safe)
+            t = np.sign(tau) / (np.abs(tau) + np.hypot(tau, 1))
+            t = np.where(tau == 0, 1, t)
+            c = 1 / np.sqrt(1 + t * t)
+            s = t * c * (gpq / a_safe)
+            c = np.where(active, c, 1).astype(G.dtype)
+            s = np.where(active, s, 0).astype(G.dtype)
+            cc, ss = c[:, None, :], s[:, None, :]
+            gp, gq = G[:, :, P].copy(), G[:, :, Q].copy()
+            G[:, :, P], G[:, :, Q] = cc * gp - ss * gq, ss * gp + cc * gq
+            vp, vq = V[:, :, P].copy(), V[:, :, Q].copy()
+            V[:, :, P], V[:, :, Q] = cc * vp - ss * vq, ss * vp + cc * vq
+            cc, ss = c[:, :, None], s[:, :, None]
+            rp, rq = G[:, P, :].copy(), G[:, Q, :].copy()
+            G[:, P, :], G[:, Q, :] = cc * rp - ss * rq, ss * rp + cc * rq
+        if off <= tol:
+            break
+    if off > tol:
+        raise RuntimeError(f"Hermitian Jacobi did not converge in {max_sweeps} sweeps")
+    w = np.diagonal(G, axis1=-2, axis2=-1).copy()
+    if padded:
+        w, V = w[:, :-1], V[:, :-1, :-1]
+    order = np.argsort(w, axis=-1, kind="stable")
+    return np.take_along_axis(w, order, 1), np.take_along_axis(V, order[:, None, :], 2), sweeps

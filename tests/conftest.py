@@ -38,6 +38,13 @@ def golden():
 
 
 @pytest.fixture(scope="session")
+def golden_eigh():
+    """The reference's jacobi_eigh outputs (h, w, v, sweeps, FP64 truth) by case."""
+    z = np.load(GOLDEN, allow_pickle=False)
+    return {str(n): {k: z[f"eigh_{n}/{k}"] for k in ("h", "w", "v", "sweeps", "truth")} for n in z["_eigh_names"]}
+
+
+@pytest.fixture(scope="session")
 def workloads():
     return importlib.import_module("pavel-s_svd_b200.workloads")
 

@@ -72,6 +72,25 @@ def cases(make_matrix):
     return out
 
 
+def eigh_cases(make_matrix):
+    """(name, batch of symmetric matrices): Grams of the reference's matrix
+    families (what gram_jacobi feeds jacobi_eigh, solvers.py:99-120), an odd
+    size (padding), an indefinite matrix and a diagonal one."""
+    out = []
+    for dt in ("float32", "float64"):
+        a = make_matrix(dict(m=24, n=10, batch=3, dtype=dt, family="gaussian"))
+        out.append((f"gram_gauss_{dt}_10", np.ascontiguousarray(np.swapaxes(a, -1, -2) @ a)))
+        a = make_matrix(dict(m=20, n=7, batch=2, dtype=dt, family="gaussian"))
+        out.append((f"gram_gauss_{dt}_7", np.ascontiguousarray(np.swapaxes(a, -1, -2) @ a)))
+    a = make_matrix(dict(m=40, n=16, dtype="float64", family="geometric", condition=1e4))
+    out.append(("gram_geometric_16", np.ascontiguousarray((a.T @ a)[None])))
+    rng = np.random.default_rng(31)
+    x = rng.standard_normal((2, 12, 12))
+    out.append(("indefinite_12", np.ascontiguousarray(x + np.swapaxes(x, -1, -2))))
+    out.append(("diagonal_6", np.diag([3.0, -1.0, 2.0, 0.0, 5.0, 1.0])[None].copy()))
+    return out
+
+
 def main():
     sys.path.insert(0, str(REF))
     import torch
@@ -98,6 +117,20 @@ def main():
         names.append(name)
         print(f"{name:28s} {str(a.shape):18s} {a.dtype}  sweeps={info['jacobi_sweeps']}")
     blob["_names"] = np.array(names)
+    # jacobi_eigh (primitives.py:370-427): symmetric inputs, the reference's
+    # w (ascending), V and sweeps
+    from svdbench.standalone import primitives as P
+    enames = []
+    for name, h in eigh_cases(make_matrix):
+        w, v, sw = P.jacobi_eigh(torch.from_numpy(h.copy()))
+        blob[f"eigh_{name}/h"] = h
+        blob[f"eigh_{name}/w"] = w.numpy()
+        blob[f"eigh_{name}/v"] = v.numpy()
+        blob[f"eigh_{name}/sweeps"] = np.array(sw)
+        blob[f"eigh_{name}/truth"] = np.stack([np.linalg.eigvalsh(x.astype(np.float64)) for x in h])
+        enames.append(name)
+        print(f"eigh {name:22s} {str(h.shape):14s} {h.dtype}  sweeps={sw}")
+    blob["_eigh_names"] = np.array(enames)
     np.savez_compressed(HERE / "reference_jacobi.npz", **blob)
     print("wrote", HERE / "reference_jacobi.npz")
 

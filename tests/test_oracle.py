@@ -143,3 +143,34 @@ def test_oracle_threads_do_not_change_results(workloads):
     r4 = C.svd_batched(x, threads=4)
     for p, q in zip(r1, r4):
         np.testing.assert_array_equal(p, q)
+
+
+def test_eigh_oracle_matches_reference(golden_eigh):
+    """The NumPy restatement of jacobi_eigh (primitives.py:370-427) against
+    the reference's own w, V and sweeps: same arithmetic dtype, so the sweep
+    counts agree and w to rounding; V column by column up to sign."""
+    for name, g in golden_eigh.items():
+        h = g["h"]
+        w, v, sw = O.jacobi_eigh(h)
+        wr, vr = g["w"], g["v"]
+        scale = float(np.abs(wr).max())
+        tol = 50 * np.finfo(h.dtype).eps
+        assert float(np.abs(w - wr).max()) <= tol * scale, name
+        assert abs(int(sw) - int(g["sweeps"])) <= 1, name
+        for b in range(h.shape[0]):
+            for j in range(h.shape[-1]):
+                gap = min([abs(wr[b, j] - wr[b, i]) for i in range(h.shape[-1]) if i != j] or [np.inf])
+                if gap <= 1e-3 * scale:
+                    continue
+                x, y = v[b][:, j], vr[b][:, j]
+                assert min(np.abs(x - y).max(), np.abs(x + y).max()) <= 1e3 * np.finfo(h.dtype).eps, name
+        # and against FP64 truth
+        truth = g["truth"]
+        assert float(np.abs(w - truth).max()) <= 10 * np.finfo(h.dtype).eps * scale * h.shape[-1], name
+
+
+def test_eigh_oracle_raises_like_reference():
+    h = np.random.default_rng(3).standard_normal((1, 9, 9))
+    h = h + h.transpose(0, 2, 1)
+    with pytest.raises(RuntimeError, match="did not converge in 1 sweeps"):
+        O.jacobi_eigh(h, max_sweeps=1)
