@@ -34,7 +34,7 @@ REFERENCE_ALGORITHMS = (
     'gram_jacobi', 'gram_dc', 'polar_qdwh', 'polar_newton_schulz',
     'polar_halley', 'polar_polynomial', 'randomized', 'subspace', 'block_krylov', 'lanczos',
 )  # svdbench/standalone/solvers.py:7-11
-ALGORITHMS = ('jacobi', 'block_jacobi')
+ALGORITHMS = ('jacobi', 'block_jacobi', 'gram_jacobi')
 PRECISIONS = ('mixed', 'fp32')
 ORDERINGS = ('block', 'round_robin')
 
@@ -143,6 +143,8 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
     rank, precision = _validate(a, algorithm, full_matrices, opts)
     if algorithm == 'block_jacobi':
         return _block_svd(a, full_matrices, values_only, return_info, rank, opts)
+    if algorithm == 'gram_jacobi':
+        return _gram_svd(a, full_matrices, values_only, return_info, rank, opts)
     max_sweeps = opts.get('max_sweeps', 60)
     tol = opts.get('tol')
     shape = a.shape[:-2]
@@ -177,6 +179,88 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
         result = (None if values_only else u.reshape(*shape, *u.shape[-2:]),
                   s.reshape(*shape, rank),
                   None if values_only else vh.reshape(*shape, *vh.shape[-2:]))
+    return (*result, stats) if return_info else result
+
+
+def _complete_null_columns(u, keep):
+    """Replace the columns of u (b, m, n) not in keep by unit vectors
+    orthogonal to the kept ones: per missing column, the coordinate vector of
+    largest leftover leverage 1 - sum |u|^2, projected out twice, normalised
+    (primitives.py:430-455, same order and the same failure)."""
+    if bool(keep.all()):
+        return u
+    u = torch.where(keep[:, None, :], u, torch.zeros_like(u))
+    b, m, n = u.shape
+    rows = torch.arange(b, device=u.device)
+    tiny = torch.finfo(u.dtype).eps * 10
+    for j in range(n):
+        missing = ~keep[:, j]
+        if not bool(missing.any()):
+            continue
+        lev = 1 - (u * u).sum(-1)
+        v = torch.zeros(b, m, 1, dtype=u.dtype, device=u.device)
+        v[rows, lev.argmax(-1), 0] = 1
+        for _ in range(2):
+            v = v - u @ (u.transpose(1, 2) @ v)
+        length = (v * v).sum(-2, keepdim=True).sqrt()
+        if bool((length[missing] < tiny).any()):
+            raise RuntimeError("null-space completion failed: supplied live columns are not independent")
+        v = v / length.clamp_min(torch.finfo(u.dtype).tiny)
+        u[:, :, j] = torch.where(missing[:, None], v[:, :, 0], u[:, :, j])
+    return u
+
+
+def _gram_svd(a, full_matrices, values_only, return_info, rank, opts):
+    """gram_jacobi (solvers.py:99-120 with the 'jacobi_eigh' branch): G = A^T A
+    (symmetrised), its eigen-decomposition by the B200 jacobi_eigh, sigma =
+    sqrt of the eigenvalues above eps * n * lambda_1 (others 0), U = A V /
+    sigma with null completion.  The products A^T A and A V are plain library
+    GEMMs in the input dtype, as the reference's matmuls; wide input is
+    solved through its transpose (:225-227), the input scaled by a power of
+    two (exact) before the squares."""
+    from .eigh import jacobi_eigh
+    m, n = a.shape[-2:]
+    shape = a.shape[:-2]
+    with torch.no_grad(), torch.cuda.device(a.device):
+        x = a.detach().reshape(-1, m, n)
+        if not bool(torch.isfinite(x).all()):
+            raise ValueError('input contains NaN or infinity')
+        wide = m < n
+        if wide:
+            x = x.transpose(1, 2)
+        amax = x.abs().amax((-2, -1), keepdim=True)
+        e = torch.where(amax > 0, torch.frexp(amax)[1], torch.zeros_like(amax, dtype=torch.int32))
+        scale = torch.ldexp(torch.ones_like(amax), e)
+        xs = x / scale
+        g = xs.transpose(1, 2) @ xs
+        g = (g + g.transpose(1, 2)) / 2
+        w, v, it = jacobi_eigh(g, max_sweeps=opts.get('max_sweeps', 60))
+        w, v = w.flip(-1), v.flip(-1)
+        nt = xs.shape[-1]
+        cut = torch.finfo(a.dtype).eps * nt * w[:, :1].clamp_min(0)
+        keep = w > cut
+        sv = torch.where(keep, w.clamp_min(0).sqrt(), torch.zeros_like(w))
+        u = (xs @ v) / torch.where(keep, sv, torch.ones_like(sv))[:, None, :]
+        u = _complete_null_columns(u, keep)
+        sv = sv * scale[:, 0, :]
+        if wide:
+            u, v = v, u
+        if full_matrices:
+            u = _complete_null_columns(torch.cat([u, torch.zeros(u.shape[0], m, m - u.shape[-1], dtype=u.dtype,
+                                                                 device=u.device)], -1),
+                                       torch.arange(m, device=u.device)[None, :].expand(u.shape[0], m) < u.shape[-1])
+            v = _complete_null_columns(torch.cat([v, torch.zeros(v.shape[0], n, n - v.shape[-1], dtype=v.dtype,
+                                                                 device=v.device)], -1),
+                                       torch.arange(n, device=v.device)[None, :].expand(v.shape[0], n) < v.shape[-1])
+        else:
+            u, sv, v = u[:, :, :rank], sv[:, :rank], v[:, :, :rank]
+        if not all(bool(torch.isfinite(t).all()) for t in (u, sv, v)):
+            raise RuntimeError('standalone solver produced nonfinite output')
+        result = (None if values_only else u.reshape(*shape, *u.shape[-2:]), sv.reshape(*shape, sv.shape[-1]),
+                  None if values_only else v.transpose(1, 2).reshape(*shape, v.shape[-1], v.shape[-2]))
+    stats = {'algorithm': 'gram_jacobi', 'vendor_factorizations': 0, 'converged': True, 'eigen_sweeps': it,
+             'gram_discarded_values': int((~keep).sum()),
+             'implementation': 'B200 sm_100a two-sided Jacobi (jacobi_eigh) on the Gram'}
     return (*result, stats) if return_info else result
 
 

@@ -67,3 +67,35 @@ def test_eigh_contract(E):
         E.jacobi_eigh(torch.randn(2, 4, 4))
     w, v, sw = E.jacobi_eigh(torch.diag(torch.tensor([3.0, -1.0, 2.0])).cuda()[None])
     assert w.cpu().tolist() == [[-1.0, 2.0, 3.0]] and sw == 1
+
+
+def test_gram_jacobi_drop_in():
+    """svd(a, 'gram_jacobi') (solvers.py:99-120): the Gram route's absolute
+    accuracy (sigma errors ~ eps ||A||^2 / sigma), U orthonormal with null
+    completion for a rank-deficient input, wide input, full_matrices and
+    values_only."""
+    pkg = importlib.import_module("pavel-s_svd_b200")
+    rng = np.random.default_rng(17)
+    for m, n, dt in ((40, 24, np.float32), (24, 40, np.float64), (64, 64, np.float64)):
+        a = rng.standard_normal((3, m, n)).astype(dt)
+        x = torch.from_numpy(a).cuda()
+        u, s, vh, info = pkg.svd(x, 'gram_jacobi', return_info=True)
+        k = min(m, n)
+        sr = np.linalg.svd(a.astype(np.float64), compute_uv=False)
+        e = np.finfo(dt).eps
+        bound = 100 * e * sr[:, :1] ** 2 / sr
+        assert bool((np.abs(s.cpu().numpy() - sr) / sr <= bound).all())
+        rec = (u.double() * s.double()[:, None, :]) @ vh.double()
+        assert float((rec - x.double()).norm() / x.double().norm()) <= 1e4 * e
+        assert info['eigen_sweeps'] >= 1 and info['gram_discarded_values'] == 0
+    # rank 3 of 10 columns: 7 values cut, their U columns completed
+    b = rng.standard_normal((30, 3)) @ rng.standard_normal((3, 10))
+    u, s, vh, info = pkg.svd(torch.from_numpy(b).cuda(), 'gram_jacobi', return_info=True)
+    assert info['gram_discarded_values'] == 7 and float(s[3:].abs().max()) == 0.0
+    uu = u.cpu().numpy()
+    assert float(np.abs(uu.T @ uu - np.eye(10)).max()) <= 1e-10
+    u, s, vh = pkg.svd(torch.from_numpy(b).cuda(), 'gram_jacobi', full_matrices=True)
+    assert u.shape == (30, 30) and vh.shape == (10, 10)
+    assert float(np.abs(u.cpu().numpy().T @ u.cpu().numpy() - np.eye(30)).max()) <= 1e-10
+    u, s, vh = pkg.svd(torch.from_numpy(b).cuda(), 'gram_jacobi', values_only=True)
+    assert u is None and vh is None and s.shape == (10,)
