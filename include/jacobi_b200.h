@@ -57,6 +57,9 @@ extern "C" {
                                    order (primitives.py:309-313) instead of the
                                    register-blocked order; same results within
                                    rounding, slower                             */
+#define JB_BLOCK_WIDTH_8    8   /* uneven batches: FP32 register sweeps with
+                                   8-column blocks (4 warps per 64 columns)
+                                   instead of 4-column blocks                   */
 
 /* ---- arithmetic of the solve ------------------------------------------- */
 #define JB_PREC_NATIVE      0   /* sweeps in the input precision (f32 or f64)   */
@@ -122,7 +125,7 @@ JB_API int jb_svd_batched_f64(const double *A, double *U, double *S, double *Vh,
  * Replaces a harness loop of svd(x, 'jacobi') over matrices of different
  * shapes. */
 JB_API size_t jb_uneven_workspace_bytes(int32_t max_m, int32_t max_n, int64_t count,
-                                        int32_t precision, int64_t scratch_floats);
+                                        int32_t precision, int32_t flags, int64_t scratch_floats);
 
 JB_API int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh,
                       const jb_matrix_desc *descs, const int32_t *order,
@@ -130,6 +133,20 @@ JB_API int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh,
                       double tol, int32_t max_sweeps, int32_t precision,
                       int32_t *sweeps, int32_t *status,
                       void *workspace, size_t workspace_bytes, void *stream);
+
+/* jb_svd_uneven_f32 with the launch choices an autotuner varies: flags
+ * JB_ROUND_ROBIN and/or JB_BLOCK_WIDTH_8 (the workspace query must get the
+ * same flags); exit_ratio, the largest pair ratio after which the FP32 phase
+ * of a mixed solve hands over to the FP64 phase (0: the default 1e-2; < 0:
+ * the FP32 phase runs to tol).  Results converge to the same tolerance
+ * whatever the choices. */
+JB_API int jb_svd_uneven_f32_ex(const float *A, float *U, float *S, float *Vh,
+                                const jb_matrix_desc *descs, const int32_t *order,
+                                int64_t count, int32_t max_m, int32_t max_n,
+                                double tol, int32_t max_sweeps, int32_t precision,
+                                int32_t flags, double exit_ratio,
+                                int32_t *sweeps, int32_t *status,
+                                void *workspace, size_t workspace_bytes, void *stream);
 
 /* ---- tensor-core building blocks (tcgen05, sm_100a) --------------------- */
 #define JB_GEMM_PLAIN   0   /* C = alpha A0 B0^T (+ C)                              */

@@ -51,6 +51,61 @@ def cost_order(m, n):
     return np.argsort(-cost, kind="stable").astype(np.int32)
 
 
+class Launch:
+    """Launch choices of an uneven solve: ``flags`` (ROUND_ROBIN pair order,
+    BLOCK_WIDTH_8 register blocks) and ``exit_ratio`` (the FP32 phase of a
+    mixed solve hands over once no pair ratio of a sweep exceeds it; 0 = the
+    library default 1e-2, < 0 = the FP32 phase runs to tol).  Every choice
+    converges to the same tolerance; they differ only in speed."""
+
+    def __init__(self, flags=0, exit_ratio=0.0):
+        self.flags, self.exit_ratio = int(flags), float(exit_ratio)
+
+    def __repr__(self):
+        names = [n for n, b in (("round_robin", N.ROUND_ROBIN), ("block_width_8", N.BLOCK_WIDTH_8)) if self.flags & b]
+        return f"Launch({'|'.join(names) or 'default'}, exit_ratio={self.exit_ratio:g})"
+
+    def key(self):
+        return (self.flags, self.exit_ratio)
+
+
+# Candidates the autotuner times (the first is the library default).
+TUNE_CANDIDATES = (Launch(), Launch(exit_ratio=3e-3), Launch(exit_ratio=-1.0), Launch(N.BLOCK_WIDTH_8),
+                   Launch(N.ROUND_ROBIN))
+_tune_cache = {}
+
+
+def tune(m, n, a_flat, *, precision="mixed", tol=None, max_sweeps=60, candidates=TUNE_CANDIDATES, repeats=3):
+    """Autotuner: time every launch choice on this batch (CUDA events, graph
+    replays after one warm-up) and return the fastest as a Launch, with the
+    timings.  The result is cached per shape multiset, precision and
+    tolerance, so a harness pays for it once, in preparation."""
+    m = np.asarray(m, np.int64)
+    n = np.asarray(n, np.int64)
+    key = (hash(m.tobytes()), hash(n.tobytes()), precision, tol, max_sweeps)
+    if key in _tune_cache:
+        return _tune_cache[key]
+    dev = a_flat.device
+    times = {}
+    for cand in candidates:
+        plan = UnevenBatch(m, n, dev, tol=tol, max_sweeps=max_sweeps, precision=precision, launch=cand)
+        g = plan.capture(a_flat)
+        g.replay()
+        plan.check()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(repeats):
+            g.replay()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        plan.check()
+        times[repr(cand)] = e0.elapsed_time(e1) / repeats
+        del g, plan
+    best = min(candidates, key=lambda c: times[repr(c)])
+    _tune_cache[key] = (best, times)
+    return best, times
+
+
 class UnevenBatch:
     """Plan and buffers for solving a fixed list of shapes repeatedly.
 
@@ -60,7 +115,7 @@ class UnevenBatch:
     the per-matrix offsets; ``result(i)`` returns views."""
 
     def __init__(self, m, n, device, *, a_off=None, tol=None, max_sweeps=60, precision="mixed",
-                 values_only=False, order="cost"):
+                 values_only=False, order="cost", launch=None):
         self.m = np.asarray(m, np.int64)
         self.n = np.asarray(n, np.int64)
         self.count = len(self.m)
@@ -73,6 +128,9 @@ class UnevenBatch:
         if precision not in ("mixed", "fp32"):
             raise ValueError("precision must be 'mixed' or 'fp32'")
         self.precision = N.PREC_MIXED if precision == "mixed" else N.PREC_NATIVE
+        # launch choices (see Launch / tune): flags JB_ROUND_ROBIN | JB_BLOCK_WIDTH_8 and the
+        # FP32-phase exit ratio of the mixed solve
+        self.launch_choice = launch or Launch()
         k = np.minimum(self.m, self.n)
         if a_off is None:
             a_off, _ = _aligned_offsets(self.m * self.n)
@@ -101,7 +159,8 @@ class UnevenBatch:
         # Workspace: the base area (ticket counters, per-CTA areas of the
         # round-robin kernels) followed, in mixed precision, by the scratch
         # floats the descriptors' x_off address.
-        ws = lib.jb_uneven_workspace_bytes(self.max_m, self.max_n, self.count, self.precision, int(xt))
+        ws = lib.jb_uneven_workspace_bytes(self.max_m, self.max_n, self.count, self.precision,
+                                           self.launch_choice.flags, int(xt))
         self.workspace = torch.empty(max(int(ws), 256), dtype=torch.uint8, device=dev)
         # memset of the work tickets + one persistent kernel per precision phase
         self.kernels_per_solve = 2 if self.precision == N.PREC_MIXED else 1
@@ -114,12 +173,13 @@ class UnevenBatch:
         lib = N.lib()
         st = stream.cuda_stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream
         ptr = lambda t: None if t is None else t.data_ptr()
-        rc = lib.jb_svd_uneven_f32(a_flat.data_ptr(), ptr(self.U), self.S.data_ptr(), ptr(self.Vh),
-                                   self.desc.data_ptr(), self.order.data_ptr(), self.count, self.max_m,
-                                   self.max_n, self.tol, self.max_sweeps, self.precision,
-                                   self.info[0].data_ptr(), self.info[1].data_ptr(), self.workspace.data_ptr(),
-                                   self.workspace.numel(), st)
-        N.check(rc, "jb_svd_uneven_f32")
+        lc = self.launch_choice
+        rc = lib.jb_svd_uneven_f32_ex(a_flat.data_ptr(), ptr(self.U), self.S.data_ptr(), ptr(self.Vh),
+                                      self.desc.data_ptr(), self.order.data_ptr(), self.count, self.max_m,
+                                      self.max_n, self.tol, self.max_sweeps, self.precision, lc.flags,
+                                      lc.exit_ratio, self.info[0].data_ptr(), self.info[1].data_ptr(),
+                                      self.workspace.data_ptr(), self.workspace.numel(), st)
+        N.check(rc, "jb_svd_uneven_f32_ex")
 
     def capture(self, a_flat: torch.Tensor) -> torch.cuda.CUDAGraph:
         """Capture one solve over the fixed buffer a_flat into a CUDA graph."""
@@ -162,7 +222,7 @@ class StreamedUneven:
     instead of compute + all transfers.  Host buffers are the flat ``pack``
     layouts of the whole batch (pinned for asynchronous copies)."""
 
-    def __init__(self, m, n, device, *, chunks=4, tol=None, max_sweeps=60, precision="mixed"):
+    def __init__(self, m, n, device, *, chunks=4, tol=None, max_sweeps=60, precision="mixed", launch=None):
         m = np.asarray(m, np.int64)
         n = np.asarray(n, np.int64)
         count = len(m)
@@ -187,7 +247,8 @@ class StreamedUneven:
 
         self.plans, self.dev_in, self.spans = [], [], []
         for lo, hi in self.ranges:
-            plan = UnevenBatch(m[lo:hi], n[lo:hi], dev, tol=tol, max_sweeps=max_sweeps, precision=precision)
+            plan = UnevenBatch(m[lo:hi], n[lo:hi], dev, tol=tol, max_sweeps=max_sweeps, precision=precision,
+                               launch=launch)
             a0, a1 = span(self.a_off, self.a_total, lo, hi)
             self.plans.append(plan)
             self.dev_in.append(torch.empty(max(a1 - a0, 1), dtype=torch.float32, device=dev))

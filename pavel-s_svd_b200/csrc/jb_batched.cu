@@ -90,6 +90,7 @@ struct Params {
     int *counter;                 // NULL: static grid-stride schedule
     int *counter2;                // ticket of the second (FP64) kernel
     int from_x32;                 // mixed round-robin solve: start from the FP32 V in x32 (large-tile K1)
+    float exit_ratio;             // mixed FP32 phase exit ratio (0: kMixedExitRatio, < 0: run to tol)
     unsigned char *gws;           // NULL: work area in shared memory
     size_t gws_stride;
     Dims maxd;                    // sizing of aux / region (largest matrix)
@@ -270,6 +271,8 @@ constexpr int kB32L = 4;  // block width of the large-tile FP32 kernel (16 warps
 // FP64 phase then converges to the requested tolerance in one rotating sweep
 // and one confirming sweep, as it does from a fully converged FP32 phase.
 constexpr float kMixedExitRatio = 1e-2f;
+// Launch choices jb_svd_uneven_f32_ex accepts in `flags` (an autotuner picks among them).
+constexpr int kTuneFlags = JB_ROUND_ROBIN | JB_BLOCK_WIDTH_8;
 constexpr int kB64 = 2;   // block width of the FP64 sweeps (16 warps for 64 columns)
 constexpr int kT32 = 256, kT64 = 512;  // threads of the two kernels
 constexpr int kMaxR = 4;  // rows per lane: mt <= 128
@@ -506,7 +509,11 @@ __global__ void __launch_bounds__(THREADS) rb32_kernel_t(Params p) {
                                         : (p.tol > 0 ? (float)p.tol : 10.0f * Lim<float>::eps());
                 bool conv;
                 ns = rb_dispatch<float, BW, MR, MRV>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true,
-                                                       ax.red, conv, MIXED ? kMixedExitRatio : 0.0f, ax.sig);
+                                                       ax.red, conv,
+                                                       MIXED ? (p.exit_ratio == 0.f ? kMixedExitRatio
+                                                                                    : fmaxf(p.exit_ratio, 0.f))
+                                                             : 0.0f,
+                                                       ax.sig);
                 if (MIXED) {
                     float *x = p.x32 + d.x_off;
                     const int nt = g.nt;
@@ -861,6 +868,7 @@ static int sm_count() {
 
 // Launch plan for one batch (sized by its largest tall shape).
 struct Plan {
+    int bw;               // block width of the FP32 register kernel (4 or 8)
     bool reg;             // register-tile path
     bool big;             // large-tile FP32 kernel (+ round-robin FP64 phase when mixed)
     size_t gram_stride;   // big + mixed: per-CTA area of the Gram FP64 kernel (0: round-robin FP64 phase)
@@ -878,6 +886,7 @@ struct Plan {
 static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags) {
     Plan pl;
     memset(&pl, 0, sizeof(pl));
+    pl.bw = (flags & JB_BLOCK_WIDTH_8) ? 8 : kB32;
     pl.d = dims_of(max_mt, max_nt, flags);
     pl.aux = aux_bytes(pl.d);
     pl.region = region_bytes(pl.d, elem, precision);
@@ -888,7 +897,7 @@ static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags
     if (t < 64) t = 64;
     if (t > 1024) t = 1024;
     pl.threads = t;
-    const RGeo r32 = rgeo(max_mt, max_nt, kB32, flags), r64 = rgeo(max_mt, max_nt, kB64, flags);
+    const RGeo r32 = rgeo(max_mt, max_nt, pl.bw, flags), r64 = rgeo(max_mt, max_nt, kB64, flags);
     pl.reg = !(flags & JB_ROUND_ROBIN) && r32.R <= kMaxR && r32.RV <= kMaxRV && r64.RV <= kMaxRV;
     if (pl.reg) {
         pl.d32 = raux_dims(r32);
@@ -989,11 +998,16 @@ static int launch_reg(Params &p, const Plan &pl, int elem, int precision, unsign
     int64_t grid;
     int rc;
     if (elem == 4) {
-        auto k1 = mixed ? rb32_kernel_t<true, kT32, kB32, kMaxR, kMaxRV> : rb32_kernel_t<false, kT32, kB32, kMaxR, kMaxRV>;
-        if ((rc = occupancy_grid(k1, kT32, pl.smem32, p.count, grid))) return rc;
+        // block width 4: 8 warps of 256 threads for 64 columns; 8: 4 warps of 128
+        auto k1 = pl.bw == 8 ? (mixed ? rb32_kernel_t<true, 128, 8, kMaxR, kMaxRV>
+                                      : rb32_kernel_t<false, 128, 8, kMaxR, kMaxRV>)
+                             : (mixed ? rb32_kernel_t<true, kT32, kB32, kMaxR, kMaxRV>
+                                      : rb32_kernel_t<false, kT32, kB32, kMaxR, kMaxRV>);
+        const int t1 = pl.bw == 8 ? 128 : kT32;
+        if ((rc = occupancy_grid(k1, t1, pl.smem32, p.count, grid))) return rc;
         p.maxd = pl.d32;
         p.region_cap = pl.reg32;
-        k1<<<(unsigned)grid, kT32, pl.smem32, st>>>(p);
+        k1<<<(unsigned)grid, t1, pl.smem32, st>>>(p);
         if (cudaGetLastError() != cudaSuccess) return JB_ECUDA;
         if (!mixed) return JB_OK;
         auto k2 = rb64_kernel<float, true>;
@@ -1181,12 +1195,12 @@ int jb_svd_batched_f64(const double *A, double *U, double *S, double *Vh, int64_
                           workspace, workspace_bytes, stream, 8);
 }
 
-size_t jb_uneven_workspace_bytes(int32_t max_m, int32_t max_n, int64_t count, int32_t precision,
+size_t jb_uneven_workspace_bytes(int32_t max_m, int32_t max_n, int64_t count, int32_t precision, int32_t flags,
                                  int64_t scratch_floats) {
     if (max_m < 1 || max_n < 1 || count < 0 || scratch_floats < 0) return 0;
     if (precision != JB_PREC_NATIVE && precision != JB_PREC_MIXED) return 0;
     const int mt = max_m > max_n ? max_m : max_n, nt = max_m > max_n ? max_n : max_m;
-    const Plan pl = make_plan(mt, nt, 4, precision, 0);
+    const Plan pl = make_plan(mt, nt, 4, precision, flags & kTuneFlags);
     size_t bytes = base_bytes(pl, count);
     if (precision == JB_PREC_MIXED) bytes += (size_t)scratch_floats * 4;
     return bytes;
@@ -1196,12 +1210,21 @@ int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh, const jb_ma
                       const int32_t *order, int64_t count, int32_t max_m, int32_t max_n, double tol,
                       int32_t max_sweeps, int32_t precision, int32_t *sweeps, int32_t *status, void *workspace,
                       size_t workspace_bytes, void *stream) {
+    return jb_svd_uneven_f32_ex(A, U, S, Vh, descs, order, count, max_m, max_n, tol, max_sweeps, precision, 0, 0.0,
+                                sweeps, status, workspace, workspace_bytes, stream);
+}
+
+int jb_svd_uneven_f32_ex(const float *A, float *U, float *S, float *Vh, const jb_matrix_desc *descs,
+                         const int32_t *order, int64_t count, int32_t max_m, int32_t max_n, double tol,
+                         int32_t max_sweeps, int32_t precision, int32_t flags, double exit_ratio, int32_t *sweeps,
+                         int32_t *status, void *workspace, size_t workspace_bytes, void *stream) {
     if (count < 0 || max_m < 1 || max_n < 1 || max_sweeps < 1 || !A || !S || !descs) return JB_EINVAL;
     if (precision != JB_PREC_NATIVE && precision != JB_PREC_MIXED) return JB_EINVAL;
+    if (flags & ~kTuneFlags) return JB_EINVAL;
     const int mt = max_m > max_n ? max_m : max_n, nt = max_m > max_n ? max_n : max_m;
     if (mt > 8192 || nt > 4096) return JB_ETOOBIG;
     if (count == 0) return JB_OK;
-    const Plan pl = make_plan(mt, nt, 4, precision, 0);
+    const Plan pl = make_plan(mt, nt, 4, precision, flags);
     if (!workspace || workspace_bytes < base_bytes(pl, count)) return JB_EWORKSPACE;
     Params p;
     memset(&p, 0, sizeof(p));
@@ -1209,6 +1232,7 @@ int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh, const jb_ma
     p.descs = descs; p.order = order; p.count = count;
     p.tol = tol; p.max_sweeps = max_sweeps; p.tol32 = tol; p.max_sweeps32 = max_sweeps;
     p.sweeps = sweeps; p.status = status;
+    p.exit_ratio = (float)exit_ratio;
     return launch_any(p, pl, 4, precision, workspace, workspace_bytes, (cudaStream_t)stream);
 }
 

@@ -15,7 +15,7 @@ from .build import library_path
 # Return codes and per-matrix status words (include/jacobi_b200.h).
 JB_OK, JB_EINVAL, JB_ETOOBIG, JB_EWORKSPACE, JB_ECUDA = 0, 1, 2, 3, 4
 ST_OK, ST_NOT_CONVERGED, ST_NONFINITE_IN, ST_NULL_FAILED, ST_NONFINITE_OUT, ST_BAD_DESC = 0, 1, 2, 3, 4, 5
-FULL_MATRICES, VALUES_ONLY, ROUND_ROBIN = 1, 2, 4
+FULL_MATRICES, VALUES_ONLY, ROUND_ROBIN, BLOCK_WIDTH_8 = 1, 2, 4, 8
 PREC_NATIVE, PREC_MIXED = 0, 1
 
 RC_NAMES = {JB_EINVAL: "invalid argument", JB_ETOOBIG: "shape too large for this entry point",
@@ -23,7 +23,8 @@ RC_NAMES = {JB_EINVAL: "invalid argument", JB_ETOOBIG: "shape too large for this
 
 # Exported symbols, in declaration order of include/jacobi_b200.h.
 SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_batched_f32",
-           "jb_svd_batched_f64", "jb_uneven_workspace_bytes", "jb_svd_uneven_f32", "jb_gemm_bf16", "jb_gemm_bf16x", "jb_gemm_bf16x_rows",
+           "jb_svd_batched_f64", "jb_uneven_workspace_bytes", "jb_svd_uneven_f32", "jb_svd_uneven_f32_ex",
+           "jb_gemm_bf16", "jb_gemm_bf16x", "jb_gemm_bf16x_rows",
            "jb_split_bf16",
            "jb_split3_bf16",
            "jb_warm_prep_f32", "jb_svd_warm_f32", "jb_transpose_bf16", "jb_bias_act", "jb_relu_backward",
@@ -57,7 +58,7 @@ def _declare(l):
     l.jb_workspace_bytes.restype = SZ
     l.jb_workspace_bytes.argtypes = [I32, I32, I64, I32, I32, I32]
     l.jb_uneven_workspace_bytes.restype = SZ
-    l.jb_uneven_workspace_bytes.argtypes = [I32, I32, I64, I32, I64]
+    l.jb_uneven_workspace_bytes.argtypes = [I32, I32, I64, I32, I32, I64]
     l.jb_eigh_workspace_bytes.restype = SZ
     l.jb_eigh_workspace_bytes.argtypes = [I32, I64]
     for name in ("jb_eigh_f32", "jb_eigh_f64"):
@@ -69,6 +70,8 @@ def _declare(l):
     l.jb_svd_batched_f64.argtypes = [P, P, P, P, I64, I32, I32, I32, I32, F64, I32, P, P, P, SZ, P]
     l.jb_svd_uneven_f32.restype = ctypes.c_int
     l.jb_svd_uneven_f32.argtypes = [P, P, P, P, P, P, I64, I32, I32, F64, I32, I32, P, P, P, SZ, P]
+    l.jb_svd_uneven_f32_ex.restype = ctypes.c_int
+    l.jb_svd_uneven_f32_ex.argtypes = [P, P, P, P, P, P, I64, I32, I32, F64, I32, I32, I32, F64, P, P, P, SZ, P]
     l.jb_gemm_bf16.restype = ctypes.c_int
     l.jb_gemm_bf16.argtypes = [P, P, P, P, I32, P, I64, I64, I64, I64, I64, I64, I64, I64, I64, I64,
                                ctypes.c_float, ctypes.c_float, I32, P, P]

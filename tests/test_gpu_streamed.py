@@ -44,3 +44,31 @@ def test_streamed_raises_on_nonfinite_input():
     st.run(hin, hu, hs, hv)
     with pytest.raises(ValueError, match="NaN or infinity"):
         st.check()
+
+
+def test_launch_choices_and_autotuner():
+    """Every launch choice the autotuner varies (pair order, block width,
+    FP32-phase exit ratio) converges to the same singular values within the
+    mixed path's bound; tune() returns the fastest of them and caches it."""
+    B = importlib.import_module("pavel-s_svd_b200.batch")
+    N = importlib.import_module("pavel-s_svd_b200.native")
+    wl = importlib.import_module("pavel-s_svd_b200.workloads")
+    mats = wl.uneven_batch(600, seed=9)
+    flat, m, n, a_off = B.pack(mats)
+    x = flat.cuda()
+    ref = None
+    for cand in B.TUNE_CANDIDATES:
+        plan = B.UnevenBatch(m, n, "cuda", a_off=a_off, launch=cand)
+        plan.launch(x)
+        sw = plan.check()
+        assert sw.min() >= 1
+        s = plan.S.cpu().numpy()
+        if ref is None:
+            ref = s
+        else:
+            assert float(np.abs(s - ref).max() / np.abs(ref).max()) <= 1e-6, repr(cand)
+    best, times = B.tune(m, n, x)
+    assert repr(best) in times and len(times) == len(B.TUNE_CANDIDATES)
+    assert times[repr(best)] == min(times.values())
+    assert B.tune(m, n, x)[0] is best                      # cached
+    assert B.Launch(N.ROUND_ROBIN | N.BLOCK_WIDTH_8).flags == 12
