@@ -311,7 +311,7 @@ def run_ours(args, rank, world, local_rank):
     line = {"metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 in/out; f32+f64 sweeps" if args.precision == "mixed" else "f32",
-            "data": "synthetic (seeded, BASELINE config 2 distribution)",
+            "data": "synthetic (seeded: n ~ U[8,64], m ~ U[n,2n], entries N(0,1))",
             "config": dict(workload_config(world), launch=repr(choice),
                            autotuner_ms={k: round(v, 3) for k, v in tune_ms.items()}),
             "accuracy": {"max_rel_sigma_err_vs_fp64": sig_err, "max_reconstruction_rel_fro": rec_err,
@@ -403,7 +403,7 @@ def run_plain_single(args):
     line = {"metric": "Jacobi SVD matrices/s (single 256x128 matrix)", "value": res["mixed"]["matrices_per_s"],
             "unit": "matrices/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": res["mixed"]["ms"], "higher_is_better": True, "scaling": "none (single matrix)",
-            "vs_baseline": None, "dtype": "f32 in/out", "data": "synthetic (seeded, BASELINE config 1)",
+            "vs_baseline": None, "dtype": "f32 in/out", "data": "synthetic (seeded: Haar U, V; s_i = 10^(-4i/127))",
             "config": {"workload": "plain_single_256x128", "tol": 1e-6, "max_sweeps": 30},
             "variants": res, "cpu_baseline": {"value": 1e3 / cpu_ms, "unit": "matrices/s", "cores": 1,
                                               "kind": "port", "sample": "the one matrix, C oracle (fp32)",
@@ -444,7 +444,8 @@ def run_blocked(args, name):
             "scaling": "none (single matrix)", "vs_baseline": None,
             "dtype": "f32 in/out; bf16x3/bf16x6 tensor; f64 eig", "config": {"workload": name, "m": m, "n": n,
                                                                               "block_size": b},
-            "data": f"synthetic (seeded, BASELINE config {'3' if name == 'clustered_large' else '4'})",
+            "data": ("synthetic (seeded: Haar U, V; 64 clusters x 16, cond 1e6)" if name == "clustered_large"
+                     else "synthetic (seeded: rank-64 Gaussian product + N(0, 1e-6) noise)"),
             "block_sweeps": info["block_sweeps"], "off_per_sweep": info["off_per_sweep"],
             "converged": info["converged"], "reached_tol": info["reached_tol"],
             "tensor_flop_per_solve": tensor_flop, "tensor_tflops_whole_solve": tensor_flop / (ms / 1e3) / 1e12,
@@ -497,7 +498,7 @@ def run_warm(args):
             "value": res["warm"]["matrices_per_s"], "unit": "matrices/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": res["warm"]["ms"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 in/out; f32+f64 sweeps; bf16 network",
-            "data": "synthetic (seeded, BASELINE config 5)", "config": {"workload": "warm_family", "train": 60000,
+            "data": "synthetic (seeded: U Haar, log-uniform s, V = expm(0.3 L(theta)))", "config": {"workload": "warm_family", "train": 60000,
                                                                          "held_out": 4096, "epochs": 15},
             "train_ms": train_ms, "loss_first_last": [hist[0], hist[-1]], "variants": res,
             "note": "plain_fp32 = the plain FP32 Jacobi from V = I; plain = the mixed-precision solver from V = I; "

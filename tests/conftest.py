@@ -51,5 +51,5 @@ def workloads():
 
 def sigma_tol(dtype):
     """Agreement bound on sigma (relative to sigma_1) between two correct
-    implementations: single precision 1e-5, double 1e-12."""
+    implementations: single precision 1e-5 (the accuracy bound of the mixed path), double 1e-12."""
     return 1e-5 if np.dtype(dtype) == np.float32 else 1e-12

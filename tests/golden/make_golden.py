@@ -38,7 +38,7 @@ def cases(make_matrix):
     """(name, input array, svd kwargs) -- mirrors the reference's own test
     inputs (tests/test_standalone.py:47-90, 187-207) in real dtypes, the
     real-valued byte-exact corpus (corpus/standalone/*.npy) and samples of
-    the BASELINE workloads."""
+    the benchmark workloads."""
     out = []
     for dt in ("float32", "float64"):
         for m, n in ((13, 7), (7, 13)):

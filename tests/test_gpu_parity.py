@@ -6,7 +6,7 @@ Tolerances, stated once:
     precision, 1e-12 * sigma_1 in double (`sigma_tol`);
   * mixed precision ('mixed', float32 input) against FP64 LAPACK: every
     singular value above twice the reference cut eps32*max(m,n)*sigma_1 within
-    1e-5 RELATIVE (the north-star bound);
+    1e-5 RELATIVE (the accuracy bound of the mixed path);
   * the reference's own test contract (tests/test_standalone.py:33-45):
     reconstruction < tol, max|Q^T Q - I| < 5 tol, spectrum < tol with
     tol = 3e-4 (single) / 2e-10 (double).
