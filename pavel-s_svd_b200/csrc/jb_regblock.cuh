@@ -426,7 +426,10 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
         }
         const bool rotate = !measure;
         int fl = 0;
+        // The step loops are unrolled so that circle_shift / shift_y become
+        // register renaming instead of moves.
         if (act && (X < live || Y < live)) {
+#pragma unroll
             for (int j = 0; j < B - 1; ++j) {
                 step<true>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
                 circle_shift(t);
@@ -444,6 +447,7 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
                 }
             }
             if (act && X < live && Y < live) {
+#pragma unroll
                 for (int j = 0; j < B; ++j) {
                     step<false>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
                     shift_y(t);
