@@ -363,10 +363,10 @@ __device__ void load_stage(const TI *A, const Geo &g, int ld, float *As) {
     }
 }
 
-template <typename T, int B, int MR = kMaxR, int MRV = kMaxRV>
+template <typename T, int B, int MR = kMaxR, int MRV = kMaxRV, bool UPD = false>
 __device__ int rb_dispatch(const RGeo &r, T *W, T *V, T tol, int max_sweeps, bool confirm, double *red,
                            bool &conv, T exit_ratio = T(0), double *colnorm = nullptr) {
-    return rb_sweeps<T, B, MR, MRV>(W, r.ldw, V, r.ldv, r.nb, r.live, tol, max_sweeps, confirm, red, conv,
+    return rb_sweeps<T, B, MR, MRV, UPD>(W, r.ldw, V, r.ldv, r.nb, r.live, tol, max_sweeps, confirm, red, conv,
                                     exit_ratio, colnorm);
 }
 
@@ -508,7 +508,11 @@ __global__ void __launch_bounds__(THREADS) rb32_kernel_t(Params p) {
                 const float tol = MIXED ? (p.tol32 > 0 ? (float)p.tol32 : 10.0f * Lim<float>::eps())
                                         : (p.tol > 0 ? (float)p.tol : 10.0f * Lim<float>::eps());
                 bool conv;
-                ns = rb_dispatch<float, BW, MR, MRV>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true,
+                // MIXED: the FP32 sweeps only precondition the FP64 phase, which
+                // decides convergence on exact dot products; they update the
+                // column norms instead of recomputing them (rb_sweeps UPD).  Not
+                // in the large tile, where the norms would not fit in registers.
+                ns = rb_dispatch<float, BW, MR, MRV, MIXED && MR <= kMaxR>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true,
                                                        ax.red, conv,
                                                        MIXED ? (p.exit_ratio == 0.f ? kMixedExitRatio
                                                                                     : fmaxf(p.exit_ratio, 0.f))

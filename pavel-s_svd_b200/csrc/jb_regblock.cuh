@@ -39,6 +39,7 @@ template <typename T, int B, int R, int RV>
 struct Tile {
     T w[2 * B][R];
     T v[2 * B][RV];
+    T nrm[2 * B];   // column norms squared (norm-update sweeps only), same on every lane
 };
 
 // Warp reduce-scatter of NV (power of two <= 32) values: afterwards x[0] on
@@ -74,17 +75,21 @@ __device__ __forceinline__ void reduce_scatter(T (&x)[NV], int lane) {
 // heuristic of rb_sweeps); bit 2: ratio > the phase exit ratio (ex2 its
 // square).  Inactive pairs get c = 1, s = 0.
 template <typename T>
-__device__ __forceinline__ int rot_params(T app, T aqq, T apq, T tol2, T big2, T ex2, T floor_, T &c, T &s);
+__device__ __forceinline__ int rot_params(T app, T aqq, T apq, T tol2, T big2, T ex2, T floor_, T &c, T &s,
+                                          T *shift = nullptr);
 
 // FP32: t from approximate reciprocal / reciprocal square root (an error of
 // a few ulp in t only leaves |apq| a few ulp of itself), c = 1/sqrt(1+t^2)
 // refined by one Newton step so that c^2 + s^2 = 1 to ~1 ulp: every applied
 // rotation stays orthogonal at FP32 precision.
+// shift (optional): t |apq|, the change of the two squared column norms
+// (app' = app - shift, aqq' = aqq + shift); 0 for an inactive pair.
 template <>
 __device__ __forceinline__ int rot_params<float>(float app, float aqq, float apq, float tol2, float big2, float ex2,
-                                                 float floor_, float &c, float &s) {
+                                                 float floor_, float &c, float &s, float *shift) {
     c = 1.f;
     s = 0.f;
+    if (shift) *shift = 0.f;
     const float apq2 = apq * apq;
     const float prod = app * aqq;
     const bool active = apq2 > tol2 * prod && fminf(app, aqq) > floor_;
@@ -98,6 +103,7 @@ __device__ __forceinline__ int rot_params<float>(float app, float aqq, float apq
     c = c0 * fmaf(-0.5f * x, c0 * c0, 1.5f);
     s = t * c;
     if (apq < 0.f) s = -s;
+    if (shift) *shift = t * fabsf(apq);
     return 1 | (apq2 > big2 * prod ? 2 : 0) | (apq2 > ex2 * prod ? 4 : 0);
 }
 
@@ -107,7 +113,7 @@ __device__ __forceinline__ int rot_params<float>(float app, float aqq, float apq
 // every applied rotation is orthogonal to FP64 precision.
 template <>
 __device__ __forceinline__ int rot_params<double>(double app, double aqq, double apq, double tol2, double big2,
-                                                  double ex2, double floor_, double &c, double &s) {
+                                                  double ex2, double floor_, double &c, double &s, double *) {
     c = 1.0;
     s = 0.0;
     const double apq2 = apq * apq;
@@ -240,9 +246,62 @@ __device__ __forceinline__ void step(Tile<T, B, R, RV> &t, T tol2, T big2, T ex2
     }
 }
 
+// Norm-update step (FP32 packed tiles): the squared column norms come from
+// t.nrm instead of two more dot products, and each rotation updates them as
+// it changes them (app - t|apq|, aqq + t|apq|); only w_p^T w_q is reduced
+// across the warp.
+template <bool INTRA, typename T, int B, int R, int RV>
+__device__ __forceinline__ void step_upd(Tile<T, B, R, RV> &t, T tol2, T big2, T ex2, T floor_, int &fl,
+                                         bool rotate, int lane, int nr, int nv) {
+    constexpr int LB = Log2<B>::value;
+    static_assert(sizeof(T) == 4 && R % 2 == 0 && RV % 2 == 0, "norm-update steps are FP32 packed tiles");
+    T pc[B];
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        const int p = pair_p<INTRA, B>(i), q = pair_q<INTRA, B>(i);
+        float c0 = 0.f, c1 = 0.f;
+#pragma unroll
+        for (int r = 0; r < R; r += 2)
+            if (r < nr) fma2(c0, c1, t.w[p][r], t.w[p][r + 1], t.w[q][r], t.w[q][r + 1]);
+        pc[i] = c0 + c1;
+    }
+    reduce_scatter<T, B>(pc, lane);
+    // this lane's pair (lane >> (5 - LB)): its two norms from the tile
+    const int li = lane >> (5 - LB);
+    T app = t.nrm[pair_p<INTRA, B>(0)], aqq = t.nrm[pair_q<INTRA, B>(0)];
+#pragma unroll
+    for (int i = 1; i < B; ++i)
+        if (li == i) { app = t.nrm[pair_p<INTRA, B>(i)]; aqq = t.nrm[pair_q<INTRA, B>(i)]; }
+    T c, s, sh;
+    const int f = rot_params<T>(app, aqq, pc[0], tol2, big2, ex2, floor_, c, s, &sh);
+    fl |= f;
+    if (!rotate || !__any_sync(FULL, f != 0)) return;
+    const T np_ = app - sh, nq_ = aqq + sh;
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+        const int src = i << (5 - LB);
+        const T ci = __shfl_sync(FULL, c, src), si = __shfl_sync(FULL, s, src);
+        const int p = pair_p<INTRA, B>(i), q = pair_q<INTRA, B>(i);
+        t.nrm[p] = __shfl_sync(FULL, np_, src);
+        t.nrm[q] = __shfl_sync(FULL, nq_, src);
+#pragma unroll
+        for (int r = 0; r < R; r += 2)
+            if (r < nr) rot2(t.w[p][r], t.w[p][r + 1], t.w[q][r], t.w[q][r + 1], ci, si);
+#pragma unroll
+        for (int r = 0; r < RV; r += 2)
+            if (r < nv) rot2(t.v[p][r], t.v[p][r + 1], t.v[q][r], t.v[q][r + 1], ci, si);
+    }
+}
+
 // y_i <- y_(i+1) (cyclic): the next CROSS step pairs x_i with the old y_(i+1).
-template <typename T, int B, int R, int RV>
+template <bool UPD, typename T, int B, int R, int RV>
 __device__ __forceinline__ void shift_y(Tile<T, B, R, RV> &t) {
+    if constexpr (UPD) {
+        const T f = t.nrm[B];
+#pragma unroll
+        for (int i = 0; i < B - 1; ++i) t.nrm[B + i] = t.nrm[B + i + 1];
+        t.nrm[2 * B - 1] = f;
+    }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
         const T f = t.w[B][r];
@@ -260,11 +319,17 @@ __device__ __forceinline__ void shift_y(Tile<T, B, R, RV> &t) {
 }
 
 // Circle rotation inside both blocks: positions 1..B-1 move one step right.
-template <typename T, int B, int R, int RV>
+template <bool UPD, typename T, int B, int R, int RV>
 __device__ __forceinline__ void circle_shift(Tile<T, B, R, RV> &t) {
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
         const int o = half * B;
+        if constexpr (UPD) {
+            const T last = t.nrm[o + B - 1];
+#pragma unroll
+            for (int i = B - 1; i >= 2; --i) t.nrm[o + i] = t.nrm[o + i - 1];
+            t.nrm[o + 1] = last;
+        }
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const T last = t.w[o + B - 1][r];
@@ -309,6 +374,29 @@ __device__ __forceinline__ void tile_io(Tile<T, B, R, RV> &t, T *W, int ldw, T *
             }
         }
     }
+}
+
+// Squared column norms of the tile's 2B columns, reduced across the warp:
+// afterwards nrm[0] on lane l is column l >> (5 - log2 2B)'s norm.
+template <typename T, int B, int R, int RV>
+__device__ __forceinline__ void tile_col_norms(const Tile<T, B, R, RV> &t, T (&nrm)[2 * B], int lane, int nr) {
+#pragma unroll
+    for (int c = 0; c < 2 * B; ++c) {
+        T a = 0;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (r < nr) a = dfma(t.w[c][r], t.w[c][r], a);
+        nrm[c] = a;
+    }
+    reduce_scatter<T, 2 * B>(nrm, lane);
+}
+
+// Norm-update sweeps: every lane gets all 2B exact norms of the tile.
+template <typename T, int B, int R, int RV>
+__device__ __forceinline__ void spread_norms(Tile<T, B, R, RV> &t, T n0) {
+    constexpr int LB2 = Log2<2 * B>::value;
+#pragma unroll
+    for (int c = 0; c < 2 * B; ++c) t.nrm[c] = __shfl_sync(FULL, n0, c << (5 - LB2));
 }
 
 // The measuring sweep as one Gram pass: every pair ratio |w_p^T w_q| /
@@ -378,7 +466,10 @@ __device__ int gram_check(const T *W, int ldw, int npb, int nr, T tol2, T floor_
 // phase that follows takes it from there (converged is then set).
 // colnorm (npb doubles of shared memory, or NULL): when given, a measuring
 // sweep is replaced by gram_check.
-template <typename T, int B, int R, int RV>
+// UPD: norm-update steps (step<.., UPD>); the norms are recomputed exactly at
+// every sweep start and whenever a warp loads a new block pair, so the
+// updates accumulate over one block round at most.
+template <typename T, int B, int R, int RV, bool UPD = false>
 __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, int max_sweeps, bool confirm,
                          double *red, bool &converged, T exit_ratio = T(0), double *colnorm = nullptr) {
     const int nr = ldw >> 5, nv = ldv >> 5;
@@ -399,16 +490,9 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
         T nmax = 0;
         if (act) {
             T nrm[2 * B];
-#pragma unroll
-            for (int c = 0; c < 2 * B; ++c) {
-                T a = 0;
-#pragma unroll
-                for (int r = 0; r < R; ++r)
-                    if (r < nr) a = dfma(t.w[c][r], t.w[c][r], a);
-                nrm[c] = a;
-            }
-            reduce_scatter<T, 2 * B>(nrm, lane);
+            tile_col_norms(t, nrm, lane, nr);
             nmax = warp_max(nrm[0]);
+            if constexpr (UPD) spread_norms(t, nrm[0]);
         }
         if (lane == 0) red[warp] = (double)nmax;
         __syncthreads();
@@ -431,8 +515,9 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
         if (act && (X < live || Y < live)) {
 #pragma unroll
             for (int j = 0; j < B - 1; ++j) {
-                step<true>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
-                circle_shift(t);
+                if constexpr (UPD) step_upd<true>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
+                else step<true>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
+                circle_shift<UPD>(t);
             }
         }
         for (int br = 0; br < nb - 1; ++br) {
@@ -444,13 +529,19 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
                     X = circ(warp, rr, nb);
                     Y = circ(nb - 1 - warp, rr, nb);
                     tile_io(t, W, ldw, V, ldv, X, Y, lane, false, nr, nv);
+                    if constexpr (UPD) {
+                        T nrm[2 * B];
+                        tile_col_norms(t, nrm, lane, nr);
+                        spread_norms(t, nrm[0]);
+                    }
                 }
             }
             if (act && X < live && Y < live) {
 #pragma unroll
                 for (int j = 0; j < B; ++j) {
-                    step<false>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
-                    shift_y(t);
+                    if constexpr (UPD) step_upd<false>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
+                    else step<false>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
+                    shift_y<UPD>(t);
                 }
             }
         }
