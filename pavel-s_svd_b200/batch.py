@@ -162,8 +162,15 @@ class UnevenBatch:
         ws = lib.jb_uneven_workspace_bytes(self.max_m, self.max_n, self.count, self.precision,
                                            self.launch_choice.flags, int(xt))
         self.workspace = torch.empty(max(int(ws), 256), dtype=torch.uint8, device=dev)
-        # memset of the work tickets + one persistent kernel per precision phase
-        self.kernels_per_solve = 2 if self.precision == N.PREC_MIXED else 1
+        # Persistent kernels per solve (after a memset of the work tickets): one
+        # per precision phase, two when the register path splits the batch
+        # into size classes (widths above and up to 32 columns run in CTAs of
+        # different sizes; the library does this for batches wider than 32
+        # that fit the register tiles: max(m, n) <= 128, min(m, n) <= 64).
+        phases = 2 if self.precision == N.PREC_MIXED else 1
+        split = (not self.launch_choice.flags & (N.ROUND_ROBIN | N.BLOCK_WIDTH_8) and self.max_m <= 128
+                 and 32 < self.max_n <= 64)
+        self.kernels_per_solve = phases * (2 if split else 1)
 
     # -- solving ----------------------------------------------------------------
     def launch(self, a_flat: torch.Tensor, stream=None):

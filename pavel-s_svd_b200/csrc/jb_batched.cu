@@ -98,6 +98,7 @@ struct Params {
     float *x32;                   // mixed scratch (V of the FP32 phase)
     int64_t x_cap;                // floats available at x32
     size_t region_cap;            // bytes of the shared-memory work area
+    int cls;                      // 0: every matrix; 1: only nt > kNarrowN; 2: only nt <= kNarrowN
 };
 
 __device__ inline jb_matrix_desc desc_of(const Params &p, int64_t mat) {
@@ -276,6 +277,10 @@ constexpr int kTuneFlags = JB_ROUND_ROBIN | JB_BLOCK_WIDTH_8;
 constexpr int kB64 = 2;   // block width of the FP64 sweeps (16 warps for 64 columns)
 constexpr int kT32 = 256, kT64 = 512;  // threads of the two kernels
 constexpr int kMaxR = 4;  // rows per lane: mt <= 128
+// Size classes of the register path: matrices with nt <= kNarrowN occupy at
+// most half of the warps of a CTA (kT32 / kT64), so they run in a second
+// launch with CTAs of half the size and twice as many CTAs per SM.
+constexpr int kNarrowN = 32;
 constexpr int kMaxRV = 2; // V rows per lane: padded width <= 64
 // Large-tile FP32 kernel (one matrix up to 256 x 128 per CTA, 16 warps).
 constexpr int kT32L = 512, kMaxRL = 8, kMaxRVL = 4;
@@ -316,6 +321,13 @@ __host__ __device__ inline Dims raux_dims(const RGeo &r) {
     Dims d;
     d.mt = r.ldw; d.nt = r.npb; d.np = r.npb; d.ncp = r.ncp; d.ldw = r.ldw; d.ldv = r.ldv;
     return d;
+}
+
+// Whether a launch with class filter cls (Params::cls) takes this matrix.
+__device__ inline bool class_takes(const jb_matrix_desc &d, int cls) {
+    if (cls == 0) return true;
+    const bool narrow = (d.m < d.n ? d.m : d.n) <= kNarrowN;
+    return cls == 2 ? narrow : !narrow;
 }
 
 __device__ inline bool rdesc_fits(const jb_matrix_desc &d, int B, int elem, const Params &p, bool mixed_scratch,
@@ -363,7 +375,7 @@ __device__ void load_stage(const TI *A, const Geo &g, int ld, float *As) {
     }
 }
 
-template <typename T, int B, int MR = kMaxR, int MRV = kMaxRV, bool UPD = false>
+template <typename T, int B, int MR = kMaxR, int MRV = kMaxRV, int UPD = 0>
 __device__ int rb_dispatch(const RGeo &r, T *W, T *V, T tol, int max_sweeps, bool confirm, double *red,
                            bool &conv, T exit_ratio = T(0), double *colnorm = nullptr) {
     return rb_sweeps<T, B, MR, MRV, UPD>(W, r.ldw, V, r.ldv, r.nb, r.live, tol, max_sweeps, confirm, red, conv,
@@ -455,7 +467,7 @@ __device__ double polar_step(double *V, int n, int ld, double *VT, double *H, do
 // 256-thread form for matrices up to 128 x 64, rb32_large_kernel the
 // 512-thread form for one matrix up to 256 x 128 per CTA.
 template <bool MIXED, int THREADS, int BW, int MR, int MRV>
-__global__ void __launch_bounds__(THREADS) rb32_kernel_t(Params p) {
+__global__ void __launch_bounds__(THREADS, (BW == kB32 && MR <= kMaxR) ? 512 / THREADS : 1) rb32_kernel_t(Params p) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_idx;
     Aux ax = carve_aux(smem, p.maxd);
@@ -466,6 +478,7 @@ __global__ void __launch_bounds__(THREADS) rb32_kernel_t(Params p) {
         if (idx >= p.count) break;
         const int64_t mat = p.order ? (int64_t)p.order[idx] : idx;
         const jb_matrix_desc d = desc_of(p, mat);
+        if (!class_takes(d, p.cls)) continue;  // the other size class's launch solves it
         if (threadIdx.x < 4) ax.flag[threadIdx.x] = 0;
         __syncthreads();
         int ns = 0, st = JB_ST_OK;
@@ -512,7 +525,7 @@ __global__ void __launch_bounds__(THREADS) rb32_kernel_t(Params p) {
                 // decides convergence on exact dot products; they update the
                 // column norms instead of recomputing them (rb_sweeps UPD).  Not
                 // in the large tile, where the norms would not fit in registers.
-                ns = rb_dispatch<float, BW, MR, MRV, MIXED && MR <= kMaxR>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true,
+                ns = rb_dispatch<float, BW, MR, MRV, (MIXED && MR <= kMaxR) ? 1 : 0>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true,
                                                        ax.red, conv,
                                                        MIXED ? (p.exit_ratio == 0.f ? kMixedExitRatio
                                                                                     : fmaxf(p.exit_ratio, 0.f))
@@ -549,8 +562,8 @@ __global__ void __launch_bounds__(THREADS) rb32_kernel_t(Params p) {
 // in FP64 from the exact input;
 // native (TI = double): start from V = I.  Runs the epilogue and writes U,
 // S, Vh in TI.
-template <typename TI, bool MIXED>
-__global__ void __launch_bounds__(kT64) rb64_kernel(Params p) {
+template <typename TI, bool MIXED, int THREADS = kT64>
+__global__ void __launch_bounds__(THREADS, kT64 / THREADS) rb64_kernel(Params p) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_idx;
     Aux ax = carve_aux(smem, p.maxd);
@@ -561,6 +574,7 @@ __global__ void __launch_bounds__(kT64) rb64_kernel(Params p) {
         if (idx >= p.count) break;
         const int64_t mat = p.order ? (int64_t)p.order[idx] : idx;
         const jb_matrix_desc d = desc_of(p, mat);
+        if (!class_takes(d, p.cls)) continue;  // the other size class's launch solves it
         if (threadIdx.x < 4) ax.flag[threadIdx.x] = 0;
         __syncthreads();
         int prev = JB_ST_OK, s1 = 0;
@@ -625,7 +639,10 @@ __global__ void __launch_bounds__(kT64) rb64_kernel(Params p) {
                 const double tol = MIXED ? (p.tol > 0 ? (double)(float)p.tol : (double)(10.0f * Lim<float>::eps()))
                                          : (p.tol > 0 ? p.tol : 10.0 * Lim<double>::eps());
                 bool conv;
-                ns += rb_dispatch<double, kB64>(r, W, V, tol, p.max_sweeps, true, ax.red, conv, 0.0, ax.sig);
+                // MIXED: norm updates carried through ax.sig (rb_sweeps UPD 2); the
+                // confirming Gram pass that ends the solve measures exact norms.
+                ns += rb_dispatch<double, kB64, kMaxR, kMaxRV, MIXED ? 2 : 0>(r, W, V, tol, p.max_sweeps, true, ax.red,
+                                                                          conv, 0.0, ax.sig);
                 if (!conv) {
                     st = JB_ST_NOT_CONVERGED;
                 } else {
@@ -888,6 +905,10 @@ struct Plan {
     // register path: one sizing per kernel
     Dims d32, d64;
     size_t smem32, smem64, reg32, reg64;
+    // size-class split (kNarrowN): a second launch per phase for narrow matrices
+    bool split;
+    Dims d64n;
+    size_t smem64n, reg64n;
 };
 
 static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags) {
@@ -914,6 +935,14 @@ static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags
         pl.smem32 = aux_bytes(pl.d32) + pl.reg32;
         pl.smem64 = aux_bytes(pl.d64) + pl.reg64;
         if (pl.smem64 > kSmemLimit || pl.smem32 > kSmemLimit) pl.reg = false;
+        pl.split = pl.reg && pl.bw == kB32 && max_nt > kNarrowN;
+        if (pl.split) {
+            const RGeo r64n = rgeo(max_mt, kNarrowN, kB64, flags);
+            pl.d64n = raux_dims(r64n);
+            pl.reg64n = (elem == 4 && precision == JB_PREC_MIXED) ? rregion_mixed64(r64n, kNarrowN)
+                                                                   : rregion_bytes(r64n, 8);
+            pl.smem64n = aux_bytes(pl.d64n) + pl.reg64n;
+        }
     }
     const RGeo r32l = rgeo(max_mt, max_nt, kB32L, flags);
     if (!pl.reg && elem == 4 && !(flags & JB_ROUND_ROBIN) && r32l.R <= kMaxRL && r32l.RV <= kMaxRVL &&
@@ -1001,7 +1030,10 @@ static int launch_reg(Params &p, const Plan &pl, int elem, int precision, unsign
         p.x32 = (float *)(ws + base);
         p.x_cap = (int64_t)((ws_bytes - base) / 4);
     }
-    if (cudaMemsetAsync(ws, 0, 2 * sizeof(int), st) != cudaSuccess) return JB_ECUDA;
+    // Shapes are known on the host only for a uniform batch, whose matrices
+    // share one class: the split applies to descriptor (uneven) batches.
+    const bool split = pl.split && p.descs != nullptr;
+    if (cudaMemsetAsync(ws, 0, 4 * sizeof(int), st) != cudaSuccess) return JB_ECUDA;
     int64_t grid;
     int rc;
     if (elem == 4) {
@@ -1014,20 +1046,47 @@ static int launch_reg(Params &p, const Plan &pl, int elem, int precision, unsign
         if ((rc = occupancy_grid(k1, t1, pl.smem32, p.count, grid))) return rc;
         p.maxd = pl.d32;
         p.region_cap = pl.reg32;
+        p.cls = split ? 1 : 0;
         k1<<<(unsigned)grid, t1, pl.smem32, st>>>(p);
         if (cudaGetLastError() != cudaSuccess) return JB_ECUDA;
+        if (split) {
+            // narrow matrices: 4 warps (nt <= 32 is at most 8 blocks of 4 columns)
+            auto k1n = mixed ? rb32_kernel_t<true, kT32 / 2, kB32, kMaxR, kMaxRV>
+                             : rb32_kernel_t<false, kT32 / 2, kB32, kMaxR, kMaxRV>;
+            if ((rc = occupancy_grid(k1n, kT32 / 2, pl.smem32, p.count, grid))) return rc;
+            p.counter = (int *)ws + 2;
+            p.cls = 2;
+            k1n<<<(unsigned)grid, kT32 / 2, pl.smem32, st>>>(p);
+            if (cudaGetLastError() != cudaSuccess) return JB_ECUDA;
+            p.counter = (int *)ws;
+        }
         if (!mixed) return JB_OK;
         auto k2 = rb64_kernel<float, true>;
         if ((rc = occupancy_grid(k2, kT64, pl.smem64, p.count, grid))) return rc;
         p.maxd = pl.d64;
         p.region_cap = pl.reg64;
+        p.cls = split ? 1 : 0;
         k2<<<(unsigned)grid, kT64, pl.smem64, st>>>(p);
-        return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+        if (cudaGetLastError() != cudaSuccess) return JB_ECUDA;
+        if (split) {
+            // narrow matrices: 8 warps (nt <= 32 is at most 16 blocks of 2 columns),
+            // work area sized for nt <= kNarrowN
+            auto k2n = rb64_kernel<float, true, kT64 / 2>;
+            if ((rc = occupancy_grid(k2n, kT64 / 2, pl.smem64n, p.count, grid))) return rc;
+            p.maxd = pl.d64n;
+            p.region_cap = pl.reg64n;
+            p.counter2 = (int *)ws + 3;
+            p.cls = 2;
+            k2n<<<(unsigned)grid, kT64 / 2, pl.smem64n, st>>>(p);
+            if (cudaGetLastError() != cudaSuccess) return JB_ECUDA;
+        }
+        return JB_OK;
     }
     auto k2 = rb64_kernel<double, false>;
     if ((rc = occupancy_grid(k2, kT64, pl.smem64, p.count, grid))) return rc;
     p.maxd = pl.d64;
     p.region_cap = pl.reg64;
+    p.cls = 0;
     k2<<<(unsigned)grid, kT64, pl.smem64, st>>>(p);
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
 }

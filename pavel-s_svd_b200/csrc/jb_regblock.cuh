@@ -246,24 +246,34 @@ __device__ __forceinline__ void step(Tile<T, B, R, RV> &t, T tol2, T big2, T ex2
     }
 }
 
-// Norm-update step (FP32 packed tiles): the squared column norms come from
-// t.nrm instead of two more dot products, and each rotation updates them as
-// it changes them (app - t|apq|, aqq + t|apq|); only w_p^T w_q is reduced
-// across the warp.
+// Norm-update step: the squared column norms come from t.nrm instead of two
+// more dot products, and each rotation updates them as it changes them; only
+// w_p^T w_q is reduced across the warp.  FP32 (packed tiles): app - t|apq|,
+// aqq + t|apq|.  FP64: the expansion c^2 app - 2cs apq + s^2 aqq (and its
+// mirror) with the applied c and s, exact whatever the accuracy of the angle.
 template <bool INTRA, typename T, int B, int R, int RV>
 __device__ __forceinline__ void step_upd(Tile<T, B, R, RV> &t, T tol2, T big2, T ex2, T floor_, int &fl,
                                          bool rotate, int lane, int nr, int nv) {
     constexpr int LB = Log2<B>::value;
-    static_assert(sizeof(T) == 4 && R % 2 == 0 && RV % 2 == 0, "norm-update steps are FP32 packed tiles");
+    constexpr bool PACK = sizeof(T) == 4 && R % 2 == 0 && RV % 2 == 0;
+    static_assert(PACK || sizeof(T) == 8, "norm-update steps: FP32 packed tiles or FP64");
     T pc[B];
 #pragma unroll
     for (int i = 0; i < B; ++i) {
         const int p = pair_p<INTRA, B>(i), q = pair_q<INTRA, B>(i);
-        float c0 = 0.f, c1 = 0.f;
+        if constexpr (PACK) {
+            float c0 = 0.f, c1 = 0.f;
 #pragma unroll
-        for (int r = 0; r < R; r += 2)
-            if (r < nr) fma2(c0, c1, t.w[p][r], t.w[p][r + 1], t.w[q][r], t.w[q][r + 1]);
-        pc[i] = c0 + c1;
+            for (int r = 0; r < R; r += 2)
+                if (r < nr) fma2(c0, c1, t.w[p][r], t.w[p][r + 1], t.w[q][r], t.w[q][r + 1]);
+            pc[i] = c0 + c1;
+        } else {
+            T c = 0;
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (r < nr) c = dfma(t.w[p][r], t.w[q][r], c);
+            pc[i] = c;
+        }
     }
     reduce_scatter<T, B>(pc, lane);
     // this lane's pair (lane >> (5 - LB)): its two norms from the tile
@@ -276,7 +286,15 @@ __device__ __forceinline__ void step_upd(Tile<T, B, R, RV> &t, T tol2, T big2, T
     const int f = rot_params<T>(app, aqq, pc[0], tol2, big2, ex2, floor_, c, s, &sh);
     fl |= f;
     if (!rotate || !__any_sync(FULL, f != 0)) return;
-    const T np_ = app - sh, nq_ = aqq + sh;
+    T np_, nq_;
+    if constexpr (PACK) {
+        np_ = app - sh;
+        nq_ = aqq + sh;
+    } else {
+        const T cc = c * c, ss = s * s, x2 = T(2) * c * s * pc[0];
+        np_ = dfma(cc, app, dfma(ss, aqq, -x2));
+        nq_ = dfma(ss, app, dfma(cc, aqq, x2));
+    }
 #pragma unroll
     for (int i = 0; i < B; ++i) {
         const int src = i << (5 - LB);
@@ -284,19 +302,38 @@ __device__ __forceinline__ void step_upd(Tile<T, B, R, RV> &t, T tol2, T big2, T
         const int p = pair_p<INTRA, B>(i), q = pair_q<INTRA, B>(i);
         t.nrm[p] = __shfl_sync(FULL, np_, src);
         t.nrm[q] = __shfl_sync(FULL, nq_, src);
+        if constexpr (PACK) {
 #pragma unroll
-        for (int r = 0; r < R; r += 2)
-            if (r < nr) rot2(t.w[p][r], t.w[p][r + 1], t.w[q][r], t.w[q][r + 1], ci, si);
+            for (int r = 0; r < R; r += 2)
+                if (r < nr) rot2(t.w[p][r], t.w[p][r + 1], t.w[q][r], t.w[q][r + 1], ci, si);
 #pragma unroll
-        for (int r = 0; r < RV; r += 2)
-            if (r < nv) rot2(t.v[p][r], t.v[p][r + 1], t.v[q][r], t.v[q][r + 1], ci, si);
+            for (int r = 0; r < RV; r += 2)
+                if (r < nv) rot2(t.v[p][r], t.v[p][r + 1], t.v[q][r], t.v[q][r + 1], ci, si);
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                if (r < nr) {
+                    const T x = t.w[p][r], y = t.w[q][r];
+                    t.w[p][r] = dfma(ci, x, -si * y);
+                    t.w[q][r] = dfma(si, x, ci * y);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < RV; ++r) {
+                if (r < nv) {
+                    const T x = t.v[p][r], y = t.v[q][r];
+                    t.v[p][r] = dfma(ci, x, -si * y);
+                    t.v[q][r] = dfma(si, x, ci * y);
+                }
+            }
+        }
     }
 }
 
 // y_i <- y_(i+1) (cyclic): the next CROSS step pairs x_i with the old y_(i+1).
-template <bool UPD, typename T, int B, int R, int RV>
+template <int UPD, typename T, int B, int R, int RV>
 __device__ __forceinline__ void shift_y(Tile<T, B, R, RV> &t) {
-    if constexpr (UPD) {
+    if constexpr (UPD != 0) {
         const T f = t.nrm[B];
 #pragma unroll
         for (int i = 0; i < B - 1; ++i) t.nrm[B + i] = t.nrm[B + i + 1];
@@ -319,12 +356,12 @@ __device__ __forceinline__ void shift_y(Tile<T, B, R, RV> &t) {
 }
 
 // Circle rotation inside both blocks: positions 1..B-1 move one step right.
-template <bool UPD, typename T, int B, int R, int RV>
+template <int UPD, typename T, int B, int R, int RV>
 __device__ __forceinline__ void circle_shift(Tile<T, B, R, RV> &t) {
 #pragma unroll
     for (int half = 0; half < 2; ++half) {
         const int o = half * B;
-        if constexpr (UPD) {
+        if constexpr (UPD != 0) {
             const T last = t.nrm[o + B - 1];
 #pragma unroll
             for (int i = B - 1; i >= 2; --i) t.nrm[o + i] = t.nrm[o + i - 1];
@@ -466,10 +503,14 @@ __device__ int gram_check(const T *W, int ldw, int npb, int nr, T tol2, T floor_
 // phase that follows takes it from there (converged is then set).
 // colnorm (npb doubles of shared memory, or NULL): when given, a measuring
 // sweep is replaced by gram_check.
-// UPD: norm-update steps (step<.., UPD>); the norms are recomputed exactly at
-// every sweep start and whenever a warp loads a new block pair, so the
-// updates accumulate over one block round at most.
-template <typename T, int B, int R, int RV, bool UPD = false>
+// UPD: norm-update steps (step_upd); the norms are recomputed exactly at every
+// sweep start, and then
+//   UPD == 1: recomputed whenever a warp loads a new block pair, so the
+//             updates accumulate over one block round at most;
+//   UPD == 2: carried with the columns through colnorm (npb doubles of shared
+//             memory) between block rounds, so they accumulate over a sweep
+//             (FP64: the updates round like the dot products they replace).
+template <typename T, int B, int R, int RV, int UPD = 0>
 __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, int max_sweeps, bool confirm,
                          double *red, bool &converged, T exit_ratio = T(0), double *colnorm = nullptr) {
     const int nr = ldw >> 5, nv = ldv >> 5;
@@ -492,7 +533,7 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
             T nrm[2 * B];
             tile_col_norms(t, nrm, lane, nr);
             nmax = warp_max(nrm[0]);
-            if constexpr (UPD) spread_norms(t, nrm[0]);
+            if constexpr (UPD != 0) spread_norms(t, nrm[0]);
         }
         if (lane == 0) red[warp] = (double)nmax;
         __syncthreads();
@@ -515,31 +556,43 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
         if (act && (X < live || Y < live)) {
 #pragma unroll
             for (int j = 0; j < B - 1; ++j) {
-                if constexpr (UPD) step_upd<true>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
+                if constexpr (UPD != 0) step_upd<true>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
                 else step<true>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
                 circle_shift<UPD>(t);
             }
         }
         for (int br = 0; br < nb - 1; ++br) {
             if (br > 0 || sweep > 1) {
-                if (act) tile_io(t, W, ldw, V, ldv, X, Y, lane, true, nr, nv);
+                if (act) {
+                    tile_io(t, W, ldw, V, ldv, X, Y, lane, true, nr, nv);
+                    if constexpr (UPD == 2) {
+                        if (lane == 0) {
+#pragma unroll
+                            for (int c = 0; c < 2 * B; ++c)
+                                colnorm[c < B ? X * B + c : Y * B + (c - B)] = (double)t.nrm[c];
+                        }
+                    }
+                }
                 __syncthreads();
                 rr = rr + 1 == nb - 1 ? 0 : rr + 1;
                 if (act) {
                     X = circ(warp, rr, nb);
                     Y = circ(nb - 1 - warp, rr, nb);
                     tile_io(t, W, ldw, V, ldv, X, Y, lane, false, nr, nv);
-                    if constexpr (UPD) {
+                    if constexpr (UPD == 1) {
                         T nrm[2 * B];
                         tile_col_norms(t, nrm, lane, nr);
                         spread_norms(t, nrm[0]);
+                    } else if constexpr (UPD == 2) {
+#pragma unroll
+                        for (int c = 0; c < 2 * B; ++c) t.nrm[c] = (T)colnorm[c < B ? X * B + c : Y * B + (c - B)];
                     }
                 }
             }
             if (act && X < live && Y < live) {
 #pragma unroll
                 for (int j = 0; j < B; ++j) {
-                    if constexpr (UPD) step_upd<false>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
+                    if constexpr (UPD != 0) step_upd<false>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
                     else step<false>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
                     shift_y<UPD>(t);
                 }
