@@ -215,21 +215,32 @@ class UnevenBatch:
         return u, s, vh
 
 
+def chunk_weights(chunks):
+    """Relative cost of the chunks of a StreamedUneven: doubling from the
+    first and towards the last chunk, at most 4 (8 chunks: 1 2 4 4 4 4 2 1).
+    The first chunk's input copy and the last chunk's output copy are the
+    only transfers left exposed, so those two chunks are the smallest."""
+    return [float(min(2 ** i, 2 ** (chunks - 1 - i), 4)) for i in range(chunks)]
+
+
 class StreamedUneven:
     """Host-to-host solve of an uneven batch with the transfers overlapped
     with the compute.
 
     The matrices (in ``pack`` order) are split into ``chunks`` contiguous
-    groups of about equal cost, each with its own UnevenBatch.  Per chunk:
-    the host->device copy of its inputs on one copy stream, its solve on the
-    compute stream once that copy has landed, the device->host copy of its
-    U, S, Vh and status on another copy stream once the solve is done.
-    Chunk i+1's input copy and chunk i-1's output copy overlap chunk i's
-    solve, so a step costs about the compute plus one chunk's transfers
-    instead of compute + all transfers.  Host buffers are the flat ``pack``
-    layouts of the whole batch (pinned for asynchronous copies)."""
+    groups with costs in the proportions of ``chunk_weights`` (small first and
+    last chunks), each with its own UnevenBatch.  Per chunk: the host->device
+    copy of its inputs on one copy stream, its solve once that copy has landed,
+    the device->host copy of its U, S, Vh and status on another copy stream
+    once the solve is done.  Chunks alternate between two compute streams, so
+    the first CTAs of chunk i+1 start on the SMs that chunk i's last matrices
+    leave idle.  The input copy of chunk i+1 and the output copy of chunk i-1
+    overlap chunk i's solve, so a step costs about the compute plus the first
+    chunk's input copy and the last chunk's output copy.  Host buffers are the
+    flat ``pack`` layouts of the whole batch (pinned for asynchronous
+    copies)."""
 
-    def __init__(self, m, n, device, *, chunks=4, tol=None, max_sweeps=60, precision="mixed", launch=None):
+    def __init__(self, m, n, device, *, chunks=8, tol=None, max_sweeps=60, precision="mixed", launch=None):
         m = np.asarray(m, np.int64)
         n = np.asarray(n, np.int64)
         count = len(m)
@@ -245,7 +256,8 @@ class StreamedUneven:
         mt, nt = np.maximum(m, n), np.minimum(m, n)
         cost = np.cumsum(nt.astype(np.float64) ** 2 * (7 * mt + 4 * nt))
         chunks = max(1, min(int(chunks), count))
-        cuts = [0] + [int(np.searchsorted(cost, cost[-1] * c / chunks)) + 1 for c in range(1, chunks)] + [count]
+        frac = np.cumsum(chunk_weights(chunks)) / np.sum(chunk_weights(chunks))
+        cuts = [0] + [int(np.searchsorted(cost, cost[-1] * f)) + 1 for f in frac[:-1]] + [count]
         cuts = sorted(set(min(max(x, 0), count) for x in cuts))
         self.ranges = [(lo, hi) for lo, hi in zip(cuts[:-1], cuts[1:]) if hi > lo]
 
@@ -262,7 +274,7 @@ class StreamedUneven:
             self.spans.append((span(self.a_off, self.a_total, lo, hi), span(self.u_off, self.u_total, lo, hi),
                                span(self.s_off, self.s_total, lo, hi), span(self.v_off, self.v_total, lo, hi)))
         self.s_in = torch.cuda.Stream(dev)
-        self.s_comp = torch.cuda.Stream(dev)
+        self.s_comp = [torch.cuda.Stream(dev), torch.cuda.Stream(dev)]
         self.s_out = torch.cuda.Stream(dev)
         self.host_info = [torch.empty(2, max(hi - lo, 1), dtype=torch.int32).pin_memory() for lo, hi in self.ranges]
 
@@ -276,7 +288,7 @@ class StreamedUneven:
         the caller's current stream waits for all of it.  Call check() to
         synchronise and raise the reference's errors."""
         main = torch.cuda.current_stream(self.device)
-        for s in (self.s_in, self.s_comp, self.s_out):
+        for s in (self.s_in, *self.s_comp, self.s_out):
             s.wait_stream(main)
         landed, solved = [], []
         for (a, _, _, _), d in zip(self.spans, self.dev_in):
@@ -285,11 +297,12 @@ class StreamedUneven:
                 ev = torch.cuda.Event()
                 ev.record(self.s_in)
             landed.append(ev)
-        for plan, d, ev in zip(self.plans, self.dev_in, landed):
-            self.s_comp.wait_event(ev)
-            plan.launch(d, stream=self.s_comp)
+        for i, (plan, d, ev) in enumerate(zip(self.plans, self.dev_in, landed)):
+            comp = self.s_comp[i % 2]
+            comp.wait_event(ev)
+            plan.launch(d, stream=comp)
             done = torch.cuda.Event()
-            done.record(self.s_comp)
+            done.record(comp)
             solved.append(done)
         for plan, (_, u, s_, v), ev, info in zip(self.plans, self.spans, solved, self.host_info):
             self.s_out.wait_event(ev)

@@ -1,6 +1,8 @@
 """Host-side contract of the drop-in svd(): validation order, exception
 types and messages of svdbench/standalone/solvers.py:264-310 -- CPU only
 (every call here fails before any device work)."""
+import importlib
+
 import numpy as np
 import pytest
 import torch
@@ -67,3 +69,12 @@ def test_uneven_offsets_and_order():
     assert (off % 4 == 0).all() and total >= (m * n).sum()
     order = B.cost_order(m, n)
     assert order[0] == 2 and sorted(order.tolist()) == [0, 1, 2, 3]
+
+
+def test_streamed_chunk_weights():
+    """StreamedUneven's chunk costs: small first and last chunks (their input
+    and output copies are the exposed transfers), doubling to at most 4."""
+    B = importlib.import_module("pavel-s_svd_b200.batch")
+    assert B.chunk_weights(1) == [1.0]
+    assert B.chunk_weights(3) == [1.0, 2.0, 1.0]
+    assert B.chunk_weights(8) == [1.0, 2.0, 4.0, 4.0, 4.0, 4.0, 2.0, 1.0]

@@ -19,7 +19,7 @@ def test_streamed_equals_single_launch():
     ref = B.UnevenBatch(m, n, "cuda", a_off=a_off)
     ref.launch(flat.cuda())
     sweeps_ref = ref.check()
-    for chunks in (1, 3, 7):
+    for chunks in (1, 3, 8):
         st = B.StreamedUneven(m, n, "cuda", chunks=chunks)
         hin, hu, hs, hv = st.host_buffers()
         hin.copy_(flat[:hin.numel()])
