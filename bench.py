@@ -45,9 +45,10 @@ METRIC = "Jacobi SVD matrices/s at sigma-rel-err<=1e-5 vs FP64 (uneven batch)"
 WORKLOAD = "uneven_batch_8192"
 COUNT = 8192
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one solve of
-# this workload, rb32_kernel + rb64_kernel, from one ncu --set full capture
-# of `bench.py --steps 1 --warmup 3 --no-cpu-baseline`.
-MEASURED_TRAFFIC_PER_SOLVE = 313.8e6
+# this workload, the four launches of the two size classes (rb32_kernel_t
+# 256- and 128-thread, rb64_kernel 512- and 256-thread), from one ncu capture
+# (those metrics only) of `bench.py --steps 1 --warmup 3 --no-cpu-baseline`.
+MEASURED_TRAFFIC_PER_SOLVE = 289.5e6
 
 
 def workload_config(n_gpus):
@@ -139,6 +140,71 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
                 "samples": len(sm), "reasons": sorted(reasons)}
+
+
+class NvmlClockSampler:
+    """SM clock and clock-event reasons read through NVML every 5 ms on a
+    background thread while the timed region runs (reads only).  Falls back
+    to nvidia-smi (ClockSampler) when NVML is unavailable."""
+
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
+
+    def __init__(self, device, index):
+        self.device, self.index = device, index
+        self.samples, self.smax, self.fallback = [], None, None
+        self._stop = threading.Event()
+
+    def _handle(self, nv):
+        import torch
+        try:
+            pr = torch.cuda.get_device_properties(self.device)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return nv.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nv.nvmlDeviceGetHandleByIndex(self.index)
+
+    def __enter__(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nv, self.h = nv, self._handle(nv)
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+        except Exception:
+            self.fallback = ClockSampler(self.index).__enter__()
+            return self
+        self.thread = threading.Thread(target=self._poll, daemon=True)
+        self.thread.start()
+        return self
+
+    def _poll(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                sm = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                rs = int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))
+                self.samples.append((sm, rs))
+            except Exception:
+                pass
+            self._stop.wait(0.005)
+
+    def __exit__(self, *exc):
+        if self.fallback is not None:
+            return self.fallback.__exit__(*exc)
+        self._stop.set()
+        self.thread.join(timeout=2)
+        try:
+            self.nv.nvmlShutdown()
+        except Exception:
+            pass
+
+    def summary(self):
+        if self.fallback is not None:
+            return self.fallback.summary()
+        sm = [a for a, _ in self.samples]
+        reasons = sorted({nm for _, r in self.samples for nm, bit in self.REASONS if r & bit})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax,
+                "samples": len(sm), "reasons": reasons, "source": "nvml, every 5 ms"}
 
 
 def peaks():
@@ -247,7 +313,7 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize(dev)
     times = []
-    with ClockSampler(local_rank) as clocks:
+    with NvmlClockSampler(dev, local_rank) as clocks:
         for step in range(args.steps):
             flush.fill_(step & 0xff)
             e0 = torch.cuda.Event(enable_timing=True)
