@@ -323,6 +323,20 @@ JB_API int jb_eigh_f64(const double *H, double *W, double *V, int32_t *sweeps, i
                        int64_t batch, int32_t n, double tol, int32_t max_sweeps,
                        void *workspace, size_t workspace_bytes, void *stream);
 
+/* Batched Householder QR of tall matrices (m >= n): replaces the reference's
+ * primitives.qr, svdbench/standalone/primitives.py:74-89 (reflectors by
+ * householder_vec :41-59, the LAPACK xLARFG convention; Q by backward
+ * accumulation), the QR of its 'qr', 'tsqr' and projected solvers
+ * (solvers.py:71-96, 185-220, 245-248).  A (batch, m, n) row-major in;
+ * Q (batch, m, n) and R (batch, n, n, upper triangular) row-major out;
+ * computed in the input type.  Workspace: jb_qr_workspace_bytes (0 when a
+ * matrix and its Q fit in shared memory). */
+JB_API size_t jb_qr_workspace_bytes(int32_t m, int32_t n, int64_t batch, int32_t elem);
+JB_API int jb_qr_f32(const float *A, float *Q, float *R, int64_t batch, int32_t m, int32_t n,
+                     void *workspace, size_t workspace_bytes, void *stream);
+JB_API int jb_qr_f64(const double *A, double *Q, double *R, int64_t batch, int32_t m, int32_t n,
+                     void *workspace, size_t workspace_bytes, void *stream);
+
 /* Size of the fixed device scratch array of jb_svd_batched_f32_noalloc. */
 #define JB_NOALLOC_SCRATCH_BYTES (16u << 20)
 

@@ -14,8 +14,12 @@ exactly like the PyTorch original:
   jacobi_eigh            svdbench/standalone/primitives.py:370-427 (real dtypes)
   complete_null_columns  svdbench/standalone/primitives.py:430-455
   complete_basis         svdbench/standalone/primitives.py:458-467
-  svd                    svdbench/standalone/solvers.py:264-310 ('jacobi' only)
-  raw                    svdbench/standalone/solvers.py:224-230
+  householder_vec / qr   svdbench/standalone/primitives.py:41-89
+  tsqr                   svdbench/standalone/solvers.py:71-96
+  partial                svdbench/standalone/solvers.py:185-220 (given initial_basis)
+  svd                    svdbench/standalone/solvers.py:264-310 ('jacobi', 'qr', 'tsqr',
+                         'randomized', 'subspace', 'block_krylov')
+  raw                    svdbench/standalone/solvers.py:224-248
   reference / validate   svdbench/metrics.py:6-66 (FP64 LAPACK gesvd truth)
 
 Parity of this restatement is pinned against fixtures produced by the
@@ -26,7 +30,7 @@ from __future__ import annotations
 import numpy as np
 
 __all__ = ["round_robin", "jacobi_svd", "jacobi_eigh", "complete_null_columns", "complete_basis",
-           "svd", "raw", "reference", "validate", "eps"]
+           "householder_vec", "qr", "tsqr", "partial", "svd", "raw", "reference", "validate", "eps"]
 
 
 def _real(dt):
@@ -163,21 +167,154 @@ def complete_basis(q, size):
     return complete_null_columns(np.concatenate([q, z], -1), keep)
 
 
-def raw(x, opts, stats):
-    """Wide inputs are solved through their adjoint (solvers.py:224-230)."""
-    if x.shape[-2] < x.shape[-1]:
-        u, s, v = raw(np.conj(np.swapaxes(x, -1, -2)), opts, stats)
+def householder_vec(x):
+    """Reflector of the rows of x (b, k), LAPACK xLARFG convention
+    (primitives.py:41-59): v (v_0 = 1), tau, beta with
+    (I - tau v v^H)^H x = beta e_1; a row with nothing below its first entry
+    (and a real first entry) gets v = 0, tau = 0, beta = x_0."""
+    b, k = x.shape
+    rdt = _real(x.dtype)
+    alpha = x[:, 0]
+    xnorm = np.sqrt((np.abs(x[:, 1:]) ** 2).sum(-1)).astype(rdt) if k > 1 else np.zeros(b, rdt)
+    ar = alpha.real.astype(rdt)
+    ai = alpha.imag.astype(rdt) if np.iscomplexobj(x) else np.zeros_like(ar)
+    beta = (-np.sign(ar + (ar == 0)) * np.hypot(np.abs(alpha).astype(rdt), xnorm)).astype(rdt)
+    trivial = (xnorm == 0) & (ai == 0)
+    beta = np.where(trivial, ar, beta).astype(rdt)
+    bx = beta.astype(x.dtype)
+    denom = np.where(trivial, np.ones_like(alpha), alpha - bx)
+    tau = np.where(trivial, np.zeros_like(alpha), (bx - alpha) / np.where(beta != 0, bx, np.ones_like(bx)))
+    v = x / denom[:, None]
+    v[:, 0] = 1
+    v = np.where(trivial[:, None], np.zeros_like(v), v)
+    return v.astype(x.dtype), tau.astype(x.dtype), beta
+
+
+def _apply_left(A, v, tau):
+    """(I - tau v v^H) A for A (b, k, c) (primitives.py:62-65)."""
+    w = (np.conj(v)[:, :, None] * A).sum(-2)
+    return A - tau[:, None, None] * v[:, :, None] * w[:, None, :]
+
+
+def qr(A):
+    """Householder QR of tall A (b, m, n): Q (b, m, n), R (b, n, n), Q by
+    backward accumulation (primitives.py:74-89)."""
+    A = np.array(A, copy=True)
+    b, m, n = A.shape
+    vs, taus = [], []
+    for j in range(n):
+        v, tau, beta = householder_vec(A[:, j:, j])
+        A[:, j:, j + 1:] = _apply_left(A[:, j:, j + 1:], v, np.conj(tau))
+        A[:, j, j] = beta
+        A[:, j + 1:, j] = 0
+        vs.append(v)
+        taus.append(tau)
+    R = np.triu(A[:, :n, :])
+    Q = np.zeros((b, m, n), A.dtype)
+    Q[:, :n, :] = np.eye(n, dtype=A.dtype)
+    for j in range(n - 1, -1, -1):
+        Q[:, j:, :] = _apply_left(Q[:, j:, :], vs[j], taus[j])
+    return Q, R
+
+
+def tsqr(a, rows, stats):
+    """Tall-skinny QR: QR of row tiles of `rows` rows (a short last tile joins
+    the one before), a binary reduction tree over the stacked R factors and
+    the tree back-transformation of Q (solvers.py:71-96)."""
+    b, m, n = a.shape
+    rows = max(rows, n)
+    if m <= rows:
+        return qr(a)
+    leaves = []
+    for start in range(0, m, rows):
+        end = min(start + rows, m)
+        if end - start < n:
+            start = leaves.pop()[0]
+        q, r = qr(a[:, start:end])
+        leaves.append((start, q, r))
+    stats["tsqr_leaves"] = len(leaves)
+    nodes = [(q, r) for _, q, r in leaves]
+    while len(nodes) > 1:
+        nxt = []
+        for i in range(0, len(nodes), 2):
+            if i + 1 == len(nodes):
+                nxt.append(nodes[i])
+                continue
+            (q1, r1), (q2, r2) = nodes[i], nodes[i + 1]
+            q, r = qr(np.concatenate([r1, r2], -2))
+            nxt.append((np.concatenate([q1 @ q[:, :n], q2 @ q[:, n:]], -2), r))
+        nodes = nxt
+    return nodes[0]
+
+
+def partial(a, stats, opts, method):
+    """Projected solvers 'randomized', 'subspace', 'block_krylov'
+    (solvers.py:185-220) from a given start basis opts['initial_basis']
+    (b, n, rank + oversample): the reference draws it from torch's generator
+    otherwise, which NumPy cannot reproduce."""
+    k = opts.get("rank", min(a.shape[-2:]))
+    ell = min(k + opts.get("oversample", 8), min(a.shape[-2:]))
+    omega = np.asarray(opts["initial_basis"])
+    if omega.ndim == 2:
+        omega = omega[None]
+    if omega.shape != (a.shape[0], a.shape[-1], ell):
+        raise ValueError("initial_basis shape must match batch, n, rank+oversample")
+    omega = omega.astype(a.dtype)
+    stats["warm_started"] = True
+    q, _ = qr(a @ omega)
+    bases = [q]
+    iterations = opts.get("iterations", 2)
+    ah = np.conj(np.swapaxes(a, -1, -2))
+    for _ in range(iterations):
+        z, _ = qr(ah @ q)
+        y = a @ z
+        if method == "block_krylov":
+            joined = np.concatenate(bases, -1)
+            available = a.shape[-2] - joined.shape[-1]
+            if available <= 0:
+                break
+            jh = np.conj(np.swapaxes(joined, -1, -2))
+            for _ in range(2):
+                y = y - joined @ (jh @ y)
+            q, _ = qr(y[:, :, :min(ell, available)])
+            bases.append(q)
+        else:
+            q, _ = qr(y)
+    if method == "block_krylov":
+        q, _ = qr(np.concatenate(bases, -1))
+    small = np.conj(np.swapaxes(q, -1, -2)) @ a
+    u, s, v = raw(small, opts, stats, "jacobi")
+    stats.update(sketch_columns=ell, range_columns=q.shape[-1], power_iterations=iterations)
+    return (q @ u)[:, :, :k], s[:, :k], v[:, :, :k]
+
+
+PARTIAL = ("randomized", "subspace", "block_krylov")
+
+
+def raw(x, opts, stats, method="jacobi"):
+    """Wide inputs are solved through their adjoint, except by the projected
+    solvers (solvers.py:224-230); then 'jacobi' (:229-230), 'qr' / 'tsqr'
+    (:245-248) or the projected solvers (:253-254)."""
+    if x.shape[-2] < x.shape[-1] and method not in PARTIAL:
+        u, s, v = raw(np.conj(np.swapaxes(x, -1, -2)), opts, stats, method)
         return v, s, u
+    if method in ("qr", "tsqr"):
+        q, r = qr(x) if method == "qr" else tsqr(x, opts.get("tile_rows", 4 * x.shape[-1]), stats)
+        u, s, v = raw(r, opts, stats, "jacobi")
+        return q @ u, s, v
+    if method in PARTIAL:
+        return partial(x, stats, opts, method)
     u, s, v, sweeps = jacobi_svd(x, tol=opts.get("tol"), max_sweeps=opts.get("max_sweeps", 60))
     stats["jacobi_sweeps"] = max(stats.get("jacobi_sweeps", 0), sweeps)   # solvers.py:24-27
     return u, s, v
 
 
 def svd(a, algorithm="jacobi", *, full_matrices=False, values_only=False, return_info=False, **opts):
-    """NumPy restatement of the public entry (solvers.py:264-310), 'jacobi' only."""
+    """NumPy restatement of the public entry (solvers.py:264-310) for the
+    Jacobi-based algorithms."""
     a = np.asarray(a)
-    if algorithm != "jacobi":
-        raise ValueError("the oracle restates the 'jacobi' family only")
+    if algorithm not in ("jacobi", "qr", "tsqr") + PARTIAL:
+        raise ValueError("the oracle restates the Jacobi-based algorithms only")
     if a.ndim < 2 or min(a.shape[-2:]) < 1:
         raise ValueError("nonempty matrix dimensions required")
     if a.dtype not in (np.float32, np.float64, np.complex64, np.complex128):
@@ -200,7 +337,7 @@ def svd(a, algorithm="jacobi", *, full_matrices=False, values_only=False, return
     scale = np.abs(x).max((-2, -1), keepdims=True)                # solvers.py:294-295
     scale = np.where(scale > 0, scale, 1).astype(_real(a.dtype))
     stats = {"algorithm": algorithm, "vendor_factorizations": 0, "converged": True}
-    u, s, v = raw((x / scale).astype(a.dtype), opts, stats)
+    u, s, v = raw((x / scale).astype(a.dtype), opts, stats, algorithm)
     s = s * scale[:, 0, 0][:, None]
     if full_matrices:
         u = complete_basis(u, a.shape[-2])

@@ -34,7 +34,7 @@ REFERENCE_ALGORITHMS = (
     'gram_jacobi', 'gram_dc', 'polar_qdwh', 'polar_newton_schulz',
     'polar_halley', 'polar_polynomial', 'randomized', 'subspace', 'block_krylov', 'lanczos',
 )  # svdbench/standalone/solvers.py:7-11
-ALGORITHMS = ('jacobi', 'block_jacobi', 'gram_jacobi')
+ALGORITHMS = ('jacobi', 'block_jacobi', 'gram_jacobi', 'qr', 'tsqr', 'randomized', 'subspace', 'block_krylov')
 PRECISIONS = ('mixed', 'fp32')
 ORDERINGS = ('block', 'round_robin')
 
@@ -138,13 +138,18 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
     solvers.py:24-27), ``rank``, ``precision`` and ``ordering``; other
     options are accepted and ignored, as the reference's Jacobi ignores them.
     algorithm='block_jacobi' (solvers.py:30-68) runs the tensor-core blocked
-    solver on each matrix of the batch (see _block_svd).
+    solver on each matrix of the batch (see _block_svd); 'gram_jacobi' the
+    GPU jacobi_eigh of the Gram (_gram_svd); 'qr', 'tsqr', 'randomized',
+    'subspace' and 'block_krylov' the GPU Householder QR around the batched
+    Jacobi (_qr_family_svd).
     Input is never overwritten."""
     rank, precision = _validate(a, algorithm, full_matrices, opts)
     if algorithm == 'block_jacobi':
         return _block_svd(a, full_matrices, values_only, return_info, rank, opts)
     if algorithm == 'gram_jacobi':
         return _gram_svd(a, full_matrices, values_only, return_info, rank, opts)
+    if algorithm in ('qr', 'tsqr', 'randomized', 'subspace', 'block_krylov'):
+        return _qr_family_svd(a, algorithm, full_matrices, values_only, return_info, rank, opts)
     max_sweeps = opts.get('max_sweeps', 60)
     tol = opts.get('tol')
     shape = a.shape[:-2]
@@ -261,6 +266,59 @@ def _gram_svd(a, full_matrices, values_only, return_info, rank, opts):
     stats = {'algorithm': 'gram_jacobi', 'vendor_factorizations': 0, 'converged': True, 'eigen_sweeps': it,
              'gram_discarded_values': int((~keep).sum()),
              'implementation': 'B200 sm_100a two-sided Jacobi (jacobi_eigh) on the Gram'}
+    return (*result, stats) if return_info else result
+
+
+def _complete_basis(q, size):
+    """Extend the orthonormal columns of q (b, m, k) to `size` columns by
+    null completion (primitives.py:458-467)."""
+    b, m, k = q.shape
+    if size == k:
+        return q
+    z = torch.zeros(b, m, size - k, dtype=q.dtype, device=q.device)
+    keep = torch.arange(size, device=q.device)[None, :].expand(b, size) < k
+    return _complete_null_columns(torch.cat([q, z], -1), keep)
+
+
+def _qr_family_svd(a, algorithm, full_matrices, values_only, return_info, rank, opts):
+    """'qr', 'tsqr' (solvers.py:71-96, 245-248) and the projected solvers
+    'randomized', 'subspace', 'block_krylov' (:185-220) through the public
+    entry (:264-310): the batch scaled by a power of two (exact) before any
+    sums of squares, the method (qr.raw: GPU Householder QRs, library GEMMs in
+    the input dtype, the batched Jacobi of the small factor), then sigma
+    rescaled, full bases completed or the rank truncated, the output checked.
+    Options: those of the reference's method (tile_rows, rank, oversample,
+    iterations, seed, initial_basis) and of the Jacobi solve (tol,
+    max_sweeps, precision, ordering)."""
+    from . import qr as Q
+    m, n = a.shape[-2:]
+    shape = a.shape[:-2]
+    stats = {'algorithm': algorithm, 'vendor_factorizations': 0, 'converged': True}
+    jopts = {key: opts[key] for key in ('tol', 'max_sweeps', 'precision', 'ordering') if key in opts}
+
+    def jacobi(y):
+        u, s, vh, info = svd(y.contiguous(), 'jacobi', return_info=True, **jopts)
+        stats['jacobi_sweeps'] = max(stats.get('jacobi_sweeps', 0), info['jacobi_sweeps'])
+        return u, s, vh.mH
+
+    with torch.no_grad(), torch.cuda.device(a.device):
+        x = a.detach().reshape(-1, m, n)
+        if not bool(torch.isfinite(x).all()):
+            raise ValueError('input contains NaN or infinity')
+        amax = x.abs().amax((-2, -1), keepdim=True)
+        e = torch.where(amax > 0, torch.frexp(amax)[1], torch.zeros_like(amax, dtype=torch.int32))
+        scale = torch.ldexp(torch.ones_like(amax), e)
+        u, sv, v = Q.raw((x / scale).contiguous(), algorithm, stats, opts, jacobi)
+        sv = sv * scale[:, 0, :]
+        if full_matrices:
+            u, v = _complete_basis(u, m), _complete_basis(v, n)
+        else:
+            u, sv, v = u[:, :, :rank], sv[:, :rank], v[:, :, :rank]
+        if not all(bool(torch.isfinite(t).all()) for t in (u, sv, v)):
+            raise RuntimeError('standalone solver produced nonfinite output')
+        result = (None if values_only else u.reshape(*shape, *u.shape[-2:]), sv.reshape(*shape, sv.shape[-1]),
+                  None if values_only else v.mH.reshape(*shape, v.shape[-1], v.shape[-2]))
+    stats['implementation'] = 'B200 sm_100a Householder QR + batched one-sided Jacobi'
     return (*result, stats) if return_info else result
 
 

@@ -44,6 +44,33 @@ def golden_eigh():
     return {str(n): {k: z[f"eigh_{n}/{k}"] for k in ("h", "w", "v", "sweeps", "truth")} for n in z["_eigh_names"]}
 
 
+def golden_qr():
+    """The reference's primitives.qr outputs (a, q, r) by case."""
+    z = np.load(GOLDEN, allow_pickle=False)
+    return {str(n): {k: z[f"qr_{n}/{k}"] for k in ("a", "q", "r")} for n in z["_qr_names"]}
+
+
+def golden_methods():
+    """The reference's svd() through its QR-based methods: input, algorithm,
+    options (with the stored start basis of the projected solvers), U, s, Vh,
+    FP64 truth."""
+    z = np.load(GOLDEN, allow_pickle=False)
+    out = {}
+    for n in z["_meth_names"]:
+        c = {k: z[f"meth_{n}/{k}"] for k in ("a", "u", "s", "vh", "truth")}
+        c["alg"] = str(z[f"meth_{n}/alg"])
+        c["kw"] = eval(str(z[f"meth_{n}/kw"]))
+        if f"meth_{n}/initial_basis" in z.files:
+            c["initial_basis"] = z[f"meth_{n}/initial_basis"]
+        out[str(n)] = c
+    return out
+
+
+# Columns of Q (and rows of R) fixed by the input, by QR case: beyond them a
+# rank-deficient input leaves Q to rounding noise.
+QR_DETERMINED = {"deficient_f64": 4}
+
+
 @pytest.fixture(scope="session")
 def workloads():
     return importlib.import_module("pavel-s_svd_b200.workloads")

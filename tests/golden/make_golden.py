@@ -9,8 +9,10 @@ It imports the reference's ``svdbench.standalone.svd`` and
 ``svdbench.matrices.make_matrix`` unchanged, runs ``svd(x, 'jacobi', ...)``
 on CPU (1 thread, as the reference's own tests do) and writes
 ``tests/golden/reference_jacobi.npz``: for every case the input, the
-reference's U, s, Vh, jacobi_sweeps, and SciPy FP64 singular values.  The
-GPU box never runs this script; tests read only the .npz.
+reference's U, s, Vh, jacobi_sweeps, and SciPy FP64 singular values; the
+reference's jacobi_eigh, qr and QR-based solvers ('qr', 'tsqr' and the
+projected ones from a stored start basis) on their own cases.  The GPU box
+never runs this script; tests read only the .npz.
 """
 from __future__ import annotations
 
@@ -91,6 +93,47 @@ def eigh_cases(make_matrix):
     return out
 
 
+def qr_cases(make_matrix):
+    """(name, batch of tall matrices) for primitives.qr (primitives.py:74-89):
+    Gaussian in both dtypes, square, a zero column and a repeated column (the
+    reflector's trivial and rank-deficient branches), a tall f32 batch."""
+    out = []
+    for dt in ("float32", "float64"):
+        out.append((f"gauss_{dt}", make_matrix(dict(m=20, n=7, batch=3, dtype=dt, family="gaussian"))))
+    out.append(("square_f64", make_matrix(dict(m=16, n=16, batch=2, dtype="float64", family="gaussian"))))
+    a = make_matrix(dict(m=18, n=6, batch=2, dtype="float64", family="gaussian")).copy()
+    a[:, :, 2] = 0.0
+    a[:, :, 4] = a[:, :, 1]
+    a[1, 3:, 5] = 0.0
+    out.append(("deficient_f64", a))
+    out.append(("tall_f32", make_matrix(dict(m=130, n=33, batch=2, dtype="float32", family="gaussian"))))
+    return out
+
+
+def method_cases(make_matrix):
+    """(name, input, algorithm, kwargs) for the Jacobi-based methods built on
+    QR: 'qr' and 'tsqr' (solvers.py:71-96, 245-248), tall and wide, with
+    tiles that force several leaves and a merged short last leaf; the
+    projected solvers (solvers.py:185-220) from a stored start basis
+    (initial_basis), since their own sketch comes from torch's generator."""
+    rng = np.random.default_rng(41)
+    out = []
+    for dt in ("float32", "float64"):
+        out.append((f"qr_{dt}", make_matrix(dict(m=40, n=12, batch=3, dtype=dt, family="gaussian")), "qr", {}))
+        out.append((f"qr_wide_{dt}", make_matrix(dict(m=9, n=20, batch=2, dtype=dt, family="gaussian")), "qr", {}))
+        out.append((f"tsqr_{dt}", make_matrix(dict(m=53, n=8, batch=2, dtype=dt, family="gaussian")), "tsqr",
+                    {"tile_rows": 10}))
+        a = make_matrix(dict(m=30, n=12, batch=2, dtype=dt, family="geometric", condition=1e3))
+        for alg, rank, over, it in (("randomized", 4, 3, 2), ("subspace", 5, 2, 3), ("block_krylov", 3, 2, 2)):
+            om = rng.standard_normal((2, 12, rank + over)).astype(dt)
+            out.append((f"{alg}_{dt}", a, alg, {"rank": rank, "oversample": over, "iterations": it,
+                                                "initial_basis": om}))
+    a = make_matrix(dict(m=10, n=26, batch=2, dtype="float64", family="gaussian"))
+    out.append(("randomized_wide_float64", a, "randomized",
+                {"rank": 4, "oversample": 4, "initial_basis": rng.standard_normal((2, 26, 8))}))
+    return out
+
+
 def main():
     sys.path.insert(0, str(REF))
     import torch
@@ -131,6 +174,33 @@ def main():
         enames.append(name)
         print(f"eigh {name:22s} {str(h.shape):14s} {h.dtype}  sweeps={sw}")
     blob["_eigh_names"] = np.array(enames)
+    # primitives.qr: the reference's Q and R
+    qnames = []
+    for name, a in qr_cases(make_matrix):
+        a = np.ascontiguousarray(a)
+        q, r = P.qr(torch.from_numpy(a.copy()))
+        blob[f"qr_{name}/a"], blob[f"qr_{name}/q"], blob[f"qr_{name}/r"] = a, q.numpy(), r.numpy()
+        qnames.append(name)
+        print(f"qr {name:24s} {str(a.shape):14s} {a.dtype}")
+    blob["_qr_names"] = np.array(qnames)
+    # the QR-based solvers through the public svd()
+    mnames = []
+    for name, a, alg, kw in method_cases(make_matrix):
+        a = np.ascontiguousarray(a)
+        tkw = {k: (torch.from_numpy(np.ascontiguousarray(v)) if isinstance(v, np.ndarray) else v) for k, v in kw.items()}
+        u, s, vh, info = svd(torch.from_numpy(a.copy()), alg, return_info=True, **tkw)
+        flat = a.reshape(-1, *a.shape[-2:]).astype(np.float64)
+        blob[f"meth_{name}/a"] = a
+        blob[f"meth_{name}/u"], blob[f"meth_{name}/s"], blob[f"meth_{name}/vh"] = u.numpy(), s.numpy(), vh.numpy()
+        blob[f"meth_{name}/truth"] = np.stack([scipy.linalg.svd(x, compute_uv=False, lapack_driver="gesvd")
+                                               for x in flat])
+        blob[f"meth_{name}/alg"] = np.array(alg)
+        blob[f"meth_{name}/kw"] = np.array(repr({k: v for k, v in kw.items() if k != "initial_basis"}))
+        if "initial_basis" in kw:
+            blob[f"meth_{name}/initial_basis"] = np.ascontiguousarray(kw["initial_basis"])
+        mnames.append(name)
+        print(f"{alg} {name:24s} {str(a.shape):14s} {a.dtype}  sweeps={info.get('jacobi_sweeps')}")
+    blob["_meth_names"] = np.array(mnames)
     np.savez_compressed(HERE / "reference_jacobi.npz", **blob)
     print("wrote", HERE / "reference_jacobi.npz")
 

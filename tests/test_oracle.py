@@ -5,7 +5,7 @@ import pytest
 
 from oracle import jacobi_oracle as O
 from oracle import c_oracle as C
-from conftest import sigma_tol
+from conftest import QR_DETERMINED, golden_methods, golden_qr, sigma_tol
 
 
 def _cmp_sigma(s, ref, dtype, factor=1.0):
@@ -174,3 +174,42 @@ def test_eigh_oracle_raises_like_reference():
     h = h + h.transpose(0, 2, 1)
     with pytest.raises(RuntimeError, match="did not converge in 1 sweeps"):
         O.jacobi_eigh(h, max_sweeps=1)
+
+
+def test_qr_oracle_matches_reference():
+    """The NumPy restatement of primitives.qr (primitives.py:41-89) against
+    the reference's own Q and R: the same reflectors in the same dtype agree
+    to rounding.  Where a rank-deficient input leaves columns of Q to
+    rounding noise, those are checked by Q R = A and Q^T Q = I only."""
+    for name, g in golden_qr().items():
+        a, qr_, rr = g["a"], g["q"], g["r"]
+        q, r = O.qr(a)
+        k = QR_DETERMINED.get(name, a.shape[-1])
+        tol = 50 * np.finfo(a.dtype).eps * max(1.0, float(np.abs(a).max()))
+        assert float(np.abs(q[..., :k] - qr_[..., :k]).max()) <= tol, name
+        assert float(np.abs(r[..., :k, :] - rr[..., :k, :]).max()) <= tol * a.shape[-2], name
+        assert float(np.abs(q @ r - a).max()) <= tol * a.shape[-2], name
+        eye = np.eye(a.shape[-1])
+        assert float(np.abs(np.swapaxes(q, -1, -2) @ q - eye).max()) <= tol * a.shape[-2], name
+        assert np.array_equal(r, np.triu(r)), name
+
+
+def test_qr_methods_oracle_matches_reference():
+    """svd() through 'qr', 'tsqr' and the projected solvers (solvers.py:71-96,
+    185-220, 245-248), restated in NumPy, against the reference's U, s, Vh on
+    the same inputs and start bases."""
+    for name, g in golden_methods().items():
+        kw = dict(g["kw"])
+        if "initial_basis" in g:
+            kw["initial_basis"] = g["initial_basis"]
+        u, s, vh = O.svd(g["a"], g["alg"], **kw)
+        dt = g["a"].dtype
+        _cmp_sigma(s, g["s"], dt)
+        _cmp_vectors(u, g["u"], g["s"], dt, -1)
+        _cmp_vectors(vh, g["vh"], g["s"], dt, -2)
+        # as accurate against FP64 truth as the reference (the projected
+        # solvers are approximations: their own error is the bar)
+        k = s.shape[-1]
+        err = float(np.abs(s - g["truth"][..., :k]).max() / g["truth"].max())
+        err_ref = float(np.abs(g["s"] - g["truth"][..., :k]).max() / g["truth"].max())
+        assert err <= max(2 * err_ref, 10 * sigma_tol(dt)), name
