@@ -337,6 +337,24 @@ JB_API int jb_qr_f32(const float *A, float *Q, float *R, int64_t batch, int32_t 
 JB_API int jb_qr_f64(const double *A, double *Q, double *R, int64_t batch, int32_t m, int32_t n,
                      void *workspace, size_t workspace_bytes, void *stream);
 
+/* Batched one-sided Jacobi SVD of complex matrices: replaces the reference's
+ * jacobi_svd for complex64 / complex128 (svdbench/standalone/primitives.py:
+ * 316-367, with the phase-aware rotation s = t c apq / |apq| of :345-351),
+ * in its round-robin order and input precision.  A (batch, m, n), m >= n
+ * (a wide matrix is solved through its conjugate transpose by the caller),
+ * interleaved (re, im), row-major; U (batch, m, n) with zero columns where
+ * sigma is cut (the caller completes them), S (batch, n) real, descending,
+ * 0 where cut; Vh (batch, n, n).  Workspace: jb_svd_complex_workspace_bytes
+ * (elem = 8 for complex64, 16 for complex128; 0 when W and V fit in
+ * shared memory). */
+JB_API size_t jb_svd_complex_workspace_bytes(int32_t m, int32_t n, int64_t batch, int32_t elem);
+JB_API int jb_svd_batched_c64(const void *A, void *U, float *S, void *Vh, int64_t batch, int32_t m, int32_t n,
+                              double tol, int32_t max_sweeps, int32_t *sweeps, int32_t *status,
+                              void *workspace, size_t workspace_bytes, void *stream);
+JB_API int jb_svd_batched_c128(const void *A, void *U, double *S, void *Vh, int64_t batch, int32_t m, int32_t n,
+                               double tol, int32_t max_sweeps, int32_t *sweeps, int32_t *status,
+                               void *workspace, size_t workspace_bytes, void *stream);
+
 /* Size of the fixed device scratch array of jb_svd_batched_f32_noalloc. */
 #define JB_NOALLOC_SCRATCH_BYTES (16u << 20)
 

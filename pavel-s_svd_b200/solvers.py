@@ -66,8 +66,8 @@ def _validate(a, algorithm, full_matrices, opts):
         raise Unsupported(f'{algorithm!r} is not implemented by the B200 solver (implemented: {ALGORITHMS})')
     if a.device.type != 'cuda':
         raise Unsupported('the B200 Jacobi solver runs on CUDA tensors only; there is no CPU fallback')
-    if a.is_complex():
-        raise Unsupported('complex Jacobi is not implemented by the B200 solver yet')
+    if a.is_complex() and algorithm != 'jacobi':
+        raise Unsupported(f'complex input runs through jacobi only in the B200 solver, not {algorithm!r}')
     precision = opts.get('precision', 'mixed')
     if precision not in PRECISIONS:
         raise ValueError(f'precision must be one of {PRECISIONS}')
@@ -144,6 +144,8 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
     Jacobi (_qr_family_svd).
     Input is never overwritten."""
     rank, precision = _validate(a, algorithm, full_matrices, opts)
+    if a.is_complex():
+        return _complex_svd(a, full_matrices, values_only, return_info, rank, opts)
     if algorithm == 'block_jacobi':
         return _block_svd(a, full_matrices, values_only, return_info, rank, opts)
     if algorithm == 'gram_jacobi':
@@ -197,20 +199,21 @@ def _complete_null_columns(u, keep):
     u = torch.where(keep[:, None, :], u, torch.zeros_like(u))
     b, m, n = u.shape
     rows = torch.arange(b, device=u.device)
-    tiny = torch.finfo(u.dtype).eps * 10
+    real = u.real.dtype if u.is_complex() else u.dtype
+    tiny = torch.finfo(real).eps * 10
     for j in range(n):
         missing = ~keep[:, j]
         if not bool(missing.any()):
             continue
-        lev = 1 - (u * u).sum(-1)
+        lev = 1 - (u.abs() ** 2).sum(-1)
         v = torch.zeros(b, m, 1, dtype=u.dtype, device=u.device)
         v[rows, lev.argmax(-1), 0] = 1
         for _ in range(2):
-            v = v - u @ (u.transpose(1, 2) @ v)
-        length = (v * v).sum(-2, keepdim=True).sqrt()
+            v = v - u @ (u.mH @ v)
+        length = (v.abs() ** 2).sum(-2, keepdim=True).sqrt()
         if bool((length[missing] < tiny).any()):
             raise RuntimeError("null-space completion failed: supplied live columns are not independent")
-        v = v / length.clamp_min(torch.finfo(u.dtype).tiny)
+        v = v / length.clamp_min(torch.finfo(real).tiny)
         u[:, :, j] = torch.where(missing[:, None], v[:, :, 0], u[:, :, j])
     return u
 
@@ -266,6 +269,69 @@ def _gram_svd(a, full_matrices, values_only, return_info, rank, opts):
     stats = {'algorithm': 'gram_jacobi', 'vendor_factorizations': 0, 'converged': True, 'eigen_sweeps': it,
              'gram_discarded_values': int((~keep).sum()),
              'implementation': 'B200 sm_100a two-sided Jacobi (jacobi_eigh) on the Gram'}
+    return (*result, stats) if return_info else result
+
+
+def _complex_svd(a, full_matrices, values_only, return_info, rank, opts):
+    """'jacobi' on complex64 / complex128 (primitives.py:316-367 in the input
+    precision, round-robin order; solvers.py:264-310 around it): the batch
+    scaled by a power of two (exact), a wide matrix solved through its
+    conjugate transpose (:224-227), one launch of jb_svd_batched_c64/_c128,
+    then the cut columns of U completed (primitives.py:430-455), sigma
+    rescaled, full bases completed or the rank truncated, the output
+    checked.  Options tol and max_sweeps; the FP32/mixed and ordering options
+    of the real path do not apply."""
+    m, n = a.shape[-2:]
+    shape = a.shape[:-2]
+    max_sweeps = opts.get('max_sweeps', 60)
+    with torch.no_grad(), torch.cuda.device(a.device):
+        x = a.detach().reshape(-1, m, n)
+        if not bool(torch.isfinite(x).all()):
+            raise ValueError('input contains NaN or infinity')
+        amax = x.abs().amax((-2, -1), keepdim=True)
+        e = torch.where(amax > 0, torch.frexp(amax)[1], torch.zeros_like(amax, dtype=torch.int32))
+        scale = torch.ldexp(torch.ones_like(amax), e)
+        wide = m < n
+        xs = (x / scale).mH if wide else x / scale
+        xs = xs.resolve_conj().contiguous()   # the kernel reads memory: no lazy conjugate view
+        b, mt, nt = xs.shape
+        real = a.real.dtype
+        u = torch.empty(b, mt, nt, dtype=a.dtype, device=a.device)
+        sv = torch.empty(b, nt, dtype=real, device=a.device)
+        vh = torch.empty(b, nt, nt, dtype=a.dtype, device=a.device)
+        info = torch.zeros(2, max(b, 1), dtype=torch.int32, device=a.device)
+        if b:
+            lib = N.lib()
+            elem = xs.element_size()
+            ws = _default_ws.setdefault(a.device, Workspace()).get(
+                lib.jb_svd_complex_workspace_bytes(mt, nt, b, elem), a.device)
+            fn = lib.jb_svd_batched_c64 if a.dtype == torch.complex64 else lib.jb_svd_batched_c128
+            N.check(fn(xs.data_ptr(), u.data_ptr(), sv.data_ptr(), vh.data_ptr(), b, mt, nt,
+                       float(opts.get('tol') or 0.0), max_sweeps, info[0].data_ptr(), info[1].data_ptr(),
+                       ws.data_ptr(), ws.numel(), torch.cuda.current_stream(a.device).cuda_stream),
+                    'jb_svd_batched_complex')
+            host = info[:, :b].cpu()
+            raise_for_status(host[1], max_sweeps)
+            sweeps = int(host[0].max())
+        else:
+            sweeps = 0
+        u = _complete_null_columns(u, sv > 0)
+        sv = sv * scale[:, 0, :]
+        v = vh.mH
+        if wide:
+            u, v = v, u
+        if full_matrices:
+            u, v = _complete_basis(u, m), _complete_basis(v, n)
+        else:
+            u, sv, v = u[:, :, :rank], sv[:, :rank], v[:, :, :rank]
+        if not all(bool(torch.isfinite(t).all()) for t in (u, sv, v)):
+            raise RuntimeError('standalone solver produced nonfinite output')
+        result = (None if values_only else u.resolve_conj().reshape(*shape, *u.shape[-2:]),
+                  sv.reshape(*shape, sv.shape[-1]),
+                  None if values_only else v.mH.resolve_conj().reshape(*shape, v.shape[-1], v.shape[-2]))
+    stats = {'algorithm': 'jacobi', 'vendor_factorizations': 0, 'converged': True, 'jacobi_sweeps': sweeps,
+             'precision': 'fp32' if a.dtype == torch.complex64 else 'fp64',
+             'implementation': 'B200 sm_100a complex one-sided Jacobi (round-robin, one launch)'}
     return (*result, stats) if return_info else result
 
 

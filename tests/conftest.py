@@ -66,6 +66,19 @@ def golden_methods():
     return out
 
 
+def golden_complex():
+    """The reference's svd(x, 'jacobi') on complex inputs: a, U, s, Vh,
+    sweeps, FP64 truth, options."""
+    z = np.load(GOLDEN, allow_pickle=False)
+    out = {}
+    for n in z["_cx_names"]:
+        c = {k: z[f"cx_{n}/{k}"] for k in ("a", "u", "s", "vh", "truth")}
+        c["sweeps"] = int(z[f"cx_{n}/sweeps"])
+        c["kw"] = eval(str(z[f"cx_{n}/kw"]))
+        out[str(n)] = c
+    return out
+
+
 # Columns of Q (and rows of R) fixed by the input, by QR case: beyond them a
 # rank-deficient input leaves Q to rounding noise.
 QR_DETERMINED = {"deficient_f64": 4}
@@ -79,4 +92,4 @@ def workloads():
 def sigma_tol(dtype):
     """Agreement bound on sigma (relative to sigma_1) between two correct
     implementations: single precision 1e-5 (the accuracy bound of the mixed path), double 1e-12."""
-    return 1e-5 if np.dtype(dtype) == np.float32 else 1e-12
+    return 1e-5 if np.dtype(dtype) in (np.float32, np.complex64) else 1e-12

@@ -134,6 +134,31 @@ def method_cases(make_matrix):
     return out
 
 
+def complex_cases(make_matrix):
+    """(name, input, svd kwargs) for 'jacobi' on complex dtypes: the
+    reference's own complex test inputs (tests/test_standalone.py:47-54,
+    68-80, 92-98, 187-194) -- Gaussian tall and wide batches in both
+    precisions, full bases of small shapes, a rank-4 matrix (cut values and
+    null completion), a multi-dimensional batch -- plus a zero matrix and a
+    truncated rank."""
+    out = []
+    for dt in ("complex64", "complex128"):
+        for m, n in ((13, 7), (7, 13)):
+            out.append((f"gauss_{dt}_{m}x{n}_b2", make_matrix(dict(m=m, n=n, batch=2, dtype=dt, family="gaussian")),
+                        {}))
+    for shape in ((1, 1), (8, 1), (1, 8), (10, 4), (4, 10)):
+        a = make_matrix(dict(m=shape[0], n=shape[1], family="gaussian", dtype="complex128"))
+        out.append((f"full_{shape[0]}x{shape[1]}", a, {"full_matrices": True}))
+    out.append(("rank4_40x25", make_matrix(dict(m=40, n=25, dtype="complex128", family="low_rank", rank=4, tail=0)),
+                {}))
+    rng = np.random.default_rng(23)
+    out.append(("multidim_2x3x9x5", rng.normal(size=(2, 3, 9, 5)) + 1j * rng.normal(size=(2, 3, 9, 5)), {}))
+    out.append(("zero_9x5", np.zeros((9, 5), np.complex128), {}))
+    out.append(("rank3_of_c64_13x7", make_matrix(dict(m=13, n=7, dtype="complex64", family="gaussian")),
+                {"rank": 3}))
+    return out
+
+
 def main():
     sys.path.insert(0, str(REF))
     import torch
@@ -201,6 +226,23 @@ def main():
         mnames.append(name)
         print(f"{alg} {name:24s} {str(a.shape):14s} {a.dtype}  sweeps={info.get('jacobi_sweeps')}")
     blob["_meth_names"] = np.array(mnames)
+    # 'jacobi' on complex inputs
+    cnames = []
+    for name, a, kw in complex_cases(make_matrix):
+        a = np.ascontiguousarray(a)
+        u, s, vh, info = svd(torch.from_numpy(a.copy()), "jacobi", return_info=True, **kw)
+        flat = a.reshape(-1, *a.shape[-2:]).astype(np.complex128)
+        blob[f"cx_{name}/a"] = a
+        blob[f"cx_{name}/u"] = u.resolve_conj().numpy()
+        blob[f"cx_{name}/s"] = s.numpy()
+        blob[f"cx_{name}/vh"] = vh.resolve_conj().numpy()
+        blob[f"cx_{name}/sweeps"] = np.array(info["jacobi_sweeps"])
+        blob[f"cx_{name}/truth"] = np.stack([scipy.linalg.svd(x, compute_uv=False, lapack_driver="gesvd")
+                                             for x in flat])
+        blob[f"cx_{name}/kw"] = np.array(repr(kw))
+        cnames.append(name)
+        print(f"complex {name:24s} {str(a.shape):14s} {a.dtype}  sweeps={info['jacobi_sweeps']}")
+    blob["_cx_names"] = np.array(cnames)
     np.savez_compressed(HERE / "reference_jacobi.npz", **blob)
     print("wrote", HERE / "reference_jacobi.npz")
 

@@ -5,7 +5,7 @@ import pytest
 
 from oracle import jacobi_oracle as O
 from oracle import c_oracle as C
-from conftest import QR_DETERMINED, golden_methods, golden_qr, sigma_tol
+from conftest import QR_DETERMINED, golden_complex, golden_methods, golden_qr, sigma_tol
 
 
 def _cmp_sigma(s, ref, dtype, factor=1.0):
@@ -213,3 +213,41 @@ def test_qr_methods_oracle_matches_reference():
         err = float(np.abs(s - g["truth"][..., :k]).max() / g["truth"].max())
         err_ref = float(np.abs(g["s"] - g["truth"][..., :k]).max() / g["truth"].max())
         assert err <= max(2 * err_ref, 10 * sigma_tol(dt)), name
+
+
+def _cmp_vectors_phase(u, ref, s, dtype, axis):
+    """Complex columns (axis=-1) or rows (axis=-2) agree up to a unit phase
+    where the singular value is simple (gap > 1e-3 relative)."""
+    ref = np.asarray(ref, np.complex128).reshape(-1, *np.shape(ref)[-2:])
+    u = np.asarray(u, np.complex128).reshape(ref.shape)
+    s = np.asarray(s, np.float64).reshape(ref.shape[0], -1)
+    tol = 1e-3 if np.dtype(dtype) == np.complex64 else 1e-8
+    worst = 0.0
+    for b in range(u.shape[0]):
+        sb = s[b]
+        ncols = ref.shape[-1] if axis == -1 else ref.shape[-2]
+        for j in range(min(len(sb), ncols)):
+            gap = min([abs(sb[j] - sb[i]) for i in range(len(sb)) if i != j] or [np.inf])
+            if sb[j] == 0 or gap <= 1e-3 * sb[0]:
+                continue
+            x = u[b][:, j] if axis == -1 else u[b][j, :]
+            y = ref[b][:, j] if axis == -1 else ref[b][j, :]
+            ph = np.vdot(x, y)
+            ph = ph / abs(ph) if abs(ph) > 0 else 1.0
+            worst = max(worst, float(np.abs(x * ph - y).max()))
+    assert worst <= tol, worst
+    return worst
+
+
+def test_complex_oracle_matches_reference():
+    """The NumPy restatement of jacobi_svd on complex inputs against the
+    reference's U, s, Vh and sweep counts (same arithmetic and order)."""
+    for name, g in golden_complex().items():
+        a = g["a"]
+        u, s, vh, info = O.svd(a, "jacobi", return_info=True, **g["kw"])
+        real = np.float32 if a.dtype == np.complex64 else np.float64
+        _cmp_sigma(s, g["s"], real)
+        assert abs(info["jacobi_sweeps"] - g["sweeps"]) <= 1, name
+        if s.ndim and np.asarray(g["s"]).max() > 0:
+            _cmp_vectors_phase(u, g["u"], g["s"], a.dtype, -1)
+            _cmp_vectors_phase(vh, g["vh"], g["s"], a.dtype, -2)
