@@ -4,13 +4,15 @@ Mirrors svdbench/standalone/solvers.py:264-324 of uncle-Slava/Pavel-s_SVD:
 same argument names and meaning, same validation order, same exception types
 and messages, same output contract (U (...,m,k), s (...,k), Vh (...,k,n);
 ``None`` for U and Vh with ``values_only``; the info dict with ``return_info``).
-The numeric work is ONE launch of the sm_100a batched kernel per call
-(``jb_svd_batched_f32`` / ``_f64``); the host reads back only the per-matrix
-status and sweep words to raise the reference's errors.
+For 'jacobi' the numeric work is ONE launch of the sm_100a batched kernel
+per call (``jb_svd_batched_f32`` / ``_f64``, ``_c64`` / ``_c128`` for
+complex input); the host reads back only the per-matrix status and sweep
+words to raise the reference's errors.
 
 Differences, by design:
-  * CUDA tensors only.  Other devices, complex dtypes and the other reference
-    families raise ``Unsupported`` (svdbench/algorithms.py:12-13) instead of
+  * CUDA tensors only.  Other devices, the reference families not built here
+    (bidiag_*, gram_dc, polar_*, lanczos) and complex input to any family but
+    'jacobi' raise ``Unsupported`` (svdbench/algorithms.py:12-13) instead of
     running elsewhere: there is no CPU fallback.
   * ``precision`` option for float32 input: ``'mixed'`` (default) runs FP32
     sweeps and then FP64 sweeps from the Householder re-orthonormalised V, so
