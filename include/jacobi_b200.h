@@ -355,6 +355,19 @@ JB_API int jb_svd_batched_c128(const void *A, void *U, double *S, void *Vh, int6
                                double tol, int32_t max_sweeps, int32_t *sweeps, int32_t *status,
                                void *workspace, size_t workspace_bytes, void *stream);
 
+/* Rounds [round_begin, round_end) of one-sided Jacobi sweeps applied in place
+ * to ONE matrix: replaces the laboratory's jacobi_rotation over its schedule
+ * (algorithm_laboratory/algorithms.py:81-102, 121-126: the round-robin
+ * tournament on n + n % 2 players without the pairs past n), so that its
+ * jacobi (:105-157) can run on the GPU while its trace sees W and V after
+ * every sweep or round.  W (m x n, m >= n) and V (n x n) row-major device
+ * arrays of dtype 0 float32, 1 float64, 2 complex64, 3 complex128
+ * (interleaved re, im); n <= 8192; 0 <= round_begin <= round_end <= n + n % 2
+ * - 1; tol > 0.  *off (a device double) becomes max(*off, the largest ratio
+ * of an active pair in these rounds). */
+JB_API int jb_jacobi_rounds(void *W, void *V, int32_t dtype, int32_t m, int32_t n, int32_t round_begin,
+                            int32_t round_end, double tol, double *off, void *stream);
+
 /* Size of the fixed device scratch array of jb_svd_batched_f32_noalloc. */
 #define JB_NOALLOC_SCRATCH_BYTES (16u << 20)
 

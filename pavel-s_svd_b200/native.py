@@ -31,7 +31,7 @@ SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_bat
            "jb_col_sum", "jb_mse_grad", "jb_adam", "jb_gram_sketch", "jb_block_eig_f64", "jb_rows_scatter",
            "jb_rows_combine", "jb_gemm_f64acc", "jb_block_finish", "jb_eigh_workspace_bytes", "jb_eigh_f32",
            "jb_eigh_f64", "jb_qr_workspace_bytes", "jb_qr_f32", "jb_qr_f64", "jb_svd_complex_workspace_bytes",
-           "jb_svd_batched_c64", "jb_svd_batched_c128", "jb_svd_batched_f32_noalloc")
+           "jb_svd_batched_c64", "jb_svd_batched_c128", "jb_jacobi_rounds", "jb_svd_batched_f32_noalloc")
 GEMM_PLAIN, GEMM_SPLIT3, GEMM_SPLIT6, GEMM_B_MN, GEMM_CHAIN128, GEMM_SYRK = 0, 1, 2, 4, 8, 16
 NOALLOC_SCRATCH_BYTES = 16 << 20  # JB_NOALLOC_SCRATCH_BYTES
 
@@ -75,6 +75,8 @@ def _declare(l):
     for name in ("jb_svd_batched_c64", "jb_svd_batched_c128"):
         getattr(l, name).restype = ctypes.c_int
         getattr(l, name).argtypes = [P, P, P, P, I64, I32, I32, F64, I32, P, P, P, SZ, P]
+    l.jb_jacobi_rounds.restype = ctypes.c_int
+    l.jb_jacobi_rounds.argtypes = [P, P, I32, I32, I32, I32, I32, F64, P, P]
     l.jb_svd_batched_f32.restype = ctypes.c_int
     l.jb_svd_batched_f32.argtypes = [P, P, P, P, I64, I32, I32, I32, I32, F64, I32, I32, P, P, P, SZ, P]
     l.jb_svd_batched_f64.restype = ctypes.c_int

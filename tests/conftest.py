@@ -79,6 +79,22 @@ def golden_complex():
     return out
 
 
+def golden_lab():
+    """The laboratory's jacobi with a recording trace: a, U, s, Vh, the
+    per-sweep largest active ratio, sweeps, options, and (with
+    record_rotations) W after every round of sweep 1."""
+    z = np.load(GOLDEN, allow_pickle=False)
+    out = {}
+    for n in z["_lab_names"]:
+        c = {k: z[f"lab_{n}/{k}"] for k in ("a", "u", "s", "vh", "offs")}
+        c["sweeps"] = int(z[f"lab_{n}/sweeps"])
+        c["kw"] = eval(str(z[f"lab_{n}/kw"]))
+        if f"lab_{n}/rounds" in z.files:
+            c["rounds"] = z[f"lab_{n}/rounds"]
+        out[str(n)] = c
+    return out
+
+
 # Columns of Q (and rows of R) fixed by the input, by QR case: beyond them a
 # rank-deficient input leaves Q to rounding noise.
 QR_DETERMINED = {"deficient_f64": 4}

@@ -159,6 +159,47 @@ def complex_cases(make_matrix):
     return out
 
 
+class _Recorder:
+    """A laboratory trace (svdbench/laboratory/trace.py interface) that keeps
+    the per-sweep off, the convergence record and W after every round of
+    sweep 1."""
+    enabled = True
+
+    def __init__(self):
+        self.offs, self.rounds, self.conv = [], [], None
+
+    def wants(self, iteration=None):
+        return True
+
+    def stage(self, *args, **kwargs):
+        from contextlib import nullcontext
+        return nullcontext()
+
+    def checkpoint(self, name, iteration=None, tensors=None, scalars=None, factors=None):
+        if name == "sweep":
+            self.offs.append(float(scalars["max_active_pair_correlation"]))
+        if name.startswith("rotation_") and iteration == 1:
+            self.rounds.append(tensors["W"].clone().resolve_conj().numpy())
+
+    def record(self, name, iteration=None, **scalars):
+        self.conv = scalars
+
+
+def lab_cases():
+    """(name, matrix, kwargs) for the laboratory's jacobi
+    (algorithm_laboratory/algorithms.py:105-157): odd and even widths, both
+    real precisions, a wide complex matrix, a rank-deficient one."""
+    rng = np.random.default_rng(51)
+    out = [("odd_f64_12x7", rng.standard_normal((12, 7)), {"record_rotations": True}),
+           ("even_f32_16x10", rng.standard_normal((16, 10)).astype(np.float32), {}),
+           ("wide_c128_6x11", rng.standard_normal((6, 11)) + 1j * rng.standard_normal((6, 11)),
+            {"record_rotations": True}),
+           ("c64_9x5", (rng.standard_normal((9, 5)) + 1j * rng.standard_normal((9, 5))).astype(np.complex64), {})]
+    b = rng.standard_normal((10, 3)) @ rng.standard_normal((3, 6))
+    out.append(("rank3_f64_10x6", b, {}))
+    return out
+
+
 def main():
     sys.path.insert(0, str(REF))
     import torch
@@ -243,6 +284,25 @@ def main():
         cnames.append(name)
         print(f"complex {name:24s} {str(a.shape):14s} {a.dtype}  sweeps={info['jacobi_sweeps']}")
     blob["_cx_names"] = np.array(cnames)
+    # the laboratory's jacobi with a recording trace
+    from algorithm_laboratory import algorithms as L
+    lnames = []
+    for name, a, kw in lab_cases():
+        a = np.ascontiguousarray(a)
+        rec = _Recorder()
+        u, s, vh = L.jacobi(torch.from_numpy(a.copy()), rec, **kw)
+        blob[f"lab_{name}/a"] = a
+        blob[f"lab_{name}/u"] = u.resolve_conj().numpy()
+        blob[f"lab_{name}/s"] = s.numpy()
+        blob[f"lab_{name}/vh"] = vh.resolve_conj().numpy()
+        blob[f"lab_{name}/offs"] = np.array(rec.offs)
+        blob[f"lab_{name}/sweeps"] = np.array(rec.conv["sweeps"])
+        blob[f"lab_{name}/kw"] = np.array(repr(kw))
+        if rec.rounds:
+            blob[f"lab_{name}/rounds"] = np.stack(rec.rounds)
+        lnames.append(name)
+        print(f"lab {name:20s} {str(a.shape):10s} {a.dtype}  sweeps={rec.conv['sweeps']} rounds={len(rec.rounds)}")
+    blob["_lab_names"] = np.array(lnames)
     np.savez_compressed(HERE / "reference_jacobi.npz", **blob)
     print("wrote", HERE / "reference_jacobi.npz")
 
