@@ -17,6 +17,10 @@ events) so every step starts with a cold L2.
   tall_lowrank     8192x2048 f32 rank 64 + noise, blocked Jacobi b = 64
   warm_family      65536 x 128x64 f32 family: network trained on 60000,
                    warm vs plain timed on 4096 held-out matrices
+  extensions       the paths around the Jacobi kernels (complex Jacobi,
+                   the QR-based solvers, gram_jacobi, jacobi_eigh, the
+                   laboratory's traced Jacobi): one line each, with accuracy
+                   against LAPACK and the NumPy oracle timed beside it
 
 --impl reference: the reference algorithm's CPU implementation, timed on the
 host cores of this machine (the C restatement in oracle/, all threads; the
@@ -575,6 +579,138 @@ def run_warm(args):
     print(json.dumps(line), flush=True)
 
 
+def _time_gpu(fn, steps, warmup):
+    """Median ms of fn() over `steps` runs, each bracketed by CUDA events on
+    the current stream, a 256 MiB write between runs (outside the events)."""
+    import torch
+    flush = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    times = []
+    for i in range(steps):
+        flush.fill_(i & 0xff)
+        e0, e1 = _events()
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    return statistics.median(times)
+
+
+def _time_cpu(fn, count, seconds=3.0):
+    """Matrices/s of fn() (which solves `count` matrices) over about
+    `seconds` of wall time, at least once."""
+    t0 = time.perf_counter()
+    runs = 0
+    while True:
+        fn()
+        runs += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            return runs * count / el
+
+
+def run_extensions(args):
+    """One line per path around the Jacobi kernels, on seeded synthetic
+    batches: the device time of the public call (inputs resident), the
+    largest relative sigma error against FP64 LAPACK on the batch, and the
+    NumPy oracle (the reference's algorithm restated, one host thread) on a
+    sample of the same batch."""
+    import torch
+    pkg = importlib.import_module("pavel-s_svd_b200")
+    eigh = importlib.import_module("pavel-s_svd_b200.eigh")
+    qrm = importlib.import_module("pavel-s_svd_b200.qr")
+    lab = importlib.import_module("pavel-s_svd_b200.lab")
+    from oracle import jacobi_oracle as O
+    rng = np.random.default_rng(61)
+
+    def sig_err(a, s, k=None):
+        a64 = a.astype(np.complex128 if np.iscomplexobj(a) else np.float64)
+        sr = np.linalg.svd(a64, compute_uv=False)
+        k = k or s.shape[-1]
+        s = np.asarray(s, np.float64)[..., :k]
+        return float((np.abs(s - sr[..., :k]) / sr[..., :1]).max())
+
+    def line(row, a_np, ms, acc, cpu_rate, cpu_sample, config, dtype):
+        b = a_np.shape[0]
+        print(json.dumps({"metric": f"{row} matrices/s", "value": b / (ms / 1e3), "unit": "matrices/s",
+                          "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+                          "data": "synthetic (seeded: N(0,1) entries; the projected solvers s_i = 0.8^i)",
+                          "config": dict(workload=row, **config),
+                          "accuracy": acc, "cpu_baseline": {"value": cpu_rate, "unit": "matrices/s", "cores": 1,
+                                                            "kind": "port", "sample": cpu_sample}}), flush=True)
+
+    # complex Jacobi
+    for dt, tdt in ((np.complex64, torch.complex64), (np.complex128, torch.complex128)):
+        a = (rng.standard_normal((1024, 48, 32)) + 1j * rng.standard_normal((1024, 48, 32))).astype(dt)
+        t = torch.from_numpy(a).cuda()
+        ms = _time_gpu(lambda: pkg.svd(t, "jacobi"), args.steps, args.warmup)
+        _, s, _ = pkg.svd(t, "jacobi")
+        cpu = _time_cpu(lambda: O.svd(a[:8], "jacobi"), 8)
+        line(f"complex Jacobi {np.dtype(dt).name}", a, ms, {"max_rel_sigma_err_vs_lapack": sig_err(a, s.cpu().numpy())},
+             cpu, "8 matrices, NumPy oracle jacobi_svd", {"shape": [1024, 48, 32]}, np.dtype(dt).name)
+    # QR-based solvers
+    # the projected solvers approximate the leading triplets: inputs with a
+    # decaying spectrum (s_i = 0.8^i, Haar-like factors) where that is meaningful
+    uu = np.linalg.qr(rng.standard_normal((256, 256, 96)))[0]
+    vv = np.linalg.qr(rng.standard_normal((256, 96, 96)))[0]
+    decaying = (uu * 0.8 ** np.arange(96)) @ np.swapaxes(vv, 1, 2)
+    cases = (("qr", rng.standard_normal((1024, 96, 32)).astype(np.float32), {}),
+             ("tsqr", rng.standard_normal((128, 1024, 32)), {"tile_rows": 128}),
+             ("randomized", decaying, {"rank": 8, "iterations": 2}),
+             ("block_krylov", decaying, {"rank": 8, "iterations": 2}))
+    for alg, a, kw in cases:
+        t = torch.from_numpy(a).cuda()
+        ms = _time_gpu(lambda: pkg.svd(t, alg, **kw), args.steps, args.warmup)
+        _, s, _ = pkg.svd(t, alg, **kw)
+        k = kw.get("rank")
+        okw = dict(kw)
+        if alg in ("randomized", "block_krylov"):
+            ell = min(k + 8, min(a.shape[-2:]))
+            okw["initial_basis"] = rng.standard_normal((4, a.shape[-1], ell)).astype(a.dtype)
+        cpu = _time_cpu(lambda: O.svd(a[:4], alg, **okw), 4)
+        line(f"svd '{alg}'", a, ms, {"max_rel_sigma_err_vs_lapack": sig_err(a, s.cpu().numpy(), k)}, cpu,
+             "4 matrices, NumPy oracle", {"shape": list(a.shape), **kw}, a.dtype.name)
+    # the QR kernel alone
+    a = rng.standard_normal((1024, 128, 64)).astype(np.float32)
+    t = torch.from_numpy(a).cuda()
+    ms = _time_gpu(lambda: qrm.qr(t), args.steps, args.warmup)
+    q, r = qrm.qr(t)
+    q64, r64 = q.cpu().numpy().astype(np.float64), r.cpu().numpy().astype(np.float64)
+    acc = {"max_abs_QR_minus_A": float(np.abs(q64 @ r64 - a).max()),
+           "max_abs_QtQ_minus_I": float(np.abs(np.swapaxes(q64, 1, 2) @ q64 - np.eye(64)).max())}
+    cpu = _time_cpu(lambda: O.qr(a[:16]), 16)
+    line("Householder QR (jb_qr_f32)", a, ms, acc, cpu, "16 matrices, NumPy oracle qr", {"shape": [1024, 128, 64]},
+         "float32")
+    # gram_jacobi and jacobi_eigh
+    a = rng.standard_normal((1024, 64, 32))
+    t = torch.from_numpy(a).cuda()
+    ms = _time_gpu(lambda: pkg.svd(t, "gram_jacobi"), args.steps, args.warmup)
+    _, s, _ = pkg.svd(t, "gram_jacobi")
+    g = np.swapaxes(a, 1, 2) @ a
+    cpu = _time_cpu(lambda: O.jacobi_eigh(g[:8]), 8)
+    line("svd 'gram_jacobi'", a, ms, {"max_rel_sigma_err_vs_lapack": sig_err(a, s.cpu().numpy())}, cpu,
+         "8 Grams, NumPy oracle jacobi_eigh", {"shape": [1024, 64, 32]}, "float64")
+    h = torch.from_numpy(g).cuda()
+    ms = _time_gpu(lambda: eigh.jacobi_eigh(h), args.steps, args.warmup)
+    w, _, _ = eigh.jacobi_eigh(h)
+    wr = np.linalg.eigvalsh(g)
+    line("jacobi_eigh", g, ms, {"max_rel_eig_err_vs_lapack": float((np.abs(w.cpu().numpy() - wr) /
+                                                                     np.abs(wr).max(-1, keepdims=True)).max())},
+         cpu, "8 matrices, NumPy oracle jacobi_eigh", {"shape": [1024, 32, 32]}, "float64")
+    # the laboratory's Jacobi (one matrix, no trace: a sweep per launch)
+    a = rng.standard_normal((1, 128, 64))
+    t = torch.from_numpy(a[0]).cuda()
+    ms = _time_gpu(lambda: lab.jacobi(t), args.steps, args.warmup)
+    _, s, _ = lab.jacobi(t)
+    cpu = _time_cpu(lambda: O.svd(a, "jacobi"), 1)
+    line("laboratory jacobi (one matrix)", a, ms, {"max_rel_sigma_err_vs_lapack": sig_err(a, s.cpu().numpy()[None])},
+         cpu, "the one matrix, NumPy oracle jacobi_svd", {"shape": [128, 64]}, "float64")
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -582,7 +718,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", choices=("uneven_batch", "plain_single", "clustered_large", "tall_lowrank",
-                                           "warm_family"), default="uneven_batch")
+                                           "warm_family", "extensions"), default="uneven_batch")
     ap.add_argument("--precision", choices=("mixed", "fp32"), default="mixed")
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -599,7 +735,7 @@ def main():
         run_reference(args, rank, world)
         return
     if args.workload != "uneven_batch":
-        {"plain_single": run_plain_single, "warm_family": run_warm}.get(
+        {"plain_single": run_plain_single, "warm_family": run_warm, "extensions": run_extensions}.get(
             args.workload, lambda a: run_blocked(a, args.workload))(args)
         return
     if world > 1:
