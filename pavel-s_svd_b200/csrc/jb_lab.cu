@@ -15,10 +15,12 @@
 // largest active ratio is folded into *off (a max), so one call per round or
 // per sweep gives the laboratory's per-sweep off.  Real inputs run through
 // the same complex formulas with zero imaginary parts, which add nothing.
-// One CTA (the laboratory solves one matrix at a time).
+// One CTA (the laboratory solves one matrix at a time); W and V are copied to
+// shared memory (column-major) for the launch when they fit, and back after.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <math.h>
+#include <type_traits>
 #include "jacobi_b200.h"
 
 namespace jb {
@@ -71,8 +73,20 @@ __device__ __forceinline__ void rr_pair(int r, int k, int np, int &p, int &q) {
 }
 
 template <typename R, bool CPLX>
-__global__ void __launch_bounds__(kThreads) rounds_kernel(void *W, void *V, int m, int n, int r0, int r1, R tol,
-                                                          double *off_out) {
+__host__ __device__ inline size_t pair_bytes(int n) {
+    const int half = (n + (n & 1)) / 2;
+    return ((size_t)(2 * half + (half & 1)) * sizeof(R) + (size_t)half * sizeof(C<R>) + 15) & ~(size_t)15;
+}
+
+// Element (i, col) of a matrix with `rows` rows: column-major in shared
+// memory, row-major (n columns) in the caller's arrays.
+__device__ __forceinline__ size_t at(bool staged, int i, int col, int rows, int n) {
+    return staged ? (size_t)col * rows + i : (size_t)i * n + col;
+}
+
+template <typename R, bool CPLX>
+__global__ void __launch_bounds__(kThreads) rounds_kernel(void *Wg, void *Vg, int m, int n, int r0, int r1, R tol,
+                                                          double *off_out, int staged) {
     extern __shared__ __align__(16) unsigned char smem[];
     const int np = n + (n & 1), half = np / 2;
     R *app = (R *)smem;
@@ -80,6 +94,22 @@ __global__ void __launch_bounds__(kThreads) rounds_kernel(void *W, void *V, int 
     C<R> *apq = (C<R> *)(aqq + half + (half & 1));   // an even count of R before it
     __shared__ double red[32];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    using E = typename std::conditional<CPLX, C<R>, R>::type;
+    void *W = Wg, *V = Vg;
+    if (staged) {
+        E *ws = (E *)(smem + pair_bytes<R, CPLX>(n)), *vs = ws + (size_t)m * n;
+        for (size_t k = threadIdx.x; k < (size_t)m * n; k += blockDim.x) {
+            const int i = (int)(k / n), c = (int)(k - (size_t)i * n);
+            ws[(size_t)c * m + i] = ((const E *)Wg)[k];
+        }
+        for (size_t k = threadIdx.x; k < (size_t)n * n; k += blockDim.x) {
+            const int i = (int)(k / n), c = (int)(k - (size_t)i * n);
+            vs[(size_t)c * n + i] = ((const E *)Vg)[k];
+        }
+        W = ws;
+        V = vs;
+        __syncthreads();
+    }
     R off = R(0);
     for (int r = r0; r < r1; ++r) {
         for (int k = warp; k < half; k += nw) {
@@ -88,7 +118,7 @@ __global__ void __launch_bounds__(kThreads) rounds_kernel(void *W, void *V, int 
             if (q >= n) continue;                      // dropped pair
             R sp = 0, sq = 0, cr = 0, ci = 0;
             for (int i = lane; i < m; i += 32) {
-                const C<R> x = ld<R, CPLX>(W, (size_t)i * n + p), y = ld<R, CPLX>(W, (size_t)i * n + q);
+                const C<R> x = ld<R, CPLX>(W, at(staged, i, p, m, n)), y = ld<R, CPLX>(W, at(staged, i, q, m, n));
                 sp += x.re * x.re + x.im * x.im;
                 sq += y.re * y.re + y.im * y.im;
                 cr += x.re * y.re + x.im * y.im;
@@ -124,15 +154,27 @@ __global__ void __launch_bounds__(kThreads) rounds_kernel(void *W, void *V, int 
                 void *X = pass == 0 ? W : V;
                 const int rows = pass == 0 ? m : n;
                 for (int i = lane; i < rows; i += 32) {
-                    const C<R> x = ld<R, CPLX>(X, (size_t)i * n + p), y = ld<R, CPLX>(X, (size_t)i * n + q);
-                    st<R, CPLX>(X, (size_t)i * n + p,
+                    const size_t ip = at(staged, i, p, rows, n), iq = at(staged, i, q, rows, n);
+                    const C<R> x = ld<R, CPLX>(X, ip), y = ld<R, CPLX>(X, iq);
+                    st<R, CPLX>(X, ip,
                                 C<R>{c * x.re - (s.re * y.re + s.im * y.im), c * x.im - (s.re * y.im - s.im * y.re)});
-                    st<R, CPLX>(X, (size_t)i * n + q,
+                    st<R, CPLX>(X, iq,
                                 C<R>{(s.re * x.re - s.im * x.im) + c * y.re, (s.re * x.im + s.im * x.re) + c * y.im});
                 }
             }
         }
         __syncthreads();
+    }
+    if (staged) {
+        const E *ws = (const E *)W, *vs = (const E *)V;
+        for (size_t k = threadIdx.x; k < (size_t)m * n; k += blockDim.x) {
+            const int i = (int)(k / n), c = (int)(k - (size_t)i * n);
+            ((E *)Wg)[k] = ws[(size_t)c * m + i];
+        }
+        for (size_t k = threadIdx.x; k < (size_t)n * n; k += blockDim.x) {
+            const int i = (int)(k / n), c = (int)(k - (size_t)i * n);
+            ((E *)Vg)[k] = vs[(size_t)c * n + i];
+        }
     }
     const R o = wmax(off);
     if (lane == 0) red[warp] = (double)o;
@@ -146,13 +188,14 @@ __global__ void __launch_bounds__(kThreads) rounds_kernel(void *W, void *V, int 
 
 template <typename R, bool CPLX>
 static int launch(void *W, void *V, int m, int n, int r0, int r1, double tol, double *off, cudaStream_t st) {
-    const int np = n + (n & 1), half = np / 2;
-    const size_t smem = (size_t)(2 * half + (half & 1)) * sizeof(R) + (size_t)half * sizeof(C<R>);
+    const size_t esz = CPLX ? sizeof(C<R>) : sizeof(R);
+    const size_t base = pair_bytes<R, CPLX>(n), work = ((size_t)m * n + (size_t)n * n) * esz;
+    const bool staged = base + work <= 227 * 1024;
+    const size_t smem = staged ? base + work : base;
     auto kern = rounds_kernel<R, CPLX>;
-    if (smem > 48 * 1024 &&
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return JB_ECUDA;
-    kern<<<1, kThreads, smem, st>>>(W, V, m, n, r0, r1, (R)tol, off);
+    kern<<<1, kThreads, smem, st>>>(W, V, m, n, r0, r1, (R)tol, off, staged ? 1 : 0);
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
 }
 

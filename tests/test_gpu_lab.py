@@ -81,15 +81,20 @@ def test_lab_jacobi_matches_reference_laboratory():
 
 def test_whole_sweep_launches_equal_per_round():
     """With a trace that records nothing a sweep is one launch; the rounds
-    are the same kernel work in the same order, so the results are equal."""
+    are the same kernel work in the same order, so the results are equal.
+    The last matrix is too large to stage in shared memory (the kernel then
+    works on the caller's arrays): checked against LAPACK too."""
     L = _lab()
     rng = np.random.default_rng(5)
     for a in (rng.standard_normal((40, 23)), (rng.standard_normal((30, 17)) + 1j * rng.standard_normal((30, 17)))
-              .astype(np.complex64)):
+              .astype(np.complex64), rng.standard_normal((260, 130))):
         t = torch.from_numpy(a).to(DEV)
         u1, s1, vh1 = L.jacobi(t)
         u2, s2, vh2 = L.jacobi(t, Recorder())
         assert torch.equal(s1, s2) and torch.equal(u1, u2) and torch.equal(vh1, vh2)
+        truth = np.linalg.svd(a.astype(np.complex128), compute_uv=False)
+        tol = 1e-5 if a.dtype == np.complex64 else 1e-12
+        assert float(np.abs(s1.cpu().numpy() - truth).max() / truth[0]) <= tol
 
 
 def test_lab_jacobi_errors():
