@@ -99,6 +99,7 @@ struct Params {
     int64_t x_cap;                // floats available at x32
     size_t region_cap;            // bytes of the shared-memory work area
     int cls;                      // 0: every matrix; 1: only nt > kNarrowN; 2: only nt <= kNarrowN
+    int xchg;                     // register FP32 kernels: tile exchange area after the work area (tile_x)
 };
 
 __device__ inline jb_matrix_desc desc_of(const Params &p, int64_t mat) {
@@ -377,9 +378,9 @@ __device__ void load_stage(const TI *A, const Geo &g, int ld, float *As) {
 
 template <typename T, int B, int MR = kMaxR, int MRV = kMaxRV, int UPD = 0>
 __device__ int rb_dispatch(const RGeo &r, T *W, T *V, T tol, int max_sweeps, bool confirm, double *red,
-                           bool &conv, T exit_ratio = T(0), double *colnorm = nullptr) {
+                           bool &conv, T exit_ratio = T(0), double *colnorm = nullptr, T *xbuf = nullptr) {
     return rb_sweeps<T, B, MR, MRV, UPD>(W, r.ldw, V, r.ldv, r.nb, r.live, tol, max_sweeps, confirm, red, conv,
-                                    exit_ratio, colnorm);
+                                    exit_ratio, colnorm, xbuf);
 }
 
 __device__ inline Geo reg_geo(const jb_matrix_desc &d, const RGeo &r) {
@@ -472,6 +473,7 @@ __global__ void __launch_bounds__(THREADS, (BW == kB32 && MR <= kMaxR) ? 512 / T
     __shared__ int s_idx;
     Aux ax = carve_aux(smem, p.maxd);
     unsigned char *region = smem + aux_bytes(p.maxd);
+    float *xbuf = p.xchg ? (float *)(region + align16(p.region_cap)) : nullptr;   // tile exchange area
     for (;;) {
         int64_t idx;
         next_ticket(p.counter, s_idx, idx);
@@ -525,12 +527,11 @@ __global__ void __launch_bounds__(THREADS, (BW == kB32 && MR <= kMaxR) ? 512 / T
                 // decides convergence on exact dot products; they update the
                 // column norms instead of recomputing them (rb_sweeps UPD).  Not
                 // in the large tile, where the norms would not fit in registers.
-                ns = rb_dispatch<float, BW, MR, MRV, (MIXED && MR <= kMaxR) ? 1 : 0>(r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true,
-                                                       ax.red, conv,
-                                                       MIXED ? (p.exit_ratio == 0.f ? kMixedExitRatio
-                                                                                    : fmaxf(p.exit_ratio, 0.f))
-                                                             : 0.0f,
-                                                       ax.sig);
+                const float exit_ratio =
+                    MIXED ? (p.exit_ratio == 0.f ? kMixedExitRatio : fmaxf(p.exit_ratio, 0.f)) : 0.0f;
+                ns = rb_dispatch<float, BW, MR, MRV, (MIXED && MR <= kMaxR) ? 1 : 0>(
+                    r, W, V, tol, MIXED ? p.max_sweeps32 : p.max_sweeps, true, ax.red, conv, exit_ratio, ax.sig,
+                    xbuf);
                 if (MIXED) {
                     float *x = p.x32 + d.x_off;
                     const int nt = g.nt;
@@ -907,8 +908,8 @@ struct Plan {
     size_t smem32, smem64, reg32, reg64;
     // size-class split (kNarrowN): a second launch per phase for narrow matrices
     bool split;
-    Dims d64n;
-    size_t smem64n, reg64n;
+    Dims d64n, d32n;
+    size_t smem64n, reg64n, smem32n, reg32n;
 };
 
 static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags) {
@@ -932,11 +933,16 @@ static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags
         pl.d64 = raux_dims(r64);
         pl.reg32 = rregion_bytes(r32, 4);
         pl.reg64 = (elem == 4 && precision == JB_PREC_MIXED) ? rregion_mixed64(r64, max_nt) : rregion_bytes(r64, 8);
-        pl.smem32 = aux_bytes(pl.d32) + pl.reg32;
+        // FP32 kernels: work area, then the tile exchange area (tile_x)
+        pl.smem32 = aux_bytes(pl.d32) + pl.reg32 + xchg_bytes(r32.npb, kMaxR, kMaxRV);
         pl.smem64 = aux_bytes(pl.d64) + pl.reg64;
         if (pl.smem64 > kSmemLimit || pl.smem32 > kSmemLimit) pl.reg = false;
         pl.split = pl.reg && pl.bw == kB32 && max_nt > kNarrowN;
         if (pl.split) {
+            const RGeo r32n = rgeo(max_mt, kNarrowN, kB32, flags);
+            pl.d32n = raux_dims(r32n);
+            pl.reg32n = rregion_bytes(r32n, 4);
+            pl.smem32n = aux_bytes(pl.d32n) + pl.reg32n + xchg_bytes(r32n.npb, kMaxR, kMaxRV);
             const RGeo r64n = rgeo(max_mt, kNarrowN, kB64, flags);
             pl.d64n = raux_dims(r64n);
             pl.reg64n = (elem == 4 && precision == JB_PREC_MIXED) ? rregion_mixed64(r64n, kNarrowN)
@@ -1047,19 +1053,23 @@ static int launch_reg(Params &p, const Plan &pl, int elem, int precision, unsign
         p.maxd = pl.d32;
         p.region_cap = pl.reg32;
         p.cls = split ? 1 : 0;
+        p.xchg = 1;
         k1<<<(unsigned)grid, t1, pl.smem32, st>>>(p);
         if (cudaGetLastError() != cudaSuccess) return JB_ECUDA;
         if (split) {
             // narrow matrices: 4 warps (nt <= 32 is at most 8 blocks of 4 columns)
             auto k1n = mixed ? rb32_kernel_t<true, kT32 / 2, kB32, kMaxR, kMaxRV>
                              : rb32_kernel_t<false, kT32 / 2, kB32, kMaxR, kMaxRV>;
-            if ((rc = occupancy_grid(k1n, kT32 / 2, pl.smem32, p.count, grid))) return rc;
+            if ((rc = occupancy_grid(k1n, kT32 / 2, pl.smem32n, p.count, grid))) return rc;
             p.counter = (int *)ws + 2;
             p.cls = 2;
-            k1n<<<(unsigned)grid, kT32 / 2, pl.smem32, st>>>(p);
+            p.maxd = pl.d32n;
+            p.region_cap = pl.reg32n;
+            k1n<<<(unsigned)grid, kT32 / 2, pl.smem32n, st>>>(p);
             if (cudaGetLastError() != cudaSuccess) return JB_ECUDA;
             p.counter = (int *)ws;
         }
+        p.xchg = 0;
         if (!mixed) return JB_OK;
         auto k2 = rb64_kernel<float, true>;
         if ((rc = occupancy_grid(k2, kT64, pl.smem64, p.count, grid))) return rc;

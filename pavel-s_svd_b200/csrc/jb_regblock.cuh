@@ -413,6 +413,46 @@ __device__ __forceinline__ void tile_io(Tile<T, B, R, RV> &t, T *W, int ldw, T *
     }
 }
 
+// The tile through the exchange area between block rounds (FP32, R a
+// multiple of 4, RV of 2): lane-major, so that a lane's R rows of a W column
+// are one 16-byte access and its RV rows of a V column one 8-byte access,
+// instead of R + RV scalar accesses per column in the column-major W / V.
+// Area: W part npb x 32 x R floats, then V part npb x 32 x RV floats.
+template <typename T, int B, int R, int RV>
+__device__ __forceinline__ void tile_x(Tile<T, B, R, RV> &t, T *xw, int npb, int X, int Y, int lane, bool store) {
+    static_assert(sizeof(T) == 4 && R % 4 == 0 && RV % 2 == 0, "exchange area: FP32 tiles, R % 4 == 0, RV % 2 == 0");
+    T *xv = xw + (size_t)npb * 32 * R;
+#pragma unroll
+    for (int c = 0; c < 2 * B; ++c) {
+        const int col = (c < B ? X * B + c : Y * B + (c - B));
+        float4 *pw = (float4 *)(xw + ((size_t)col * 32 + lane) * R);
+        float2 *pv = (float2 *)(xv + ((size_t)col * 32 + lane) * RV);
+#pragma unroll
+        for (int k = 0; k < R / 4; ++k) {
+            if (store) {
+                pw[k] = make_float4(t.w[c][4 * k], t.w[c][4 * k + 1], t.w[c][4 * k + 2], t.w[c][4 * k + 3]);
+            } else {
+                const float4 v = pw[k];
+                t.w[c][4 * k] = v.x; t.w[c][4 * k + 1] = v.y; t.w[c][4 * k + 2] = v.z; t.w[c][4 * k + 3] = v.w;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < RV / 2; ++k) {
+            if (store) {
+                pv[k] = make_float2(t.v[c][2 * k], t.v[c][2 * k + 1]);
+            } else {
+                const float2 v = pv[k];
+                t.v[c][2 * k] = v.x; t.v[c][2 * k + 1] = v.y;
+            }
+        }
+    }
+}
+
+// Bytes of the exchange area for npb columns.
+__host__ __device__ inline size_t xchg_bytes(int npb, int R, int RV) {
+    return (size_t)npb * 32 * (R + RV) * 4;
+}
+
 // Squared column norms of the tile's 2B columns, reduced across the warp:
 // afterwards nrm[0] on lane l is column l >> (5 - log2 2B)'s norm.
 template <typename T, int B, int R, int RV>
@@ -510,9 +550,14 @@ __device__ int gram_check(const T *W, int ldw, int npb, int nr, T tol2, T floor_
 //   UPD == 2: carried with the columns through colnorm (npb doubles of shared
 //             memory) between block rounds, so they accumulate over a sweep
 //             (FP64: the updates round like the dot products they replace).
+// xbuf (FP32 tiles, or NULL): the exchange area (tile_x) that carries the
+// tiles between block rounds; W and V are then read at the start and written
+// at the end and before each Gram pass only, every layout change separated
+// from the last access of the other layout by a CTA barrier.
 template <typename T, int B, int R, int RV, int UPD = 0>
 __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, int max_sweeps, bool confirm,
-                         double *red, bool &converged, T exit_ratio = T(0), double *colnorm = nullptr) {
+                         double *red, bool &converged, T exit_ratio = T(0), double *colnorm = nullptr,
+                         T *xbuf = nullptr) {
     const int nr = ldw >> 5, nv = ldv >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nw = nwarps();
@@ -564,7 +609,12 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
         for (int br = 0; br < nb - 1; ++br) {
             if (br > 0 || sweep > 1) {
                 if (act) {
-                    tile_io(t, W, ldw, V, ldv, X, Y, lane, true, nr, nv);
+                    if constexpr (sizeof(T) == 4 && R == 4 && RV == 2) {   // the 128 x 64 tiles
+                        if (xbuf) tile_x(t, xbuf, nb * B, X, Y, lane, true);
+                        else tile_io(t, W, ldw, V, ldv, X, Y, lane, true, nr, nv);
+                    } else {
+                        tile_io(t, W, ldw, V, ldv, X, Y, lane, true, nr, nv);
+                    }
                     if constexpr (UPD == 2) {
                         if (lane == 0) {
 #pragma unroll
@@ -578,7 +628,12 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
                 if (act) {
                     X = circ(warp, rr, nb);
                     Y = circ(nb - 1 - warp, rr, nb);
-                    tile_io(t, W, ldw, V, ldv, X, Y, lane, false, nr, nv);
+                    if constexpr (sizeof(T) == 4 && R == 4 && RV == 2) {   // the 128 x 64 tiles
+                        if (xbuf) tile_x(t, xbuf, nb * B, X, Y, lane, false);
+                        else tile_io(t, W, ldw, V, ldv, X, Y, lane, false, nr, nv);
+                    } else {
+                        tile_io(t, W, ldw, V, ldv, X, Y, lane, false, nr, nv);
+                    }
                     if constexpr (UPD == 1) {
                         T nrm[2 * B];
                         tile_col_norms(t, nrm, lane, nr);
