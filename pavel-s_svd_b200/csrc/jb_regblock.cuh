@@ -448,9 +448,10 @@ __device__ __forceinline__ void tile_x(Tile<T, B, R, RV> &t, T *xw, int npb, int
     }
 }
 
-// Bytes of the exchange area for npb columns.
+// Bytes of the exchange area for npb columns: the tiles, then one float per
+// column for the squared norms of the norm-update sweeps.
 __host__ __device__ inline size_t xchg_bytes(int npb, int R, int RV) {
-    return (size_t)npb * 32 * (R + RV) * 4;
+    return (size_t)npb * (32 * (R + RV) + 1) * 4;
 }
 
 // Squared column norms of the tile's 2B columns, reduced across the warp:
@@ -545,8 +546,10 @@ __device__ int gram_check(const T *W, int ldw, int npb, int nr, T tol2, T floor_
 // sweep is replaced by gram_check.
 // UPD: norm-update steps (step_upd); the norms are recomputed exactly at every
 // sweep start, and then
-//   UPD == 1: recomputed whenever a warp loads a new block pair, so the
-//             updates accumulate over one block round at most;
+//   UPD == 1: recomputed whenever a warp loads a new block pair from W / V,
+//             so the updates accumulate over one block round at most; with
+//             the exchange area (xbuf) carried with the tiles instead, so
+//             they accumulate over a sweep (FP32 preconditioning sweeps);
 //   UPD == 2: carried with the columns through colnorm (npb doubles of shared
 //             memory) between block rounds, so they accumulate over a sweep
 //             (FP64: the updates round like the dot products they replace).
@@ -610,8 +613,19 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
             if (br > 0 || sweep > 1) {
                 if (act) {
                     if constexpr (sizeof(T) == 4 && R == 4 && RV == 2) {   // the 128 x 64 tiles
-                        if (xbuf) tile_x(t, xbuf, nb * B, X, Y, lane, true);
-                        else tile_io(t, W, ldw, V, ldv, X, Y, lane, true, nr, nv);
+                        if (xbuf) {
+                            tile_x(t, xbuf, nb * B, X, Y, lane, true);
+                            if constexpr (UPD == 1) {
+                                // the updated norms travel with the tiles
+                                T *xn = xbuf + (size_t)nb * B * 32 * (R + RV);
+                                if (lane == 0) {
+#pragma unroll
+                                    for (int c = 0; c < 2 * B; ++c) xn[c < B ? X * B + c : Y * B + (c - B)] = t.nrm[c];
+                                }
+                            }
+                        } else {
+                            tile_io(t, W, ldw, V, ldv, X, Y, lane, true, nr, nv);
+                        }
                     } else {
                         tile_io(t, W, ldw, V, ldv, X, Y, lane, true, nr, nv);
                     }
@@ -635,9 +649,15 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
                         tile_io(t, W, ldw, V, ldv, X, Y, lane, false, nr, nv);
                     }
                     if constexpr (UPD == 1) {
-                        T nrm[2 * B];
-                        tile_col_norms(t, nrm, lane, nr);
-                        spread_norms(t, nrm[0]);
+                        if (xbuf) {
+                            const T *xn = xbuf + (size_t)nb * B * 32 * (R + RV);
+#pragma unroll
+                            for (int c = 0; c < 2 * B; ++c) t.nrm[c] = xn[c < B ? X * B + c : Y * B + (c - B)];
+                        } else {
+                            T nrm[2 * B];
+                            tile_col_norms(t, nrm, lane, nr);
+                            spread_norms(t, nrm[0]);
+                        }
                     } else if constexpr (UPD == 2) {
 #pragma unroll
                         for (int c = 0; c < 2 * B; ++c) t.nrm[c] = (T)colnorm[c < B ? X * B + c : Y * B + (c - B)];
