@@ -99,7 +99,9 @@ struct Params {
     int64_t x_cap;                // floats available at x32
     size_t region_cap;            // bytes of the shared-memory work area
     int cls;                      // 0: every matrix; 1: only nt > kNarrowN; 2: only nt <= kNarrowN
-    int xchg;                     // register FP32 kernels: tile exchange area after the work area (tile_x)
+    int xchg;                     // register FP32 kernels: tile exchange area (tile_x) ...
+    size_t xchg_off;              // ... at this byte offset in the work area (after W / V; it may share the
+                                  //     warm-start staging of A, which is dead once the sweeps start)
 };
 
 __device__ inline jb_matrix_desc desc_of(const Params &p, int64_t mat) {
@@ -473,7 +475,7 @@ __global__ void __launch_bounds__(THREADS, (BW == kB32 && MR <= kMaxR) ? 512 / T
     __shared__ int s_idx;
     Aux ax = carve_aux(smem, p.maxd);
     unsigned char *region = smem + aux_bytes(p.maxd);
-    float *xbuf = p.xchg ? (float *)(region + align16(p.region_cap)) : nullptr;   // tile exchange area
+    float *xbuf = p.xchg ? (float *)(region + p.xchg_off) : nullptr;   // tile exchange area
     for (;;) {
         int64_t idx;
         next_ticket(p.counter, s_idx, idx);
@@ -910,6 +912,8 @@ struct Plan {
     bool split;
     Dims d64n, d32n;
     size_t smem64n, reg64n, smem32n, reg32n;
+    // FP32 tile exchange areas: offsets in the work area and size
+    size_t xoff32, xoff32n, xbytes32;
 };
 
 static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags) {
@@ -934,7 +938,9 @@ static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags
         pl.reg32 = rregion_bytes(r32, 4);
         pl.reg64 = (elem == 4 && precision == JB_PREC_MIXED) ? rregion_mixed64(r64, max_nt) : rregion_bytes(r64, 8);
         // FP32 kernels: work area, then the tile exchange area (tile_x)
-        pl.smem32 = aux_bytes(pl.d32) + pl.reg32 + xchg_bytes(r32.npb, kMaxR, kMaxRV);
+        pl.xoff32 = pl.reg32;
+        pl.xbytes32 = xchg_bytes(r32.npb, kMaxR, kMaxRV);
+        pl.smem32 = aux_bytes(pl.d32) + pl.reg32 + pl.xbytes32;
         pl.smem64 = aux_bytes(pl.d64) + pl.reg64;
         if (pl.smem64 > kSmemLimit || pl.smem32 > kSmemLimit) pl.reg = false;
         pl.split = pl.reg && pl.bw == kB32 && max_nt > kNarrowN;
@@ -942,6 +948,7 @@ static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags
             const RGeo r32n = rgeo(max_mt, kNarrowN, kB32, flags);
             pl.d32n = raux_dims(r32n);
             pl.reg32n = rregion_bytes(r32n, 4);
+            pl.xoff32n = pl.reg32n;
             pl.smem32n = aux_bytes(pl.d32n) + pl.reg32n + xchg_bytes(r32n.npb, kMaxR, kMaxRV);
             const RGeo r64n = rgeo(max_mt, kNarrowN, kB64, flags);
             pl.d64n = raux_dims(r64n);
@@ -1054,6 +1061,7 @@ static int launch_reg(Params &p, const Plan &pl, int elem, int precision, unsign
         p.region_cap = pl.reg32;
         p.cls = split ? 1 : 0;
         p.xchg = 1;
+        p.xchg_off = pl.xoff32;
         k1<<<(unsigned)grid, t1, pl.smem32, st>>>(p);
         if (cudaGetLastError() != cudaSuccess) return JB_ECUDA;
         if (split) {
@@ -1065,6 +1073,7 @@ static int launch_reg(Params &p, const Plan &pl, int elem, int precision, unsign
             p.cls = 2;
             p.maxd = pl.d32n;
             p.region_cap = pl.reg32n;
+            p.xchg_off = pl.xoff32n;
             k1n<<<(unsigned)grid, kT32 / 2, pl.smem32n, st>>>(p);
             if (cudaGetLastError() != cudaSuccess) return JB_ECUDA;
             p.counter = (int *)ws;
@@ -1343,8 +1352,10 @@ int jb_svd_warm_f32(const float *A, const float *Vstart, float *U, float *S, flo
     Plan pl = make_plan(m, n, 4, precision, flags);
     if (!pl.reg) return JB_ETOOBIG;
     const size_t stage = align16((size_t)32 * ((m + 31) / 32) * n * 4);
+    // the staging of A follows W / V; the tile exchange area, used only once
+    // the sweeps start, shares its space
     pl.reg32 += stage;
-    pl.smem32 += stage;
+    pl.smem32 = aux_bytes(pl.d32) + (pl.reg32 > pl.xoff32 + pl.xbytes32 ? pl.reg32 : pl.xoff32 + pl.xbytes32);
     if (pl.smem32 > kSmemLimit) return JB_ETOOBIG;
     if (workspace_bytes < uniform_workspace(m, n, batch, 4, precision, flags)) return JB_EWORKSPACE;
     Params p;
