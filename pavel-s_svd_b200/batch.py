@@ -1,12 +1,13 @@
-"""Uneven batches: thousands of matrices of different shapes in ONE launch.
+"""Uneven batches: thousands of matrices of different shapes in ONE call.
 
 The reference can only batch equal shapes (svdbench/standalone/solvers.py:
 289-290); a harness solving matrices of different sizes loops over
 ``svd(x, 'jacobi')`` one call per matrix.  ``UnevenBatch`` replaces that loop:
 shapes are fixed when the plan is built (descriptors, output offsets, a
 largest-first processing order and the workspace are made once), and every
-solve is one persistent-kernel launch (``jb_svd_uneven_f32``) that can be
-captured in a CUDA graph and replayed.
+solve is one call of ``jb_svd_uneven_f32`` -- one persistent kernel per
+precision phase and size class -- that can be captured in a CUDA graph and
+replayed.
 """
 from __future__ import annotations
 
@@ -328,7 +329,7 @@ class StreamedUneven:
 
 
 def svd_uneven(mats, *, tol=None, max_sweeps=60, precision="mixed", values_only=False):
-    """Solve a list of float32 CUDA matrices of different shapes in one launch.
+    """Solve a list of float32 CUDA matrices of different shapes in one call.
     Returns a list of (U, s, Vh) like svd() of each matrix would."""
     if not mats:
         return []

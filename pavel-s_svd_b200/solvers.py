@@ -4,10 +4,11 @@ Mirrors svdbench/standalone/solvers.py:264-324 of uncle-Slava/Pavel-s_SVD:
 same argument names and meaning, same validation order, same exception types
 and messages, same output contract (U (...,m,k), s (...,k), Vh (...,k,n);
 ``None`` for U and Vh with ``values_only``; the info dict with ``return_info``).
-For 'jacobi' the numeric work is ONE launch of the sm_100a batched kernel
-per call (``jb_svd_batched_f32`` / ``_f64``, ``_c64`` / ``_c128`` for
-complex input); the host reads back only the per-matrix status and sweep
-words to raise the reference's errors.
+For 'jacobi' the numeric work is ONE call of the sm_100a batched solver
+(``jb_svd_batched_f32`` / ``_f64``, ``_c64`` / ``_c128`` for complex input:
+one persistent kernel, two for the FP32 and FP64 phases of the mixed
+precision); the host reads back only the per-matrix status and sweep words
+to raise the reference's errors.
 
 Differences, by design:
   * CUDA tensors only.  Other devices, the reference families not built here
@@ -184,7 +185,7 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
         stats = {'algorithm': algorithm, 'vendor_factorizations': 0, 'converged': True,
                  'jacobi_sweeps': sweeps,
                  'precision': 'fp64' if a.dtype == torch.float64 else precision,
-                 'implementation': 'B200 sm_100a batched one-sided Jacobi (one launch)'}
+                 'implementation': 'B200 sm_100a batched one-sided Jacobi (one call, persistent kernels)'}
         result = (None if values_only else u.reshape(*shape, *u.shape[-2:]),
                   s.reshape(*shape, rank),
                   None if values_only else vh.reshape(*shape, *vh.shape[-2:]))
@@ -278,7 +279,7 @@ def _complex_svd(a, full_matrices, values_only, return_info, rank, opts):
     """'jacobi' on complex64 / complex128 (primitives.py:316-367 in the input
     precision, round-robin order; solvers.py:264-310 around it): the batch
     scaled by a power of two (exact), a wide matrix solved through its
-    conjugate transpose (:224-227), one launch of jb_svd_batched_c64/_c128,
+    conjugate transpose (:224-227), one call of jb_svd_batched_c64/_c128,
     then the cut columns of U completed (primitives.py:430-455), sigma
     rescaled, full bases completed or the rank truncated, the output
     checked.  Options tol and max_sweeps; the FP32/mixed and ordering options
@@ -333,7 +334,7 @@ def _complex_svd(a, full_matrices, values_only, return_info, rank, opts):
                   None if values_only else v.mH.resolve_conj().reshape(*shape, v.shape[-1], v.shape[-2]))
     stats = {'algorithm': 'jacobi', 'vendor_factorizations': 0, 'converged': True, 'jacobi_sweeps': sweeps,
              'precision': 'fp32' if a.dtype == torch.complex64 else 'fp64',
-             'implementation': 'B200 sm_100a complex one-sided Jacobi (round-robin, one launch)'}
+             'implementation': 'B200 sm_100a complex one-sided Jacobi (round-robin, one kernel)'}
     return (*result, stats) if return_info else result
 
 
@@ -466,6 +467,6 @@ def factory(a, spec):
         return u, s, vh
     run.metadata = {'implementation': 'B200 sm_100a one-sided Jacobi, hand-written CUDA via C ABI',
                     'vendor_factorizations': False, 'values_only_forms_vectors': True, 'rng_in_solve': False,
-                    'gpu_control': 'one persistent launch per call; per-matrix convergence on device; '
+                    'gpu_control': 'one C-ABI call per solve (persistent kernels); per-matrix convergence on device; '
                                    'one status read-back per call'}
     return run
