@@ -328,14 +328,20 @@ JB_API int jb_eigh_f64(const double *H, double *W, double *V, int32_t *sweeps, i
  * householder_vec :41-59, the LAPACK xLARFG convention; Q by backward
  * accumulation), the QR of its 'qr', 'tsqr' and projected solvers
  * (solvers.py:71-96, 185-220, 245-248).  A (batch, m, n) row-major in;
- * Q (batch, m, n) and R (batch, n, n, upper triangular) row-major out;
- * computed in the input type.  Workspace: jb_qr_workspace_bytes (0 when a
- * matrix and its Q fit in shared memory). */
+ * Q (batch, m, n) and R (batch, n, n, upper triangular, real diagonal)
+ * row-major out; computed in the input type; _c64 / _c128 take interleaved
+ * complex.  Workspace: jb_qr_workspace_bytes with elem the element size (4,
+ * 8 for float64 and complex64, 16 for complex128; 0 when a matrix and its Q
+ * fit in shared memory). */
 JB_API size_t jb_qr_workspace_bytes(int32_t m, int32_t n, int64_t batch, int32_t elem);
 JB_API int jb_qr_f32(const float *A, float *Q, float *R, int64_t batch, int32_t m, int32_t n,
                      void *workspace, size_t workspace_bytes, void *stream);
 JB_API int jb_qr_f64(const double *A, double *Q, double *R, int64_t batch, int32_t m, int32_t n,
                      void *workspace, size_t workspace_bytes, void *stream);
+JB_API int jb_qr_c64(const void *A, void *Q, void *R, int64_t batch, int32_t m, int32_t n,
+                     void *workspace, size_t workspace_bytes, void *stream);
+JB_API int jb_qr_c128(const void *A, void *Q, void *R, int64_t batch, int32_t m, int32_t n,
+                      void *workspace, size_t workspace_bytes, void *stream);
 
 /* Batched one-sided Jacobi SVD of complex matrices: replaces the reference's
  * jacobi_svd for complex64 / complex128 (svdbench/standalone/primitives.py:

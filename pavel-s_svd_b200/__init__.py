@@ -8,11 +8,11 @@ harness plug-in name (svdbench/algorithms.py:90-93).
 """
 import sys as _sys
 
-from .solvers import ALGORITHMS, REFERENCE_ALGORITHMS, Unsupported, svd, factory
+from .solvers import ALGORITHMS, COMPLEX_ALGORITHMS, REFERENCE_ALGORITHMS, Unsupported, svd, factory
 from .batch import UnevenBatch, svd_uneven
 from . import native
 
 _sys.modules.setdefault("pavel_s_svd_b200", _sys.modules[__name__])
 
-__all__ = ["ALGORITHMS", "REFERENCE_ALGORITHMS", "Unsupported", "svd", "factory", "UnevenBatch",
+__all__ = ["ALGORITHMS", "COMPLEX_ALGORITHMS", "REFERENCE_ALGORITHMS", "Unsupported", "svd", "factory", "UnevenBatch",
            "svd_uneven", "native"]

@@ -135,6 +135,120 @@ __global__ void __launch_bounds__(kThreads) qr_kernel(const T *A, T *Qo, T *Ro, 
     }
 }
 
+// Complex input (complex64 / complex128, interleaved re, im): the same
+// algorithm with the reference's complex reflector (householder_vec for
+// complex x: beta = -sign(Re alpha) hypot(|alpha|, ||x_2:||), real; the
+// column is left alone only when nothing is below the diagonal AND alpha is
+// real; tau = (beta - alpha) / beta and v = x / (alpha - beta) complex), the
+// factorisation applying (I - conj(tau) v v^H) and Q accumulating
+// (I - tau v v^H) as primitives.py:80-87 do.
+template <typename R> struct Cx { R re, im; };
+template <typename R> __device__ __forceinline__ Cx<R> cmul(Cx<R> a, Cx<R> b) {
+    return Cx<R>{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <typename R> __device__ __forceinline__ Cx<R> cmulc(Cx<R> a, Cx<R> b) {   // conj(a) b
+    return Cx<R>{a.re * b.re + a.im * b.im, a.re * b.im - a.im * b.re};
+}
+template <typename R> __device__ __forceinline__ Cx<R> cdiv(Cx<R> a, Cx<R> b) {
+    const R d = b.re * b.re + b.im * b.im;
+    return Cx<R>{(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d};
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads) cqr_kernel(const Cx<R> *A, Cx<R> *Qo, Cx<R> *Ro, int64_t batch, int m,
+                                                       int n, int in_smem, Cx<R> *gws) {
+    using C = Cx<R>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    double *red = (double *)smem;
+    C *tau = (C *)(smem + 32 * 8);
+    const size_t mn = (size_t)m * n;
+    C *Wk = in_smem ? (C *)(smem + 32 * 8 + align16z((size_t)n * sizeof(C))) : gws + (size_t)blockIdx.x * 2 * mn;
+    C *Qk = Wk + mn;
+    const C zero{R(0), R(0)}, one{R(1), R(0)};
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int64_t z = blockIdx.x; z < batch; z += gridDim.x) {
+        const C *a = A + z * (int64_t)mn;
+        __syncthreads();
+        for (size_t idx = threadIdx.x; idx < mn; idx += blockDim.x) {
+            const int r = (int)(idx / n), c = (int)(idx - (size_t)r * n);
+            Wk[(size_t)c * m + r] = a[idx];
+        }
+        __syncthreads();
+        for (int j = 0; j < n; ++j) {
+            C *x = Wk + (size_t)j * m;
+            R part = R(0);
+            for (int i = j + 1 + threadIdx.x; i < m; i += blockDim.x) part += x[i].re * x[i].re + x[i].im * x[i].im;
+            const R xnorm = sqrt(block_sum(part, red));   // block_sum ends with a barrier
+            const C alpha = x[j];
+            const bool trivial = xnorm == R(0) && alpha.im == R(0);
+            const R beta = trivial ? alpha.re
+                                   : (alpha.re < R(0) ? R(1) : R(-1)) * hyp(hyp(alpha.re, alpha.im), xnorm);
+            const C denom = trivial ? one : C{alpha.re - beta, alpha.im};
+            const R bd = beta != R(0) ? beta : R(1);
+            const C t = trivial ? zero : C{(beta - alpha.re) / bd, -alpha.im / bd};
+            __syncthreads();
+            for (int i = j + 1 + threadIdx.x; i < m; i += blockDim.x) x[i] = trivial ? zero : cdiv(x[i], denom);
+            if (threadIdx.x == 0) { tau[j] = t; x[j] = C{beta, R(0)}; }
+            __syncthreads();
+            if (t.re != R(0) || t.im != R(0)) {
+                // columns j+1..n-1, rows j..m-1: y <- y - conj(tau) v (v^H y), v_j = 1
+                const C tc{t.re, -t.im};
+                for (int c = j + 1 + warp; c < n; c += nw) {
+                    C *y = Wk + (size_t)c * m;
+                    C w = zero;
+                    for (int i = j + lane; i < m; i += 32) {
+                        const C p = cmulc(i == j ? one : x[i], y[i]);
+                        w.re += p.re; w.im += p.im;
+                    }
+                    w.re = warp_sum(w.re); w.im = warp_sum(w.im);
+                    const C tw = cmul(tc, w);
+                    for (int i = j + lane; i < m; i += 32) {
+                        const C d = cmul(i == j ? one : x[i], tw);
+                        y[i].re -= d.re; y[i].im -= d.im;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        C *r = Ro + z * (int64_t)n * n;
+        for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+            const int i = idx / n, c = idx - i * n;
+            r[idx] = i <= c ? Wk[(size_t)c * m + i] : zero;
+        }
+        for (size_t idx = threadIdx.x; idx < mn; idx += blockDim.x) {
+            const int c = (int)(idx / m), i = (int)(idx - (size_t)c * m);
+            Qk[idx] = i == c ? one : zero;
+        }
+        __syncthreads();
+        for (int j = n - 1; j >= 0; --j) {
+            const C t = tau[j];
+            if (t.re != R(0) || t.im != R(0)) {
+                const C *v = Wk + (size_t)j * m;
+                for (int c = j + warp; c < n; c += nw) {
+                    C *y = Qk + (size_t)c * m;
+                    C w = zero;
+                    for (int i = j + lane; i < m; i += 32) {
+                        const C p = cmulc(i == j ? one : v[i], y[i]);
+                        w.re += p.re; w.im += p.im;
+                    }
+                    w.re = warp_sum(w.re); w.im = warp_sum(w.im);
+                    const C tw = cmul(t, w);
+                    for (int i = j + lane; i < m; i += 32) {
+                        const C d = cmul(i == j ? one : v[i], tw);
+                        y[i].re -= d.re; y[i].im -= d.im;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        C *q = Qo + z * (int64_t)mn;
+        for (size_t idx = threadIdx.x; idx < mn; idx += blockDim.x) {
+            const int i = (int)(idx / n), c = (int)(idx - (size_t)i * n);
+            q[idx] = Qk[(size_t)c * m + i];
+        }
+    }
+}
+
 static int sm_count_of_device() {
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))
@@ -156,12 +270,11 @@ static size_t workspace_bytes(int m, int n, int64_t batch) {
     return (size_t)grid * 2 * (size_t)m * n * sizeof(T);
 }
 
-template <typename T>
-static int launch(const T *A, T *Q, T *R, int64_t batch, int m, int n, void *workspace, size_t ws_bytes,
+template <typename T, typename K>
+static int launch(K kern, const T *A, T *Q, T *R, int64_t batch, int m, int n, void *workspace, size_t ws_bytes,
                   cudaStream_t st) {
     const bool in_smem = fits_smem<T>(m, n);
     const size_t smem = smem_bytes<T>(m, n, in_smem);
-    auto kern = qr_kernel<T>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return JB_ECUDA;
     int per_sm = 0;
@@ -182,13 +295,13 @@ static int launch(const T *A, T *Q, T *R, int64_t batch, int m, int n, void *wor
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
 }
 
-template <typename T>
-static int entry(const T *A, T *Q, T *R, int64_t batch, int32_t m, int32_t n, void *workspace, size_t ws_bytes,
-                 void *stream) {
+template <typename T, typename K>
+static int entry(K kern, const T *A, T *Q, T *R, int64_t batch, int32_t m, int32_t n, void *workspace,
+                 size_t ws_bytes, void *stream) {
     if (!A || !Q || !R || batch < 0 || n < 1 || m < n) return JB_EINVAL;
     if ((int64_t)m * n > ((int64_t)1 << 31)) return JB_ETOOBIG;
     if (batch == 0) return JB_OK;
-    return launch<T>(A, Q, R, batch, m, n, workspace, ws_bytes, (cudaStream_t)stream);
+    return launch<T>(kern, A, Q, R, batch, m, n, workspace, ws_bytes, (cudaStream_t)stream);
 }
 
 }  // namespace qr
@@ -198,17 +311,33 @@ extern "C" {
 
 size_t jb_qr_workspace_bytes(int32_t m, int32_t n, int64_t batch, int32_t elem) {
     if (n < 1 || m < n || batch < 0) return 0;
+    if (elem == 16) return jb::qr::workspace_bytes<jb::qr::Cx<double>>(m, n, batch);
     return elem == 8 ? jb::qr::workspace_bytes<double>(m, n, batch) : jb::qr::workspace_bytes<float>(m, n, batch);
 }
 
 int jb_qr_f32(const float *A, float *Q, float *R, int64_t batch, int32_t m, int32_t n, void *workspace,
               size_t workspace_bytes, void *stream) {
-    return jb::qr::entry<float>(A, Q, R, batch, m, n, workspace, workspace_bytes, stream);
+    return jb::qr::entry<float>(jb::qr::qr_kernel<float>, A, Q, R, batch, m, n, workspace, workspace_bytes, stream);
 }
 
 int jb_qr_f64(const double *A, double *Q, double *R, int64_t batch, int32_t m, int32_t n, void *workspace,
               size_t workspace_bytes, void *stream) {
-    return jb::qr::entry<double>(A, Q, R, batch, m, n, workspace, workspace_bytes, stream);
+    return jb::qr::entry<double>(jb::qr::qr_kernel<double>, A, Q, R, batch, m, n, workspace, workspace_bytes,
+                                 stream);
+}
+
+int jb_qr_c64(const void *A, void *Q, void *R, int64_t batch, int32_t m, int32_t n, void *workspace,
+              size_t workspace_bytes, void *stream) {
+    using E = jb::qr::Cx<float>;
+    return jb::qr::entry<E>(jb::qr::cqr_kernel<float>, (const E *)A, (E *)Q, (E *)R, batch, m, n, workspace,
+                            workspace_bytes, stream);
+}
+
+int jb_qr_c128(const void *A, void *Q, void *R, int64_t batch, int32_t m, int32_t n, void *workspace,
+               size_t workspace_bytes, void *stream) {
+    using E = jb::qr::Cx<double>;
+    return jb::qr::entry<E>(jb::qr::cqr_kernel<double>, (const E *)A, (E *)Q, (E *)R, batch, m, n, workspace,
+                            workspace_bytes, stream);
 }
 
 }  // extern "C"

@@ -30,7 +30,7 @@ SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_bat
            "jb_warm_prep_f32", "jb_svd_warm_f32", "jb_transpose_bf16", "jb_bias_act", "jb_relu_backward",
            "jb_col_sum", "jb_mse_grad", "jb_adam", "jb_gram_sketch", "jb_block_eig_f64", "jb_rows_scatter",
            "jb_rows_combine", "jb_gemm_f64acc", "jb_block_finish", "jb_eigh_workspace_bytes", "jb_eigh_f32",
-           "jb_eigh_f64", "jb_qr_workspace_bytes", "jb_qr_f32", "jb_qr_f64", "jb_svd_complex_workspace_bytes",
+           "jb_eigh_f64", "jb_qr_workspace_bytes", "jb_qr_f32", "jb_qr_f64", "jb_qr_c64", "jb_qr_c128", "jb_svd_complex_workspace_bytes",
            "jb_svd_batched_c64", "jb_svd_batched_c128", "jb_jacobi_rounds", "jb_svd_batched_f32_noalloc")
 GEMM_PLAIN, GEMM_SPLIT3, GEMM_SPLIT6, GEMM_B_MN, GEMM_CHAIN128, GEMM_SYRK = 0, 1, 2, 4, 8, 16
 NOALLOC_SCRATCH_BYTES = 16 << 20  # JB_NOALLOC_SCRATCH_BYTES
@@ -67,7 +67,7 @@ def _declare(l):
         getattr(l, name).argtypes = [P, P, P, P, P, I64, I32, F64, I32, P, SZ, P]
     l.jb_qr_workspace_bytes.restype = SZ
     l.jb_qr_workspace_bytes.argtypes = [I32, I32, I64, I32]
-    for name in ("jb_qr_f32", "jb_qr_f64"):
+    for name in ("jb_qr_f32", "jb_qr_f64", "jb_qr_c64", "jb_qr_c128"):
         getattr(l, name).restype = ctypes.c_int
         getattr(l, name).argtypes = [P, P, P, I64, I32, I32, P, SZ, P]
     l.jb_svd_complex_workspace_bytes.restype = SZ

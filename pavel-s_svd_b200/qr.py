@@ -4,7 +4,7 @@ and the projected 'randomized', 'subspace' and 'block_krylov' solvers (a
 range basis from QRs of sketches, then the Jacobi of the projected matrix).
 
 Mirrors svdbench/standalone of uncle-Slava/Pavel-s_SVD:
-  qr       primitives.py:41-89 (householder_vec, qr) -> jb_qr_f32 / jb_qr_f64
+  qr       primitives.py:41-89 (householder_vec, qr) -> jb_qr_f32 / _f64 / _c64 / _c128
   tsqr     solvers.py:71-96
   partial  solvers.py:185-220 (with _sketch, :179-182)
   raw      solvers.py:224-230, 245-248, 253-254 for these methods
@@ -19,6 +19,8 @@ import torch
 from . import native as N
 
 PARTIAL = ('randomized', 'subspace', 'block_krylov')
+_QR = {torch.float32: 'jb_qr_f32', torch.float64: 'jb_qr_f64', torch.complex64: 'jb_qr_c64',
+       torch.complex128: 'jb_qr_c128'}
 METHODS = ('qr', 'tsqr') + PARTIAL
 
 _ws = {}
@@ -34,18 +36,18 @@ def _workspace(nbytes, device):
 
 
 def qr(a: torch.Tensor):
-    """Householder QR of a batch of tall matrices (b, m, n), m >= n, float32
-    or float64 on a CUDA device: Q (b, m, n), R (b, n, n) upper triangular,
-    in the input dtype (primitives.py:74-89, computed as the reference does,
-    in that dtype)."""
+    """Householder QR of a batch of tall matrices (b, m, n), m >= n, float32,
+    float64, complex64 or complex128 on a CUDA device: Q (b, m, n), R (b, n,
+    n) upper triangular, in the input dtype (primitives.py:74-89, computed as
+    the reference does, in that dtype)."""
     if a.ndim != 3 or a.shape[-2] < a.shape[-1]:
         raise ValueError('qr expects a (batch, m, n) tensor with m >= n')
-    if a.dtype not in (torch.float32, torch.float64):
-        raise TypeError('qr supports float32 and float64')
+    if a.dtype not in _QR:
+        raise TypeError('qr supports float32, float64, complex64 and complex128')
     if a.device.type != 'cuda':
         raise RuntimeError('the B200 QR runs on CUDA tensors only; there is no CPU fallback')
     b, m, n = a.shape
-    x = a.contiguous()
+    x = a.resolve_conj().contiguous()   # the kernel reads memory: no lazy conjugate view
     q = torch.empty(b, m, n, dtype=a.dtype, device=a.device)
     r = torch.empty(b, n, n, dtype=a.dtype, device=a.device)
     if b == 0:
@@ -54,7 +56,7 @@ def qr(a: torch.Tensor):
     elem = x.element_size()
     ws = _workspace(lib.jb_qr_workspace_bytes(m, n, b, elem), a.device)
     stream = torch.cuda.current_stream(a.device).cuda_stream
-    fn = lib.jb_qr_f32 if a.dtype == torch.float32 else lib.jb_qr_f64
+    fn = getattr(lib, _QR[a.dtype])
     N.check(fn(x.data_ptr(), q.data_ptr(), r.data_ptr(), b, m, n, ws.data_ptr(), ws.numel(), stream), 'jb_qr')
     return q, r
 
@@ -151,7 +153,7 @@ def raw(x: torch.Tensor, method: str, stats: dict, opts: dict, jacobi):
     253-254): wide input through its transpose except for the projected
     solvers; 'qr' / 'tsqr' solve R by Jacobi and return U = Q U_R."""
     if x.shape[-2] < x.shape[-1] and method not in PARTIAL:
-        u, s, v = raw(x.mH.contiguous(), method, stats, opts, jacobi)
+        u, s, v = raw(x.mH.resolve_conj().contiguous(), method, stats, opts, jacobi)
         return v, s, u
     if method in ('qr', 'tsqr'):
         q, r = qr(x) if method == 'qr' else tsqr(x, opts.get('tile_rows', 4 * x.shape[-1]), stats)

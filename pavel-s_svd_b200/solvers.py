@@ -38,6 +38,7 @@ REFERENCE_ALGORITHMS = (
     'polar_halley', 'polar_polynomial', 'randomized', 'subspace', 'block_krylov', 'lanczos',
 )  # svdbench/standalone/solvers.py:7-11
 ALGORITHMS = ('jacobi', 'block_jacobi', 'gram_jacobi', 'qr', 'tsqr', 'randomized', 'subspace', 'block_krylov')
+COMPLEX_ALGORITHMS = ('jacobi', 'qr', 'tsqr', 'randomized', 'subspace', 'block_krylov')
 PRECISIONS = ('mixed', 'fp32')
 ORDERINGS = ('block', 'round_robin')
 
@@ -69,8 +70,8 @@ def _validate(a, algorithm, full_matrices, opts):
         raise Unsupported(f'{algorithm!r} is not implemented by the B200 solver (implemented: {ALGORITHMS})')
     if a.device.type != 'cuda':
         raise Unsupported('the B200 Jacobi solver runs on CUDA tensors only; there is no CPU fallback')
-    if a.is_complex() and algorithm != 'jacobi':
-        raise Unsupported(f'complex input runs through jacobi only in the B200 solver, not {algorithm!r}')
+    if a.is_complex() and algorithm not in COMPLEX_ALGORITHMS:
+        raise Unsupported(f'complex input runs through {COMPLEX_ALGORITHMS} in the B200 solver, not {algorithm!r}')
     precision = opts.get('precision', 'mixed')
     if precision not in PRECISIONS:
         raise ValueError(f'precision must be one of {PRECISIONS}')
@@ -147,7 +148,7 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
     Jacobi (_qr_family_svd).
     Input is never overwritten."""
     rank, precision = _validate(a, algorithm, full_matrices, opts)
-    if a.is_complex():
+    if a.is_complex() and algorithm == 'jacobi':
         return _complex_svd(a, full_matrices, values_only, return_info, rank, opts)
     if algorithm == 'block_jacobi':
         return _block_svd(a, full_matrices, values_only, return_info, rank, opts)
@@ -385,8 +386,9 @@ def _qr_family_svd(a, algorithm, full_matrices, values_only, return_info, rank, 
             u, sv, v = u[:, :, :rank], sv[:, :rank], v[:, :, :rank]
         if not all(bool(torch.isfinite(t).all()) for t in (u, sv, v)):
             raise RuntimeError('standalone solver produced nonfinite output')
-        result = (None if values_only else u.reshape(*shape, *u.shape[-2:]), sv.reshape(*shape, sv.shape[-1]),
-                  None if values_only else v.mH.reshape(*shape, v.shape[-1], v.shape[-2]))
+        result = (None if values_only else u.resolve_conj().reshape(*shape, *u.shape[-2:]),
+                  sv.reshape(*shape, sv.shape[-1]),
+                  None if values_only else v.mH.resolve_conj().reshape(*shape, v.shape[-1], v.shape[-2]))
     stats['implementation'] = 'B200 sm_100a Householder QR + batched one-sided Jacobi'
     return (*result, stats) if return_info else result
 

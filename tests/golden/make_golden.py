@@ -107,6 +107,8 @@ def qr_cases(make_matrix):
     a[1, 3:, 5] = 0.0
     out.append(("deficient_f64", a))
     out.append(("tall_f32", make_matrix(dict(m=130, n=33, batch=2, dtype="float32", family="gaussian"))))
+    for dt in ("complex64", "complex128"):
+        out.append((f"gauss_{dt}", make_matrix(dict(m=21, n=8, batch=2, dtype=dt, family="gaussian"))))
     return out
 
 
@@ -131,6 +133,15 @@ def method_cases(make_matrix):
     a = make_matrix(dict(m=10, n=26, batch=2, dtype="float64", family="gaussian"))
     out.append(("randomized_wide_float64", a, "randomized",
                 {"rank": 4, "oversample": 4, "initial_basis": rng.standard_normal((2, 26, 8))}))
+    # complex inputs (tests/test_standalone.py:47-54 runs every family on them)
+    for dt in ("complex64", "complex128"):
+        out.append((f"qr_{dt}", make_matrix(dict(m=13, n=7, batch=2, dtype=dt, family="gaussian")), "qr", {}))
+        out.append((f"tsqr_wide_{dt}", make_matrix(dict(m=7, n=13, batch=2, dtype=dt, family="gaussian")), "tsqr",
+                    {"tile_rows": 7}))
+        a = make_matrix(dict(m=24, n=10, batch=2, dtype=dt, family="geometric", condition=1e3))
+        om = (rng.standard_normal((2, 10, 6)) + 1j * rng.standard_normal((2, 10, 6))).astype(dt)
+        out.append((f"subspace_{dt}", a, "subspace", {"rank": 3, "oversample": 3, "iterations": 2,
+                                                      "initial_basis": om}))
     return out
 
 
@@ -245,7 +256,7 @@ def main():
     for name, a in qr_cases(make_matrix):
         a = np.ascontiguousarray(a)
         q, r = P.qr(torch.from_numpy(a.copy()))
-        blob[f"qr_{name}/a"], blob[f"qr_{name}/q"], blob[f"qr_{name}/r"] = a, q.numpy(), r.numpy()
+        blob[f"qr_{name}/a"], blob[f"qr_{name}/q"], blob[f"qr_{name}/r"] = a, q.resolve_conj().numpy(), r.resolve_conj().numpy()
         qnames.append(name)
         print(f"qr {name:24s} {str(a.shape):14s} {a.dtype}")
     blob["_qr_names"] = np.array(qnames)
@@ -255,9 +266,11 @@ def main():
         a = np.ascontiguousarray(a)
         tkw = {k: (torch.from_numpy(np.ascontiguousarray(v)) if isinstance(v, np.ndarray) else v) for k, v in kw.items()}
         u, s, vh, info = svd(torch.from_numpy(a.copy()), alg, return_info=True, **tkw)
-        flat = a.reshape(-1, *a.shape[-2:]).astype(np.float64)
+        flat = a.reshape(-1, *a.shape[-2:]).astype(np.complex128 if np.iscomplexobj(a) else np.float64)
         blob[f"meth_{name}/a"] = a
-        blob[f"meth_{name}/u"], blob[f"meth_{name}/s"], blob[f"meth_{name}/vh"] = u.numpy(), s.numpy(), vh.numpy()
+        blob[f"meth_{name}/u"] = u.resolve_conj().numpy()
+        blob[f"meth_{name}/s"] = s.numpy()
+        blob[f"meth_{name}/vh"] = vh.resolve_conj().numpy()
         blob[f"meth_{name}/truth"] = np.stack([scipy.linalg.svd(x, compute_uv=False, lapack_driver="gesvd")
                                                for x in flat])
         blob[f"meth_{name}/alg"] = np.array(alg)
