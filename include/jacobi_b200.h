@@ -322,6 +322,18 @@ JB_API int jb_eigh_f32(const float *H, float *W, float *V, int32_t *sweeps, int3
 JB_API int jb_eigh_f64(const double *H, double *W, double *V, int32_t *sweeps, int32_t *status,
                        int64_t batch, int32_t n, double tol, int32_t max_sweeps,
                        void *workspace, size_t workspace_bytes, void *stream);
+/* The same for complex Hermitian H (complex64 / complex128, interleaved re,
+ * im), computed in complex128: the reference's complex branch of jacobi_eigh
+ * (primitives.py:393-421, s = t c g_pq / |g_pq|, G <- J^H G J).  W real
+ * (batch, n) ascending, V complex (batch, n, n).  Workspace:
+ * jb_eigh_complex_workspace_bytes (0 while G and V fit in shared memory). */
+JB_API size_t jb_eigh_complex_workspace_bytes(int32_t n, int64_t batch);
+JB_API int jb_eigh_c64(const void *H, float *W, void *V, int32_t *sweeps, int32_t *status,
+                       int64_t batch, int32_t n, double tol, int32_t max_sweeps,
+                       void *workspace, size_t workspace_bytes, void *stream);
+JB_API int jb_eigh_c128(const void *H, double *W, void *V, int32_t *sweeps, int32_t *status,
+                        int64_t batch, int32_t n, double tol, int32_t max_sweeps,
+                        void *workspace, size_t workspace_bytes, void *stream);
 
 /* Batched Householder QR of tall matrices (m >= n): replaces the reference's
  * primitives.qr, svdbench/standalone/primitives.py:74-89 (reflectors by

@@ -408,9 +408,9 @@ def validate(a, result, refs):
 
 
 def jacobi_eigh(H, tol=None, max_sweeps=30):
-    """Two-sided cyclic Jacobi of real symmetric H (b, n, n): w ascending, V,
-    sweeps.  Restates primitives.py:370-427 for real input, in the input's
-    dtype, batched in lock-step: zero-padding to even n (:384-386), tol =
+    """Two-sided cyclic Jacobi of Hermitian H (b, n, n), real or complex: w
+    ascending (real), V, sweeps.  Restates primitives.py:370-427 in the
+    input's dtype, batched in lock-step: zero-padding to even n (:384-386), tol =
     10 eps (:388), per round the scale max|G| (:395), active pairs
     |g_pq| > tol scale (:396), off = max |g_pq| / scale (:397), the rotation
     (:398-405), G <- G J then G <- J^T G (:407-414), V <- V J (:410-411),
@@ -433,7 +433,7 @@ def jacobi_eigh(H, tol=None, max_sweeps=30):
     for sweeps in range(1, max_sweeps + 1):
         off = 0.0
         for P, Q in sched:
-            gpp, gqq, gpq = G[bi, P, P], G[bi, Q, Q], G[bi, P, Q]
+            gpp, gqq, gpq = G[bi, P, P].real, G[bi, Q, Q].real, G[bi, P, Q]
             a = np.abs(gpq)
             scale = np.broadcast_to(np.abs(G).max(axis=(-2, -1))[:, None], a.shape)
             active = a > tol * scale
@@ -448,17 +448,17 @@ def jacobi_eigh(H, tol=None, max_sweeps=30):
             s = np.where(active, s, 0).astype(G.dtype)
             cc, ss = c[:, None, :], s[:, None, :]
             gp, gq = G[:, :, P].copy(), G[:, :, Q].copy()
-            G[:, :, P], G[:, :, Q] = cc * gp - ss * gq, ss * gp + cc * gq
+            G[:, :, P], G[:, :, Q] = cc * gp - np.conj(ss) * gq, ss * gp + cc * gq
             vp, vq = V[:, :, P].copy(), V[:, :, Q].copy()
-            V[:, :, P], V[:, :, Q] = cc * vp - ss * vq, ss * vp + cc * vq
+            V[:, :, P], V[:, :, Q] = cc * vp - np.conj(ss) * vq, ss * vp + cc * vq
             cc, ss = c[:, :, None], s[:, :, None]
             rp, rq = G[:, P, :].copy(), G[:, Q, :].copy()
-            G[:, P, :], G[:, Q, :] = cc * rp - ss * rq, ss * rp + cc * rq
+            G[:, P, :], G[:, Q, :] = cc * rp - ss * rq, np.conj(ss) * rp + cc * rq
         if off <= tol:
             break
     if off > tol:
         raise RuntimeError(f"Hermitian Jacobi did not converge in {max_sweeps} sweeps")
-    w = np.diagonal(G, axis1=-2, axis2=-1).copy()
+    w = np.diagonal(G, axis1=-2, axis2=-1).real.copy()
     if padded:
         w, V = w[:, :-1], V[:, :-1, :-1]
     order = np.argsort(w, axis=-1, kind="stable")

@@ -151,7 +151,176 @@ __global__ void __launch_bounds__(kThreads) eigh_kernel(const T *H, T *W, T *Vou
     }
 }
 
+// Complex Hermitian H (complex64 / complex128, interleaved re, im), computed
+// in complex128: the reference's complex branch (primitives.py:393-421) --
+// g_pp, g_qq real, s = t c g_pq / |g_pq|, G <- G J on columns (c g_p -
+// conj(s) g_q, s g_p + c g_q), G <- J^H G on rows (c r_p - s r_q, conj(s) r_p
+// + c r_q), V <- V J; the same round-robin pairs, scale and convergence test
+// as the real kernel.  Shared memory: G (and V) as double pairs when they fit.
+struct Z { double re, im; };
+__device__ __forceinline__ Z zmul(Z a, Z b) { return Z{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+__device__ __forceinline__ Z zconj(Z a) { return Z{a.re, -a.im}; }
+__device__ __forceinline__ Z zaxpby(double ca, Z x, Z sb, Z y) {   // ca x + sb y
+    const Z t = zmul(sb, y);
+    return Z{ca * x.re + t.re, ca * x.im + t.im};
+}
+
+__host__ __device__ inline size_t zsmem_bytes(int np, int mode) {
+    return (size_t)np * np * 16 * mode + (size_t)np * 24 + (size_t)np + 32 * 8 + (size_t)np * 4 + 64;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads) zeigh_kernel(const R *H, R *W, R *Vout, int32_t *sweeps_out,
+                                                         int32_t *status, int64_t batch, int n, double tol,
+                                                         int max_sweeps, int mode, Z *gv) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int np = n + (n & 1), half = np / 2;
+    const size_t nn = (size_t)np * np;
+    Z *area = gv ? gv + (size_t)blockIdx.x * nn * (2 - mode) : nullptr;
+    Z *G = mode >= 1 ? (Z *)smem : area;                      // G[col * np + row]
+    Z *V = mode == 2 ? (Z *)smem + nn : (mode == 1 ? area : area + nn);
+    double *cs = (double *)((Z *)smem + nn * mode);           // c[half]
+    Z *sv = (Z *)(cs + half + (half & 1));                    // s[half]
+    double *red = (double *)(sv + half);                      // 32 warp partials
+    int *perm = (int *)(red + 32);                            // np
+    unsigned char *pq = (unsigned char *)(perm + np);         // p[half], q[half]
+    __shared__ int s_any;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int64_t z = blockIdx.x; z < batch; z += gridDim.x) {
+        const R *h = H + z * (int64_t)n * n * 2;
+        __syncthreads();
+        for (int i = threadIdx.x; i < np * np; i += blockDim.x) {
+            const int c = i / np, r = i - c * np;
+            Z g{0.0, 0.0};
+            if (r < n && c < n) {   // (H + H^H) / 2
+                const double ar = (double)h[2 * ((size_t)r * n + c)], ai = (double)h[2 * ((size_t)r * n + c) + 1];
+                const double br = (double)h[2 * ((size_t)c * n + r)], bi = (double)h[2 * ((size_t)c * n + r) + 1];
+                g = Z{0.5 * (ar + br), 0.5 * (ai - bi)};
+            }
+            G[i] = g;
+            V[i] = Z{(r == c) ? 1.0 : 0.0, 0.0};
+        }
+        int sweep = 0, converged = 0;
+        for (sweep = 1; sweep <= max_sweeps; ++sweep) {
+            __syncthreads();
+            double mx = 0.0;
+            for (int i = threadIdx.x; i < np * np; i += blockDim.x) mx = fmax(mx, hypot(G[i].re, G[i].im));
+            for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            if (lane == 0) red[warp] = mx;
+            if (threadIdx.x == 0) s_any = 0;
+            __syncthreads();
+            double scale = 0.0;
+            for (int w = 0; w < nw; ++w) scale = fmax(scale, red[w]);
+            const double thr = tol * scale;
+            for (int r = 0; r < np - 1; ++r) {
+                __syncthreads();
+                for (int t = threadIdx.x; t < half; t += blockDim.x) {
+                    int p = circ(t, r, np), q = circ(np - 1 - t, r, np);
+                    if (p > q) { const int x = p; p = q; q = x; }
+                    const double gpp = G[(size_t)p * np + p].re, gqq = G[(size_t)q * np + q].re;
+                    const Z gpq = G[(size_t)q * np + p];                  // row p, column q
+                    const double a = hypot(gpq.re, gpq.im);
+                    double c = 1.0;
+                    Z s{0.0, 0.0};
+                    if (a > thr) {
+                        const double tau = (gqq - gpp) / (2.0 * a);
+                        const double tt = tau == 0.0 ? 1.0 : copysign(1.0, tau) / (fabs(tau) + hypot(tau, 1.0));
+                        c = 1.0 / sqrt(1.0 + tt * tt);
+                        s = Z{tt * c * gpq.re / a, tt * c * gpq.im / a};
+                        s_any = 1;
+                    }
+                    cs[t] = c;
+                    sv[t] = s;
+                    pq[t] = (unsigned char)p;
+                    pq[half + t] = (unsigned char)q;
+                }
+                __syncthreads();
+                // G <- J^H G J (2 x 2 blocks: row pair a, column pair b); V <- V J
+                for (int b = warp; b < half; b += nw) {
+                    const int u = pq[b], v = pq[half + b];
+                    const double cb = cs[b];
+                    const Z sb = sv[b], sbc = zconj(sb), msbc = Z{-sb.re, sb.im};
+                    Z *cu = G + (size_t)u * np, *cv = G + (size_t)v * np;
+                    for (int a = lane; a < half; a += 32) {
+                        const int p = pq[a], q = pq[half + a];
+                        const double ca = cs[a];
+                        const Z sa = sv[a], msa = Z{-sa.re, -sa.im}, sac = zconj(sa);
+                        const Z gpu = cu[p], gqu = cu[q], gpv = cv[p], gqv = cv[q];
+                        // rows: r_p = c r_p - s r_q, r_q = conj(s) r_p + c r_q
+                        const Z rpu = zaxpby(ca, gpu, msa, gqu), rqu = zaxpby(ca, gqu, sac, gpu);
+                        const Z rpv = zaxpby(ca, gpv, msa, gqv), rqv = zaxpby(ca, gqv, sac, gpv);
+                        // columns: g_u = c g_u - conj(s) g_v, g_v = s g_u + c g_v
+                        cu[p] = zaxpby(cb, rpu, msbc, rpv);
+                        cv[p] = zaxpby(cb, rpv, sb, rpu);
+                        cu[q] = zaxpby(cb, rqu, msbc, rqv);
+                        cv[q] = zaxpby(cb, rqv, sb, rqu);
+                    }
+                    if (cb != 1.0 || sb.re != 0.0 || sb.im != 0.0) {
+                        Z *vu = V + (size_t)u * np, *vv = V + (size_t)v * np;
+                        for (int i = lane; i < np; i += 32) {
+                            const Z x = vu[i], y = vv[i];
+                            vu[i] = zaxpby(cb, x, msbc, y);
+                            vv[i] = zaxpby(cb, y, sb, x);
+                        }
+                    }
+                    (void)sbc;
+                }
+            }
+            __syncthreads();
+            if (!s_any) { converged = 1; break; }
+        }
+        __syncthreads();
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const double dj = G[(size_t)j * np + j].re;
+            int rk = 0;
+            for (int i = 0; i < n; ++i) {
+                const double di = G[(size_t)i * np + i].re;
+                rk += (di < dj) || (di == dj && i < j);
+            }
+            perm[rk] = j;
+        }
+        __syncthreads();
+        R *w = W + z * (int64_t)n;
+        R *vo = Vout + z * (int64_t)n * n * 2;
+        for (int k = threadIdx.x; k < n; k += blockDim.x) w[k] = (R)G[(size_t)perm[k] * np + perm[k]].re;
+        for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+            const int i = k / n, j = k - i * n;
+            const Z x = V[(size_t)perm[j] * np + i];
+            vo[2 * k] = (R)x.re;
+            vo[2 * k + 1] = (R)x.im;
+        }
+        if (threadIdx.x == 0) {
+            if (sweeps_out) sweeps_out[z] = sweep > max_sweeps ? max_sweeps : sweep;
+            if (status) status[z] = converged ? JB_ST_OK : JB_ST_NOT_CONVERGED;
+        }
+    }
+}
+
 constexpr size_t kSmemLimit = 227 * 1024;
+
+template <typename R>
+static int zlaunch(const R *H, R *W, R *V, int32_t *sweeps, int32_t *status, int64_t batch, int n, double tol,
+                   int max_sweeps, void *workspace, size_t ws_bytes, cudaStream_t st) {
+    const int np = n + (n & 1);
+    const int mode = zsmem_bytes(np, 2) <= kSmemLimit ? 2 : (zsmem_bytes(np, 1) <= kSmemLimit ? 1 : 0);
+    const size_t smem = zsmem_bytes(np, mode);
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))
+        return JB_ECUDA;
+    int64_t grid = batch < (int64_t)sms * 4 ? batch : (int64_t)sms * 4;
+    Z *gv = nullptr;
+    if (mode < 2) {
+        const int64_t fit = (int64_t)(ws_bytes / ((size_t)np * np * 16 * (2 - mode)));
+        if (!workspace || fit < 1) return JB_EWORKSPACE;
+        if (grid > fit) grid = fit;
+        gv = (Z *)workspace;
+    }
+    auto kern = zeigh_kernel<R>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return JB_ECUDA;
+    kern<<<(unsigned)grid, kThreads, smem, st>>>(H, W, V, sweeps, status, batch, n, tol, max_sweeps, mode, gv);
+    return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+}
 
 template <typename T>
 static int launch(const T *H, T *W, T *V, int32_t *sweeps, int32_t *status, int64_t batch, int n, double tol,
@@ -202,6 +371,37 @@ int jb_eigh_f32(const float *H, float *W, float *V, int32_t *sweeps, int32_t *st
     if (tol <= 0) tol = 10.0 * 1.1920928955078125e-07;
     return jb::eigh::launch<float>(H, W, V, sweeps, status, batch, n, tol, max_sweeps, workspace, workspace_bytes,
                                    (cudaStream_t)stream);
+}
+
+size_t jb_eigh_complex_workspace_bytes(int32_t n, int64_t batch) {
+    if (n < 1 || batch < 0) return 0;
+    const int np = n + (n & 1);
+    const int mode = jb::eigh::zsmem_bytes(np, 2) <= jb::eigh::kSmemLimit ? 2
+                   : (jb::eigh::zsmem_bytes(np, 1) <= jb::eigh::kSmemLimit ? 1 : 0);
+    if (mode == 2) return 0;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev))
+        sms = 148;
+    const int64_t grid = batch < (int64_t)sms * 4 ? batch : (int64_t)sms * 4;
+    return (size_t)grid * np * np * 16 * (2 - mode);
+}
+
+int jb_eigh_c64(const void *H, float *W, void *V, int32_t *sweeps, int32_t *status, int64_t batch, int32_t n,
+                double tol, int32_t max_sweeps, void *workspace, size_t workspace_bytes, void *stream) {
+    if (!H || !W || !V || batch < 0 || n < 1 || n > 255 || max_sweeps < 1) return JB_EINVAL;
+    if (batch == 0) return JB_OK;
+    if (tol <= 0) tol = 10.0 * 1.1920928955078125e-07;
+    return jb::eigh::zlaunch<float>((const float *)H, W, (float *)V, sweeps, status, batch, n, tol, max_sweeps,
+                                    workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int jb_eigh_c128(const void *H, double *W, void *V, int32_t *sweeps, int32_t *status, int64_t batch, int32_t n,
+                 double tol, int32_t max_sweeps, void *workspace, size_t workspace_bytes, void *stream) {
+    if (!H || !W || !V || batch < 0 || n < 1 || n > 255 || max_sweeps < 1) return JB_EINVAL;
+    if (batch == 0) return JB_OK;
+    if (tol <= 0) tol = 10.0 * 2.220446049250313e-16;
+    return jb::eigh::zlaunch<double>((const double *)H, W, (double *)V, sweeps, status, batch, n, tol, max_sweeps,
+                                     workspace, workspace_bytes, (cudaStream_t)stream);
 }
 
 int jb_eigh_f64(const double *H, double *W, double *V, int32_t *sweeps, int32_t *status, int64_t batch, int32_t n,

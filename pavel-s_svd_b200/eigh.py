@@ -7,9 +7,10 @@ two-sided cyclic Jacobi with round-robin pairs, one plane rotation per
 active pair (|g_pq| > tol * max|G|), V accumulated, eigenvalues ascending.
 Same signature, return value ``(w, V, sweeps)`` and error
 (``RuntimeError('Hermitian Jacobi did not converge in N sweeps')``).  Real
-float32/float64 CUDA tensors of shape (b, n, n), n <= 255; the arithmetic is
-FP64 for both dtypes.  Complex input and other devices raise Unsupported:
-there is no CPU fallback.
+float32/float64 or complex64/complex128 (Hermitian) CUDA tensors of shape
+(b, n, n), n <= 255; the arithmetic is FP64 (complex128) for all of them;
+eigenvalues come out real.  Other devices raise Unsupported: there is no CPU
+fallback.
 """
 from __future__ import annotations
 
@@ -24,25 +25,25 @@ def jacobi_eigh(H: torch.Tensor, tol=None, max_sweeps=30):
         raise ValueError('jacobi_eigh takes a (b, n, n) batch of square matrices')
     if H.device.type != 'cuda':
         raise Unsupported('the B200 eigen-solver runs on CUDA tensors only; there is no CPU fallback')
-    if H.is_complex():
-        raise Unsupported('complex Hermitian Jacobi is not implemented by the B200 solver yet')
-    if H.dtype not in (torch.float32, torch.float64):
-        raise TypeError('supported dtypes: float32/64')
+    if H.dtype not in (torch.float32, torch.float64, torch.complex64, torch.complex128):
+        raise TypeError('supported dtypes: float32/64, complex64/128')
     if max_sweeps < 1:
         raise ValueError('max_sweeps must be positive')
     b, n, _ = H.shape
     if n > 255:
         raise Unsupported('jacobi_eigh on the B200 solver takes n <= 255')
-    x = H.detach().contiguous()
-    w = torch.empty(b, n, dtype=H.dtype, device=H.device)
+    x = H.detach().resolve_conj().contiguous()      # the kernel reads memory: no lazy conjugate view
+    real = H.real.dtype if H.is_complex() else H.dtype
+    w = torch.empty(b, n, dtype=real, device=H.device)
     V = torch.empty(b, n, n, dtype=H.dtype, device=H.device)
     info = torch.zeros(2, max(b, 1), dtype=torch.int32, device=H.device)
     if b == 0:
         return w, V, 0
     lib = N.lib()
-    ws_bytes = int(lib.jb_eigh_workspace_bytes(n, b))
+    ws_bytes = int(lib.jb_eigh_complex_workspace_bytes(n, b) if H.is_complex() else lib.jb_eigh_workspace_bytes(n, b))
     ws = torch.empty(max(ws_bytes, 8), dtype=torch.uint8, device=H.device)
-    fn = lib.jb_eigh_f32 if H.dtype == torch.float32 else lib.jb_eigh_f64
+    fn = {torch.float32: lib.jb_eigh_f32, torch.float64: lib.jb_eigh_f64, torch.complex64: lib.jb_eigh_c64,
+          torch.complex128: lib.jb_eigh_c128}[H.dtype]
     with torch.cuda.device(H.device):
         st = torch.cuda.current_stream(H.device).cuda_stream
         N.check(fn(x.data_ptr(), w.data_ptr(), V.data_ptr(), info[0].data_ptr(), info[1].data_ptr(), b, n,

@@ -24,14 +24,14 @@ RC_NAMES = {JB_EINVAL: "invalid argument", JB_ETOOBIG: "shape too large for this
 # Exported symbols, in declaration order of include/jacobi_b200.h.
 SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_batched_f32",
            "jb_svd_batched_f64", "jb_uneven_workspace_bytes", "jb_svd_uneven_f32", "jb_svd_uneven_f32_ex",
-           "jb_gemm_bf16", "jb_gemm_bf16x", "jb_gemm_bf16x_rows",
-           "jb_split_bf16",
-           "jb_split3_bf16",
+           "jb_gemm_bf16", "jb_gemm_bf16x", "jb_gemm_bf16x_rows", "jb_split_bf16", "jb_split3_bf16",
            "jb_warm_prep_f32", "jb_svd_warm_f32", "jb_transpose_bf16", "jb_bias_act", "jb_relu_backward",
            "jb_col_sum", "jb_mse_grad", "jb_adam", "jb_gram_sketch", "jb_block_eig_f64", "jb_rows_scatter",
            "jb_rows_combine", "jb_gemm_f64acc", "jb_block_finish", "jb_eigh_workspace_bytes", "jb_eigh_f32",
-           "jb_eigh_f64", "jb_qr_workspace_bytes", "jb_qr_f32", "jb_qr_f64", "jb_qr_c64", "jb_qr_c128", "jb_svd_complex_workspace_bytes",
-           "jb_svd_batched_c64", "jb_svd_batched_c128", "jb_jacobi_rounds", "jb_svd_batched_f32_noalloc")
+           "jb_eigh_f64", "jb_eigh_complex_workspace_bytes", "jb_eigh_c64", "jb_eigh_c128",
+           "jb_qr_workspace_bytes", "jb_qr_f32", "jb_qr_f64", "jb_qr_c64", "jb_qr_c128",
+           "jb_svd_complex_workspace_bytes", "jb_svd_batched_c64", "jb_svd_batched_c128", "jb_jacobi_rounds",
+           "jb_svd_batched_f32_noalloc")
 GEMM_PLAIN, GEMM_SPLIT3, GEMM_SPLIT6, GEMM_B_MN, GEMM_CHAIN128, GEMM_SYRK = 0, 1, 2, 4, 8, 16
 NOALLOC_SCRATCH_BYTES = 16 << 20  # JB_NOALLOC_SCRATCH_BYTES
 
@@ -62,7 +62,9 @@ def _declare(l):
     l.jb_uneven_workspace_bytes.argtypes = [I32, I32, I64, I32, I32, I64]
     l.jb_eigh_workspace_bytes.restype = SZ
     l.jb_eigh_workspace_bytes.argtypes = [I32, I64]
-    for name in ("jb_eigh_f32", "jb_eigh_f64"):
+    l.jb_eigh_complex_workspace_bytes.restype = SZ
+    l.jb_eigh_complex_workspace_bytes.argtypes = [I32, I64]
+    for name in ("jb_eigh_f32", "jb_eigh_f64", "jb_eigh_c64", "jb_eigh_c128"):
         getattr(l, name).restype = ctypes.c_int
         getattr(l, name).argtypes = [P, P, P, P, P, I64, I32, F64, I32, P, SZ, P]
     l.jb_qr_workspace_bytes.restype = SZ

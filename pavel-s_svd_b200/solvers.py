@@ -38,7 +38,7 @@ REFERENCE_ALGORITHMS = (
     'polar_halley', 'polar_polynomial', 'randomized', 'subspace', 'block_krylov', 'lanczos',
 )  # svdbench/standalone/solvers.py:7-11
 ALGORITHMS = ('jacobi', 'block_jacobi', 'gram_jacobi', 'qr', 'tsqr', 'randomized', 'subspace', 'block_krylov')
-COMPLEX_ALGORITHMS = ('jacobi', 'qr', 'tsqr', 'randomized', 'subspace', 'block_krylov')
+COMPLEX_ALGORITHMS = ('jacobi', 'gram_jacobi', 'qr', 'tsqr', 'randomized', 'subspace', 'block_krylov')
 PRECISIONS = ('mixed', 'fp32')
 ORDERINGS = ('block', 'round_robin')
 
@@ -239,17 +239,17 @@ def _gram_svd(a, full_matrices, values_only, return_info, rank, opts):
             raise ValueError('input contains NaN or infinity')
         wide = m < n
         if wide:
-            x = x.transpose(1, 2)
+            x = x.mH
         amax = x.abs().amax((-2, -1), keepdim=True)
         e = torch.where(amax > 0, torch.frexp(amax)[1], torch.zeros_like(amax, dtype=torch.int32))
         scale = torch.ldexp(torch.ones_like(amax), e)
         xs = x / scale
-        g = xs.transpose(1, 2) @ xs
-        g = (g + g.transpose(1, 2)) / 2
+        g = xs.mH @ xs
+        g = (g + g.mH) / 2
         w, v, it = jacobi_eigh(g, max_sweeps=opts.get('max_sweeps', 60))
         w, v = w.flip(-1), v.flip(-1)
         nt = xs.shape[-1]
-        cut = torch.finfo(a.dtype).eps * nt * w[:, :1].clamp_min(0)
+        cut = torch.finfo(w.dtype).eps * nt * w[:, :1].clamp_min(0)
         keep = w > cut
         sv = torch.where(keep, w.clamp_min(0).sqrt(), torch.zeros_like(w))
         u = (xs @ v) / torch.where(keep, sv, torch.ones_like(sv))[:, None, :]
@@ -268,8 +268,9 @@ def _gram_svd(a, full_matrices, values_only, return_info, rank, opts):
             u, sv, v = u[:, :, :rank], sv[:, :rank], v[:, :, :rank]
         if not all(bool(torch.isfinite(t).all()) for t in (u, sv, v)):
             raise RuntimeError('standalone solver produced nonfinite output')
-        result = (None if values_only else u.reshape(*shape, *u.shape[-2:]), sv.reshape(*shape, sv.shape[-1]),
-                  None if values_only else v.transpose(1, 2).reshape(*shape, v.shape[-1], v.shape[-2]))
+        result = (None if values_only else u.resolve_conj().reshape(*shape, *u.shape[-2:]),
+                  sv.reshape(*shape, sv.shape[-1]),
+                  None if values_only else v.mH.resolve_conj().reshape(*shape, v.shape[-1], v.shape[-2]))
     stats = {'algorithm': 'gram_jacobi', 'vendor_factorizations': 0, 'converged': True, 'eigen_sweeps': it,
              'gram_discarded_values': int((~keep).sum()),
              'implementation': 'B200 sm_100a two-sided Jacobi (jacobi_eigh) on the Gram'}

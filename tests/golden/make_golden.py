@@ -90,6 +90,10 @@ def eigh_cases(make_matrix):
     x = rng.standard_normal((2, 12, 12))
     out.append(("indefinite_12", np.ascontiguousarray(x + np.swapaxes(x, -1, -2))))
     out.append(("diagonal_6", np.diag([3.0, -1.0, 2.0, 0.0, 5.0, 1.0])[None].copy()))
+    for dt in ("complex64", "complex128"):     # Hermitian Grams (gram_jacobi on complex input)
+        a = make_matrix(dict(m=20, n=9, batch=2, dtype=dt, family="gaussian"))
+        g = np.conj(np.swapaxes(a, -1, -2)) @ a
+        out.append((f"gram_gauss_{dt}_9", np.ascontiguousarray((g + np.conj(np.swapaxes(g, -1, -2))) / 2)))
     return out
 
 
@@ -142,6 +146,10 @@ def method_cases(make_matrix):
         om = (rng.standard_normal((2, 10, 6)) + 1j * rng.standard_normal((2, 10, 6))).astype(dt)
         out.append((f"subspace_{dt}", a, "subspace", {"rank": 3, "oversample": 3, "iterations": 2,
                                                       "initial_basis": om}))
+        out.append((f"gram_{dt}", make_matrix(dict(m=15, n=8, batch=2, dtype=dt, family="gaussian")), "gram_jacobi",
+                    {}))
+        out.append((f"gram_wide_{dt}", make_matrix(dict(m=6, n=11, batch=2, dtype=dt, family="gaussian")),
+                    "gram_jacobi", {}))
     return out
 
 
@@ -245,9 +253,10 @@ def main():
         w, v, sw = P.jacobi_eigh(torch.from_numpy(h.copy()))
         blob[f"eigh_{name}/h"] = h
         blob[f"eigh_{name}/w"] = w.numpy()
-        blob[f"eigh_{name}/v"] = v.numpy()
+        blob[f"eigh_{name}/v"] = v.resolve_conj().numpy()
         blob[f"eigh_{name}/sweeps"] = np.array(sw)
-        blob[f"eigh_{name}/truth"] = np.stack([np.linalg.eigvalsh(x.astype(np.float64)) for x in h])
+        blob[f"eigh_{name}/truth"] = np.stack([np.linalg.eigvalsh(x.astype(np.complex128 if np.iscomplexobj(x)
+                                                                           else np.float64)) for x in h])
         enames.append(name)
         print(f"eigh {name:22s} {str(h.shape):14s} {h.dtype}  sweeps={sw}")
     blob["_eigh_names"] = np.array(enames)

@@ -1,5 +1,5 @@
-"""jacobi_eigh on the GPU (jb_eigh_f32/_f64) against the reference's own
-outputs (golden fixtures) and FP64 LAPACK.
+"""jacobi_eigh on the GPU (jb_eigh_f32/_f64, _c64/_c128 for Hermitian input)
+against the reference's own outputs (golden fixtures) and FP64 LAPACK.
 
 Bounds: eigenvalues within 10 n eps(dtype) max|w| of FP64 truth (the
 reference's absolute criterion delivers eps * lambda_max accuracy); columns of
@@ -24,13 +24,14 @@ def E():
 def _check(h, w, v, truth):
     n = h.shape[-1]
     e = np.finfo(h.dtype).eps
+    wide = np.complex128 if np.iscomplexobj(h) else np.float64
     w = w.cpu().numpy().astype(np.float64)
-    v = v.cpu().numpy().astype(np.float64)
+    v = v.resolve_conj().cpu().numpy().astype(wide)
     scale = np.abs(truth).max(axis=-1, keepdims=True)
     assert float((np.abs(w - truth) / scale).max()) <= 10 * n * e
     eye = np.eye(n)
-    assert float(np.abs(np.swapaxes(v, -1, -2) @ v - eye).max()) <= 100 * n * e
-    res = np.abs(h.astype(np.float64) @ v - v * w[:, None, :]).max(axis=(-2, -1)) / scale[:, 0]
+    assert float(np.abs(np.conj(np.swapaxes(v, -1, -2)) @ v - eye).max()) <= 100 * n * e
+    res = np.abs(h.astype(wide) @ v - v * w[:, None, :]).max(axis=(-2, -1)) / scale[:, 0]
     assert float(res.max()) <= 100 * n * e
 
 
@@ -38,20 +39,23 @@ def test_eigh_matches_reference_golden(E, golden_eigh):
     for name, g in golden_eigh.items():
         h = g["h"]
         w, v, sw = E.jacobi_eigh(torch.from_numpy(h).cuda())
-        assert w.dtype == torch.from_numpy(h).dtype
+        assert w.dtype == torch.from_numpy(h).real.dtype and v.dtype == torch.from_numpy(h).dtype
         _check(h, w, v, g["truth"])
         assert abs(sw - int(g["sweeps"])) <= 2, name
 
 
 @pytest.mark.parametrize("n,batch,dtype", [(64, 5, torch.float32), (127, 2, torch.float64), (200, 2, torch.float32),
-                                           (1, 3, torch.float64), (2, 4, torch.float32)])
+                                           (1, 3, torch.float64), (2, 4, torch.float32), (48, 3, torch.complex64),
+                                           (101, 2, torch.complex128), (130, 2, torch.complex128)])
 def test_eigh_sizes(E, n, batch, dtype):
-    """Even, odd (padded) and large sizes; V in global memory above n = 118."""
+    """Even, odd (padded) and large sizes; V (and G for the largest) in
+    global memory above the shared-memory limit; Hermitian input."""
     g = torch.Generator().manual_seed(n)
-    x = torch.randn(batch, n, n, generator=g, dtype=torch.float64)
-    h = (x + x.transpose(1, 2)).to(dtype)
+    cdt = torch.complex128 if dtype.is_complex else torch.float64
+    x = torch.randn(batch, n, n, generator=g, dtype=cdt)
+    h = (x + x.mH).to(dtype)
     w, v, sw = E.jacobi_eigh(h.cuda())
-    truth = np.linalg.eigvalsh(h.double().numpy())
+    truth = np.linalg.eigvalsh(h.to(cdt).numpy())
     _check(h.numpy(), w, v, truth)
     assert sw >= 1
 

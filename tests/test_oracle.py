@@ -163,7 +163,9 @@ def test_eigh_oracle_matches_reference(golden_eigh):
                 if gap <= 1e-3 * scale:
                     continue
                 x, y = v[b][:, j], vr[b][:, j]
-                assert min(np.abs(x - y).max(), np.abs(x + y).max()) <= 1e3 * np.finfo(h.dtype).eps, name
+                ph = np.vdot(x, y)                        # a unit phase (a sign for real input)
+                ph = ph / abs(ph) if abs(ph) > 0 else 1.0
+                assert np.abs(x * ph - y).max() <= 1e3 * np.finfo(h.dtype).eps, name
         # and against FP64 truth
         truth = g["truth"]
         assert float(np.abs(w - truth).max()) <= 10 * np.finfo(h.dtype).eps * scale * h.shape[-1], name
@@ -199,6 +201,8 @@ def test_qr_methods_oracle_matches_reference():
     185-220, 245-248), restated in NumPy, against the reference's U, s, Vh on
     the same inputs and start bases."""
     for name, g in golden_methods().items():
+        if g["alg"] == "gram_jacobi":      # restated through jacobi_eigh (test_eigh_oracle_matches_reference)
+            continue
         kw = dict(g["kw"])
         if "initial_basis" in g:
             kw["initial_basis"] = g["initial_basis"]
