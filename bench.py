@@ -702,6 +702,20 @@ def run_extensions(args):
     line("jacobi_eigh", g, ms, {"max_rel_eig_err_vs_lapack": float((np.abs(w.cpu().numpy() - wr) /
                                                                      np.abs(wr).max(-1, keepdims=True)).max())},
          cpu, "8 matrices, NumPy oracle jacobi_eigh", {"shape": [1024, 32, 32]}, "float64")
+    # block_jacobi in rounds (float64 and complex input): one batched Jacobi
+    # call per round of the block tournament
+    for dt in (np.float64, np.complex64):
+        a = rng.standard_normal((256, 96, 64))
+        if dt == np.complex64:
+            a = a + 1j * rng.standard_normal((256, 96, 64))
+        a = a.astype(dt)
+        t = torch.from_numpy(a).cuda()
+        ms = _time_gpu(lambda: pkg.svd(t, "block_jacobi", block_size=8), args.steps, args.warmup)
+        _, s, _ = pkg.svd(t, "block_jacobi", block_size=8)
+        cpu = _time_cpu(lambda: O.svd(a[:2], "block_jacobi", block_size=8), 2)
+        line(f"svd 'block_jacobi' rounds {np.dtype(dt).name}", a, ms,
+             {"max_rel_sigma_err_vs_lapack": sig_err(a, s.cpu().numpy())}, cpu, "2 matrices, NumPy oracle",
+             {"shape": [256, 96, 64], "block_size": 8}, np.dtype(dt).name)
     # the laboratory's Jacobi (one matrix, no trace: a sweep per launch)
     a = rng.standard_normal((1, 128, 64))
     t = torch.from_numpy(a[0]).cuda()

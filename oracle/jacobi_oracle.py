@@ -17,8 +17,10 @@ exactly like the PyTorch original:
   householder_vec / qr   svdbench/standalone/primitives.py:41-89
   tsqr                   svdbench/standalone/solvers.py:71-96
   partial                svdbench/standalone/solvers.py:185-220 (given initial_basis)
-  svd                    svdbench/standalone/solvers.py:264-310 ('jacobi', 'qr', 'tsqr',
-                         'randomized', 'subspace', 'block_krylov')
+  finish_columns         svdbench/standalone/solvers.py:18-21
+  block_jacobi           svdbench/standalone/solvers.py:30-68
+  svd                    svdbench/standalone/solvers.py:264-310 ('jacobi', 'block_jacobi', 'qr',
+                         'tsqr', 'randomized', 'subspace', 'block_krylov')
   raw                    svdbench/standalone/solvers.py:224-248
   reference / validate   svdbench/metrics.py:6-66 (FP64 LAPACK gesvd truth)
 
@@ -291,10 +293,72 @@ def partial(a, stats, opts, method):
 PARTIAL = ("randomized", "subspace", "block_krylov")
 
 
+def finish_columns(w, s):
+    """U = W / sigma above eps * max(m, n) * sigma_1, the rest completed
+    (solvers.py:18-21)."""
+    keep = s > s.dtype.type(eps(w.dtype)) * max(w.shape[-2:]) * s[:, :1]
+    u = w / np.where(keep, s, s.dtype.type(1))[:, None, :]
+    return complete_null_columns(u, keep), np.where(keep, s, s.dtype.type(0))
+
+
+def block_jacobi(a, stats, opts):
+    """Block one-sided Jacobi (solvers.py:30-68): column groups of
+    block_size in a round-robin tournament, each pair orthogonalised by the
+    Jacobi SVD of its columns, until the largest correlation of live columns
+    is at most tol (40 eps by default); pairs applied one after the other
+    as in the reference."""
+    b, m, n = a.shape
+    width = opts.get("block_size", 4)                              # :32
+    if width < 1:
+        raise ValueError("block_size must be positive")
+    groups = [list(range(j, min(j + width, n))) for j in range(0, n, width)]   # :35
+    if len(groups) == 1:                                           # :36-37
+        return raw(a, opts, stats, "jacobi")
+    if len(groups) % 2:                                            # :38-39
+        groups.append([])
+    w = a.copy()
+    v = np.broadcast_to(np.eye(n, dtype=a.dtype), (b, n, n)).copy()
+    e = eps(a.dtype)
+    tol = opts.get("tol") or 40 * e                               # :41
+    rdt = _real(a.dtype)
+    for sweep in range(opts.get("max_sweeps", 30)):               # :42
+        for pairs in round_robin(len(groups)):                     # :43-44
+            for i, j in pairs:
+                cols = groups[i] + groups[j]
+                if len(cols) < 2:                                  # :46-47
+                    continue
+                _, _, vv, sweeps = jacobi_svd(w[:, :, cols], tol=opts.get("tol"),
+                                              max_sweeps=opts.get("max_sweeps", 60))   # :48, :24-27
+                stats["jacobi_sweeps"] = max(stats.get("jacobi_sweeps", 0), sweeps)
+                w[:, :, cols] = w[:, :, cols] @ vv                 # :49
+                v[:, :, cols] = v[:, :, cols] @ vv                 # :50
+        g = np.conj(np.swapaxes(w, -1, -2)) @ w                    # :51
+        d = np.clip(np.real(np.diagonal(g, axis1=-2, axis2=-1)), 0, None)   # :52
+        denom = np.sqrt(d)[:, :, None] * np.sqrt(d)[:, None, :]     # :53
+        g = g.copy()
+        idx = np.arange(n)
+        g[:, idx, idx] = 0                                         # :54
+        live = d > (e * max(m, n)) ** 2 * d.max(-1, keepdims=True)  # :55
+        corr = np.where(live[:, :, None] & live[:, None, :],
+                        np.abs(g) / np.maximum(denom, tiny(rdt)), 0)   # :56
+        if corr.max() <= tol:                                      # :57-58
+            break
+    else:
+        raise RuntimeError("block Jacobi did not converge")       # :59-60
+    s = np.sqrt((np.abs(w) ** 2).sum(1, dtype=rdt))               # :61
+    order = np.argsort(-s, axis=1, kind="stable")                 # :62
+    s = np.take_along_axis(s, order, 1)
+    w = np.take_along_axis(w, order[:, None, :], 2)
+    v = np.take_along_axis(v, order[:, None, :], 2)
+    u, s = finish_columns(w, s)                                    # :66
+    stats["block_sweeps"] = sweep + 1                             # :67
+    return u, s, v
+
+
 def raw(x, opts, stats, method="jacobi"):
     """Wide inputs are solved through their adjoint, except by the projected
-    solvers (solvers.py:224-230); then 'jacobi' (:229-230), 'qr' / 'tsqr'
-    (:245-248) or the projected solvers (:253-254)."""
+    solvers (solvers.py:224-230); then 'jacobi' (:229-230), 'block_jacobi'
+    (:231-232), 'qr' / 'tsqr' (:245-248) or the projected solvers (:253-254)."""
     if x.shape[-2] < x.shape[-1] and method not in PARTIAL:
         u, s, v = raw(np.conj(np.swapaxes(x, -1, -2)), opts, stats, method)
         return v, s, u
@@ -304,6 +368,8 @@ def raw(x, opts, stats, method="jacobi"):
         return q @ u, s, v
     if method in PARTIAL:
         return partial(x, stats, opts, method)
+    if method == "block_jacobi":
+        return block_jacobi(x, stats, opts)
     u, s, v, sweeps = jacobi_svd(x, tol=opts.get("tol"), max_sweeps=opts.get("max_sweeps", 60))
     stats["jacobi_sweeps"] = max(stats.get("jacobi_sweeps", 0), sweeps)   # solvers.py:24-27
     return u, s, v
@@ -313,7 +379,7 @@ def svd(a, algorithm="jacobi", *, full_matrices=False, values_only=False, return
     """NumPy restatement of the public entry (solvers.py:264-310) for the
     Jacobi-based algorithms."""
     a = np.asarray(a)
-    if algorithm not in ("jacobi", "qr", "tsqr") + PARTIAL:
+    if algorithm not in ("jacobi", "block_jacobi", "qr", "tsqr") + PARTIAL:
         raise ValueError("the oracle restates the Jacobi-based algorithms only")
     if a.ndim < 2 or min(a.shape[-2:]) < 1:
         raise ValueError("nonempty matrix dimensions required")

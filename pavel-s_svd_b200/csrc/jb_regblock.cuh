@@ -135,6 +135,47 @@ __device__ __forceinline__ int rot_params<double>(double app, double aqq, double
     return 1 | (apq2 > big2 * prod ? 2 : 0) | (apq2 > ex2 * prod ? 4 : 0);
 }
 
+// FP64 at the reference's precision (the float64 solve, tol 10 eps): the same
+// rotation with t and c accurate to FP64 rounding, so that one rotation
+// leaves the pair orthogonal to rounding level as the reference's FP64
+// arithmetic does (an FP32 angle leaves a ratio ~1e-7 of the one it removed,
+// near 10 eps in the last rotating sweep, and costs a sweep).  With the
+// exponent-scaled dd = |d| scl, aa = 2|apq| scl (max of the two in [1, 2)),
+// t is the positive root of g(t) = aa t^2 + 2 dd t - aa: the FP32 estimate,
+// then two Newton steps t -= g(t) / g'(t) with g'/2 = aa t + dd >= 1/2
+// inverted once in FP32 (each step multiplies the error by ~1e-7; g(t) is
+// evaluated to rounding of its largest term, ~aa, so small angles keep
+// their relative accuracy); c = 1/sqrt(1 + t^2) from the FP32 estimate and
+// two Newton steps.
+__device__ __forceinline__ int rot_params_exact(double app, double aqq, double apq, double tol2, double big2,
+                                                double ex2, double floor_, double &c, double &s) {
+    c = 1.0;
+    s = 0.0;
+    const double apq2 = apq * apq;
+    const double prod = app * aqq;
+    const bool active = apq2 > tol2 * prod && fmin(app, aqq) > floor_;
+    if (!active) return 0;
+    const double d = aqq - app, a2 = 2.0 * fabs(apq);
+    const int ex = (__double2hiint(fmax(fabs(d), a2)) >> 20) & 0x7ff;
+    const double scl = __hiloint2double((2046 - ex) << 20, 0);
+    const double dd = fabs(d) * scl, aa = a2 * scl;
+    const float df = (float)dd, af = (float)aa;
+    const float hf = fmaf(df, df, af * af);
+    double t = (double)__fdividef(af, df + hf * rsqrtf(hf));
+    const double r = 0.5 * (double)__frcp_rn((float)fma(aa, t, dd));
+#pragma unroll
+    for (int k = 0; k < 2; ++k) t -= fma(aa * t, t, fma(2.0 * dd, t, -aa)) * r;
+    if (d < 0.0) t = -t;
+    const double x = fma(t, t, 1.0), hx = -0.5 * x;
+    double c0 = (double)rsqrtf((float)x);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) c0 *= fma(hx, c0 * c0, 1.5);
+    c = c0;
+    s = t * c;
+    if (apq < 0.0) s = -s;
+    return 1 | (apq2 > big2 * prod ? 2 : 0) | (apq2 > ex2 * prod ? 4 : 0);
+}
+
 // Packed FP32 (two rows per instruction): a += x * y for (a0, a1), and the
 // rotation pair (x, y) <- (c x - s y, s x + c y) for two rows at once.
 __device__ __forceinline__ void fma2(float &a0, float &a1, float x0, float x1, float y0, float y1) {
@@ -210,7 +251,9 @@ __device__ __forceinline__ void step(Tile<T, B, R, RV> &t, T tol2, T big2, T ex2
     reduce_scatter<T, B>(pb, lane);
     reduce_scatter<T, B>(pc, lane);
     T c, s;
-    const int f = rot_params<T>(pa[0], pb[0], pc[0], tol2, big2, ex2, floor_, c, s);
+    int f;
+    if constexpr (sizeof(T) == 8) f = rot_params_exact(pa[0], pb[0], pc[0], tol2, big2, ex2, floor_, c, s);
+    else f = rot_params<T>(pa[0], pb[0], pc[0], tol2, big2, ex2, floor_, c, s);
     fl |= f;
     if (!rotate || !__any_sync(FULL, f != 0)) return;
 #pragma unroll

@@ -12,9 +12,9 @@ to raise the reference's errors.
 
 Differences, by design:
   * CUDA tensors only.  Other devices, the reference families not built here
-    (bidiag_*, gram_dc, polar_*, lanczos) and complex input to any family but
-    'jacobi' raise ``Unsupported`` (svdbench/algorithms.py:12-13) instead of
-    running elsewhere: there is no CPU fallback.
+    (bidiag_*, gram_dc, polar_*, lanczos) raise ``Unsupported``
+    (svdbench/algorithms.py:12-13) instead of running elsewhere: there is no
+    CPU fallback.
   * ``precision`` option for float32 input: ``'mixed'`` (default) runs FP32
     sweeps and then FP64 sweeps from the Householder re-orthonormalised V, so
     singular values meet a 1e-5 relative bound against FP64 LAPACK even where
@@ -38,7 +38,8 @@ REFERENCE_ALGORITHMS = (
     'polar_halley', 'polar_polynomial', 'randomized', 'subspace', 'block_krylov', 'lanczos',
 )  # svdbench/standalone/solvers.py:7-11
 ALGORITHMS = ('jacobi', 'block_jacobi', 'gram_jacobi', 'qr', 'tsqr', 'randomized', 'subspace', 'block_krylov')
-COMPLEX_ALGORITHMS = ('jacobi', 'gram_jacobi', 'qr', 'tsqr', 'randomized', 'subspace', 'block_krylov')
+COMPLEX_ALGORITHMS = ('jacobi', 'block_jacobi', 'gram_jacobi', 'qr', 'tsqr', 'randomized', 'subspace',
+                      'block_krylov')
 PRECISIONS = ('mixed', 'fp32')
 ORDERINGS = ('block', 'round_robin')
 
@@ -145,7 +146,7 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
     solver on each matrix of the batch (see _block_svd); 'gram_jacobi' the
     GPU jacobi_eigh of the Gram (_gram_svd); 'qr', 'tsqr', 'randomized',
     'subspace' and 'block_krylov' the GPU Householder QR around the batched
-    Jacobi (_qr_family_svd).
+    Jacobi (_composed_svd).
     Input is never overwritten."""
     rank, precision = _validate(a, algorithm, full_matrices, opts)
     if a.is_complex() and algorithm == 'jacobi':
@@ -155,7 +156,7 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
     if algorithm == 'gram_jacobi':
         return _gram_svd(a, full_matrices, values_only, return_info, rank, opts)
     if algorithm in ('qr', 'tsqr', 'randomized', 'subspace', 'block_krylov'):
-        return _qr_family_svd(a, algorithm, full_matrices, values_only, return_info, rank, opts)
+        return _composed_svd(a, algorithm, full_matrices, values_only, return_info, rank, opts)
     max_sweeps = opts.get('max_sweeps', 60)
     tol = opts.get('tol')
     shape = a.shape[:-2]
@@ -351,16 +352,20 @@ def _complete_basis(q, size):
     return _complete_null_columns(torch.cat([q, z], -1), keep)
 
 
-def _qr_family_svd(a, algorithm, full_matrices, values_only, return_info, rank, opts):
-    """'qr', 'tsqr' (solvers.py:71-96, 245-248) and the projected solvers
-    'randomized', 'subspace', 'block_krylov' (:185-220) through the public
-    entry (:264-310): the batch scaled by a power of two (exact) before any
-    sums of squares, the method (qr.raw: GPU Householder QRs, library GEMMs in
-    the input dtype, the batched Jacobi of the small factor), then sigma
-    rescaled, full bases completed or the rank truncated, the output checked.
-    Options: those of the reference's method (tile_rows, rank, oversample,
-    iterations, seed, initial_basis) and of the Jacobi solve (tol,
-    max_sweeps, precision, ordering)."""
+def _composed_svd(a, algorithm, full_matrices, values_only, return_info, rank, opts):
+    """The methods composed on the host from this library's kernels, through
+    the public entry (solvers.py:264-310): 'qr', 'tsqr' (:71-96, 245-248) and
+    the projected 'randomized', 'subspace', 'block_krylov' (:185-220) by
+    qr.raw (GPU Householder QRs, the batched Jacobi of the small factor);
+    'block_jacobi' in rounds (:30-68) by block_rounds.raw (one batched Jacobi
+    call per round).  The batch is scaled by a power of two (exact) before
+    any sums of squares; after the method sigma is rescaled, full bases
+    completed or the rank truncated, the output checked.  Products between
+    the kernels' results are library GEMMs in the input dtype.  Options:
+    those of the reference's method (tile_rows, rank, oversample, iterations,
+    seed, initial_basis; block_size, tol, max_sweeps) and of the Jacobi solve
+    (tol, max_sweeps, precision, ordering)."""
+    from . import block_rounds as BR
     from . import qr as Q
     m, n = a.shape[-2:]
     shape = a.shape[:-2]
@@ -379,7 +384,11 @@ def _qr_family_svd(a, algorithm, full_matrices, values_only, return_info, rank, 
         amax = x.abs().amax((-2, -1), keepdim=True)
         e = torch.where(amax > 0, torch.frexp(amax)[1], torch.zeros_like(amax, dtype=torch.int32))
         scale = torch.ldexp(torch.ones_like(amax), e)
-        u, sv, v = Q.raw((x / scale).contiguous(), algorithm, stats, opts, jacobi)
+        y = (x / scale).contiguous()
+        if algorithm == 'block_jacobi':
+            u, sv, v = BR.raw(y, stats, opts, jacobi, _complete_null_columns)
+        else:
+            u, sv, v = Q.raw(y, algorithm, stats, opts, jacobi)
         sv = sv * scale[:, 0, :]
         if full_matrices:
             u, v = _complete_basis(u, m), _complete_basis(v, n)
@@ -390,26 +399,33 @@ def _qr_family_svd(a, algorithm, full_matrices, values_only, return_info, rank, 
         result = (None if values_only else u.resolve_conj().reshape(*shape, *u.shape[-2:]),
                   sv.reshape(*shape, sv.shape[-1]),
                   None if values_only else v.mH.resolve_conj().reshape(*shape, v.shape[-1], v.shape[-2]))
-    stats['implementation'] = 'B200 sm_100a Householder QR + batched one-sided Jacobi'
+    stats['implementation'] = ('B200 sm_100a batched one-sided Jacobi per block round' if algorithm == 'block_jacobi'
+                               else 'B200 sm_100a Householder QR + batched one-sided Jacobi')
     return (*result, stats) if return_info else result
 
 
 _block_plans = {}
 
 
+TENSOR_CORE_MIN = 65   # float32 block_jacobi on the tensor cores from this min(m, n) up
+
+
 def _block_svd(a, full_matrices, values_only, return_info, rank, opts):
-    """block_jacobi (solvers.py:30-68) on the tensor cores, one matrix at a
-    time (blocked.BlockJacobi).  Like the reference: block_size defaults to 4
-    and must be positive (:32-34); a matrix whose tall view has a single block
-    is solved by the plain Jacobi (:36-37); tol defaults to 40 eps (:41);
-    max_sweeps (default 30) bounds the block sweeps and exhausting it raises
-    RuntimeError('block Jacobi did not converge') (:59-60); wide matrices are
-    solved transposed (:225-227).  The block width only shapes the schedule:
-    widths the tensor-core kernels do not take (not a multiple of 8 in
-    [8, 64]) run with width 32, reported as info['block_size_used'].  float32
-    only (the products are 3xBF16 / 6xBF16); float64 input and
-    full_matrices raise Unsupported."""
-    from .blocked import BlockJacobi
+    """block_jacobi (solvers.py:30-68).  Like the reference: block_size
+    defaults to 4 and must be positive (:32-34); a matrix whose tall view has
+    a single block is solved by the plain Jacobi (:36-37); tol defaults to 40
+    eps (:41); max_sweeps (default 30) bounds the block sweeps and exhausting
+    it raises RuntimeError('block Jacobi did not converge') (:59-60); wide
+    matrices are solved transposed (:225-227).
+
+    float32 matrices with min(m, n) >= TENSOR_CORE_MIN run the tensor-core
+    solver, one matrix at a time (blocked.BlockJacobi, products on 3xBF16 /
+    6xBF16 splits, FP64 block eigen-solves); there the block width only
+    shapes the schedule: widths the tensor-core kernels do not take (not a
+    multiple of 8 in [8, 64]) run with width 32, reported as
+    info['block_size_used'].  float64, complex and smaller float32 batches
+    run the reference's rounds with the given block_size, each round's pair
+    subproblems one batched Jacobi call (block_rounds, via _composed_svd)."""
     width = opts.get('block_size', 4)
     if width < 1:
         raise ValueError('block_size must be positive')
@@ -418,10 +434,9 @@ def _block_svd(a, full_matrices, values_only, return_info, rank, opts):
         rest = {k: v for k, v in opts.items() if k != 'block_size'}
         return svd(a, 'jacobi', full_matrices=full_matrices, values_only=values_only, return_info=return_info,
                    **rest)
-    if a.dtype != torch.float32:
-        raise Unsupported('block_jacobi runs float32 on the tensor cores; use jacobi for float64')
-    if full_matrices:
-        raise Unsupported('block_jacobi does not complete full bases on the B200 solver; use jacobi')
+    if a.dtype != torch.float32 or min(m, n) < TENSOR_CORE_MIN:
+        return _composed_svd(a, 'block_jacobi', full_matrices, values_only, return_info, rank, opts)
+    from .blocked import BlockJacobi
     used = width if (width % 8 == 0 and 8 <= width <= 64) else 32
     tol = opts.get('tol') or 40 * 1.1920928955078125e-07
     max_sweeps = opts.get('max_sweeps', 30)
@@ -443,8 +458,11 @@ def _block_svd(a, full_matrices, values_only, return_info, rank, opts):
             us.append(u[:, :rank]); ss.append(s_[:rank]); vs.append(vh[:rank])
             sweeps = max(sweeps, info['block_sweeps'])
         s = torch.stack(ss).reshape(*shape, rank)
-        u = None if values_only else torch.stack(us).reshape(*shape, m, rank).contiguous()
-        vh = None if values_only else torch.stack(vs).reshape(*shape, rank, n).contiguous()
+        uu, vv = torch.stack(us), torch.stack(vs).mT
+        if full_matrices:
+            uu, vv = _complete_basis(uu, m), _complete_basis(vv, n)
+        u = None if values_only else uu.reshape(*shape, m, uu.shape[-1]).contiguous()
+        vh = None if values_only else vv.mT.reshape(*shape, vv.shape[-1], n).contiguous()
         if not all(bool(torch.isfinite(t).all()) for t in (s,) + (() if values_only else (u, vh))):
             raise RuntimeError('standalone solver produced nonfinite output')
     stats = {'algorithm': 'block_jacobi', 'vendor_factorizations': 0, 'converged': True, 'block_sweeps': sweeps,

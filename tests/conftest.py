@@ -62,6 +62,8 @@ def golden_methods():
         c["kw"] = eval(str(z[f"meth_{n}/kw"]))
         if f"meth_{n}/initial_basis" in z.files:
             c["initial_basis"] = z[f"meth_{n}/initial_basis"]
+        if f"meth_{n}/block_sweeps" in z.files:
+            c["block_sweeps"] = int(z[f"meth_{n}/block_sweeps"])
         out[str(n)] = c
     return out
 

@@ -150,6 +150,21 @@ def method_cases(make_matrix):
                     {}))
         out.append((f"gram_wide_{dt}", make_matrix(dict(m=6, n=11, batch=2, dtype=dt, family="gaussian")),
                     "gram_jacobi", {}))
+    # block_jacobi (solvers.py:30-68): ragged last group, an odd group count
+    # (padded with an empty group), wide input, a rank-deficient matrix
+    # (cut columns completed), both real and both complex dtypes
+    out.append(("block_float64", make_matrix(dict(m=20, n=11, batch=2, dtype="float64", family="gaussian")),
+                "block_jacobi", {"block_size": 3}))
+    out.append(("block_wide_float64", make_matrix(dict(m=9, n=22, batch=2, dtype="float64", family="gaussian")),
+                "block_jacobi", {}))
+    out.append(("block_float32", make_matrix(dict(m=24, n=10, batch=2, dtype="float32", family="gaussian")),
+                "block_jacobi", {}))
+    out.append(("block_lowrank_float64", make_matrix(dict(m=18, n=8, dtype="float64", family="low_rank", rank=3,
+                                                          tail=0)), "block_jacobi", {"block_size": 2}))
+    out.append(("block_complex64", make_matrix(dict(m=15, n=9, batch=2, dtype="complex64", family="gaussian")),
+                "block_jacobi", {}))
+    out.append(("block_wide_complex128", make_matrix(dict(m=8, n=14, batch=2, dtype="complex128",
+                                                          family="gaussian")), "block_jacobi", {"block_size": 3}))
     return out
 
 
@@ -283,6 +298,8 @@ def main():
         blob[f"meth_{name}/truth"] = np.stack([scipy.linalg.svd(x, compute_uv=False, lapack_driver="gesvd")
                                                for x in flat])
         blob[f"meth_{name}/alg"] = np.array(alg)
+        if "block_sweeps" in info:
+            blob[f"meth_{name}/block_sweeps"] = np.array(info["block_sweeps"])
         blob[f"meth_{name}/kw"] = np.array(repr({k: v for k, v in kw.items() if k != "initial_basis"}))
         if "initial_basis" in kw:
             blob[f"meth_{name}/initial_basis"] = np.ascontiguousarray(kw["initial_basis"])

@@ -116,5 +116,80 @@ def test_block_jacobi_drop_in():
     assert info['algorithm'] == 'jacobi' and s.shape == (3, 24)
     with pytest.raises(ValueError):
         pkg.svd(x, 'block_jacobi', block_size=0)
-    with pytest.raises(pkg.Unsupported):
-        pkg.svd(x.double(), 'block_jacobi', block_size=32)
+    # full bases on the tensor-core path: the reference's null completion
+    u, s, vh = pkg.svd(x, 'block_jacobi', block_size=32, full_matrices=True)
+    assert u.shape == (256, 256) and vh.shape == (384, 384)
+    for q in (u.double(), vh.double()):
+        assert float((q.mT @ q - torch.eye(q.shape[0], dtype=torch.float64, device="cuda")).abs().max()) <= 1e-4
+
+
+def _lapack_check(a, u, s, vh, tol):
+    a64 = a.astype(np.complex128 if np.iscomplexobj(a) else np.float64).reshape(-1, *a.shape[-2:])
+    truth = np.stack([np.linalg.svd(x, compute_uv=False) for x in a64])
+    k = min(a.shape[-2:])
+    assert float(np.abs(s.reshape(-1, s.shape[-1])[:, :k] - truth).max() / truth.max()) <= tol
+    u = u.reshape(-1, *u.shape[-2:]).astype(a64.dtype)
+    vh = vh.reshape(-1, *vh.shape[-2:]).astype(a64.dtype)
+    rec = (u[..., :k] * s.reshape(-1, s.shape[-1])[:, None, :k]) @ vh[..., :k, :]
+    assert float(np.abs(rec - a64).max() / np.abs(a64).max()) <= 10 * tol
+    for q, eye in ((np.conj(np.swapaxes(u, -1, -2)) @ u, u.shape[-1]), (vh @ np.conj(np.swapaxes(vh, -1, -2)),
+                                                                        vh.shape[-2])):
+        assert float(np.abs(q - np.eye(eye)).max()) <= 10 * tol
+
+
+def test_block_jacobi_rounds_golden(pkg):
+    """The rounds path against the reference's own block_jacobi runs: block
+    sweeps within one of the reference's (the pair solves are this library's
+    Jacobi, whose rounding differs), sigma and vectors as in the reference."""
+    from conftest import golden_methods, sigma_tol
+    from test_oracle import _cmp_sigma, _cmp_vectors, _cmp_vectors_phase
+    seen = 0
+    for name, g in golden_methods().items():
+        if g["alg"] != "block_jacobi":
+            continue
+        seen += 1
+        a = g["a"]
+        u, s, vh, info = pkg.svd(torch.from_numpy(a).cuda(), "block_jacobi", return_info=True, **g["kw"])
+        assert abs(info["block_sweeps"] - g["block_sweeps"]) <= 1, name
+        assert info["jacobi_sweeps"] >= 1 and "block_size_used" not in info
+        u, s, vh = u.resolve_conj().cpu().numpy(), s.cpu().numpy(), vh.resolve_conj().cpu().numpy()
+        _cmp_sigma(s, g["s"], a.dtype)
+        cmp = _cmp_vectors_phase if np.iscomplexobj(a) else _cmp_vectors
+        cmp(u, g["u"], g["s"], a.dtype, -1)
+        cmp(vh, g["vh"], g["s"], a.dtype, -2)
+        err = float(np.abs(s - g["truth"]).max() / g["truth"].max())
+        assert err <= max(2 * float(np.abs(g["s"] - g["truth"]).max() / g["truth"].max()), 10 * sigma_tol(a.dtype))
+    assert seen >= 6
+
+
+@pytest.mark.parametrize("shape,dtype,bs", [((3, 200, 120), np.float64, 16), ((2, 90, 140), np.complex128, 8),
+                                            ((4, 64, 40), np.complex64, 5), ((8, 48, 33), np.float32, 4)])
+def test_block_jacobi_rounds_against_lapack(pkg, shape, dtype, bs):
+    """Larger batches through the rounds path (float64, complex, float32 below
+    the tensor-core size), tall and wide, ragged groups."""
+    rng = np.random.default_rng(shape[-1])
+    a = rng.standard_normal(shape)
+    if np.issubdtype(dtype, np.complexfloating):
+        a = a + 1j * rng.standard_normal(shape)
+    a = a.astype(dtype)
+    u, s, vh, info = pkg.svd(torch.from_numpy(a).cuda(), "block_jacobi", block_size=bs, return_info=True)
+    assert info["block_sweeps"] >= 2
+    tol = 1e-12 if dtype in (np.float64, np.complex128) else 2e-5
+    _lapack_check(a, u.resolve_conj().cpu().numpy(), s.cpu().numpy(), vh.resolve_conj().cpu().numpy(), tol)
+
+
+def test_block_jacobi_rounds_contract(pkg):
+    """Full bases (wide, complex), values only, a truncated rank, the
+    reference's non-convergence error."""
+    rng = np.random.default_rng(5)
+    a = (rng.standard_normal((2, 12, 30)) + 1j * rng.standard_normal((2, 12, 30))).astype(np.complex128)
+    x = torch.from_numpy(a).cuda()
+    u, s, vh = pkg.svd(x, "block_jacobi", full_matrices=True, block_size=4)
+    assert u.shape == (2, 12, 12) and vh.shape == (2, 30, 30)
+    _lapack_check(a, u.cpu().numpy(), s.cpu().numpy(), vh.cpu().numpy(), 1e-12)
+    u, s2, vh = pkg.svd(x, "block_jacobi", values_only=True, block_size=4)
+    assert u is None and vh is None and torch.allclose(s2, s, rtol=0, atol=1e-12)
+    u, s3, vh = pkg.svd(x.real.contiguous(), "block_jacobi", rank=5, block_size=4)
+    assert u.shape == (2, 12, 5) and s3.shape == (2, 5) and vh.shape == (2, 5, 30)
+    with pytest.raises(RuntimeError, match="block Jacobi did not converge"):
+        pkg.svd(x.real.contiguous(), "block_jacobi", block_size=1, max_sweeps=2)

@@ -67,7 +67,7 @@ def test_complex_sizes_against_lapack(pkg, shape, dtype):
     _contract(a, u.cpu().numpy(), s.cpu().numpy(), vh.cpu().numpy(), 3e-4 if dtype == np.complex64 else 2e-10)
 
 
-def test_complex_errors_and_unsupported(pkg):
+def test_complex_errors(pkg):
     rng = np.random.default_rng(0)
     a = torch.from_numpy(rng.standard_normal((12, 9)) + 1j * rng.standard_normal((12, 9))).to(DEV)
     with pytest.raises(RuntimeError, match="did not converge in 1 sweeps"):
@@ -76,6 +76,5 @@ def test_complex_errors_and_unsupported(pkg):
     b[3, 4] = complex(float("nan"), 0.0)
     with pytest.raises(ValueError, match="NaN or infinity"):
         pkg.svd(b, "jacobi")
-    for alg in ("block_jacobi",):
-        with pytest.raises(pkg.Unsupported):
-            pkg.svd(a, alg)
+    with pytest.raises(RuntimeError, match="block Jacobi did not converge"):
+        pkg.svd(a, "block_jacobi", block_size=1, max_sweeps=2)     # 2-column pairs converge, the blocks not

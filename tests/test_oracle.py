@@ -197,17 +197,20 @@ def test_qr_oracle_matches_reference():
 
 
 def test_qr_methods_oracle_matches_reference():
-    """svd() through 'qr', 'tsqr' and the projected solvers (solvers.py:71-96,
-    185-220, 245-248), restated in NumPy, against the reference's U, s, Vh on
-    the same inputs and start bases."""
+    """svd() through 'qr', 'tsqr', the projected solvers and 'block_jacobi'
+    (solvers.py:30-68, 71-96, 185-220, 245-248), restated in NumPy, against
+    the reference's U, s, Vh (and block sweeps) on the same inputs and start
+    bases."""
     for name, g in golden_methods().items():
         if g["alg"] == "gram_jacobi":      # restated through jacobi_eigh (test_eigh_oracle_matches_reference)
             continue
         kw = dict(g["kw"])
         if "initial_basis" in g:
             kw["initial_basis"] = g["initial_basis"]
-        u, s, vh = O.svd(g["a"], g["alg"], **kw)
+        u, s, vh, info = O.svd(g["a"], g["alg"], return_info=True, **kw)
         dt = g["a"].dtype
+        if "block_sweeps" in g:
+            assert info["block_sweeps"] == g["block_sweeps"], name
         _cmp_sigma(s, g["s"], dt)
         cmp = _cmp_vectors_phase if np.iscomplexobj(g["a"]) else _cmp_vectors
         cmp(u, g["u"], g["s"], dt, -1)
