@@ -78,6 +78,9 @@ def block_jacobi(a, stats, opts, jacobi, complete):
     Raises RuntimeError('block Jacobi did not converge') after max_sweeps
     (default 30) sweeps (solvers.py:59-60)."""
     b, m, n = a.shape
+    if b == 0:
+        stats['block_sweeps'] = 0
+        return a.new_zeros(b, m, n), a.real.new_zeros(b, n), a.new_zeros(b, n, n)
     width = opts.get('block_size', 4)
     dev = a.device
     rounds = schedule(n, width, dev)

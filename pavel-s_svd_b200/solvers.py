@@ -407,7 +407,13 @@ def _composed_svd(a, algorithm, full_matrices, values_only, return_info, rank, o
 _block_plans = {}
 
 
-TENSOR_CORE_MIN = 65   # float32 block_jacobi on the tensor cores from this min(m, n) up
+# float32 block_jacobi runs on the tensor cores (one matrix at a time) when
+# min(m, n) >= TENSOR_CORE_MIN and either max(m, n) > TENSOR_CORE_ROWS (the
+# rounds engine's pair subproblems then leave the register kernels) or the
+# batch holds at most TENSOR_CORE_BATCH matrices.  Measured on B200, block
+# width 32: 64 x 256x128 takes 15 ms in rounds vs 220 ms on the tensor cores,
+# 1 x 256x128 11.3 vs 5.5 ms, 16 x 512x256 302 vs 120 ms.
+TENSOR_CORE_MIN, TENSOR_CORE_ROWS, TENSOR_CORE_BATCH = 65, 256, 2
 
 
 def _block_svd(a, full_matrices, values_only, return_info, rank, opts):
@@ -418,12 +424,12 @@ def _block_svd(a, full_matrices, values_only, return_info, rank, opts):
     it raises RuntimeError('block Jacobi did not converge') (:59-60); wide
     matrices are solved transposed (:225-227).
 
-    float32 matrices with min(m, n) >= TENSOR_CORE_MIN run the tensor-core
+    Large float32 matrices (see TENSOR_CORE_MIN) run the tensor-core
     solver, one matrix at a time (blocked.BlockJacobi, products on 3xBF16 /
     6xBF16 splits, FP64 block eigen-solves); there the block width only
     shapes the schedule: widths the tensor-core kernels do not take (not a
     multiple of 8 in [8, 64]) run with width 32, reported as
-    info['block_size_used'].  float64, complex and smaller float32 batches
+    info['block_size_used'].  float64, complex and the other float32 batches
     run the reference's rounds with the given block_size, each round's pair
     subproblems one batched Jacobi call (block_rounds, via _composed_svd)."""
     width = opts.get('block_size', 4)
@@ -434,7 +440,10 @@ def _block_svd(a, full_matrices, values_only, return_info, rank, opts):
         rest = {k: v for k, v in opts.items() if k != 'block_size'}
         return svd(a, 'jacobi', full_matrices=full_matrices, values_only=values_only, return_info=return_info,
                    **rest)
-    if a.dtype != torch.float32 or min(m, n) < TENSOR_CORE_MIN:
+    batch = a.numel() // (m * n)
+    tensor_cores = (a.dtype == torch.float32 and min(m, n) >= TENSOR_CORE_MIN and batch > 0
+                    and (max(m, n) > TENSOR_CORE_ROWS or batch <= TENSOR_CORE_BATCH))
+    if not tensor_cores:
         return _composed_svd(a, 'block_jacobi', full_matrices, values_only, return_info, rank, opts)
     from .blocked import BlockJacobi
     used = width if (width % 8 == 0 and 8 <= width <= 64) else 32

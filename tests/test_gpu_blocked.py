@@ -163,7 +163,8 @@ def test_block_jacobi_rounds_golden(pkg):
 
 
 @pytest.mark.parametrize("shape,dtype,bs", [((3, 200, 120), np.float64, 16), ((2, 90, 140), np.complex128, 8),
-                                            ((4, 64, 40), np.complex64, 5), ((8, 48, 33), np.float32, 4)])
+                                            ((4, 64, 40), np.complex64, 5), ((8, 48, 33), np.float32, 4),
+                                            ((6, 200, 100), np.float32, 16)])
 def test_block_jacobi_rounds_against_lapack(pkg, shape, dtype, bs):
     """Larger batches through the rounds path (float64, complex, float32 below
     the tensor-core size), tall and wide, ragged groups."""
@@ -173,7 +174,7 @@ def test_block_jacobi_rounds_against_lapack(pkg, shape, dtype, bs):
         a = a + 1j * rng.standard_normal(shape)
     a = a.astype(dtype)
     u, s, vh, info = pkg.svd(torch.from_numpy(a).cuda(), "block_jacobi", block_size=bs, return_info=True)
-    assert info["block_sweeps"] >= 2
+    assert info["block_sweeps"] >= 2 and "block_size_used" not in info     # the rounds engine
     tol = 1e-12 if dtype in (np.float64, np.complex128) else 2e-5
     _lapack_check(a, u.resolve_conj().cpu().numpy(), s.cpu().numpy(), vh.resolve_conj().cpu().numpy(), tol)
 
@@ -193,3 +194,8 @@ def test_block_jacobi_rounds_contract(pkg):
     assert u.shape == (2, 12, 5) and s3.shape == (2, 5) and vh.shape == (2, 5, 30)
     with pytest.raises(RuntimeError, match="block Jacobi did not converge"):
         pkg.svd(x.real.contiguous(), "block_jacobi", block_size=1, max_sweeps=2)
+    for dt, shape in ((torch.float64, (0, 12, 30)), (torch.float32, (2, 0, 80, 70))):   # empty batches
+        u, s, vh = pkg.svd(torch.zeros(shape, dtype=dt, device="cuda"), "block_jacobi", block_size=4)
+        k = min(shape[-2:])
+        assert u.shape == (*shape[:-2], shape[-2], k) and s.shape == (*shape[:-2], k)
+        assert vh.shape == (*shape[:-2], k, shape[-1])
