@@ -13,6 +13,11 @@ the other (the reference) or all at once (here) gives the same result:
     of this library's batched Jacobi (b x pairs matrices of m x |cols|,
     jb_svd_batched_f64 / _c64 / _c128, or the mixed FP32/FP64 kernels for
     float32), instead of one solve per pair;
+  * only V_ij of a pair solve is used, and a one-sided Jacobi sees its matrix
+    only through the column Gram W^H W; so pair subproblems taller than
+    QR_ROWS are first reduced to their R factor (this library's Householder
+    QR, W = Q R, R^H R = W^H W) and the Jacobi runs on the |cols| x |cols| R:
+    the same rotations and sweeps in exact arithmetic, far less work;
   * the rotations W[:, cols] V_ij and V[:, cols] V_ij and the convergence
     check's Gram W^H W are library GEMMs in the input dtype, as the
     reference's matmuls are.
@@ -24,6 +29,10 @@ sorted by norm and normalised, null columns completed (solvers.py:18-21).
 from __future__ import annotations
 
 import torch
+
+from . import qr as Q
+
+QR_ROWS = 128   # pair subproblems with more rows than this are reduced to R first
 
 
 def round_robin(n):
@@ -99,7 +108,10 @@ def block_jacobi(a, stats, opts, jacobi, complete):
                 flat = idx.reshape(-1)
                 wy = w[:, :, flat].reshape(b, m, k, c).permute(2, 0, 1, 3)     # (pairs, b, m, c)
                 vy = v[:, :, flat].reshape(b, n, k, c).permute(2, 0, 1, 3)
-                _, _, vv = jacobi(wy.reshape(k * b, m, c))
+                y = wy.reshape(k * b, m, c)
+                if m > QR_ROWS:
+                    y = Q.qr(y)[1]
+                _, _, vv = jacobi(y)
                 vv = vv.reshape(k, b, c, c)
                 w[:, :, flat] = (wy @ vv).permute(1, 2, 0, 3).reshape(b, m, k * c)
                 v[:, :, flat] = (vy @ vv).permute(1, 2, 0, 3).reshape(b, n, k * c)

@@ -408,12 +408,12 @@ _block_plans = {}
 
 
 # float32 block_jacobi runs on the tensor cores (one matrix at a time) when
-# min(m, n) >= TENSOR_CORE_MIN and either max(m, n) > TENSOR_CORE_ROWS (the
-# rounds engine's pair subproblems then leave the register kernels) or the
-# batch holds at most TENSOR_CORE_BATCH matrices.  Measured on B200, block
-# width 32: 64 x 256x128 takes 15 ms in rounds vs 220 ms on the tensor cores,
-# 1 x 256x128 11.3 vs 5.5 ms, 16 x 512x256 302 vs 120 ms.
-TENSOR_CORE_MIN, TENSOR_CORE_ROWS, TENSOR_CORE_BATCH = 65, 256, 2
+# min(m, n) >= TENSOR_CORE_MIN and the batch holds at most
+# max(m, n) / TENSOR_CORE_ROWS_PER_MATRIX matrices; otherwise the rounds
+# engine solves the whole batch at once.  Measured on B200, block width 32
+# (tensor cores vs rounds): 4 x 256x128 15.3 vs 14.1 ms, 8 x 512x256 62 vs
+# 63 ms, 4 x 1024x512 68 vs 261 ms, 1 x 2048x512 17 vs 535 ms.
+TENSOR_CORE_MIN, TENSOR_CORE_ROWS_PER_MATRIX = 65, 64
 
 
 def _block_svd(a, full_matrices, values_only, return_info, rank, opts):
@@ -441,8 +441,8 @@ def _block_svd(a, full_matrices, values_only, return_info, rank, opts):
         return svd(a, 'jacobi', full_matrices=full_matrices, values_only=values_only, return_info=return_info,
                    **rest)
     batch = a.numel() // (m * n)
-    tensor_cores = (a.dtype == torch.float32 and min(m, n) >= TENSOR_CORE_MIN and batch > 0
-                    and (max(m, n) > TENSOR_CORE_ROWS or batch <= TENSOR_CORE_BATCH))
+    tensor_cores = (a.dtype == torch.float32 and min(m, n) >= TENSOR_CORE_MIN
+                    and 0 < batch <= max(m, n) / TENSOR_CORE_ROWS_PER_MATRIX)
     if not tensor_cores:
         return _composed_svd(a, 'block_jacobi', full_matrices, values_only, return_info, rank, opts)
     from .blocked import BlockJacobi
