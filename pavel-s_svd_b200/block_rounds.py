@@ -78,14 +78,16 @@ def finish_columns(w, s, complete):
     return complete(u, keep), torch.where(keep, s, torch.zeros_like(s))
 
 
-def block_jacobi(a, stats, opts, jacobi, complete):
+def block_jacobi(a, stats, opts, jacobi, check, complete):
     """Block Jacobi of a batch of tall matrices a (b, m, n), m >= n, with at
-    least two column groups.  `jacobi(y)` solves a batch of pair
-    subproblems and returns (u, s, v) with v (., c, c) orthogonal / unitary,
-    columns by descending sigma; `complete(u, keep)` fills the columns of u
-    not in keep.  Returns U (b, m, n), sigma (b, n) descending, V (b, n, n).
-    Raises RuntimeError('block Jacobi did not converge') after max_sweeps
-    (default 30) sweeps (solvers.py:59-60)."""
+    least two column groups.  `jacobi(y)` enqueues the one-sided Jacobi of a
+    batch of pair subproblems and returns (_, _, v) with v (., c, c)
+    orthogonal / unitary, columns by descending sigma; `check()` raises the
+    errors of the solves enqueued since its last call (called once per
+    sweep); `complete(u, keep)` fills the columns of u not in keep.  Returns
+    U (b, m, n), sigma (b, n) descending, V (b, n, n).  Raises
+    RuntimeError('block Jacobi did not converge') after max_sweeps (default
+    30) sweeps (solvers.py:59-60)."""
     b, m, n = a.shape
     if b == 0:
         stats['block_sweeps'] = 0
@@ -115,6 +117,7 @@ def block_jacobi(a, stats, opts, jacobi, complete):
                 vv = vv.reshape(k, b, c, c)
                 w[:, :, flat] = (wy @ vv).permute(1, 2, 0, 3).reshape(b, m, k * c)
                 v[:, :, flat] = (vy @ vv).permute(1, 2, 0, 3).reshape(b, n, k * c)
+        check()
         g = w.mH @ w
         d = g.diagonal(dim1=-2, dim2=-1).real.clamp_min(0)
         root = d.sqrt()
@@ -138,12 +141,11 @@ def block_jacobi(a, stats, opts, jacobi, complete):
     return u, s, v
 
 
-def raw(x, stats, opts, jacobi, complete):
-    """Wide input through its conjugate transpose (solvers.py:224-227); a
-    single column group is the plain Jacobi (:36-37)."""
+def raw(x, stats, opts, jacobi, check, complete):
+    """Wide input through its conjugate transpose (solvers.py:224-227).  The
+    caller sends a matrix with a single column group to the plain Jacobi
+    (:36-37)."""
     if x.shape[-2] < x.shape[-1]:
-        u, s, v = raw(x.mH.resolve_conj().contiguous(), stats, opts, jacobi, complete)
+        u, s, v = raw(x.mH.resolve_conj().contiguous(), stats, opts, jacobi, check, complete)
         return v, s, u
-    if -(-x.shape[-1] // opts.get('block_size', 4)) == 1:
-        return jacobi(x)
-    return block_jacobi(x, stats, opts, jacobi, complete)
+    return block_jacobi(x, stats, opts, jacobi, check, complete)

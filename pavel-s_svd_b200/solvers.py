@@ -352,6 +352,53 @@ def _complete_basis(q, size):
     return _complete_null_columns(torch.cat([q, z], -1), keep)
 
 
+def _pair_solver(jopts, stats):
+    """The pair solves of the block rounds (block_rounds.block_jacobi): V of
+    each subproblem of a batch from one call of the batched kernel
+    (jb_svd_batched_f32 / _f64 / _c64 / _c128), with the per-matrix status
+    and sweep words left on the device; `check()` reads them all at once and
+    raises the reference's errors (primitives.py:354-355), so the rounds of
+    a block sweep are enqueued without host round trips.  The subproblems
+    are columns of the already scaled, checked W: no rescaling or input
+    scan, as the reference's inner _jacobi does none (solvers.py:24-27)."""
+    pending = []
+    tol = float(jopts.get('tol') or 0.0)
+    max_sweeps = jopts.get('max_sweeps', 60)
+    precision = jopts.get('precision', 'mixed')
+    flags = N.ROUND_ROBIN if jopts.get('ordering', 'block') == 'round_robin' else 0
+
+    def solve(y):
+        y = y.resolve_conj().contiguous()
+        b, m, c = y.shape
+        dev = y.device
+        info = torch.zeros(2, b, dtype=torch.int32, device=dev)
+        u = torch.empty(b, m, c, dtype=y.dtype, device=dev)
+        s = torch.empty(b, c, dtype=y.real.dtype, device=dev)
+        vh = torch.empty(b, c, c, dtype=y.dtype, device=dev)
+        ws = _default_ws.setdefault(dev, Workspace())
+        if y.is_complex():
+            lib = N.lib()
+            buf = ws.get(lib.jb_svd_complex_workspace_bytes(m, c, b, y.element_size()), dev)
+            fn = lib.jb_svd_batched_c64 if y.dtype == torch.complex64 else lib.jb_svd_batched_c128
+            N.check(fn(y.data_ptr(), u.data_ptr(), s.data_ptr(), vh.data_ptr(), b, m, c, tol, max_sweeps,
+                       info[0].data_ptr(), info[1].data_ptr(), buf.data_ptr(), buf.numel(),
+                       torch.cuda.current_stream(dev).cuda_stream), 'jb_svd_batched_complex')
+        else:
+            launch_batched(y, c, flags, tol, max_sweeps, precision if y.dtype == torch.float32 else 'fp64',
+                           (u, s, vh), info, ws)
+        pending.append(info)
+        return None, None, vh.mH
+
+    def check():
+        if not pending:
+            return
+        host = torch.cat(pending, 1).cpu()
+        pending.clear()
+        raise_for_status(host[1], max_sweeps)
+        stats['jacobi_sweeps'] = max(stats.get('jacobi_sweeps', 0), int(host[0].max()))
+    return solve, check
+
+
 def _composed_svd(a, algorithm, full_matrices, values_only, return_info, rank, opts):
     """The methods composed on the host from this library's kernels, through
     the public entry (solvers.py:264-310): 'qr', 'tsqr' (:71-96, 245-248) and
@@ -386,7 +433,8 @@ def _composed_svd(a, algorithm, full_matrices, values_only, return_info, rank, o
         scale = torch.ldexp(torch.ones_like(amax), e)
         y = (x / scale).contiguous()
         if algorithm == 'block_jacobi':
-            u, sv, v = BR.raw(y, stats, opts, jacobi, _complete_null_columns)
+            pair_v, check = _pair_solver(jopts, stats)
+            u, sv, v = BR.raw(y, stats, opts, pair_v, check, _complete_null_columns)
         else:
             u, sv, v = Q.raw(y, algorithm, stats, opts, jacobi)
         sv = sv * scale[:, 0, :]
