@@ -149,6 +149,8 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
     Jacobi (_composed_svd).
     Input is never overwritten."""
     rank, precision = _validate(a, algorithm, full_matrices, opts)
+    if algorithm == 'jacobi' and _qr_first(a):
+        return _tall_svd(a, full_matrices, values_only, return_info, rank, precision, opts)
     if a.is_complex() and algorithm == 'jacobi':
         return _complex_svd(a, full_matrices, values_only, return_info, rank, opts)
     if algorithm == 'block_jacobi':
@@ -157,8 +159,6 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
         return _gram_svd(a, full_matrices, values_only, return_info, rank, opts)
     if algorithm in ('qr', 'tsqr', 'randomized', 'subspace', 'block_krylov'):
         return _composed_svd(a, algorithm, full_matrices, values_only, return_info, rank, opts)
-    if _qr_first(a):
-        return _tall_svd(a, full_matrices, values_only, return_info, rank, precision, opts)
     max_sweeps = opts.get('max_sweeps', 60)
     tol = opts.get('tol')
     shape = a.shape[:-2]
@@ -196,29 +196,31 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
     return (*result, stats) if return_info else result
 
 
-# Real 'jacobi' input taller than this (tall view) and at least twice as tall
-# as wide is reduced to its R factor first (_tall_svd): beyond these rows the
-# register and large-tile kernels do not take the matrix.
-QR_FIRST_ROWS = {torch.float32: 256, torch.float64: 128}
+# 'jacobi' input taller than this (tall view) and at least twice as tall as
+# wide is reduced to its R factor first (_tall_svd): beyond these rows the
+# register and large-tile kernels (real) or a shared-memory work area
+# (complex, 48 x 32 to 128 x 64) no longer hold the matrix.
+QR_FIRST_ROWS = {torch.float32: 256, torch.float64: 128, torch.complex64: 128, torch.complex128: 128}
 
 
 def _qr_first(a):
     mt, nt = max(a.shape[-2:]), min(a.shape[-2:])
-    return not a.is_complex() and mt > QR_FIRST_ROWS[a.dtype] and mt >= 2 * nt and a.numel() > 0
+    return mt > QR_FIRST_ROWS[a.dtype] and mt >= 2 * nt and a.numel() > 0
 
 
 def _tall_svd(a, full_matrices, values_only, return_info, rank, precision, opts):
-    """'jacobi' on real matrices taller than the register and large-tile
-    kernels take (QR_FIRST_ROWS).  A one-sided Jacobi sees its matrix only
-    through the column Gram W^T W, and R^T R of a QR equals it, so the
-    Jacobi of the small factor R rotates as the Jacobi of A would: the same
-    V, sigma and sweeps in exact arithmetic, and U = Q U_R
-    (primitives.py:316-367 on A).  Steps:
+    """'jacobi' on matrices taller than the register and large-tile kernels
+    (real) or the shared-memory work area (complex) take (QR_FIRST_ROWS).  A
+    one-sided Jacobi sees its matrix only through the column Gram W^H W, and
+    R^H R of a QR equals it, so the Jacobi of the small factor R rotates as
+    the Jacobi of A would: the same V, sigma and sweeps in exact arithmetic,
+    and U = Q U_R (primitives.py:316-367 on A).  Steps:
       * the batch scaled by a power of two (exact), NaN / Inf rejected as by
         the reference (solvers.py:291-292);
-      * Householder QR on the GPU (jb_qr_f32 / _f64) of the tall view, in
-        FP64 for the mixed precision of float32 input (the 1e-5 sigma bound
-        of that mode rests on FP64 arithmetic from the exact input);
+      * Householder QR on the GPU (jb_qr_f32 / _f64 / _c64 / _c128) of the
+        tall view (the conjugate transpose of a wide matrix), in FP64 for
+        the mixed precision of float32 input (the 1e-5 sigma bound of that
+        mode rests on FP64 arithmetic from the exact input);
       * the Jacobi of R by the batched kernels, with the input dtype's
         tolerance (10 eps, primitives.py:325);
       * U = Q U_R (library GEMM), cast to the input dtype, then the
@@ -231,6 +233,7 @@ def _tall_svd(a, full_matrices, values_only, return_info, rank, precision, opts)
     wide = m < n
     mt, nt = max(m, n), min(m, n)
     eps = torch.finfo(a.dtype).eps
+    real = a.real.dtype
     tol = opts.get('tol') or 10 * eps
     max_sweeps = opts.get('max_sweeps', 60)
     with torch.no_grad(), torch.cuda.device(a.device):
@@ -242,14 +245,16 @@ def _tall_svd(a, full_matrices, values_only, return_info, rank, precision, opts)
         scale = torch.ldexp(torch.ones_like(amax), e)
         xs = x / scale
         if wide:
-            xs = xs.mT
-        work = torch.float64 if (a.dtype == torch.float64 or precision == 'mixed') else torch.float32
-        q, r = Q.qr(xs.to(work).contiguous())
+            xs = xs.mH
+        work = a.dtype
+        if a.dtype == torch.float32 and precision == 'mixed':
+            work = torch.float64
+        q, r = Q.qr(xs.to(work).resolve_conj().contiguous())
         ur, sv, vhr, info = svd(r, 'jacobi', return_info=True, tol=tol, max_sweeps=max_sweeps, precision='fp32',
                                 ordering=opts.get('ordering', 'block'))
         keep = sv > eps * max(mt, nt + nt % 2) * sv[:, :1]
-        sv = (torch.where(keep, sv, torch.zeros_like(sv)) * scale[:, 0, :].to(sv.dtype)).to(a.dtype)
-        v = vhr.mT.to(a.dtype)
+        sv = (torch.where(keep, sv, torch.zeros_like(sv)) * scale[:, 0, :].to(sv.dtype)).to(real)
+        v = vhr.mH.to(a.dtype)
         u = None if values_only else _complete_null_columns((q @ ur).to(a.dtype), keep)
         if wide:
             u, v = v, u
@@ -262,12 +267,12 @@ def _tall_svd(a, full_matrices, values_only, return_info, rank, precision, opts)
         sv = sv[:, :rank] if not full_matrices else sv
         if not all(bool(torch.isfinite(t).all()) for t in (sv,) + (() if values_only else (u, v))):
             raise RuntimeError('standalone solver produced nonfinite output')
-        result = (None if values_only else u.reshape(*shape, *u.shape[-2:]),
+        result = (None if values_only else u.resolve_conj().reshape(*shape, *u.shape[-2:]),
                   sv.reshape(*shape, sv.shape[-1]),
-                  None if values_only else v.mT.reshape(*shape, v.shape[-1], v.shape[-2]))
+                  None if values_only else v.mH.resolve_conj().reshape(*shape, v.shape[-1], v.shape[-2]))
     stats = {'algorithm': 'jacobi', 'vendor_factorizations': 0, 'converged': True,
              'jacobi_sweeps': info['jacobi_sweeps'],
-             'precision': 'fp64' if a.dtype == torch.float64 else precision, 'qr_first': True,
+             'precision': {torch.float32: precision, torch.complex64: 'fp32'}.get(a.dtype, 'fp64'), 'qr_first': True,
              'implementation': 'B200 sm_100a Householder QR + batched one-sided Jacobi of R (tall input)'}
     return (*result, stats) if return_info else result
 

@@ -15,7 +15,7 @@ import torch
 
 from conftest import sigma_tol
 from oracle import jacobi_oracle as O
-from test_oracle import _cmp_sigma, _cmp_vectors
+from test_oracle import _cmp_sigma, _cmp_vectors, _cmp_vectors_phase
 
 pytestmark = pytest.mark.gpu
 DEV = "cuda"
@@ -45,6 +45,30 @@ def test_tall_matches_oracle(pkg, shape, dtype, precision):
     if precision == "mixed":      # the mixed bound: 1e-5 of sigma against FP64 LAPACK
         truth = np.linalg.svd(a.astype(np.float64), compute_uv=False)
         assert float(np.abs(s - truth).max() / truth.max()) <= 1e-5
+
+
+@pytest.mark.parametrize("shape,dtype", [((2, 300, 20), np.complex64), ((2, 20, 400), np.complex128)])
+def test_tall_complex_matches_oracle(pkg, shape, dtype):
+    """Complex input through the complex QR: tall, and wide through the
+    conjugate transpose; vectors up to a unit phase."""
+    rng = np.random.default_rng(shape[-2])
+    a = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(dtype)
+    u, s, vh, info = pkg.svd(torch.from_numpy(a).to(DEV), "jacobi", return_info=True)
+    assert info["qr_first"]
+    uo, so, vho, io = O.svd(a, "jacobi", return_info=True)
+    s, u, vh = s.cpu().numpy(), u.resolve_conj().cpu().numpy(), vh.resolve_conj().cpu().numpy()
+    _cmp_sigma(s, so, a.dtype)
+    _cmp_vectors_phase(u, uo, so, a.dtype, -1)
+    _cmp_vectors_phase(vh, vho, so, a.dtype, -2)
+    assert abs(info["jacobi_sweeps"] - io["jacobi_sweeps"]) <= 2
+    k = min(shape[-2:])
+    rec = (u.astype(np.complex128) * s[:, None, :]) @ vh.astype(np.complex128)
+    assert float(np.abs(rec - a).max() / np.abs(a).max()) <= (1e-5 if dtype == np.complex64 else 1e-13)
+    uf, sf, vhf = pkg.svd(torch.from_numpy(a).to(DEV), "jacobi", full_matrices=True)
+    q = (vhf if shape[-1] > shape[-2] else uf).cpu().numpy().astype(np.complex128)
+    assert q.shape[-1] == max(shape[-2:]) and k == s.shape[-1]
+    assert float(np.abs(np.conj(np.swapaxes(q, 1, 2)) @ q - np.eye(q.shape[-1])).max()) <= (
+        1e-5 if dtype == np.complex64 else 1e-12)
 
 
 def test_tall_rank_deficient_cut_and_full(pkg):
