@@ -27,11 +27,14 @@ _ws = {}
 
 
 def _workspace(nbytes, device):
-    buf = _ws.get(device)
+    """The QR scratch of the current stream on `device` (launches on different
+    streams may run at the same time and must not share it)."""
+    key = (torch.device(device), torch.cuda.current_stream(device).cuda_stream)
+    buf = _ws.get(key)
     nbytes = max(int(nbytes), 256)
     if buf is None or buf.numel() < nbytes:
         buf = torch.empty(nbytes, dtype=torch.uint8, device=device)
-        _ws[device] = buf
+        _ws[key] = buf
     return buf
 
 

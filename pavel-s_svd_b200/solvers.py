@@ -135,6 +135,14 @@ def launch_batched(x, rank, flags, tol, max_sweeps, precision, out, info, worksp
 _default_ws = {}
 
 
+def _stream_ws(device):
+    """The default workspace of the current stream on `device`.  Launches on
+    different streams may run at the same time, so they must not share the
+    ticket counters and scratch that a workspace holds."""
+    key = (torch.device(device), torch.cuda.current_stream(device).cuda_stream)
+    return _default_ws.setdefault(key, Workspace())
+
+
 def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return_info=False, **opts):
     """Return U, s, Vh (and optionally diagnostics) for real batched CUDA tensors.
 
@@ -177,7 +185,7 @@ def svd(a, algorithm='jacobi', *, full_matrices=False, values_only=False, return
         vh = None if values_only else torch.empty(b, vrows, n, dtype=a.dtype, device=dev)
         s = torch.empty(b, rank, dtype=a.dtype, device=dev)
         info = torch.empty(2, max(b, 1), dtype=torch.int32, device=dev)
-        ws = opts.get('workspace') or _default_ws.setdefault(dev, Workspace())
+        ws = opts.get('workspace') or _stream_ws(dev)
         if b:
             launch_batched(x, rank, flags, tol, max_sweeps, precision if a.dtype == torch.float32 else 'fp64',
                            (u, s, vh), info, ws)
@@ -414,7 +422,7 @@ def _complex_svd(a, full_matrices, values_only, return_info, rank, opts):
         if b:
             lib = N.lib()
             elem = xs.element_size()
-            ws = _default_ws.setdefault(a.device, Workspace()).get(
+            ws = _stream_ws(a.device).get(
                 lib.jb_svd_complex_workspace_bytes(mt, nt, b, elem), a.device)
             fn = lib.jb_svd_batched_c64 if a.dtype == torch.complex64 else lib.jb_svd_batched_c128
             N.check(fn(xs.data_ptr(), u.data_ptr(), sv.data_ptr(), vh.data_ptr(), b, mt, nt,
@@ -480,7 +488,7 @@ def _pair_solver(jopts, stats):
         u = torch.empty(b, m, c, dtype=y.dtype, device=dev)
         s = torch.empty(b, c, dtype=y.real.dtype, device=dev)
         vh = torch.empty(b, c, c, dtype=y.dtype, device=dev)
-        ws = _default_ws.setdefault(dev, Workspace())
+        ws = _stream_ws(dev)
         if y.is_complex():
             lib = N.lib()
             buf = ws.get(lib.jb_svd_complex_workspace_bytes(m, c, b, y.element_size()), dev)
