@@ -113,7 +113,10 @@ class UnevenBatch:
     ``m``, ``n``: per-matrix shapes.  ``a_off``: element offsets of each
     matrix in the flat input (default: ``pack``'s layout).  Outputs are flat
     buffers ``U``, ``S``, ``Vh`` (reduced SVD, rank = min(m, n)) addressed by
-    the per-matrix offsets; ``result(i)`` returns views."""
+    the per-matrix offsets; ``result(i)`` returns views.  The plan owns its
+    workspace (ticket counters, the FP32 V hand-off) and output buffers, so
+    one plan serves one stream at a time; solves on several streams at once
+    take one plan each."""
 
     def __init__(self, m, n, device, *, a_off=None, tol=None, max_sweeps=60, precision="mixed",
                  values_only=False, order="cost", launch=None):
