@@ -294,16 +294,16 @@ class StreamedUneven:
         main = torch.cuda.current_stream(self.device)
         for s in (self.s_in, *self.s_comp, self.s_out):
             s.wait_stream(main)
-        landed, solved = [], []
-        for (a, _, _, _), d in zip(self.spans, self.dev_in):
+        solved = []
+        # each chunk's solve is enqueued right after its input copy, so the
+        # first solve starts as soon as the (small) first chunk has landed
+        for i, ((a, _, _, _), d, plan) in enumerate(zip(self.spans, self.dev_in, self.plans)):
             with torch.cuda.stream(self.s_in):
                 d[:a[1] - a[0]].copy_(host_in[a[0]:a[1]], non_blocking=True)
-                ev = torch.cuda.Event()
-                ev.record(self.s_in)
-            landed.append(ev)
-        for i, (plan, d, ev) in enumerate(zip(self.plans, self.dev_in, landed)):
+                landed = torch.cuda.Event()
+                landed.record(self.s_in)
             comp = self.s_comp[i % 2]
-            comp.wait_event(ev)
+            comp.wait_event(landed)
             plan.launch(d, stream=comp)
             done = torch.cuda.Event()
             done.record(comp)
@@ -320,11 +320,12 @@ class StreamedUneven:
     def check(self):
         """Synchronise; raise for any failed matrix; return the sweep counts."""
         self.s_out.synchronize()
-        sweeps = []
-        for plan, info in zip(self.plans, self.host_info):
-            raise_for_status(info[1, :plan.count], self.max_sweeps)
-            sweeps.append(info[0, :plan.count].numpy().copy())
-        return np.concatenate(sweeps) if sweeps else np.zeros(0, np.int32)
+        if not self.plans:
+            return np.zeros(0, np.int32)
+        info = np.concatenate([h[:, :p.count].numpy() for p, h in zip(self.plans, self.host_info)], axis=1)
+        if info[1].any():
+            raise_for_status(torch.from_numpy(info[1]), self.max_sweeps)
+        return info[0].copy()
 
     def device_bytes_per_run(self):
         """Bytes copied host->device and device->host by one run."""
