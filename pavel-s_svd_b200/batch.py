@@ -332,21 +332,40 @@ class StreamedUneven:
         return 4 * self.a_total, 4 * (self.u_total + self.s_total + self.v_total) + 8 * self.count
 
 
+REGISTER_ROWS, REGISTER_COLS = 128, 64   # tall-view limits of the register kernels
+
+
 def svd_uneven(mats, *, tol=None, max_sweeps=60, precision="mixed", values_only=False):
     """Solve a list of float32 CUDA matrices of different shapes in one call.
-    Returns a list of (U, s, Vh) like svd() of each matrix would."""
+    Returns a list of (U, s, Vh) like svd() of each matrix would.  The
+    matrices the register kernels take (tall view up to REGISTER_ROWS x
+    REGISTER_COLS) are one persistent launch; larger ones, which would move
+    the whole launch to the general kernels, go through svd() one by one
+    (large tiles, QR first)."""
     if not mats:
         return []
     dev = mats[0].device
     for a in mats:
         if a.dtype != torch.float32 or a.ndim != 2 or a.device != dev:
             raise TypeError("svd_uneven takes 2-D float32 tensors on one CUDA device")
-    m = np.array([a.shape[0] for a in mats], np.int64)
-    n = np.array([a.shape[1] for a in mats], np.int64)
-    plan = UnevenBatch(m, n, dev, tol=tol, max_sweeps=max_sweeps, precision=precision, values_only=values_only)
-    flat = torch.zeros(int(plan.a_off[-1] + m[-1] * n[-1] + 4), dtype=torch.float32, device=dev)
-    for a, o in zip(mats, plan.a_off):
-        flat[int(o):int(o) + a.numel()] = a.reshape(-1)
-    plan.launch(flat)
-    plan.check()
-    return [plan.result(i) for i in range(len(mats))]
+    fits = [max(a.shape) <= REGISTER_ROWS and min(a.shape) <= REGISTER_COLS for a in mats]
+    out = [None] * len(mats)
+    idx = [i for i, f in enumerate(fits) if f]
+    if idx:
+        m = np.array([mats[i].shape[0] for i in idx], np.int64)
+        n = np.array([mats[i].shape[1] for i in idx], np.int64)
+        plan = UnevenBatch(m, n, dev, tol=tol, max_sweeps=max_sweeps, precision=precision, values_only=values_only)
+        flat = torch.zeros(int(plan.a_off[-1] + m[-1] * n[-1] + 4), dtype=torch.float32, device=dev)
+        for i, o in zip(idx, plan.a_off):
+            flat[int(o):int(o) + mats[i].numel()] = mats[i].reshape(-1)
+        plan.launch(flat)
+        plan.check()
+        for j, i in enumerate(idx):
+            out[i] = plan.result(j)
+    if len(idx) < len(mats):
+        from .solvers import svd
+        for i, f in enumerate(fits):
+            if not f:
+                out[i] = svd(mats[i], "jacobi", tol=tol, max_sweeps=max_sweeps, precision=precision,
+                             values_only=values_only)
+    return out

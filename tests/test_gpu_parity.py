@@ -224,12 +224,21 @@ def test_uneven_batch_mixed_meets_bound_and_graph_replay(pkg, workloads):
 
 
 def test_svd_uneven_list_api(pkg, workloads):
-    mats = workloads.uneven_batch(16)
-    res = pkg.svd_uneven([torch.from_numpy(a).to(DEV) for a in mats], precision="fp32")
-    for a, (u, s, vh) in zip(mats, res):
-        u2, s2, vh2 = pkg.svd(torch.from_numpy(a).to(DEV), precision="fp32")
-        # different launch shapes sum in a different order: agree to fp32 accuracy
-        torch.testing.assert_close(s, s2, rtol=0, atol=1e-5 * float(s2[0]))
+    """The list API, with matrices beyond the register kernels mixed in (a
+    300 x 20, a 20 x 300, a 100 x 100): those go through svd() one by one,
+    the rest in one launch; every result in input order."""
+    mats = list(workloads.uneven_batch(16))
+    rng = np.random.default_rng(3)
+    mats[3:3] = [rng.standard_normal((300, 20)).astype(np.float32), rng.standard_normal((20, 300)).astype(np.float32)]
+    mats.append(rng.standard_normal((100, 100)).astype(np.float32))
+    for precision in ("fp32", "mixed"):
+        res = pkg.svd_uneven([torch.from_numpy(a).to(DEV) for a in mats], precision=precision)
+        assert len(res) == len(mats)
+        for a, (u, s, vh) in zip(mats, res):
+            u2, s2, vh2 = pkg.svd(torch.from_numpy(a).to(DEV), precision=precision)
+            assert u.shape == u2.shape and vh.shape == vh2.shape
+            # different launch shapes sum in a different order: agree to fp32 accuracy
+            torch.testing.assert_close(s, s2, rtol=0, atol=1e-5 * float(s2[0]))
 
 
 @pytest.mark.parametrize("precision", ["mixed", "fp32"])
