@@ -642,22 +642,51 @@ def _block_svd(a, full_matrices, values_only, return_info, rank, opts):
     return (*result, stats) if return_info else result
 
 
+_GPU_CONTROL = {
+    'jacobi': 'one C-ABI call per solve (persistent kernels, per-matrix convergence on the device) and one '
+              'status read-back; input taller than the register kernels takes a GPU QR (or TSQR) first',
+    'block_jacobi': 'large float32 matrices: the tensor-core engine, a host loop over block sweeps replaying CUDA '
+                    'graphs of the rounds; otherwise the block rounds on the host, one batched Jacobi call per '
+                    'round, status words read once per block sweep',
+    'gram_jacobi': 'a library GEMM for the Gram, one batched jacobi_eigh call, a library GEMM for U',
+    'qr': 'one GPU Householder QR launch, one batched Jacobi call for R, a library GEMM for U',
+    'tsqr': 'GPU Householder QR launches (equal-height leaves and each tree level batched), one batched Jacobi '
+            'call for R, library GEMMs',
+}
+for _m in ('randomized', 'subspace', 'block_krylov'):
+    _GPU_CONTROL[_m] = ('the sketch drawn on the device in the solve (unless initial_basis), GPU QRs of the '
+                        'sketches and power iterations, one batched Jacobi call, library GEMMs')
+
+
 def factory(a, spec):
     """Adapter for ``python -m svdbench`` (svdbench/algorithms.py:90-93), the
     counterpart of solvers.py:313-324: ``spec['method']`` selects the
     algorithm, ``spec['mode']`` the output form, other keys are options.
-    The workspace is sized here, in preparation, and reused by every run."""
+    For 'jacobi' on a CUDA tensor the device workspace is sized here, in
+    preparation, and reused by every run.  ``metadata`` describes the method
+    that runs."""
     opts = {k: v for k, v in spec.items() if k not in ('name', 'method', 'mode', 'seed_offset')}
     method = spec.get('method', 'jacobi')
+    full, values = spec.get('mode') == 'full', spec.get('mode') == 'values'
     ws = Workspace()
+    if (method == 'jacobi' and getattr(a, 'is_cuda', False) and a.dtype in (torch.float32, torch.float64)
+            and a.ndim >= 2 and a.numel() > 0 and not _qr_first(a)):
+        m, n = a.shape[-2:]
+        precision = opts.get('precision', 'mixed') if a.dtype == torch.float32 else 'fp64'
+        flags = (N.FULL_MATRICES if full else 0) | (N.VALUES_ONLY if values else 0)
+        if opts.get('ordering', 'block') == 'round_robin':
+            flags |= N.ROUND_ROBIN
+        prec = N.PREC_MIXED if precision == 'mixed' else N.PREC_NATIVE
+        ws.get(N.lib().jb_workspace_bytes(m, n, a.numel() // (m * n), a.element_size(), prec, flags), a.device)
 
     def run():
-        u, s, vh, info = svd(a, method, full_matrices=spec.get('mode') == 'full',
-                             values_only=spec.get('mode') == 'values', return_info=True, workspace=ws, **opts)
+        u, s, vh, info = svd(a, method, full_matrices=full, values_only=values, return_info=True, workspace=ws,
+                             **opts)
         run.diagnostics = info
         return u, s, vh
-    run.metadata = {'implementation': 'B200 sm_100a one-sided Jacobi, hand-written CUDA via C ABI',
-                    'vendor_factorizations': False, 'values_only_forms_vectors': True, 'rng_in_solve': False,
-                    'gpu_control': 'one C-ABI call per solve (persistent kernels); per-matrix convergence on device; '
-                                   'one status read-back per call'}
+    run.metadata = {'implementation': f'B200 sm_100a {method}, hand-written CUDA via C ABI',
+                    'vendor_factorizations': False, 'values_only_forms_vectors': True,
+                    'rng_in_solve': method in ('randomized', 'subspace', 'block_krylov')
+                                    and opts.get('initial_basis') is None,
+                    'gpu_control': _GPU_CONTROL.get(method, _GPU_CONTROL['jacobi'])}
     return run

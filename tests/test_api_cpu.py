@@ -54,6 +54,13 @@ def test_factory_contract(pkg):
     assert callable(run) and run.metadata["vendor_factorizations"] is False
     with pytest.raises(pkg.Unsupported):
         run()  # CPU tensor: unsupported, never a silent fallback
+    # metadata describes the method that runs (the harness saves it)
+    for method in pkg.ALGORITHMS:
+        md = pkg.factory(a, {"method": method}).metadata
+        assert method in md["implementation"] and md["gpu_control"]
+        assert md["rng_in_solve"] == (method in ("randomized", "subspace", "block_krylov"))
+    md = pkg.factory(a, {"method": "randomized", "initial_basis": torch.randn(4, 3)}).metadata
+    assert md["rng_in_solve"] is False
 
 
 def test_plugin_alias_importable(pkg):
