@@ -85,3 +85,16 @@ def test_streamed_chunk_weights():
     assert B.chunk_weights(1) == [1.0]
     assert B.chunk_weights(3) == [1.0, 2.0, 1.0]
     assert B.chunk_weights(8) == [1.0, 2.0, 4.0, 4.0, 4.0, 4.0, 2.0, 1.0]
+
+
+def test_tall_routing_thresholds(pkg):
+    """Which 'jacobi' inputs take the QR-first path: beyond the register /
+    large-tile rows (float32 256, float64 and complex 128) and at least twice
+    as tall as wide, either orientation; empty batches never."""
+    from importlib import import_module
+    S = import_module("pavel-s_svd_b200.solvers")
+    z = lambda *s, dt=torch.float32: torch.zeros(*s, dtype=dt)
+    assert not S._qr_first(z(256, 128)) and S._qr_first(z(257, 128)) and S._qr_first(z(128, 600))
+    assert not S._qr_first(z(300, 200))                       # not twice as tall as wide
+    assert S._qr_first(z(129, 64, dt=torch.float64)) and not S._qr_first(z(128, 64, dt=torch.float64))
+    assert S._qr_first(z(2, 200, 30, dt=torch.complex64)) and not S._qr_first(z(0, 400, 30))
