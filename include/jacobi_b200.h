@@ -391,15 +391,19 @@ JB_API int jb_jacobi_rounds(void *W, void *V, int32_t dtype, int32_t m, int32_t 
 
 /* jb_svd_batched_f32 without a workspace argument: allocates nothing.
  * No counterpart in the reference (its Python solver always allocates); this
- * is for callers that cannot allocate device memory when they solve, e.g.
- * code running while a CUDA graph is being captured (cudaMalloc is illegal
- * then) or plug-ins whose host framework owns all device allocations.
+ * is for callers that cannot allocate device memory when they solve: plug-ins
+ * whose host framework owns every device allocation through its own pool,
+ * and latency-bound paths that must not call cudaMalloc/cudaFree (which can
+ * synchronise the whole device).
  *   - Scratch is one file-scope __device__ array of JB_NOALLOC_SCRATCH_BYTES
  *     (16 MiB) that every GPU loading the library keeps until process exit.
- *   - Requests whose scratch would exceed it return JB_ETOOBIG: equal shapes
- *     need about 256 bytes plus, with JB_PREC_MIXED, 4*batch*min(m,n)^2
- *     bytes (e.g. at most 1023 matrices of 64 columns); shapes above 128 x 64
- *     (tall view) run only if their work area fits in shared memory.
+ *   - The limit: a call runs exactly when
+ *     jb_workspace_bytes(m, n, batch, 4, precision, flags) <=
+ *     JB_NOALLOC_SCRATCH_BYTES, and returns JB_ETOOBIG otherwise; callers can
+ *     query that before calling.  For shapes of the register kernels (tall
+ *     view up to 128 x 64) that is about 256 bytes plus, with JB_PREC_MIXED,
+ *     4*batch*min(m,n)^2 bytes (e.g. at most 1023 matrices of 64 columns);
+ *     larger shapes also need per-CTA work areas (about one per SM).
  *   - The first call on a device looks up the array's device address
  *     (cudaGetSymbolAddress) and caches it; make that first call before any
  *     stream capture.

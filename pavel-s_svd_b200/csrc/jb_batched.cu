@@ -1019,7 +1019,11 @@ static int launch_rr(Params &p, const Plan &pl, unsigned char *ws, size_t ws_byt
     if (pl.global_region) {
         const size_t stride = align16(pl.region) + 256;
         if (ws_bytes < kCounterBytes + stride) return JB_EWORKSPACE;
-        const int64_t max_grid = (int64_t)((ws_bytes - kCounterBytes) / stride);
+        // With an FP32-phase V hand-off (x32) in the same workspace, the
+        // per-CTA areas may use only the span base_bytes reserved before it.
+        const size_t span = p.x32 ? base_bytes(pl, p.count) - kCounterBytes : ws_bytes - kCounterBytes;
+        const int64_t max_grid = (int64_t)(span / stride);
+        if (max_grid < 1) return JB_EWORKSPACE;
         if (grid > max_grid) grid = max_grid;
         p.gws = ws + kCounterBytes;
         p.gws_stride = stride;
@@ -1196,10 +1200,10 @@ static size_t uniform_workspace(int32_t m, int32_t n, int64_t count, int32_t ele
 // Allocation-free variant of jb_svd_batched_f32.
 //
 // Some callers cannot allocate device memory at the moment they need an SVD:
-// code running while another library captures the stream into a CUDA graph
-// (cudaMalloc is not allowed during capture), plug-ins whose host framework
-// owns every device allocation, or real-time paths that must not touch the
-// allocator.  This entry point takes only inputs and outputs; its scratch
+// plug-ins whose host framework owns every device allocation through its own
+// pool (a raw cudaMalloc would bypass its accounting and limits), and
+// latency-bound paths that must not call cudaMalloc/cudaFree, which can
+// synchronise the whole device.  This entry point takes only inputs and outputs; its scratch
 // (the kernels' work tickets and, in mixed precision, the FP32-phase V of
 // every matrix) is the fixed array below, which every GPU that loads this
 // library holds until the process exits.

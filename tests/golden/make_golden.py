@@ -1,9 +1,9 @@
 """Generate the golden fixtures of the Jacobi path from the reference itself.
 
-Run once, in a container where uncle-Slava/Pavel-s_SVD is checked out (its
-path is given by REFERENCE_ROOT, default /root/reference):
+Run once, in a container where uncle-Slava/Pavel-s_SVD is checked out, with
+the path of that checkout as the argument or in REFERENCE_ROOT:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py <path of the reference checkout>
 
 It imports the reference's ``svdbench.standalone.svd`` and
 ``svdbench.matrices.make_matrix`` unchanged, runs ``svd(x, 'jacobi', ...)``
@@ -24,7 +24,7 @@ from pathlib import Path
 
 import numpy as np
 
-REF = Path(os.environ.get("REFERENCE_ROOT", "/root/reference"))
+REF: Path | None = None   # the reference checkout, set by main()
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
 
@@ -235,6 +235,11 @@ def lab_cases():
 
 
 def main():
+    global REF
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py <reference checkout> (or set REFERENCE_ROOT)")
+    REF = Path(root)
     sys.path.insert(0, str(REF))
     import torch
     import scipy.linalg

@@ -1,8 +1,9 @@
 """The allocation-free entry point jb_svd_batched_f32_noalloc, through the C ABI.
 
-It serves callers that cannot allocate device memory when they solve: code
-running while a CUDA graph is being captured (cudaMalloc is illegal then) or
-plug-ins whose host framework owns every device allocation.  Its scratch is a
+It serves callers that cannot allocate device memory when they solve:
+plug-ins whose host framework owns every device allocation through its own
+pool, and latency-bound paths that must not call cudaMalloc/cudaFree (which
+can synchronise the whole device).  Its scratch is a
 fixed 16 MiB device array inside the library, so its results must equal
 those of jb_svd_batched_f32 with a caller-provided workspace, call after call
 (the array keeps the previous call's contents).
