@@ -3,10 +3,19 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Workload (one step): the uneven batch of 8192 float32 matrices, n ~ U{8..64},
-m ~ U{n..2n}, entries N(0,1), seed 1 (rank r > 0 of a multi-GPU run uses seed
-1 + 1000 r: independent matrices, same distribution), solved by ONE persistent
-launch replayed from a captured CUDA graph, in the mixed precision that meets
+m ~ U{n..2n}, entries N(0,1), seed 1, solved by ONE persistent launch
+replayed from a captured CUDA graph, in the mixed precision that meets
 sigma-rel-err <= 1e-5 against FP64 LAPACK (checked on rank 0 after timing).
+The same batch is then timed in plain FP32 (the reference's arithmetic) for
+the mixed / plain factor.
+
+--gpus N (N > 1) without a torchrun environment starts N ranks itself (one
+process per GPU, torch.distributed.run on 127.0.0.1).  --scaling weak (the
+default): every rank solves its own batch of 8192 (rank r > 0 uses seed
+1 + 1000 r: independent matrices, same distribution); --scaling strong: the
+one seed-1 batch is split across the ranks by cost (batch.shard_by_cost).
+No collective touches the data: the ranks share only barriers and the
+max-over-ranks timing.
 Metric: matrices/s (whole job).  Each step is timed with CUDA events on the
 launching stream; a 256 MiB buffer is written between steps (outside the
 events) so every step starts with a cold L2.
@@ -23,9 +32,13 @@ events) so every step starts with a cold L2.
                    against LAPACK and the NumPy oracle timed beside it
 
 --impl reference: the reference algorithm's CPU implementation, timed on the
-host cores of this machine (the C restatement in oracle/, all threads; the
-reference itself is Python/PyTorch and is not present here), on a bounded
-sample of the same workload.  Under torchrun only rank 0 runs it.
+host cores of this machine on a bounded sample of the same workload: the C
+restatement in oracle/ (all threads; the reference is Python, so nothing of
+it compiles into a native library) gives the line's value, and the
+reference's own svdbench.standalone.svd(x, 'jacobi') (PyTorch on CPU, all
+threads, one call per matrix as a harness runs it; imported unchanged from
+the install in baseline/_ref when present) is timed beside it.  Under
+torchrun only rank 0 runs it.
 """
 from __future__ import annotations
 
@@ -53,20 +66,60 @@ COUNT = 8192
 # 256- and 128-thread, rb64_kernel 512- and 256-thread), from one ncu capture
 # (those metrics only) of `bench.py --steps 1 --warmup 3 --no-cpu-baseline`.
 MEASURED_TRAFFIC_PER_SOLVE = 289.5e6
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the four solve launches of one step, "
+                  "captured at the library of commit 520108d (profiles/rb_uneven_batch_8192.md)")
 
 
-def workload_config(n_gpus):
-    return {"workload": WORKLOAD, "matrices_per_gpu": COUNT, "n_range": [8, 64], "m_range": "[n, 2n]",
+MIXED = ("mixed (FP32 sweeps, then FP64 sweeps from the Newton-Schulz orthogonalised V, "
+         "W = A V recomputed in FP64)")
+
+
+def workload_config(n_gpus, scaling="weak", precision=MIXED):
+    per_gpu = COUNT if scaling == "weak" else f"{COUNT} / {n_gpus}, split by cost (batch.shard_by_cost)"
+    return {"workload": WORKLOAD, "matrices_per_gpu": per_gpu, "n_range": [8, 64], "m_range": "[n, 2n]",
             "dtype": "float32", "seed": 1, "tol": "10*eps32 (reference default)", "max_sweeps": 60,
-            "precision": "mixed (FP32 sweeps, then FP64 sweeps from the Newton-Schulz orthogonalised V, "
-                         "W = A V recomputed in FP64)",
+            "precision": precision, "scaling_mode": scaling,
             "parallelism": f"dp{n_gpus} (independent matrices per GPU, no collective)",
             "l2": "256 MiB write between steps, outside the timed events"}
 
 
-def load_matrices(rank):
+def load_matrices(rank, world=1, scaling="weak"):
+    """This rank's matrices: its own seeded batch (weak scaling), or its
+    cost-balanced share of the one seed-1 batch (strong scaling)."""
     wl = importlib.import_module("pavel-s_svd_b200.workloads")
+    if scaling == "strong":
+        B = importlib.import_module("pavel-s_svd_b200.batch")
+        mats = wl.uneven_batch(COUNT, seed=1)
+        m = np.array([a.shape[0] for a in mats])
+        n = np.array([a.shape[1] for a in mats])
+        return [mats[i] for i in B.shard_by_cost(m, n, world)[rank]]
     return wl.uneven_batch(COUNT, seed=1 if rank == 0 else 1 + 1000 * rank)
+
+
+def rank_command(nprocs, script, argv, port):
+    """The command that starts `nprocs` ranks of `script` on this node, one
+    per GPU, rendezvous on 127.0.0.1."""
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={nprocs}",
+            "--master-addr=127.0.0.1", f"--master-port={port}", str(script), *argv]
+
+
+def launch_ranks(nprocs, script, argv, timeout=None):
+    """Run `script` as `nprocs` ranks and return their launcher's exit code."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    return subprocess.run(rank_command(nprocs, script, argv, port), timeout=timeout).returncode
+
+
+def cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def reduce_max(x, device):
@@ -244,8 +297,34 @@ def cpu_port_sample(mats, seconds=12.0, threads=0):
     return done / elapsed, done, threads, elapsed
 
 
+def reference_pytorch_sample(mats, seconds=10.0):
+    """Time the reference's own svd(x, 'jacobi') (svdbench.standalone,
+    PyTorch on CPU, imported unchanged from the install in baseline/_ref)
+    one call per matrix, as a harness loops over matrices of different
+    shapes, on consecutive matrices of the workload for about `seconds`.
+    Returns (matrices/s, matrices, threads, seconds) or None when the
+    install is absent."""
+    ref = ROOT / "baseline" / "_ref"
+    if not (ref / "svdbench").is_dir():
+        return None
+    import torch
+    if str(ref) not in sys.path:
+        sys.path.insert(0, str(ref))
+    from svdbench.standalone import svd as ref_svd
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    ref_svd(torch.from_numpy(mats[0]), 'jacobi')                       # warm-up
+    done, t0 = 0, time.perf_counter()
+    while done < len(mats) and time.perf_counter() - t0 < seconds:
+        ref_svd(torch.from_numpy(mats[done]), 'jacobi')
+        done += 1
+    el = time.perf_counter() - t0
+    return done / el, done, threads, el
+
+
 def run_reference(args, rank, world):
-    """The CPU reference arm: rank 0 times the oracle port; other ranks exit."""
+    """The CPU reference arm: rank 0 times the oracle port (the line's value)
+    and the reference's own PyTorch CPU Jacobi beside it; other ranks exit."""
     if rank != 0:
         return
     mats = load_matrices(0)
@@ -258,15 +337,57 @@ def run_reference(args, rank, world):
             per_step.append(rate)
             sample = done
     value = statistics.median(per_step)
+    fp32 = "fp32 (the reference's FP32 Jacobi arithmetic, solvers.py:24-27)"
     line = {"metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * sample / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": workload_config(world), "impl": "reference",
+            "config": workload_config(world, "weak", fp32), "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "matrices/s", "cores": threads, "kind": "port",
+                             "cpu": cpu_model(),
                              "sample": f"first {sample} matrices of the workload per step (~{args.ref_seconds:.0f} s),"
                                        " C restatement of the reference Jacobi (oracle/), fp32 as the reference"},
             "e2e": {"value": value, "unit": "matrices/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_reference_pytorch:
+        got = reference_pytorch_sample(mats, seconds=args.ref_seconds)
+        if got is None:
+            line["reference_pytorch"] = {"unavailable": "baseline/_ref holds no install of the reference"}
+        else:
+            rate, done, thr, el = got
+            line["reference_pytorch"] = {
+                "value": rate, "unit": "matrices/s", "cores": thr, "kind": "reference", "cpu": cpu_model(),
+                "sample": f"first {done} matrices of the workload ({el:.1f} s), svdbench.standalone.svd(x, "
+                          "'jacobi') imported unchanged, one call per matrix (the reference batches only "
+                          "equal shapes), torch.set_num_threads(all host threads)",
+                "c_port_over_reference": value / rate}
     print(json.dumps(line), flush=True)
+
+
+def measure_fp_peaks(dev):
+    """FP32 (scalar and packed) and FP64 CUDA-core peaks of this GPU, TFLOP/s:
+    jb_fma_loop (independent FMA chains, registers only), best of 3 runs
+    timed with CUDA events."""
+    import torch
+    N = importlib.import_module("pavel-s_svd_b200.native")
+    lib = N.lib()
+    sink = torch.zeros(1 << 16, dtype=torch.float32, device=dev)
+    blocks = torch.cuda.get_device_properties(dev).multi_processor_count * 8
+    out = {}
+    for mode, name, iters in ((0, "fp32_scalar_tflops", 40000), (1, "fp32_packed_tflops", 40000),
+                              (2, "fp64_tflops", 8000)):
+        best = float("inf")
+        for _ in range(4):
+            e0, e1 = _events()
+            e0.record()
+            N.check(lib.jb_fma_loop(mode, blocks, iters, sink.data_ptr(), torch.cuda.current_stream(dev).cuda_stream),
+                    "jb_fma_loop")
+            e1.record()
+            torch.cuda.synchronize(dev)
+            best = min(best, e0.elapsed_time(e1))
+        out[name] = lib.jb_fma_loop_flops(blocks, iters) / (best / 1e3) / 1e12
+    out["fp32_tflops"] = max(out["fp32_scalar_tflops"], out["fp32_packed_tflops"])
+    out["how"] = ("jb_fma_loop: 8 CTAs x 256 threads per SM, 16 independent FMA chains per thread, best of 4 "
+                  "CUDA-event timings")
+    return out
 
 
 def check_accuracy(plan, mats, limit=None):
@@ -291,6 +412,23 @@ def check_accuracy(plan, mats, limit=None):
     return worst_sig, worst_rec
 
 
+def time_replays(graph, flush, stream, steps):
+    """CUDA-event times (ms) of `steps` graph replays, L2 flushed between them
+    (outside the events)."""
+    import torch
+    times = []
+    for step in range(steps):
+        flush.fill_(step & 0xff)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        graph.replay()
+        e1.record(stream)
+        times.append((e0, e1))
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in times]
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -298,7 +436,8 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     pkg = importlib.import_module("pavel-s_svd_b200")
     B = importlib.import_module("pavel-s_svd_b200.batch")
-    mats = load_matrices(rank)
+    mats = load_matrices(rank, world, args.scaling)
+    total = COUNT * world if args.scaling == "weak" else COUNT
     flat_host, m, n, a_off = B.pack(mats)
     flat = flat_host.to(dev)
     # launch choices picked by the autotuner on this batch, in preparation (outside every timed region)
@@ -316,23 +455,13 @@ def run_ours(args, rank, world, local_rank):
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize(dev)
-    times = []
     with NvmlClockSampler(dev, local_rank) as clocks:
-        for step in range(args.steps):
-            flush.fill_(step & 0xff)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            graph.replay()
-            e1.record(stream)
-            times.append((e0, e1))
-        torch.cuda.synchronize(dev)
+        step_ms = time_replays(graph, flush, stream, args.steps)
     if world > 1:
         dist.barrier()
-    step_ms = [a.elapsed_time(b) for a, b in times]
     total_ms = reduce_max(sum(step_ms), dev)
     ms_per_step = total_ms / args.steps
-    value = COUNT * world / (ms_per_step / 1e3)
+    value = total / (ms_per_step / 1e3)
 
     # End to end through the public host-to-host API (batch.StreamedUneven):
     # pinned host input -> device, solve, U/S/Vh and status -> pinned host,
@@ -365,7 +494,7 @@ def run_ours(args, rank, world, local_rank):
         e2e_ev.append((e0, e1))
     torch.cuda.synchronize(dev)
     e2e_ms = reduce_max(sum(a.elapsed_time(b) for a, b in e2e_ev), dev)
-    e2e_value = COUNT * world / (e2e_ms / args.steps / 1e3)
+    e2e_value = total / (e2e_ms / args.steps / 1e3)
     # the host-to-host result equals the device solve's (same kernels per matrix)
     e2e_same = bool(torch.equal(host_s[:plan.S.numel()], plan.S.cpu()))
 
@@ -379,24 +508,50 @@ def run_ours(args, rank, world, local_rank):
     achieved_gbs = nbytes / (ms_per_step / 1e3) / 1e9
     flop = float((flop_per_sweep * sweeps).sum())
     fp_tflops = flop / (ms_per_step / 1e3) / 1e12
+    fp_peaks = measure_fp_peaks(dev)
+    del graph
+    # The same batch in plain FP32 (the reference's arithmetic, V = I start,
+    # its tolerance), timed the same way on this GPU: the mixed / plain factor.
+    plain = None
+    if args.precision == "mixed":
+        p32 = B.UnevenBatch(m, n, dev, a_off=a_off, precision="fp32")
+        g32 = p32.capture(flat)
+        for _ in range(args.warmup):
+            flush.fill_(1)
+            g32.replay()
+        ms32 = statistics.mean(time_replays(g32, flush, stream, args.steps))
+        sw32 = p32.check()
+        err32, rec32 = check_accuracy(p32, mats, limit=2048)
+        rate32 = len(mats) / (ms32 / 1e3)
+        plain = {"matrices_per_s_this_gpu": rate32, "ms_per_step": ms32, "sweeps_mean": float(sw32.mean()),
+                 "max_rel_sigma_err_vs_fp64": err32, "max_reconstruction_rel_fro": rec32,
+                 "meets_1e-5": bool(err32 <= 1e-5), "matrices_checked": 2048,
+                 "mixed_over_plain_fp32": (len(mats) / (ms_per_step / 1e3)) / rate32,
+                 "note": "plain FP32 one-sided Jacobi (precision='fp32', the reference's arithmetic) on the same "
+                         "batch and GPU, graph replays timed like the headline"}
+        del g32
     line = {"metric": METRIC, "value": value, "unit": "matrices/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": args.scaling,
             "vs_baseline": None, "dtype": "f32 in/out; f32+f64 sweeps" if args.precision == "mixed" else "f32",
             "data": "synthetic (seeded: n ~ U[8,64], m ~ U[n,2n], entries N(0,1))",
-            "config": dict(workload_config(world), launch=repr(choice),
-                           autotuner_ms={k: round(v, 3) for k, v in tune_ms.items()}),
+            "config": dict(workload_config(world, args.scaling, MIXED if args.precision == "mixed" else "fp32"),
+                           launch=repr(choice), autotuner_ms={k: round(v, 3) for k, v in tune_ms.items()}),
             "accuracy": {"max_rel_sigma_err_vs_fp64": sig_err, "max_reconstruction_rel_fro": rec_err,
                          "matrices_checked": len(mats) if args.full_check else 2048,
                          "sweeps_mean": float(sweeps.mean()), "sweeps_max": int(sweeps.max())},
+            "plain_fp32": plain,
             "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved_gbs / hbm_peak, "peak_kind": peak_kind,
                          "traffic": args.traffic_bytes if args.traffic_bytes is not None else
                          MEASURED_TRAFFIC_PER_SOLVE,
+                         "traffic_source": TRAFFIC_SOURCE,
                          "algorithmic_bytes_per_launch": nbytes,
                          "note": "compulsory bytes only; the path is bound by the FP32/FP64 pipes, see fp_pipe"},
             "fp_pipe": {"achieved_tflops": fp_tflops, "flop_per_launch": flop,
-                        "fp32_nominal_tflops": 74.4, "fp64_nominal_tflops": 37.2,
-                        "note": "algorithmic flop = sum over matrices of sweeps x nt(nt-1)/2 (12 mt + 6 nt)"},
+                        "measured_peaks": fp_peaks,
+                        "frac_of_measured_fp32": fp_tflops / fp_peaks["fp32_tflops"],
+                        "note": "algorithmic flop = sum over matrices of sweeps x nt(nt-1)/2 (12 mt + 6 nt), FP32 "
+                                "and FP64 sweeps together, against the measured FP32 peak"},
             "clocks": clocks.summary(), "gpu_launches": args.steps * plan.kernels_per_solve,
             "e2e": {"value": e2e_value, "unit": "matrices/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "api": "batch.StreamedUneven (8 chunks of cost 1:2:4:4:4:4:2:1, two compute streams, copies overlapped "
@@ -405,10 +560,10 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_cpu_baseline:
         rate, done, threads, el = cpu_port_sample(mats, seconds=args.ref_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": "matrices/s", "cores": threads, "kind": "port",
+                                "cpu": cpu_model(),
                                 "sample": f"first {done} of the 8192 matrices ({el:.1f} s), C restatement of the "
                                           "reference Jacobi (oracle/), fp32 like the reference"}
     print(json.dumps(line), flush=True)
-    del graph
 
 
 def _events():
@@ -735,6 +890,10 @@ def main():
     ap.add_argument("--workload", choices=("uneven_batch", "plain_single", "clustered_large", "tall_lowrank",
                                            "warm_family", "extensions"), default="uneven_batch")
     ap.add_argument("--precision", choices=("mixed", "fp32"), default="mixed")
+    ap.add_argument("--scaling", choices=("weak", "strong"), default="weak",
+                    help="weak: a batch of 8192 per GPU; strong: one batch of 8192 split across the GPUs by cost")
+    ap.add_argument("--no-reference-pytorch", action="store_true",
+                    help="reference arm: skip timing the reference's own PyTorch CPU Jacobi")
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--full-check", action="store_true")
@@ -743,9 +902,14 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("at least 3 warm-up steps")
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        # one process per GPU: start the ranks (the same command line under torchrun)
+        sys.exit(launch_ranks(args.gpus, Path(__file__).resolve(), sys.argv[1:]))
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if world != args.gpus:
+        ap.error(f"--gpus {args.gpus} but WORLD_SIZE is {world}: one rank per GPU")
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

@@ -49,6 +49,7 @@ extern "C" {
 #define JB_ST_NULL_FAILED   3   /* null completion failed (primitives.py:451-452)     */
 #define JB_ST_NONFINITE_OUT 4   /* NaN/Inf in an output (solvers.py:305-306)          */
 #define JB_ST_BAD_DESC      5   /* descriptor outside the launch's max sizes/flags    */
+#define JB_ST_TIMEOUT       6   /* a bounded wait inside a multi-CTA kernel ran out   */
 
 /* ---- flags ---------------------------------------------------------------- */
 #define JB_FULL_MATRICES    1   /* U is m x m and Vh is n x n (complete_basis)  */
@@ -385,6 +386,29 @@ JB_API int jb_svd_batched_c128(const void *A, void *U, double *S, void *Vh, int6
  * of an active pair in these rounds). */
 JB_API int jb_jacobi_rounds(void *W, void *V, int32_t dtype, int32_t m, int32_t n, int32_t round_begin,
                             int32_t round_end, double tol, double *off, void *stream);
+
+/* Null-space completion of U, svdbench/standalone/primitives.py:430-455
+ * (complete_null_columns; complete_basis :458-467 and _finish_columns,
+ * solvers.py:18-21, call it).  U: batch x m x n row-major device array of
+ * dtype 0 float32, 1 float64, 2 complex64, 3 complex128 (interleaved);
+ * keep: batch x n bytes (nonzero = keep the column).  In place, in
+ * ascending column order, every column not kept becomes the coordinate
+ * vector of largest leftover leverage 1 - sum_c |u_ic|^2, projected out
+ * against the kept and already completed columns, normalised; a projected
+ * length below 10 eps of the dtype sets status[z] = JB_ST_NULL_FAILED
+ * (primitives.py:451-452).  status[z] is written for every matrix.
+ * n <= 8192; workspace of jb_complete_null_workspace_bytes bytes. */
+JB_API size_t jb_complete_null_workspace_bytes(int32_t dtype, int64_t batch, int64_t m, int64_t n);
+JB_API int jb_complete_null(void *U, const uint8_t *keep, int32_t dtype, int64_t batch, int64_t m, int64_t n,
+                            int32_t *status, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Measurement kernel for the rooflines of the FP32/FP64 Jacobi kernels (no
+ * counterpart in the reference): `blocks` CTAs of 256 threads, each thread
+ * 16 independent fused multiply-add chains of `iters` steps; mode 0 FP32
+ * (fma.rn.f32), 1 packed FP32 (fma.rn.f32x2), 2 FP64.  jb_fma_loop_flops
+ * gives the launch's flops (2 per multiply-add) for timing it. */
+JB_API double jb_fma_loop_flops(int32_t blocks, int32_t iters);
+JB_API int jb_fma_loop(int32_t mode, int32_t blocks, int32_t iters, float *sink, void *stream);
 
 /* Size of the fixed device scratch array of jb_svd_batched_f32_noalloc. */
 #define JB_NOALLOC_SCRATCH_BYTES (16u << 20)

@@ -47,9 +47,37 @@ def pack(mats, device=None, dtype=np.float32):
 def cost_order(m, n):
     """Processing order, largest estimated cost first (LPT on the persistent
     grid): one sweep of one-sided Jacobi on the tall view costs ~ nt^2 (7 mt + 4 nt)."""
+    return np.argsort(-matrix_cost(np.asarray(m), np.asarray(n)), kind="stable").astype(np.int32)
+
+
+def matrix_cost(m, n):
+    """Estimated cost of one matrix: one sweep of one-sided Jacobi on the tall
+    view costs ~ nt^2 (7 mt + 4 nt) (the sweep count varies little)."""
     mt, nt = np.maximum(m, n), np.minimum(m, n)
-    cost = nt.astype(np.float64) ** 2 * (7 * mt + 4 * nt)
-    return np.argsort(-cost, kind="stable").astype(np.int32)
+    return nt.astype(np.float64) ** 2 * (7 * mt + 4 * nt)
+
+
+def shard_by_cost(m, n, parts):
+    """Split one uneven batch into `parts` shards of about equal cost, for
+    solving it on several devices with no exchange between them: the
+    cost-ordered work list (cost_order, largest first) is dealt greedily,
+    every matrix to the shard with the least cost so far (LPT, within one
+    matrix's cost of the best split).  Returns `parts` sorted index arrays;
+    every matrix is in exactly one shard."""
+    import heapq
+    parts = int(parts)
+    if parts < 1:
+        raise ValueError("parts must be >= 1")
+    m = np.asarray(m, np.int64)
+    n = np.asarray(n, np.int64)
+    cost = matrix_cost(m, n)
+    heap = [(0.0, p) for p in range(parts)]
+    owner = np.empty(len(m), np.int64)
+    for i in cost_order(m, n):
+        load, p = heapq.heappop(heap)
+        owner[i] = p
+        heapq.heappush(heap, (load + float(cost[i]), p))
+    return [np.flatnonzero(owner == p) for p in range(parts)]
 
 
 class Launch:
@@ -330,6 +358,66 @@ class StreamedUneven:
     def device_bytes_per_run(self):
         """Bytes copied host->device and device->host by one run."""
         return 4 * self.a_total, 4 * (self.u_total + self.s_total + self.v_total) + 8 * self.count
+
+
+class ShardedUneven:
+    """One uneven batch solved on several devices at once.
+
+    The batch is split by shard_by_cost into one share per device; each
+    device gets an UnevenBatch over its share and solves it on its own
+    current stream.  Nothing is exchanged between devices: every device reads
+    its own inputs and writes its own outputs, and the host only gathers
+    them.  One host thread enqueues every device's launch (they are
+    asynchronous), so the devices run concurrently."""
+
+    def __init__(self, m, n, devices, *, tol=None, max_sweeps=60, precision="mixed", values_only=False,
+                 launch=None):
+        self.m = np.asarray(m, np.int64)
+        self.n = np.asarray(n, np.int64)
+        self.count = len(self.m)
+        self.devices = [torch.device(d) for d in devices]
+        if not self.devices:
+            raise ValueError("at least one device")
+        self.shards = shard_by_cost(self.m, self.n, len(self.devices))
+        self.max_sweeps = int(max_sweeps)
+        self.plans = [UnevenBatch(self.m[idx], self.n[idx], dev, tol=tol, max_sweeps=max_sweeps,
+                                  precision=precision, values_only=values_only, launch=launch)
+                      if len(idx) else None for idx, dev in zip(self.shards, self.devices)]
+        self.where = np.empty((self.count, 2), np.int64)      # matrix -> (shard, index in shard)
+        for p, idx in enumerate(self.shards):
+            self.where[idx, 0] = p
+            self.where[idx, 1] = np.arange(len(idx))
+
+    def pack(self, mats):
+        """Per-device flat inputs (float32) of a list of host matrices."""
+        flats = []
+        for idx, dev, plan in zip(self.shards, self.devices, self.plans):
+            if plan is None:
+                flats.append(None)
+                continue
+            flat, _, _, _ = pack([mats[i] for i in idx])
+            flats.append(flat.pin_memory().to(dev, non_blocking=True))
+        return flats
+
+    def launch(self, flats):
+        """Enqueue every device's solve on that device's current stream."""
+        for plan, flat, dev in zip(self.plans, flats, self.devices):
+            if plan is not None:
+                with torch.cuda.device(dev):
+                    plan.launch(flat)
+
+    def check(self):
+        """Synchronise every device; raise for any failed matrix; return the
+        sweep counts in the batch's order."""
+        sweeps = np.zeros(self.count, np.int32)
+        for idx, plan in zip(self.shards, self.plans):
+            if plan is not None:
+                sweeps[idx] = plan.check()
+        return sweeps
+
+    def result(self, i):
+        p, j = self.where[i]
+        return self.plans[p].result(int(j))
 
 
 REGISTER_ROWS, REGISTER_COLS = 128, 64   # tall-view limits of the register kernels

@@ -27,7 +27,8 @@ off <= tol_phase1 (the reference's 40 eps32, solvers.py:41,55-57).
 
 Finish: V orthogonalised again, W = A V with FP64 accumulation, sigma =
 column norms in FP64, sorted descending, values below eps32 * max(m, n) *
-sigma_1 reported as 0 (solvers.py:18-21, 61-66).  With V orthogonal to ~1e-6
+sigma_1 reported as 0 and their U columns replaced by the reference's null
+completion (solvers.py:18-21, 61-66; jb_complete_null).  With V orthogonal to ~1e-6
 and W's columns orthogonal to ~tol_phase1, every sigma above the cut keeps a
 relative error of a few 1e-6.
 """
@@ -279,8 +280,12 @@ class BlockJacobi:
         N.check(lib.jb_block_finish(wt.data_ptr(), vt.data_ptr(), U.data_ptr(), S.data_ptr(), Vh.data_ptr(),
                                     sig.data_ptr(), perm.data_ptr(), self.mpad, self.npad, n, e, max(m, n), st),
                 "jb_block_finish")
+        # Columns of cut sigma: the reference's completion vectors (_finish_columns,
+        # solvers.py:18-21 -> primitives.py:430-455), on the device.
+        from .solvers import _complete_null_columns
+        U = _complete_null_columns(U[:m][None], (S > 0)[None])[0]
         info = {"algorithm": "block_jacobi", "block_sweeps": sweeps, "off_per_sweep": off_hist,
                 "converged": converged, "reached_tol": off_hist[-1][0] <= tol_phase1,
                 "precision": "tensor-core sweeps (3xBF16 then 6xBF16) with FP64 block eigen-solves; "
                              "6xBF16 Newton-Schulz V, FP64-accumulated W = A V"}
-        return U[:m], S, Vh[:, :n].contiguous(), info
+        return U, S, Vh[:, :n].contiguous(), info

@@ -20,7 +20,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIBDIR = PKG / "_lib"
 LIBNAME = "libjacobi_b200.so"
-SOURCES = ["jb_batched.cu", "jb_tensor.cu", "jb_mlp.cu", "jb_block.cu", "jb_eigh.cu", "jb_qr.cu", "jb_complex.cu", "jb_lab.cu"]
+SOURCES = ["jb_batched.cu", "jb_tensor.cu", "jb_mlp.cu", "jb_block.cu", "jb_eigh.cu", "jb_qr.cu", "jb_complex.cu", "jb_lab.cu", "jb_null.cu", "jb_peak.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1,0 +1,526 @@
+// jb_null.cu - null-space completion of U on the GPU
+// (svdbench/standalone/primitives.py:430-455, complete_null_columns; used by
+// complete_basis :458-467 and by _finish_columns, solvers.py:18-21).
+//
+// For every matrix of a batch U (batch x m x n, row-major) and its keep mask
+// (batch x n bytes): the columns not kept are replaced, in ascending column
+// order, by unit vectors orthogonal to all columns before them.  Per missing
+// column, as the reference: idx = the first row of largest leftover leverage
+// 1 - sum_c |u_ic|^2 (over the kept and the already completed columns),
+// v = e_idx projected out against those columns, v / ||v||; ||v|| < 10 eps
+// of the dtype fails the matrix (JB_ST_NULL_FAILED, primitives.py:451-452).
+//
+// B200 form.  The columns that count (kept, then completed ones in the order
+// they are made) are packed into a work matrix X (m x a, row stride n), so
+// every product reads a contiguous row prefix.  U^H e_idx is row idx of X,
+// so the first projection is row-local: v_i = delta_{i,idx} - X_i . conj(X_idx).
+// The leverage is kept per row in FP64 and lowered by |v_i|^2 after each new
+// column; products accumulate in FP64 (complex: FP64 pairs).
+//   * Many matrices (team of one CTA per matrix): the second projection
+//     always runs, as in the reference.
+//   * Few large matrices: one team of CTAs (about one per SM, cooperative
+//     launch, rows split evenly) handles one matrix after another, with two
+//     grid-wide barriers per column.  The second projection runs when the
+//     first left ||v||^2 < 1/2 (Kahan-Parlett "twice is enough": otherwise
+//     v is already orthogonal to the columns to working accuracy).
+// Every barrier wait is bounded (about two seconds of globaltimer); a wait
+// that runs out marks the team's matrix JB_ST_TIMEOUT and the CTAs return.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <math.h>
+#include "jacobi_b200.h"
+
+namespace jb {
+namespace nul {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr unsigned long long kWaitNs = 2000000000ull;
+
+struct cf { float x, y; };
+struct cd { double x, y; };
+
+// Element traits: storage type S, FP64 accumulation type A.
+template <typename S> struct Tr;
+template <> struct Tr<float> {
+    using A = double;
+    static constexpr bool cplx = false;
+    static constexpr double eps = 1.1920928955078125e-07;
+    __device__ static A zero() { return 0.0; }
+    __device__ static A ld(const float *p) { return (double)*p; }
+    __device__ static A ldcg(const float *p) { return (double)__ldcg(p); }
+    __device__ static void st(float *p, A v) { *p = (float)v; }
+    __device__ static A fma_(A acc, A x, A y) { return fma(x, y, acc); }
+    __device__ static double norm2(A x) { return x * x; }
+    __device__ static A scale(A x, double s) { return x * s; }
+    __device__ static A sub(A x, A y) { return x - y; }
+    __device__ static A add(A x, A y) { return x + y; }
+    __device__ static A conj(A x) { return x; }
+    __device__ static A ldcgA(const A *p) { return __ldcg(p); }
+    __device__ static A unit() { return 1.0; }
+    __device__ static A shfl_sum(A v) {
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        return v;
+    }
+};
+template <> struct Tr<double> {
+    using A = double;
+    static constexpr bool cplx = false;
+    static constexpr double eps = 2.220446049250313e-16;
+    __device__ static A zero() { return 0.0; }
+    __device__ static A ld(const double *p) { return *p; }
+    __device__ static A ldcg(const double *p) { return __ldcg(p); }
+    __device__ static void st(double *p, A v) { *p = v; }
+    __device__ static A fma_(A acc, A x, A y) { return fma(x, y, acc); }
+    __device__ static double norm2(A x) { return x * x; }
+    __device__ static A scale(A x, double s) { return x * s; }
+    __device__ static A sub(A x, A y) { return x - y; }
+    __device__ static A add(A x, A y) { return x + y; }
+    __device__ static A conj(A x) { return x; }
+    __device__ static A ldcgA(const A *p) { return __ldcg(p); }
+    __device__ static A unit() { return 1.0; }
+    __device__ static A shfl_sum(A v) {
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        return v;
+    }
+};
+template <typename S, typename R> struct TrC {
+    using A = cd;
+    static constexpr bool cplx = true;
+    __device__ static A zero() { return {0.0, 0.0}; }
+    __device__ static A ld(const S *p) { return {(double)p->x, (double)p->y}; }
+    __device__ static A ldcg(const S *p) {
+        const R *q = (const R *)p;
+        return {(double)__ldcg(q), (double)__ldcg(q + 1)};
+    }
+    __device__ static void st(S *p, A v) { p->x = (R)v.x; p->y = (R)v.y; }
+    __device__ static A fma_(A acc, A x, A y) {                          // acc + x * y
+        return {fma(x.x, y.x, fma(-x.y, y.y, acc.x)), fma(x.x, y.y, fma(x.y, y.x, acc.y))};
+    }
+    __device__ static double norm2(A x) { return x.x * x.x + x.y * x.y; }
+    __device__ static A scale(A x, double s) { return {x.x * s, x.y * s}; }
+    __device__ static A sub(A x, A y) { return {x.x - y.x, x.y - y.y}; }
+    __device__ static A add(A x, A y) { return {x.x + y.x, x.y + y.y}; }
+    __device__ static A conj(A x) { return {x.x, -x.y}; }
+    __device__ static A ldcgA(const A *p) { return {__ldcg(&p->x), __ldcg(&p->y)}; }
+    __device__ static A unit() { return {1.0, 0.0}; }
+    __device__ static A shfl_sum(A v) {
+        for (int o = 16; o; o >>= 1) {
+            v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+            v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+        }
+        return v;
+    }
+};
+template <> struct Tr<cf> : TrC<cf, float> { static constexpr double eps = 1.1920928955078125e-07; };
+template <> struct Tr<cd> : TrC<cd, double> { static constexpr double eps = 2.220446049250313e-16; };
+
+struct Slot {            // one CTA's contribution to a team-wide reduction
+    double val;          // norm^2 partial, or the CTA's best leverage
+    int64_t idx;         // row of the best leverage (first on ties)
+};
+
+struct Params {
+    void *U;
+    const uint8_t *keep;
+    int32_t *status;
+    int64_t batch, m, n;
+    unsigned char *ws;   // per-team areas of team_bytes each
+    size_t team_bytes;
+    int G;               // CTAs per team (1: every CTA is a team)
+    int always_reorth;
+};
+
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Team-wide barrier.  G == 1: the CTA barrier.  G > 1: a generation barrier
+// over the whole (co-resident, cooperative) grid with a bounded wait.
+// Returns false once any CTA of the team has given up waiting.
+__device__ __forceinline__ bool team_sync(unsigned *bar, int *err, int G) {
+    __syncthreads();
+    if (G == 1) return true;
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        volatile unsigned *vgen = bar + 1;
+        const unsigned gen = *vgen;
+        __threadfence();
+        const unsigned arrived = atomicAdd(bar, 1u);
+        int ok = 1;
+        if (arrived == (unsigned)G - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            const unsigned long long t0 = gtimer();
+            while (*vgen == gen) {
+                if (gtimer() - t0 > kWaitNs) {
+                    ok = 0;
+                    atomicExch(err, 1);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok && !*(volatile int *)err;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Best (largest val, then smallest idx) of the CTA's candidates; result in
+// thread 0.  `red` holds kWarps slots.
+__device__ __forceinline__ Slot cta_argmax(double best, int64_t bidx, Slot *red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int64_t oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+        if (ob > best || (ob == best && oi < bidx)) { best = ob; bidx = oi; }
+    }
+    if (lane == 0) red[warp] = {best, bidx};
+    __syncthreads();
+    Slot s = red[0];
+    if (threadIdx.x == 0)
+        for (int w = 1; w < kWarps; ++w)
+            if (red[w].val > s.val || (red[w].val == s.val && red[w].idx < s.idx)) s = red[w];
+    __syncthreads();
+    return s;
+}
+
+__device__ __forceinline__ double cta_sum(double v, double *red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < kWarps; ++w) s += red[w];
+    __syncthreads();
+    return s;
+}
+
+// Per-team workspace layout (byte offsets from the team's base).  X, the
+// packed columns, exists only for multi-CTA teams.
+struct Layout {
+    size_t x, lev, y, part, cmap, slots, bar, total;
+};
+__host__ __device__ inline size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+__host__ __device__ inline Layout layout(int64_t m, int64_t n, int esz, int asz, int G) {
+    Layout L;
+    size_t o = 0;
+    L.x = o;     o += G > 1 ? al256((size_t)m * n * esz) : 0;
+    L.lev = o;   o += al256((size_t)m * 8);
+    L.y = o;     o += al256((size_t)n * asz);
+    L.part = o;  o += G > 1 ? al256((size_t)G * n * asz) : 0;
+    L.cmap = o;  o += al256((size_t)n * 4);
+    L.slots = o; o += al256((size_t)2 * G * sizeof(Slot));
+    L.bar = o;   o += 256;
+    L.total = o;
+    return L;
+}
+
+// TEAM = false: one CTA per matrix, in place on U (the columns not yet
+// completed are zero, so every product runs over all n columns, as the
+// reference's u @ (u^H v) does; the new column is excluded from the second
+// projection).  TEAM = true: a cooperative team of G CTAs, the kept and
+// completed columns packed into X (row stride n), G > 1.
+template <typename S, bool TEAM>
+__global__ void __launch_bounds__(kThreads) null_kernel(Params p) {
+    using T = Tr<S>;
+    using A = typename T::A;
+    extern __shared__ __align__(16) unsigned char smem[];
+    S *rowc = (S *)smem;                                   // row idx of X
+    __shared__ Slot s_red[kWarps];
+    __shared__ double s_dred[kWarps];
+    __shared__ int s_flag;
+    const int G = TEAM ? p.G : 1;
+    const int g = TEAM ? blockIdx.x : 0;                   // rank in the team
+    const int64_t team = TEAM ? 0 : blockIdx.x;
+    const int64_t nteams = TEAM ? 1 : gridDim.x;
+    const int64_t m = p.m, n = p.n;
+    const Layout L = layout(m, n, sizeof(S), sizeof(A), G);
+    unsigned char *base = p.ws + team * p.team_bytes;
+    double *lev = (double *)(base + L.lev);
+    A *y = (A *)(base + L.y);
+    A *part = (A *)(base + L.part);
+    int *cmap = (int *)(base + L.cmap);
+    Slot *slots = (Slot *)(base + L.slots);                // [2][G]
+    unsigned *bar = (unsigned *)(base + L.bar);
+    int *err = (int *)(bar + 2);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t r0 = m * g / G, r1 = m * (g + 1) / G;   // this CTA's rows
+    // cross-CTA data is read through L2 (ld.global.cg): L1 is not coherent
+    auto ldx = [&](const S *q) -> A { return TEAM ? T::ldcg(q) : T::ld(q); };
+    int64_t z = team;
+    for (; z < p.batch; z += nteams) {
+        S *U = (S *)p.U + z * m * n;
+        S *X = TEAM ? (S *)(base + L.x) : U;
+        const uint8_t *keep = p.keep + z * n;
+        if (warp == 0) {                                   // kept columns in order (cmap), by ballots
+            int a = 0, miss = 0;
+            for (int64_t c0 = 0; c0 < n; c0 += 32) {
+                const int64_t c = c0 + lane;
+                const bool in = c < n, kp = in && keep[c] != 0;
+                const unsigned bk = __ballot_sync(0xffffffffu, kp);
+                if (TEAM && kp) cmap[a + __popc(bk & ((1u << lane) - 1u))] = (int)c;
+                a += __popc(bk);
+                miss += __popc(__ballot_sync(0xffffffffu, in && !kp));
+            }
+            if (lane == 0) s_flag = miss ? a : -1;
+        }
+        __syncthreads();
+        const int nkept = s_flag;
+        if (nkept < 0) {                                   // nothing to complete
+            if (g == 0 && threadIdx.x == 0) p.status[z] = JB_ST_OK;
+            continue;
+        }
+        // Zero U's missing columns (primitives.py:436), pack the kept ones
+        // (TEAM), leverage of every row of this CTA in FP64.
+        double best = -1e300;
+        int64_t bidx = 0;
+        for (int64_t i = r0 + warp; i < r1; i += kWarps) {
+            S *urow = U + i * n;
+            double acc = 0.0;
+            for (int64_t c = lane; c < n; c += 32) {
+                if (!keep[c]) T::st(urow + c, T::zero());
+                else acc += T::norm2(T::ld(urow + c));
+            }
+            if (TEAM)
+                for (int k = lane; k < nkept; k += 32) X[i * n + k] = urow[cmap[k]];
+            for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            const double lv = 1.0 - acc;
+            if (lane == 0) lev[i] = lv;
+            if (lv > best) { best = lv; bidx = i; }         // lanes agree; rows ascend
+        }
+        Slot sb = cta_argmax(best, bidx, s_red);
+        if (threadIdx.x == 0) slots[g] = sb;
+        if (!team_sync(bar, err, G)) goto timeout;
+        {
+            int a = nkept;                                 // packed columns (TEAM)
+            const int span = TEAM ? 0 : (int)n;            // columns a product runs over (in place)
+            bool failed = false;
+            for (int64_t c = 0; c < n; ++c) {
+                if (keep[c]) continue;
+                const int na = TEAM ? a : span;
+                const int64_t col = TEAM ? a : c;          // where v is built
+                // idx = team-wide first argmax of the leverage
+                Slot b = {-1e300, 0};
+                for (int q = 0; q < G; ++q) {
+                    Slot s;
+                    if (TEAM) { s.val = __ldcg(&slots[q].val); s.idx = __ldcg(&slots[q].idx); }
+                    else s = slots[q];
+                    if (s.val > b.val || (s.val == b.val && s.idx < b.idx)) b = s;
+                }
+                const int64_t idx = b.idx;
+                for (int k = threadIdx.x; k < na; k += kThreads) T::st(rowc + k, ldx(X + idx * n + k));
+                __syncthreads();
+                // first projection, row-local: v_i = delta - X_i . conj(X_idx)
+                // (column col of X is still zero in every row)
+                double pn2 = 0.0;
+                for (int64_t i = r0 + warp; i < r1; i += kWarps) {
+                    const S *xrow = X + i * n;
+                    A acc = T::zero();
+                    for (int k = lane; k < na; k += 32) acc = T::fma_(acc, T::ld(xrow + k), T::conj(T::ld(rowc + k)));
+                    acc = T::shfl_sum(acc);
+                    if (lane == 0) {
+                        T::st(X + i * n + col, T::sub(i == idx ? T::unit() : T::zero(), acc));
+                        pn2 += T::norm2(T::ld(X + i * n + col));
+                    }
+                }
+                double n2 = cta_sum(pn2, s_dred);
+                if (threadIdx.x == 0) slots[G + g].val = n2;
+                if (!team_sync(bar, err, G)) goto timeout;
+                n2 = 0.0;
+                for (int q = 0; q < G; ++q) n2 += TEAM ? __ldcg(&slots[G + q].val) : slots[G + q].val;
+                if (p.always_reorth || n2 < 0.5) {
+                    // second projection: y = X^H v (without v's own column), v -= X y
+                    A *yout = TEAM ? part + (size_t)g * n : y;
+                    for (int k = threadIdx.x; k < na; k += kThreads) {
+                        A acc = T::zero();
+                        if (k != col)
+                            for (int64_t i = r0; i < r1; ++i)
+                                acc = T::fma_(acc, T::conj(T::ld(X + i * n + k)), T::ld(X + i * n + col));
+                        yout[k] = acc;
+                    }
+                    if (TEAM) {
+                        // every CTA sums the partials of its slice of y
+                        if (!team_sync(bar, err, G)) goto timeout;
+                        const int64_t k0 = (int64_t)na * g / G, k1 = (int64_t)na * (g + 1) / G;
+                        for (int64_t k = k0 + threadIdx.x; k < k1; k += kThreads) {
+                            A acc = T::zero();
+                            for (int q = 0; q < G; ++q) acc = T::add(acc, T::ldcgA(part + (size_t)q * n + k));
+                            y[k] = acc;
+                        }
+                    }
+                    if (!team_sync(bar, err, G)) goto timeout;
+                    double pn2b = 0.0;
+                    for (int64_t i = r0 + warp; i < r1; i += kWarps) {
+                        const S *xrow = X + i * n;
+                        A acc = T::zero();
+                        for (int k = lane; k < na; k += 32)
+                            acc = T::fma_(acc, T::ld(xrow + k), TEAM ? T::ldcgA(y + k) : y[k]);
+                        acc = T::shfl_sum(acc);
+                        if (lane == 0) {
+                            T::st(X + i * n + col, T::sub(T::ld(X + i * n + col), acc));
+                            pn2b += T::norm2(T::ld(X + i * n + col));
+                        }
+                    }
+                    const double s2 = cta_sum(pn2b, s_dred);
+                    if (threadIdx.x == 0) slots[G + g].val = s2;
+                    if (!team_sync(bar, err, G)) goto timeout;
+                    n2 = 0.0;
+                    for (int q = 0; q < G; ++q) n2 += TEAM ? __ldcg(&slots[G + q].val) : slots[G + q].val;
+                }
+                const double len = sqrt(n2);
+                if (len < 10.0 * T::eps) {                 // primitives.py:451-452
+                    failed = true;
+                    break;
+                }
+                // normalise, lower the leverage, next argmax
+                const double inv = 1.0 / len;
+                best = -1e300;
+                bidx = 0;
+                for (int64_t i = r0 + threadIdx.x; i < r1; i += kThreads) {
+                    T::st(X + i * n + col, T::scale(T::ld(X + i * n + col), inv));
+                    const double lv = lev[i] - T::norm2(T::ld(X + i * n + col));
+                    lev[i] = lv;
+                    if (lv > best) { best = lv; bidx = i; }
+                }
+                sb = cta_argmax(best, bidx, s_red);
+                if (threadIdx.x == 0) {
+                    slots[g] = sb;
+                    if (TEAM && g == 0) cmap[a] = (int)c;
+                }
+                ++a;
+                if (!team_sync(bar, err, G)) goto timeout;
+            }
+            if (TEAM)                                      // completed columns back into U
+                for (int64_t i = r0 + warp; i < r1; i += kWarps)
+                    for (int k = nkept + lane; k < a; k += 32) U[i * n + __ldcg(&cmap[k])] = X[i * n + k];
+            if (g == 0 && threadIdx.x == 0) p.status[z] = failed ? JB_ST_NULL_FAILED : JB_ST_OK;
+            if (!team_sync(bar, err, G)) goto timeout;
+        }
+    }
+    return;
+timeout:
+    // a barrier wait ran out: this matrix and the team's later ones fail
+    if (threadIdx.x == 0 && g == 0)
+        for (; z < p.batch; z += nteams) p.status[z] = JB_ST_TIMEOUT;
+}
+
+struct Plan {
+    int G;
+    int64_t grid;
+    size_t team_bytes, bytes, smem;
+};
+
+static int esize(int dtype) { return dtype == 0 ? 4 : dtype == 1 ? 8 : dtype == 2 ? 8 : 16; }
+
+static int dev_sms() {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) return 148;
+    return sms;
+}
+
+// One CTA per matrix unless the batch has few large matrices: then one
+// cooperative team of about one CTA per SM (at least 16 rows each).
+static Plan make_plan(int dtype, int64_t batch, int64_t m, int64_t n) {
+    Plan pl;
+    const int sms = dev_sms();
+    const int esz = esize(dtype), asz = dtype >= 2 ? 16 : 8;
+    const bool large = batch * 4 < sms && m * n >= (1 << 16) && m >= 256;
+    if (large) {
+        int64_t G = m / 16;
+        if (G > sms) G = sms;
+        if (G < 2) G = 2;
+        pl.G = (int)G;
+        pl.grid = G;
+        pl.team_bytes = layout(m, n, esz, asz, pl.G).total;
+        pl.bytes = pl.team_bytes;
+    } else {
+        pl.G = 1;
+        int64_t grid = (int64_t)sms * 4;
+        if (grid > batch) grid = batch;
+        if (grid < 1) grid = 1;
+        pl.grid = grid;
+        pl.team_bytes = layout(m, n, esz, asz, 1).total;
+        pl.bytes = pl.team_bytes * (size_t)grid;
+    }
+    pl.smem = (size_t)n * esz;
+    return pl;
+}
+
+template <typename S>
+static int launch(Params &p, const Plan &pl, cudaStream_t st) {
+    p.G = pl.G;
+    p.team_bytes = pl.team_bytes;
+    p.always_reorth = pl.G == 1;
+    if (pl.G == 1) {
+        auto kern = null_kernel<S, false>;
+        if (pl.smem > 48 * 1024 &&
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem) != cudaSuccess)
+            return JB_ECUDA;
+        kern<<<(unsigned)pl.grid, kThreads, pl.smem, st>>>(p);
+        return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+    }
+    auto kern = null_kernel<S, true>;
+    if (pl.smem > 48 * 1024 &&
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem) != cudaSuccess)
+        return JB_ECUDA;
+    // the barrier words and the error flag start at zero
+    const Layout L = layout(p.m, p.n, sizeof(S), Tr<S>::cplx ? 16 : 8, pl.G);
+    if (cudaMemsetAsync(p.ws + L.bar, 0, 16, st) != cudaSuccess) return JB_ECUDA;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, pl.smem) != cudaSuccess)
+        return JB_ECUDA;
+    if ((int64_t)per_sm * dev_sms() < pl.grid) return JB_ETOOBIG;   // every CTA must be resident
+    void *args[] = {&p};
+    if (cudaLaunchCooperativeKernel((const void *)kern, dim3((unsigned)pl.grid), dim3(kThreads), args, pl.smem,
+                                    st) != cudaSuccess)
+        return JB_ECUDA;
+    return JB_OK;
+}
+
+}  // namespace nul
+}  // namespace jb
+
+using namespace jb::nul;
+
+extern "C" {
+
+size_t jb_complete_null_workspace_bytes(int32_t dtype, int64_t batch, int64_t m, int64_t n) {
+    if (dtype < 0 || dtype > 3 || batch < 0 || m < 1 || n < 1) return 0;
+    return make_plan(dtype, batch, m, n).bytes;
+}
+
+int jb_complete_null(void *U, const uint8_t *keep, int32_t dtype, int64_t batch, int64_t m, int64_t n,
+                     int32_t *status, void *workspace, size_t workspace_bytes, void *stream) {
+    if (!U || !keep || !status || dtype < 0 || dtype > 3 || batch < 0 || m < 1 || n < 1) return JB_EINVAL;
+    if (n > 8192 || m > ((int64_t)1 << 31) / n) return JB_ETOOBIG;
+    if (batch == 0) return JB_OK;
+    const Plan pl = make_plan(dtype, batch, m, n);
+    if (pl.smem > 227 * 1024) return JB_ETOOBIG;
+    if (!workspace || workspace_bytes < pl.bytes) return JB_EWORKSPACE;
+    Params p;
+    p.U = U;
+    p.keep = keep;
+    p.status = status;
+    p.batch = batch;
+    p.m = m;
+    p.n = n;
+    p.ws = (unsigned char *)workspace;
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (dtype) {
+        case 0: return launch<float>(p, pl, st);
+        case 1: return launch<double>(p, pl, st);
+        case 2: return launch<cf>(p, pl, st);
+        default: return launch<cd>(p, pl, st);
+    }
+}
+
+}  // extern "C"

@@ -14,7 +14,8 @@ from .build import library_path
 
 # Return codes and per-matrix status words (include/jacobi_b200.h).
 JB_OK, JB_EINVAL, JB_ETOOBIG, JB_EWORKSPACE, JB_ECUDA = 0, 1, 2, 3, 4
-ST_OK, ST_NOT_CONVERGED, ST_NONFINITE_IN, ST_NULL_FAILED, ST_NONFINITE_OUT, ST_BAD_DESC = 0, 1, 2, 3, 4, 5
+ST_OK, ST_NOT_CONVERGED, ST_NONFINITE_IN, ST_NULL_FAILED, ST_NONFINITE_OUT, ST_BAD_DESC, ST_TIMEOUT = (
+    0, 1, 2, 3, 4, 5, 6)
 FULL_MATRICES, VALUES_ONLY, ROUND_ROBIN, BLOCK_WIDTH_8 = 1, 2, 4, 8
 PREC_NATIVE, PREC_MIXED = 0, 1
 
@@ -31,6 +32,7 @@ SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_bat
            "jb_eigh_f64", "jb_eigh_complex_workspace_bytes", "jb_eigh_c64", "jb_eigh_c128",
            "jb_qr_workspace_bytes", "jb_qr_f32", "jb_qr_f64", "jb_qr_c64", "jb_qr_c128",
            "jb_svd_complex_workspace_bytes", "jb_svd_batched_c64", "jb_svd_batched_c128", "jb_jacobi_rounds",
+           "jb_complete_null_workspace_bytes", "jb_complete_null", "jb_fma_loop_flops", "jb_fma_loop",
            "jb_svd_batched_f32_noalloc")
 GEMM_PLAIN, GEMM_SPLIT3, GEMM_SPLIT6, GEMM_B_MN, GEMM_CHAIN128, GEMM_SYRK = 0, 1, 2, 4, 8, 16
 NOALLOC_SCRATCH_BYTES = 16 << 20  # JB_NOALLOC_SCRATCH_BYTES
@@ -119,6 +121,14 @@ def _declare(l):
         f = getattr(l, name)
         f.restype = ctypes.c_int
         f.argtypes = args
+    l.jb_complete_null_workspace_bytes.restype = SZ
+    l.jb_complete_null_workspace_bytes.argtypes = [I32, I64, I64, I64]
+    l.jb_complete_null.restype = ctypes.c_int
+    l.jb_complete_null.argtypes = [P, P, I32, I64, I64, I64, P, P, SZ, P]
+    l.jb_fma_loop_flops.restype = F64
+    l.jb_fma_loop_flops.argtypes = [I32, I32]
+    l.jb_fma_loop.restype = ctypes.c_int
+    l.jb_fma_loop.argtypes = [I32, I32, I32, P, P]
     l.jb_svd_batched_f32_noalloc.restype = ctypes.c_int
     l.jb_svd_batched_f32_noalloc.argtypes = [P, P, P, P, I64, I32, I32, I32, I32, F64, I32, I32, P, P, P]
     return l

@@ -3,7 +3,8 @@ the group tournament and its bucketing by column count, the gather / solve /
 scatter of a round's pair subproblems, the convergence test, the sort and
 the cut.  The pair solves, which run on the GPU in the product, are done
 here by the NumPy oracle's jacobi_svd (the reference's inner solver,
-primitives.py:316-367) on the batched subproblems, so the engine must
+primitives.py:316-367) on the batched subproblems, and the null completion
+by the oracle's complete_null_columns, so the engine must
 reproduce the reference's own block_jacobi runs (golden fixtures): sigma
 within sigma_tol, block sweeps within one.  (LAPACK is no stand-in: its V
 leaves the columns correlated at ~1e-14, above the 40 eps the block
@@ -21,6 +22,12 @@ from oracle import jacobi_oracle as O
 
 def _mods():
     return importlib.import_module("pavel-s_svd_b200.block_rounds"), importlib.import_module("pavel-s_svd_b200.solvers")
+
+
+def _oracle_complete(u, keep):
+    """The oracle's null completion (primitives.py:430-455) on CPU tensors:
+    the product's runs on the GPU (jb_complete_null)."""
+    return torch.from_numpy(O.complete_null_columns(np.ascontiguousarray(u.resolve_conj().numpy()), keep.numpy()))
 
 
 def _oracle_pairs(y):
@@ -55,7 +62,7 @@ def test_rounds_engine_matches_reference_runs():
         x = torch.from_numpy(a.reshape(-1, *a.shape[-2:]).copy())
         stats = {}
         opts = dict(g["kw"])
-        u, s, v = BR.raw(x, stats, opts, _oracle_pairs, lambda: None, S._complete_null_columns)
+        u, s, v = BR.raw(x, stats, opts, _oracle_pairs, lambda: None, _oracle_complete)
         s = s.numpy().reshape(g["s"].shape)
         dt = a.dtype
         k = s.shape[-1]
@@ -75,10 +82,10 @@ def test_rounds_engine_errors():
     BR, S = _mods()
     x = torch.randn(2, 20, 12, dtype=torch.float64)
     with pytest.raises(RuntimeError, match="block Jacobi did not converge"):
-        BR.raw(x, {}, {"block_size": 3, "max_sweeps": 1}, _oracle_pairs, lambda: None, S._complete_null_columns)
+        BR.raw(x, {}, {"block_size": 3, "max_sweeps": 1}, _oracle_pairs, lambda: None, _oracle_complete)
     calls = []
-    BR.raw(x, {}, {"block_size": 3}, _oracle_pairs, lambda: calls.append(1), S._complete_null_columns)
+    BR.raw(x, {}, {"block_size": 3}, _oracle_pairs, lambda: calls.append(1), _oracle_complete)
     assert len(calls) >= 2                          # status words checked once per block sweep
     u, s, v = BR.raw(torch.zeros(0, 20, 12, dtype=torch.float64), {}, {"block_size": 3}, _oracle_pairs,
-                     lambda: None, S._complete_null_columns)
+                     lambda: None, _oracle_complete)
     assert u.shape == (0, 20, 12) and s.shape == (0, 12) and v.shape == (0, 12, 12)

@@ -199,3 +199,63 @@ def test_block_jacobi_rounds_contract(pkg):
         k = min(shape[-2:])
         assert u.shape == (*shape[:-2], shape[-2], k) and s.shape == (*shape[:-2], k)
         assert vh.shape == (*shape[:-2], k, shape[-1])
+
+
+@pytest.mark.parametrize("name,b", [("clustered_large", 32), ("tall_lowrank", 64)])
+def test_configured_sizes_against_lapack(pkg, name, b):
+    """The two blocked configurations at their full sizes through the drop-in
+    svd(a, 'block_jacobi', block_size=b): 4096 x 1024 with 64 clusters of 16
+    values (cond 1e6), and 8192 x 2048 rank 64 plus N(0, 1e-6) noise.
+
+    The reference zeroes sigma <= cut = eps32 * max(m, n) * sigma_1 and
+    completes those U columns (solvers.py:18-21).  Bounds, against SciPy
+    FP64 gesdd of the same float32 input:
+      * resolved values (sigma > 2 cut): relative error <= 1e-5;
+      * values below cut / 2 are reported as 0, every reported value is
+        within 1e-5 sigma_1 of the truth;
+      * |V^T V - I| <= 2e-5;
+      * U (kept and completed columns): |U^T U - I| <= max(2e-5,
+        2e-7 sigma_1 / sigma_min kept), the FP32-level error of the
+        smallest kept column's direction;
+      * ||A - U S V^T|| / ||A|| within 2e-5 of the cut values' own share;
+      * the completed columns are the oracle's completion of the kept ones
+        (first 40 missing columns, FP64 oracle: same pivots, 1e-5)."""
+    import scipy.linalg
+    from oracle import jacobi_oracle as O
+    wl = importlib.import_module("pavel-s_svd_b200.workloads")
+    a_np = getattr(wl, name)()
+    m, n = a_np.shape
+    a = torch.from_numpy(a_np).cuda()
+    u, s, vh, info = pkg.svd(a, 'block_jacobi', block_size=b, return_info=True)
+    assert info['block_size_used'] == b and info['converged']
+    sr = scipy.linalg.svd(a_np.astype(np.float64), compute_uv=False, lapack_driver="gesdd")
+    s_np = s.cpu().numpy().astype(np.float64)
+    cut = np.finfo(np.float32).eps * max(m, n) * sr[0]
+    res = sr > 2 * cut
+    assert res.sum() >= 64
+    rel = np.abs(s_np[res] - sr[res]) / sr[res]
+    assert float(rel.max()) <= 1e-5, float(rel.max())
+    assert bool((s_np[sr < cut / 2] == 0).all())
+    rep = s_np > 0
+    assert float(np.abs(s_np[rep] - sr[rep]).max()) <= 1e-5 * sr[0]
+    u64, vh64, a64 = u.double(), vh.double(), a.double()
+    eye = torch.eye(n, dtype=torch.float64, device="cuda")
+    assert float((vh64 @ vh64.T - eye).abs().max()) <= 2e-5
+    smin_kept = float(s_np[rep].min())
+    ou = float((u64.T @ u64 - eye).abs().max())
+    assert ou <= max(2e-5, 2e-7 * sr[0] / smin_kept), ou
+    s64 = torch.from_numpy(s_np).cuda()
+    rec = float((a64 - (u64 * s64) @ vh64).norm() / a64.norm())
+    cut_share = float(np.sqrt((sr[~rep] ** 2).sum()) / np.sqrt((sr ** 2).sum()))
+    assert rec <= cut_share + 2e-5, (rec, cut_share)
+    # completion parity: the oracle's completion of the kept columns
+    miss = np.flatnonzero(~rep)
+    assert len(miss) > 0
+    cols = np.concatenate([np.flatnonzero(rep), miss[:40]])
+    cols.sort()
+    sub = u.cpu().numpy().astype(np.float64)[:, cols]
+    keep_sub = rep[cols]
+    want = O.complete_null_columns(sub[None], keep_sub[None])[0]
+    got = sub
+    assert np.array_equal(np.abs(got[:, ~keep_sub]).argmax(0), np.abs(want[:, ~keep_sub]).argmax(0))
+    assert float(np.abs(got[:, ~keep_sub] - want[:, ~keep_sub]).max()) <= 1e-5

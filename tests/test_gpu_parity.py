@@ -223,6 +223,42 @@ def test_uneven_batch_mixed_meets_bound_and_graph_replay(pkg, workloads):
     del g
 
 
+def test_uneven_batch_full_workload(pkg, workloads):
+    """All 8192 matrices of the uneven-batch benchmark workload (n ~ U[8, 64],
+    m ~ U[n, 2n], seed 1): the mixed solve meets sigma-rel-err <= 1e-5 against
+    FP64 LAPACK on every matrix, with reconstruction <= 1e-6; the fp32 solve
+    (the reference's arithmetic) agrees with the C oracle of the reference's
+    FP32 Jacobi within sigma_tol on every matrix."""
+    mats = workloads.uneven_batch(8192)
+    B, flat, m, n, plan = _plan(pkg, mats, "mixed")
+    plan.launch(flat)
+    plan.check()
+    S, U, Vh = plan.S.cpu().numpy(), plan.U.cpu().numpy(), plan.Vh.cpu().numpy()
+    worst, worst_rec = 0.0, 0.0
+    for i in range(len(mats)):
+        k = min(m[i], n[i])
+        s = S[plan.s_off[i]:plan.s_off[i] + k]
+        worst = max(worst, mixed_bound(mats[i], s))
+        u = U[plan.u_off[i]:plan.u_off[i] + m[i] * k].reshape(m[i], k).astype(np.float64)
+        vh = Vh[plan.v_off[i]:plan.v_off[i] + k * n[i]].reshape(k, n[i]).astype(np.float64)
+        a = mats[i].astype(np.float64)
+        worst_rec = max(worst_rec, float(np.linalg.norm(a - (u * s) @ vh) / np.linalg.norm(a)))
+    assert worst <= 1e-5, worst
+    assert worst_rec <= 1e-6, worst_rec
+    B, flat, m, n, plan32 = _plan(pkg, mats, "fp32")
+    plan32.launch(flat)
+    plan32.check()
+    desc = np.frombuffer(plan32.desc.cpu().numpy().tobytes(), B.DESC_DTYPE)
+    _, s_o, _, _, st_o = C.svd_uneven(flat.cpu().numpy(), desc)
+    assert (st_o == 0).all()
+    S32 = plan32.S.cpu().numpy()
+    for i in range(len(mats)):
+        k = min(m[i], n[i])
+        so = desc["s_off"][i]
+        ref = s_o[so:so + k].astype(np.float64)
+        assert np.abs(S32[so:so + k] - ref).max() / ref[0] <= sigma_tol(np.float32), i
+
+
 def test_svd_uneven_list_api(pkg, workloads):
     """The list API, with matrices beyond the register kernels mixed in (a
     300 x 20, a 20 x 300, a 100 x 100): those go through svd() one by one,

@@ -33,6 +33,19 @@ out["shapes"] = [list(a.shape) for a in mats[:8]]
 digests = [None] * world
 dist.all_gather_object(digests, out["digest"])
 out["all_digests"] = digests
+# strong scaling: each rank's cost-balanced share of the one seed-1 batch
+import importlib
+B = importlib.import_module("pavel-s_svd_b200.batch")
+full = bench.load_matrices(0)
+fm = np.array([a.shape[0] for a in full]); fn = np.array([a.shape[1] for a in full])
+share = B.shard_by_cost(fm, fn, world)[rank]
+mine = bench.load_matrices(rank, world, "strong")
+out["share_same_matrices"] = all(np.array_equal(full[i], a) for i, a in zip(share, mine))
+out["share_cost"] = float(B.matrix_cost(fm[share], fn[share]).sum())
+out["total_cost"] = float(B.matrix_cost(fm, fn).sum())
+shares = [None] * world
+dist.all_gather_object(shares, share.tolist())
+out["all_shares"] = shares
 # the reference arm: rank 0 alone works and prints
 class A: warmup = 3; steps = 1; ref_seconds = 0.2
 if rank != 0:
@@ -71,3 +84,42 @@ def test_two_gloo_ranks_shard_and_reduce():
     assert results[0]["all_digests"] == results[1]["all_digests"]
     assert results[0]["digest"] != results[1]["digest"]
     assert results[1]["reference_returned"] is True
+    # strong scaling: every matrix exactly once over the ranks, costs balanced
+    got = sorted(results[0]["all_shares"][0] + results[0]["all_shares"][1])
+    assert got == list(range(8192))
+    assert all(r["share_same_matrices"] for r in results)
+    costs = [r["share_cost"] for r in results]
+    assert abs(sum(costs) - results[0]["total_cost"]) <= 1e-6 * results[0]["total_cost"]
+    assert max(costs) / min(costs) <= 1.001
+
+
+RANK_SCRIPT = r"""
+import datetime, json, os, torch.distributed as dist
+dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+t = __import__("torch").tensor([float(dist.get_rank() + 1)])
+dist.all_reduce(t)
+print("RANK " + json.dumps({"rank": dist.get_rank(), "world": dist.get_world_size(),
+                            "local": int(os.environ["LOCAL_RANK"]), "sum": float(t)}), flush=True)
+dist.destroy_process_group()
+"""
+
+
+def test_bench_starts_one_rank_per_gpu(tmp_path):
+    """bench.py --gpus N without a torchrun environment starts N ranks
+    through bench.launch_ranks (torch.distributed.run on 127.0.0.1, one
+    process per GPU); here the launched script is a two-rank gloo job."""
+    sys.path.insert(0, str(ROOT))
+    import bench
+    cmd = bench.rank_command(4, "x.py", ["--gpus", "4"], 29999)
+    assert cmd[1:3] == ["-m", "torch.distributed.run"] and "--nproc-per-node=4" in cmd
+    assert "--master-addr=127.0.0.1" in cmd and cmd[-3:] == ["x.py", "--gpus", "4"]
+    script = tmp_path / "ranks.py"
+    script.write_text(RANK_SCRIPT)
+    out = subprocess.run([sys.executable, "-c", f"import sys; sys.path.insert(0, {str(ROOT)!r}); import bench; "
+                          f"sys.exit(bench.launch_ranks(2, {str(script)!r}, [], timeout=200))"],
+                         capture_output=True, text=True, timeout=240,
+                         env=dict(os.environ, OMP_NUM_THREADS="1"))
+    assert out.returncode == 0, out.stderr[-2000:]
+    ranks = sorted((json.loads(x[5:]) for x in out.stdout.splitlines() if x.startswith("RANK ")),
+                   key=lambda r: r["rank"])
+    assert [(r["rank"], r["world"], r["local"], r["sum"]) for r in ranks] == [(0, 2, 0, 3.0), (1, 2, 1, 3.0)]
