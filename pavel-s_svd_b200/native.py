@@ -27,7 +27,7 @@ SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_bat
            "jb_svd_batched_f64", "jb_uneven_workspace_bytes", "jb_svd_uneven_f32", "jb_svd_uneven_f32_ex",
            "jb_gemm_bf16", "jb_gemm_bf16x", "jb_gemm_bf16x_rows", "jb_split_bf16", "jb_split3_bf16",
            "jb_warm_prep_f32", "jb_svd_warm_f32", "jb_transpose_bf16", "jb_bias_act", "jb_relu_backward",
-           "jb_col_sum", "jb_mse_grad", "jb_adam", "jb_gram_sketch", "jb_block_eig_f64", "jb_rows_scatter",
+           "jb_col_sum", "jb_mse_grad", "jb_adam", "jb_gram_sketch", "jb_block_eig_f64", "jb_block_eig_f64_ex", "jb_rows_scatter",
            "jb_rows_combine", "jb_gemm_f64acc", "jb_block_finish", "jb_eigh_workspace_bytes", "jb_eigh_f32",
            "jb_eigh_f64", "jb_eigh_complex_workspace_bytes", "jb_eigh_c64", "jb_eigh_c128",
            "jb_qr_workspace_bytes", "jb_qr_f32", "jb_qr_f64", "jb_qr_c64", "jb_qr_c128",
@@ -114,6 +114,7 @@ def _declare(l):
                        ("jb_adam", [P, P, P, P, P, P, I64, I64, FL, FL, FL, FL, I32, P]),
                        ("jb_gram_sketch", [P, P, I64, I32, I32, P]),
                        ("jb_block_eig_f64", [P, P, P, P, P, P, P, I64, I32, I32, F64, P, P]),
+                       ("jb_block_eig_f64_ex", [P, P, P, P, P, P, P, I64, I32, I32, F64, P, I32, P]),
                        ("jb_rows_scatter", [P, P, P, P, P, P, I64, I64, P]),
                        ("jb_rows_combine", [P, P, P, P, P, I64, I64, P]),
                        ("jb_gemm_f64acc", [P, P, P, I64, I64, I64, I64, I64, I64, P]),

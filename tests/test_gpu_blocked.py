@@ -89,6 +89,37 @@ def test_block_eig_f64(n):
     assert 0.0 < float(off.min())
 
 
+@pytest.mark.parametrize("n", [64, 128])
+@pytest.mark.parametrize("sweeps", [1, 2])
+def test_block_eig_cluster_equals_register_kernel(n, sweeps):
+    """The cluster eigen-solve (one cluster of 8 CTAs per slot, distributed
+    shared memory) runs the register kernel's rotations: the same Q^T parts,
+    off, dmax, bit for bit, on graded Grams."""
+    N = importlib.import_module("pavel-s_svd_b200.native")
+    g = torch.Generator(device="cuda").manual_seed(n + sweeps)
+    P = 16
+    x = torch.randn(P, n, 2 * n, device="cuda", generator=g, dtype=torch.float64)
+    x = x * torch.logspace(0, -4, n, device="cuda", dtype=torch.float64)[:, None]
+    G = (x @ x.transpose(1, 2)).float().contiguous()
+    live = torch.full((1,), 1e-12, dtype=torch.float64, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    outs = []
+    for variant in (1, 2):
+        qt = [torch.full((P, n, n), 7.0, dtype=torch.bfloat16, device="cuda") for _ in range(3)]
+        off = torch.zeros(P, device="cuda")
+        dmax = torch.zeros(P, device="cuda")
+        sw = torch.zeros(P, dtype=torch.int32, device="cuda")
+        N.check(N.lib().jb_block_eig_f64_ex(G.data_ptr(), qt[0].data_ptr(), qt[1].data_ptr(), qt[2].data_ptr(),
+                                            off.data_ptr(), dmax.data_ptr(), sw.data_ptr(), P, n, sweeps, 1e-7,
+                                            live.data_ptr(), variant, st), "jb_block_eig_f64_ex")
+        torch.cuda.synchronize()
+        outs.append((qt, off, dmax))
+    (qa, offa, da), (qb, offb, db) = outs
+    for a, b in zip(qa, qb):
+        assert torch.equal(a, b)
+    assert torch.equal(offa, offb) and torch.equal(da, db)
+
+
 def test_block_jacobi_drop_in():
     """svd(a, 'block_jacobi', ...) through the drop-in API: tall and wide
     inputs, the reference's defaults (block_size 4 -> width 32 here), the
