@@ -649,6 +649,7 @@ def run_blocked(args, name):
     m, n = a_np.shape
     a = torch.from_numpy(a_np).cuda()
     plan = BJ.BlockJacobi(m, n, b)
+    tune_ms = plan.tune(a)                               # launch choices, in preparation
     for _ in range(max(args.warmup, 2)):               # eager first sweeps, then the sweep graphs captured
         U, S, Vh, info = plan.solve(a)
     torch.cuda.synchronize()
@@ -670,8 +671,10 @@ def run_blocked(args, name):
             "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 2), "ms_per_step": ms,
             "higher_is_better": True,
             "scaling": "none (single matrix)", "vs_baseline": None,
-            "dtype": "f32 in/out; bf16x3/bf16x6 tensor; f64 eig", "config": {"workload": name, "m": m, "n": n,
-                                                                              "block_size": b},
+            "dtype": "f32 in/out; bf16x3/bf16x6 tensor; f64 eig",
+            "config": {"workload": name, "m": m, "n": n, "block_size": b,
+                       "launch": {"eig_cols_per_warp": plan.eig_variant, "gram_split": plan.gram_split},
+                       "autotuner_ms_per_sweep": {k: round(v, 3) for k, v in tune_ms.items()}},
             "data": ("synthetic (seeded: Haar U, V; 64 clusters x 16, cond 1e6)" if name == "clustered_large"
                      else "synthetic (seeded: rank-64 Gaussian product + N(0, 1e-6) noise)"),
             "block_sweeps": info["block_sweeps"], "off_per_sweep": info["off_per_sweep"],

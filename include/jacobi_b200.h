@@ -281,11 +281,11 @@ JB_API int jb_block_eig_f64(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_l
                             float *dmax, int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps,
                             double tol, const double *live_floor, void *stream);
 /* jb_block_eig_f64 with the kernel chosen: variant 0 = automatic (as
- * jb_block_eig_f64), 1 = one CTA per slot with G and Q in registers (slot
- * widths 64 and 128), 2 = one cluster of 8 CTAs per slot exchanging through
- * distributed shared memory (widths 64 and 128; exactly max_sweeps sweeps,
- * the same rotations and outputs as variant 1), 3 = the shared-memory
- * round-robin kernel (any even width up to 256). */
+ * jb_block_eig_f64), 1 = the shared-memory round-robin kernel (any even
+ * width up to 256), 4 / 8 / 16 = one CTA per slot with G and Q in registers
+ * (slot widths 64 and 128, odd-even order), that many columns per warp
+ * (n / variant warps; the same outputs, a different latency / occupancy
+ * balance, chosen by the blocked solver's autotuner). */
 JB_API int jb_block_eig_f64_ex(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
                                int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps, double tol,
                                const double *live_floor, int32_t variant, void *stream);

@@ -127,6 +127,9 @@ class BlockJacobi:
         self.live = torch.zeros(1, dtype=torch.float64, device=dev)   # live-column floor of the sweep
         # CTAs along K of the Gram products: about one wave over the SMs
         self.gram_split = max(1, torch.cuda.get_device_properties(dev).multi_processor_count // self.P)
+        # layout of the register eigen-solve: columns of G per warp (4, 8 or 16)
+        self.eig_variant = 8
+        self.tuned = None
         self._graphs, self._seen = {}, set()
 
     def _combine_v(self, cur):
@@ -167,10 +170,11 @@ class BlockJacobi:
             Vp = [x.view(P, 2 * b, self.npad) for x in self.V[cur][:parts]]
             # Grams of every slot: G_k = X_k X_k^T with X_k = 2b rows of W^T.
             gemm_parts(Wp, None, self.G, syrk=True, chain128=True, split_k=self.gram_split)
-            N.check(lib.jb_block_eig_f64(self.G.data_ptr(), self.Qt[0].data_ptr(), self.Qt[1].data_ptr(),
-                                         self.Qt[2].data_ptr() if parts == 3 else None, self.off[r].data_ptr(),
-                                         self.dmax[r].data_ptr(), self.isweeps.data_ptr(), P, 2 * b,
-                                         inner_sweeps, inner_tol, self.live.data_ptr(), st), "jb_block_eig_f64")
+            N.check(lib.jb_block_eig_f64_ex(self.G.data_ptr(), self.Qt[0].data_ptr(), self.Qt[1].data_ptr(),
+                                            self.Qt[2].data_ptr() if parts == 3 else None, self.off[r].data_ptr(),
+                                            self.dmax[r].data_ptr(), self.isweeps.data_ptr(), P, 2 * b,
+                                            inner_sweeps, inner_tol, self.live.data_ptr(),
+                                            self.eig_variant if 2 * b in (64, 128) else 0, st), "jb_block_eig_f64_ex")
             # X_k <- vv^T X_k (rows of W^T), same for V, each rotated row
             # written (as BF16 parts) straight into its next-round slot.
             nxt = 1 - cur
@@ -184,7 +188,7 @@ class BlockJacobi:
         the ~4 (nb - 1) launches of a sweep then cost one host call.  The
         graphs hold only this plan's buffers; the live floor is read on the
         device (self.live)."""
-        key = (cur, parts, inner_sweeps, inner_tol)
+        key = (cur, parts, inner_sweeps, inner_tol, self.eig_variant, self.gram_split)
         if not use_graphs or key not in self._seen:
             self._seen.add(key)
             return self._sweep(cur, parts, inner_sweeps, inner_tol)
@@ -196,6 +200,62 @@ class BlockJacobi:
             self._graphs[key] = g
         g.replay()
         return 1 - cur
+
+    def _load(self, a):
+        """Check a, scale it by 2^-e (exact), and place its columns (rows of
+        W^T) and the identity V in the slots of round 0 (buffer 0).  Returns
+        (A padded, its transpose, e)."""
+        lib = N.lib()
+        dev, st = self.device, _st(self.device)
+        m, n = self.m, self.n
+        if tuple(a.shape) != (m, n) or a.dtype != torch.float32 or a.device != dev:
+            raise ValueError("input must be a float32 (m, n) tensor on the plan's device")
+        if not bool(torch.isfinite(a).all()):
+            raise ValueError("input contains NaN or infinity")
+        amax = float(a.abs().max())
+        e = math.frexp(amax)[1] if amax > 0 else 0
+        # A padded (mpad x npad), scaled by 2^-e (exact); W^T rows = columns of A.
+        ap = torch.zeros(self.mpad, self.npad, dtype=torch.float32, device=dev)
+        ap[:m, :n] = a * (2.0 ** -e)
+        at = ap.t().contiguous()                                   # npad x mpad
+        eye = torch.eye(self.npad, dtype=torch.float32, device=dev)
+        for x in self.W + self.V:
+            x[2].zero_()
+        for buf, src, L in ((self.W[0], at, self.mpad), (self.V[0], eye, self.npad)):
+            N.check(lib.jb_rows_scatter(src.data_ptr(), self.init_map.data_ptr(), buf[0].data_ptr(), buf[1].data_ptr(),
+                                        None, None, self.npad, L, st), "scatter")
+        return ap, at, e
+
+    def tune(self, a: torch.Tensor, *, repeats=2):
+        """Autotuner of the launch choices: the register eigen-solve's layout
+        (4, 8 or 16 columns of G per warp; slot widths 64 and 128) and the
+        Gram's split along K (about one wave of CTAs over the SMs, or twice
+        that).  Each choice times `repeats` sweeps of the two-part stage on a
+        (CUDA events, after one warm-up sweep); the fastest is kept for every
+        later solve.  The choices change no result beyond rounding.  Returns
+        {choice: ms per sweep}."""
+        base_split = self.gram_split
+        variants = (4, 8, 16) if 2 * self.b in (64, 128) else (8,)
+        splits = (base_split, 2 * base_split)
+        times = {}
+        _, at, _ = self._load(a)
+        self.live.fill_(1e-4 * float((at * at).sum(1).max()))     # the two-part stage's live floor
+        cur = 0
+        for v in variants:
+            for sp in splits:
+                self.eig_variant, self.gram_split = v, sp
+                cur = self._sweep(cur, 2, 1, 1e-7)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(repeats):
+                    cur = self._sweep(cur, 2, 1, 1e-7)
+                e1.record()
+                torch.cuda.synchronize(self.device)
+                times[f"eig_cols_per_warp={v},gram_split={sp}"] = e0.elapsed_time(e1) / repeats
+        best = min(times, key=times.get)
+        self.eig_variant, self.gram_split = [int(x.split("=")[1]) for x in best.split(",")]
+        self.tuned = times
+        return times
 
     def solve(self, a: torch.Tensor, *, tol_phase1=5e-6, switch=5e-2, max_sweeps=30, max_two_part=12,
               inner_sweeps=1, inner_tol=1e-7, polar_steps=2, require_convergence=True, use_graphs=True):
@@ -217,22 +277,7 @@ class BlockJacobi:
         lib = N.lib()
         dev, st = self.device, _st(self.device)
         m, n, b, P, R = self.m, self.n, self.b, self.P, self.nb - 1
-        if tuple(a.shape) != (m, n) or a.dtype != torch.float32 or a.device != dev:
-            raise ValueError("input must be a float32 (m, n) tensor on the plan's device")
-        if not bool(torch.isfinite(a).all()):
-            raise ValueError("input contains NaN or infinity")
-        amax = float(a.abs().max())
-        e = math.frexp(amax)[1] if amax > 0 else 0
-        # A padded (mpad x npad), scaled by 2^-e (exact); W^T rows = columns of A.
-        ap = torch.zeros(self.mpad, self.npad, dtype=torch.float32, device=dev)
-        ap[:m, :n] = a * (2.0 ** -e)
-        at = ap.t().contiguous()                                   # npad x mpad
-        eye = torch.eye(self.npad, dtype=torch.float32, device=dev)
-        for x in self.W + self.V:
-            x[2].zero_()
-        for buf, src, L in ((self.W[0], at, self.mpad), (self.V[0], eye, self.npad)):
-            N.check(lib.jb_rows_scatter(src.data_ptr(), self.init_map.data_ptr(), buf[0].data_ptr(), buf[1].data_ptr(),
-                                        None, None, self.npad, L, st), "scatter")
+        ap, at, e = self._load(a)
         cur = 0
         sweeps = 0
         off_hist = []

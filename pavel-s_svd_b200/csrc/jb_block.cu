@@ -13,7 +13,6 @@
 //   jb_block_finish    sigma = column norms (FP64), descending order, cut,
 //                      U = W / sigma, Vh (solvers.py:61-66 with
 //                      _finish_columns :18-21).
-#include <cooperative_groups.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -232,20 +231,21 @@ __global__ void __launch_bounds__(kEigThreads) eig_kernel(const float *Gin, __nv
 // also swaps its two positions (J P), so after n rounds each pair of columns
 // has met exactly once (the swaps reverse the order).  With positions fixed,
 // G and Q stay in registers: lane l holds rows RPT l .. RPT l + RPT - 1 and
-// warp w columns 8 w .. 8 w + 7.  Row pairs that straddle two lanes use warp
+// warp w columns CB w .. CB w + CB - 1 (CB even: 4, 8 or 16 columns per warp,
+// n / CB warps; the outputs do not depend on CB).  Row pairs that straddle two lanes use warp
 // shuffles, column pairs that straddle two warps (odd rounds) one exchange
 // through shared memory.  Per round: warp 0 forms the angles from the
 // diagonal d and superdiagonal e (published in shared memory by their
 // owners), one barrier, rotations, (odd rounds: boundary exchange, one
 // barrier), new d / e, one barrier.
-template <int RPT>
-__global__ void __launch_bounds__(RPT * 128) eig_reg_kernel(const float *Gin, __nv_bfloat16 *Qt_hi,
+template <int RPT, int CB>
+__global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *Gin, __nv_bfloat16 *Qt_hi,
                                                             __nv_bfloat16 *Qt_lo, __nv_bfloat16 *Qt_lo2,
                                                             float *off_out, float *dmax_out, int *sweeps_out,
                                                             int max_sweeps, double tol, const double *live_floor_ptr) {
     constexpr int n = 32 * RPT;
-    constexpr int CB = 8;                      // columns per warp
     constexpr int NW = n / CB;                 // warps
+    static_assert(CB % 2 == 0 && NW >= RPT / 2, "columns per warp");
     extern __shared__ __align__(16) unsigned char smem[];
     double *sd = (double *)smem;               // d[x] = G[x][x]
     double *se = sd + n;                       // e[x] = G[x][x + 1]
@@ -487,296 +487,8 @@ __global__ void __launch_bounds__(RPT * 128) eig_reg_kernel(const float *Gin, __
     }
 }
 
-// Cluster form of eig_reg_kernel: one thread-block cluster of CL CTAs per
-// slot, every CTA holding CPC = N / CL consecutive columns of G and Q (all
-// N rows; lane l holds rows RPT l .. RPT l + RPT - 1, warp w columns
-// CB w .. CB w + CB - 1 of its CTA).  The same odd-even rounds with swap
-// folding, the same angle and rotation arithmetic, so the outputs equal
-// eig_reg_kernel's bit for bit (without its early exit: exactly
-// `max_sweeps` sweeps run; once a sweep rotates nothing, further sweeps
-// only swap positions, which the final sort undoes).
-// Per round: every CTA forms all N/2 angles from its own copy of the
-// diagonal d and superdiagonal e (published by their owners into every
-// CTA's shared memory, double-buffered by round parity), rotates rows
-// (warp shuffles across lanes) and columns; in odd rounds the column pairs
-// that straddle two warps take the neighbour's column through shared
-// memory, and across two CTAs through the neighbour's shared memory
-// (distributed shared memory), after one cluster barrier.  One more
-// cluster barrier per round publishes the new d / e.  Every barrier is
-// reached by every thread of the cluster the same number of times (the
-// loop bounds are uniform), so none can wait for a CTA that has left.
-template <int N, int CL>
-struct EigCl {
-    static constexpr int CPC = N / CL;     // columns per CTA
-    static constexpr int CB = 4;           // columns per warp
-    static constexpr int W = CPC / CB;     // warps per CTA
-    static constexpr int T = W * 32;
-    static constexpr int RPT = N / 32;     // rows per lane
-    static_assert(CPC % CB == 0 && W >= 1 && RPT >= 2 && RPT % 2 == 0, "slot width / cluster size");
-    // shared memory (bytes): sd, se [2][N] double; sc, ss [N] double;
-    // fg, lg [W][N] double; fq, lq [W][N] float; halo g [2][N] double,
-    // halo q [2][N] float; Qs [CPC][N] float; perm [N] int
-    static constexpr size_t smem = (size_t)(4 * N + 2 * N) * 8 + (size_t)2 * W * N * 12 + (size_t)2 * N * 12 +
-                                   (size_t)CPC * N * 4 + (size_t)N * 4 + 16;
-};
-
-template <int N, int CL>
-__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(EigCl<N, CL>::T)
-    eig_cluster_kernel(const float *Gin, __nv_bfloat16 *Qt_hi, __nv_bfloat16 *Qt_lo, __nv_bfloat16 *Qt_lo2,
-                       float *off_out, float *dmax_out, int *sweeps_out, int max_sweeps, double tol,
-                       const double *live_floor_ptr) {
-    namespace cg = cooperative_groups;
-    using K = EigCl<N, CL>;
-    constexpr int CB = K::CB, W = K::W, RPT = K::RPT, CPC = K::CPC;
-    extern __shared__ __align__(16) unsigned char smem[];
-    double *sd = (double *)smem;               // [2][N] d by round parity
-    double *se = sd + 2 * N;                   // [2][N] e by round parity
-    double *sc = se + 2 * N;                   // [N] c of the pair starting at position p
-    double *ss = sc + N;                       // [N] s
-    double *fg = ss + N;                       // [W][N] first G column of each warp
-    double *lg = fg + W * N;                   // [W][N] last G column of each warp
-    double *hg = lg + W * N;                   // [2][N] halo: 0 = left CTA's last, 1 = right CTA's first
-    float *fq = (float *)(hg + 2 * N);         // [W][N]
-    float *lq = fq + W * N;                    // [W][N]
-    float *hq = lq + W * N;                    // [2][N]
-    float *Qs = hq + 2 * N;                    // [CPC][N] Q columns for the write-out
-    int *perm = (int *)(Qs + (size_t)CPC * N);
-    __shared__ double s_red[W];
-    cg::cluster_group cluster = cg::this_cluster();
-    const int rank = (int)cluster.block_rank();
-    const int k = blockIdx.x / CL;             // slot
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int r0 = lane * RPT, c0 = rank * CPC + warp * CB;   // global row / column of this thread's tile
-    const double live_floor = live_floor_ptr ? *live_floor_ptr : 0.0;
-    const float *g_in = Gin + (size_t)k * N * N;
-
-    double g[RPT][CB];
-    float q[RPT][CB];
-#pragma unroll
-    for (int i = 0; i < RPT; ++i)
-#pragma unroll
-        for (int j = 0; j < CB; ++j) {
-            const int r = r0 + i, c = c0 + j;
-            g[i][j] = 0.5 * ((double)g_in[(size_t)r * N + c] + (double)g_in[(size_t)c * N + r]);
-            q[i][j] = (r == c) ? 1.f : 0.f;
-        }
-    // d[x] = G[x][x] and e[x] = G[x][x + 1] into buffer `buf` of every CTA
-    auto publish_de = [&](int buf) {
-#pragma unroll
-        for (int i = 0; i < RPT; ++i) {
-            const int x = r0 + i;
-#pragma unroll
-            for (int j = 0; j < CB; ++j) {
-                if (c0 + j == x || c0 + j == x + 1) {
-                    const double v = g[i][j];
-                    double *dst = (c0 + j == x ? sd : se) + buf * N + x;
-                    for (int rr = 0; rr < CL; ++rr) *cluster.map_shared_rank(dst, rr) = v;
-                }
-            }
-        }
-    };
-    publish_de(0);
-    cluster.sync();
-    double gmax = 0.0;
-    for (int i = 0; i < N; ++i) gmax = fmax(gmax, sd[i]);
-    const double floor_ = 2.220446049250313e-16 * 2.220446049250313e-16 * gmax;
-    const double tol2 = tol * tol;
-    double first_off = 0.0;
-    for (int sweep = 1; sweep <= max_sweeps; ++sweep) {
-        double offn = 0.0, offd = 1.0;
-        for (int r = 0; r < N; ++r) {
-            const int par = r & 1, buf = r & 1;
-            const double *d = sd + buf * N, *e = se + buf * N;
-            for (int t = threadIdx.x; t < N / 2 - par; t += K::T) {
-                const int p = 2 * t + par;
-                const double app = d[p], aqq = d[p + 1], apq = e[p];
-                double c = 1.0, sn = 0.0;
-                const double prod = app * aqq, apq2 = apq * apq;
-                if (apq2 > tol2 * prod && fmin(app, aqq) > floor_) {
-                    // off over live columns only (solvers.py:55-57)
-                    if (fmin(app, aqq) > live_floor && apq2 * offd > offn * prod) { offn = apq2; offd = prod; }
-                    const double dd = aqq - app, a2 = 2.0 * fabs(apq);
-                    const int ex = (__double2hiint(fmax(fabs(dd), a2)) >> 20) & 0x7ff;
-                    const double scl = __hiloint2double((2046 - ex) << 20, 0);
-                    const float df = fabsf((float)(dd * scl)), af = (float)(a2 * scl);
-                    const float tf = __fdividef(af, df + sqrtf(df * df + af * af));
-                    const double tt = dd < 0.0 ? -(double)tf : (double)tf;
-                    // c = 1 / sqrt(1 + t^2): FP32 estimate and one Newton step in FP64
-                    const double x = 1.0 + tt * tt;
-                    const double cg0 = (double)rsqrtf(1.f + tf * tf);
-                    c = cg0 * (1.5 - 0.5 * x * cg0 * cg0);
-                    sn = tt * c;
-                    if (apq < 0.0) sn = -sn;
-                }
-                sc[p] = c;
-                ss[p] = sn;
-            }
-            __syncthreads();
-            // Rows (J^T from the left, then the swap): (x_p, x_q) <- (s x_p + c x_q, c x_p - s x_q).
-            if (par == 0) {
-#pragma unroll
-                for (int i = 0; i < RPT; i += 2) {
-                    const double c = sc[r0 + i], sn = ss[r0 + i];
-#pragma unroll
-                    for (int j = 0; j < CB; ++j) {
-                        const double x = g[i][j], y = g[i + 1][j];
-                        g[i][j] = sn * x + c * y;
-                        g[i + 1][j] = c * x - sn * y;
-                    }
-                }
-            } else {
-                const bool has_up = lane > 0, has_down = lane < 31;
-                const double cu = has_up ? sc[r0 - 1] : 1.0, su = has_up ? ss[r0 - 1] : 0.0;
-                const double cd = has_down ? sc[r0 + RPT - 1] : 1.0, sdn = has_down ? ss[r0 + RPT - 1] : 0.0;
-#pragma unroll
-                for (int j = 0; j < CB; ++j) {
-                    const double up = __shfl_up_sync(0xffffffffu, g[RPT - 1][j], 1);   // row r0 - 1
-                    const double dn = __shfl_down_sync(0xffffffffu, g[0][j], 1);       // row r0 + RPT
-                    const double first = g[0][j], last = g[RPT - 1][j];
-                    if (has_up) g[0][j] = cu * up - su * first;
-                    if (has_down) g[RPT - 1][j] = sdn * last + cd * dn;
-                }
-#pragma unroll
-                for (int i = 1; i + 1 < RPT; i += 2) {
-                    const double c = sc[r0 + i], sn = ss[r0 + i];
-#pragma unroll
-                    for (int j = 0; j < CB; ++j) {
-                        const double x = g[i][j], y = g[i + 1][j];
-                        g[i][j] = sn * x + c * y;
-                        g[i + 1][j] = c * x - sn * y;
-                    }
-                }
-            }
-            // Columns (J from the right, then the swap), G and Q alike.
-            if (par == 0) {
-#pragma unroll
-                for (int j = 0; j < CB; j += 2) {
-                    const double c = sc[c0 + j], sn = ss[c0 + j];
-                    const float fc = (float)c, fs = (float)sn;
-#pragma unroll
-                    for (int i = 0; i < RPT; ++i) {
-                        const double x = g[i][j], y = g[i][j + 1];
-                        g[i][j] = sn * x + c * y;
-                        g[i][j + 1] = c * x - sn * y;
-                        const float u = q[i][j], v = q[i][j + 1];
-                        q[i][j] = fs * u + fc * v;
-                        q[i][j + 1] = fc * u - fs * v;
-                    }
-                }
-            } else {
-                // this warp's first and last columns (after the row rotation) to the
-                // neighbours: in this CTA through fg / lg, across CTAs into the halo
-#pragma unroll
-                for (int i = 0; i < RPT; ++i) {
-                    fg[warp * N + r0 + i] = g[i][0];
-                    lg[warp * N + r0 + i] = g[i][CB - 1];
-                    fq[warp * N + r0 + i] = q[i][0];
-                    lq[warp * N + r0 + i] = q[i][CB - 1];
-                }
-                if (warp == 0 && rank > 0) {
-                    double *dg = cluster.map_shared_rank(hg + N, rank - 1);
-                    float *dq = cluster.map_shared_rank(hq + N, rank - 1);
-#pragma unroll
-                    for (int i = 0; i < RPT; ++i) { dg[r0 + i] = g[i][0]; dq[r0 + i] = q[i][0]; }
-                }
-                if (warp == W - 1 && rank < CL - 1) {
-                    double *dg = cluster.map_shared_rank(hg, rank + 1);
-                    float *dq = cluster.map_shared_rank(hq, rank + 1);
-#pragma unroll
-                    for (int i = 0; i < RPT; ++i) { dg[r0 + i] = g[i][CB - 1]; dq[r0 + i] = q[i][CB - 1]; }
-                }
-                cluster.sync();
-                const bool has_left = c0 > 0, has_right = c0 + CB < N;
-                const double *lgc = warp > 0 ? lg + (warp - 1) * N : hg;
-                const float *lqc = warp > 0 ? lq + (warp - 1) * N : hq;
-                const double *rgc = warp < W - 1 ? fg + (warp + 1) * N : hg + N;
-                const float *rqc = warp < W - 1 ? fq + (warp + 1) * N : hq + N;
-                const double cl = has_left ? sc[c0 - 1] : 1.0, sl = has_left ? ss[c0 - 1] : 0.0;
-                const double cr = has_right ? sc[c0 + CB - 1] : 1.0, sr = has_right ? ss[c0 + CB - 1] : 0.0;
-#pragma unroll
-                for (int i = 0; i < RPT; ++i) {
-                    const int row = r0 + i;
-                    if (has_left) {                // pair (c0 - 1, c0): this warp holds the second
-                        const double x = lgc[row];
-                        const float u = lqc[row];
-                        g[i][0] = cl * x - sl * g[i][0];
-                        q[i][0] = (float)cl * u - (float)sl * q[i][0];
-                    }
-                    if (has_right) {               // pair (c0 + CB - 1, c0 + CB): this warp holds the first
-                        const double y = rgc[row];
-                        const float v = rqc[row];
-                        g[i][CB - 1] = sr * g[i][CB - 1] + cr * y;
-                        q[i][CB - 1] = (float)sr * q[i][CB - 1] + (float)cr * v;
-                    }
-                }
-#pragma unroll
-                for (int j = 1; j + 1 < CB; j += 2) {
-                    const double c = sc[c0 + j], sn = ss[c0 + j];
-                    const float fc = (float)c, fs = (float)sn;
-#pragma unroll
-                    for (int i = 0; i < RPT; ++i) {
-                        const double x = g[i][j], y = g[i][j + 1];
-                        g[i][j] = sn * x + c * y;
-                        g[i][j + 1] = c * x - sn * y;
-                        const float u = q[i][j], v = q[i][j + 1];
-                        q[i][j] = fs * u + fc * v;
-                        q[i][j + 1] = fc * u - fs * v;
-                    }
-                }
-            }
-            publish_de(buf ^ 1);
-            cluster.sync();
-        }
-        if (sweep == 1) {
-            for (int o = 16; o; o >>= 1) {
-                const double on = __shfl_xor_sync(0xffffffffu, offn, o), od = __shfl_xor_sync(0xffffffffu, offd, o);
-                if (on * offd > offn * od) { offn = on; offd = od; }
-            }
-            if (lane == 0) s_red[warp] = sqrt(offn / offd);
-            __syncthreads();
-            for (int w = 0; w < W; ++w) first_off = fmax(first_off, s_red[w]);
-        }
-    }
-    // N rounds per sweep: the final d is in buffer 0 (N even)
-#pragma unroll
-    for (int i = 0; i < RPT; ++i)
-#pragma unroll
-        for (int j = 0; j < CB; ++j) Qs[(size_t)(warp * CB + j) * N + r0 + i] = q[i][j];
-    for (int j = threadIdx.x; j < N; j += K::T) {
-        const double dj = sd[j];
-        int rk = 0;
-        for (int i = 0; i < N; ++i) {
-            const double di = sd[i];
-            rk += (di > dj) || (di == dj && i < j);
-        }
-        perm[rk] = j;
-    }
-    __syncthreads();
-    // Q^T rows in eigenvalue order: this CTA writes the rows of its columns
-    __nv_bfloat16 *qh = Qt_hi + (size_t)k * N * N, *ql = Qt_lo + (size_t)k * N * N;
-    for (int rr = 0; rr < N; ++rr) {
-        const int col = perm[rr] - rank * CPC;
-        if (col < 0 || col >= CPC) continue;
-        for (int i = threadIdx.x; i < N; i += K::T) {
-            const float x = Qs[(size_t)col * N + i];
-            const size_t t = (size_t)rr * N + i;
-            const __nv_bfloat16 h = __float2bfloat16_rn(x);
-            qh[t] = h;
-            const float rem = x - __bfloat162float(h);
-            const __nv_bfloat16 l = __float2bfloat16_rn(rem);
-            ql[t] = l;
-            if (Qt_lo2) Qt_lo2[(size_t)k * N * N + t] = __float2bfloat16_rn(rem - __bfloat162float(l));
-        }
-    }
-    if (rank == 0 && threadIdx.x == 0) {
-        if (off_out) off_out[k] = (float)first_off;
-        if (dmax_out) dmax_out[k] = (float)gmax;
-        if (sweeps_out) sweeps_out[k] = max_sweeps;
-    }
-}
-
-__host__ inline size_t eig_reg_smem_bytes(int n) {
-    const int nw = n / 8;
+__host__ inline size_t eig_reg_smem_bytes(int n, int cb) {
+    const int nw = n / cb;
     return (size_t)4 * n * 8 + (size_t)nw * 2 * n * 8 + (size_t)nw * 2 * n * 4 + (size_t)n * n * 4 + (size_t)n * 4 +
            16;
 }
@@ -915,18 +627,18 @@ __global__ void __launch_bounds__(256) gemm_f64acc_kernel(const float *A, const 
     }
 }
 
-template <int N, int CL>
-static int launch_eig_cluster(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
-                              int32_t *sweeps, int64_t pairs, int32_t max_sweeps, double tol,
-                              const double *live_floor, cudaStream_t st) {
-    using K = EigCl<N, CL>;
-    auto kern = eig_cluster_kernel<N, CL>;
-    if (K::smem > 48 * 1024 &&
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::smem) != cudaSuccess)
+template <int RPT, int CB>
+static int launch_eig_reg(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
+                          int32_t *sweeps, int64_t pairs, int32_t max_sweeps, double tol, const double *live_floor,
+                          cudaStream_t st) {
+    constexpr int n = 32 * RPT;
+    const size_t smem = eig_reg_smem_bytes(n, CB);
+    auto kern = eig_reg_kernel<RPT, CB>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return JB_ECUDA;
-    kern<<<(unsigned)(pairs * CL), K::T, K::smem, st>>>(G, (__nv_bfloat16 *)Qt_hi, (__nv_bfloat16 *)Qt_lo,
-                                                       (__nv_bfloat16 *)Qt_lo2, off, dmax, sweeps, max_sweeps, tol,
-                                                       live_floor);
+    kern<<<(unsigned)pairs, 32 * (n / CB), smem, st>>>(G, (__nv_bfloat16 *)Qt_hi, (__nv_bfloat16 *)Qt_lo,
+                                                      (__nv_bfloat16 *)Qt_lo2, off, dmax, sweeps, max_sweeps, tol,
+                                                      live_floor);
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
 }
 
@@ -940,34 +652,21 @@ extern "C" {
 int jb_block_eig_f64_ex(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
                         int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps, double tol,
                         const double *live_floor, int32_t variant, void *stream) {
-    if (!G || !Qt_hi || !Qt_lo || pairs < 1 || n < 2 || (n & 1) || max_sweeps < 1 || variant < 0 || variant > 3)
+    if (!G || !Qt_hi || !Qt_lo || pairs < 1 || n < 2 || (n & 1) || max_sweeps < 1 ||
+        !(variant == 0 || variant == 1 || variant == 4 || variant == 8 || variant == 16))
         return JB_EINVAL;
     cudaStream_t st = (cudaStream_t)stream;
-    if ((n == 64 || n == 128) && variant != 1 && variant != 3) {
-        if (pairs > 65535 / 8) return JB_ETOOBIG;
-        return n == 64 ? launch_eig_cluster<64, 8>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps,
-                                                   tol, live_floor, st)
-                       : launch_eig_cluster<128, 8>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps,
-                                                    tol, live_floor, st);
-    }
-    if ((n == 64 || n == 128) && variant != 3) {
-        const size_t smem = eig_reg_smem_bytes(n);
-        if (n == 64) {
-            if (cudaFuncSetAttribute(eig_reg_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-                cudaSuccess)
-                return JB_ECUDA;
-            eig_reg_kernel<2><<<(unsigned)pairs, 256, smem, st>>>(
-                G, (__nv_bfloat16 *)Qt_hi, (__nv_bfloat16 *)Qt_lo, (__nv_bfloat16 *)Qt_lo2, off, dmax, sweeps,
-                max_sweeps, tol, live_floor);
-        } else {
-            if (cudaFuncSetAttribute(eig_reg_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-                cudaSuccess)
-                return JB_ECUDA;
-            eig_reg_kernel<4><<<(unsigned)pairs, 512, smem, st>>>(
-                G, (__nv_bfloat16 *)Qt_hi, (__nv_bfloat16 *)Qt_lo, (__nv_bfloat16 *)Qt_lo2, off, dmax, sweeps,
-                max_sweeps, tol, live_floor);
+    if ((n == 64 || n == 128) && variant != 1) {
+        const int cb = variant == 0 ? 8 : variant;
+        switch (n * 100 + cb) {
+            case 6404: return launch_eig_reg<2, 4>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps, tol, live_floor, st);
+            case 6408: return launch_eig_reg<2, 8>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps, tol, live_floor, st);
+            case 6416: return launch_eig_reg<2, 16>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps, tol, live_floor, st);
+            case 12804: return launch_eig_reg<4, 4>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps, tol, live_floor, st);
+            case 12808: return launch_eig_reg<4, 8>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps, tol, live_floor, st);
+            case 12816: return launch_eig_reg<4, 16>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps, tol, live_floor, st);
+            default: return JB_EINVAL;
         }
-        return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
     }
     if (n > 256) return JB_ETOOBIG;                  // players are stored as bytes
     const size_t smem = eig_smem_bytes(n);

@@ -33,7 +33,7 @@
 namespace jb {
 namespace nul {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;
 constexpr int kWarps = kThreads / 32;
 constexpr unsigned long long kWaitNs = 2000000000ull;
 
@@ -137,36 +137,47 @@ __device__ __forceinline__ unsigned long long gtimer() {
     return t;
 }
 
-// Team-wide barrier.  G == 1: the CTA barrier.  G > 1: a generation barrier
-// over the whole (co-resident, cooperative) grid with a bounded wait.
-// Returns false once any CTA of the team has given up waiting.
-__device__ __forceinline__ bool team_sync(unsigned *bar, int *err, int G) {
+// Team-wide barrier.  G == 1: the CTA barrier.  G > 1: a two-level
+// generation barrier over the whole (co-resident, cooperative) grid: CTAs
+// arrive on the counter of their group of kGroupCTAs, the last of a group on
+// the counter of groups, and the last group releases everyone by bumping the
+// generation word, so no counter takes more than ~20 contending atomics.
+// Waits are bounded; returns false once any CTA of the team gave up.
+// bar[0] generation, bar[1] groups arrived, bar[2] error flag, bar[4 + k]
+// CTAs of group k arrived (the area is zeroed before the launch).
+constexpr int kGroupCTAs = 8;
+__device__ __forceinline__ bool team_sync(unsigned *bar, int G) {
     __syncthreads();
     if (G == 1) return true;
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
-        volatile unsigned *vgen = bar + 1;
+        volatile unsigned *vgen = bar;
+        volatile int *verr = (volatile int *)(bar + 2);
         const unsigned gen = *vgen;
         __threadfence();
-        const unsigned arrived = atomicAdd(bar, 1u);
+        const int grp = blockIdx.x / kGroupCTAs, ngroups = (G + kGroupCTAs - 1) / kGroupCTAs;
+        const int gsize = min(kGroupCTAs, G - grp * kGroupCTAs);
         int ok = 1;
-        if (arrived == (unsigned)G - 1) {
-            atomicExch(bar, 0u);
+        if (atomicAdd(bar + 4 + grp, 1u) == (unsigned)gsize - 1) {
+            atomicExch(bar + 4 + grp, 0u);
             __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            const unsigned long long t0 = gtimer();
-            while (*vgen == gen) {
-                if (gtimer() - t0 > kWaitNs) {
-                    ok = 0;
-                    atomicExch(err, 1);
-                    break;
-                }
-                __nanosleep(64);
+            if (atomicAdd(bar + 1, 1u) == (unsigned)ngroups - 1) {
+                atomicExch(bar + 1, 0u);
+                __threadfence();
+                atomicAdd(bar, 1u);
             }
         }
+        const unsigned long long t0 = gtimer();
+        while (*vgen == gen) {
+            if (gtimer() - t0 > kWaitNs) {
+                ok = 0;
+                atomicExch((int *)(bar + 2), 1);
+                break;
+            }
+            __nanosleep(32);
+        }
         __threadfence();
-        s_ok = ok && !*(volatile int *)err;
+        s_ok = ok && !*verr;
     }
     __syncthreads();
     return s_ok != 0;
@@ -203,6 +214,54 @@ __device__ __forceinline__ double cta_sum(double v, double *red) {
     return s;
 }
 
+// Team-wide reductions over the G slots, read by warp 0 only (one L2 read
+// per slot per CTA) and broadcast through shared memory.
+__device__ __forceinline__ int64_t team_argmax(const Slot *slots, int G, bool team, int64_t *s_idx) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp == 0) {
+        double best = -1e300;
+        int64_t bidx = 0;
+        for (int q = lane; q < G; q += 32) {
+            const double v = team ? __ldcg(&slots[q].val) : slots[q].val;
+            const int64_t i = team ? __ldcg(&slots[q].idx) : slots[q].idx;
+            if (v > best || (v == best && i < bidx)) { best = v; bidx = i; }
+        }
+        for (int o = 16; o; o >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int64_t oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+            if (ob > best || (ob == best && oi < bidx)) { best = ob; bidx = oi; }
+        }
+        if (lane == 0) *s_idx = bidx;
+    }
+    __syncthreads();
+    const int64_t r = *s_idx;
+    __syncthreads();
+    return r;
+}
+
+// Sum of slots[q].val over q < G in a fixed order (the same value in every
+// CTA): lane-strided partial sums combined by a fixed butterfly.
+__device__ __forceinline__ double team_sum(const Slot *slots, int G, bool team, double *s_val) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp == 0) {
+        double v = 0.0;
+        for (int q = lane; q < G; q += 32) v += team ? __ldcg(&slots[q].val) : slots[q].val;
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) *s_val = v;
+    }
+    __syncthreads();
+    const double r = *s_val;
+    __syncthreads();
+    return r;
+}
+
+// Row stride of the packed columns X: a multiple of 16 bytes, so that every
+// row starts aligned for 16-byte vector loads.
+__host__ __device__ inline int64_t x_stride(int64_t n, int esz) {
+    const int64_t v = 16 / esz;
+    return (n + v - 1) / v * v;
+}
+
 // Per-team workspace layout (byte offsets from the team's base).  X, the
 // packed columns, exists only for multi-CTA teams.
 struct Layout {
@@ -212,7 +271,7 @@ __host__ __device__ inline size_t al256(size_t b) { return (b + 255) & ~(size_t)
 __host__ __device__ inline Layout layout(int64_t m, int64_t n, int esz, int asz, int G) {
     Layout L;
     size_t o = 0;
-    L.x = o;     o += G > 1 ? al256((size_t)m * n * esz) : 0;
+    L.x = o;     o += G > 1 ? al256((size_t)m * x_stride(n, esz) * esz) : 0;
     L.lev = o;   o += al256((size_t)m * 8);
     L.y = o;     o += al256((size_t)n * asz);
     L.part = o;  o += G > 1 ? al256((size_t)G * n * asz) : 0;
@@ -223,25 +282,94 @@ __host__ __device__ inline Layout layout(int64_t m, int64_t n, int esz, int asz,
     return L;
 }
 
+// Rows are processed TPR threads per row, THREADS / TPR rows at a time, so a
+// CTA has many independent loads in flight (the products stream X from L2).
+constexpr int kTPR = 8;
+
+// sum_k x[k] * (CONJ ? conj(r[k]) : r[k]) over k < na, this thread's share:
+// k-chunks sub, sub + TPR, ... of VEC = 16 / sizeof(S) elements (16-byte
+// loads when VECTOR: x 16-byte aligned, r in shared memory), four chunks in
+// flight, then the scalar tail.
+template <typename S, bool VECTOR, bool CONJ>
+__device__ __forceinline__ typename Tr<S>::A row_dot(const S *x, const S *r, int na, int sub) {
+    using T = Tr<S>;
+    using A = typename T::A;
+    constexpr int V = VECTOR ? 16 / (int)sizeof(S) : 1;
+    union Pack { uint4 u; S s[16 / sizeof(S)]; };
+    A acc0 = T::zero(), acc1 = T::zero();
+    int k = 0;
+    if (VECTOR) {
+        const int nv = na / V;
+        int j = sub;
+        for (; j + 3 * kTPR < nv; j += 4 * kTPR) {
+            Pack a[4], b[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                a[u].u = *(const uint4 *)(x + (size_t)(j + u * kTPR) * V);
+                b[u].u = *(const uint4 *)(r + (size_t)(j + u * kTPR) * V);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int e = 0; e < V; ++e) {
+                    const A rv = CONJ ? T::conj(T::ld(&b[u].s[e])) : T::ld(&b[u].s[e]);
+                    if (u & 1) acc1 = T::fma_(acc1, T::ld(&a[u].s[e]), rv);
+                    else acc0 = T::fma_(acc0, T::ld(&a[u].s[e]), rv);
+                }
+        }
+        for (; j < nv; j += kTPR) {
+            Pack a, b;
+            a.u = *(const uint4 *)(x + (size_t)j * V);
+            b.u = *(const uint4 *)(r + (size_t)j * V);
+#pragma unroll
+            for (int e = 0; e < V; ++e)
+                acc0 = T::fma_(acc0, T::ld(&a.s[e]), CONJ ? T::conj(T::ld(&b.s[e])) : T::ld(&b.s[e]));
+        }
+        k = nv * V;
+    }
+#pragma unroll 4
+    for (int kk = k + sub; kk < na; kk += kTPR)
+        acc1 = T::fma_(acc1, T::ld(x + kk), CONJ ? T::conj(T::ld(r + kk)) : T::ld(r + kk));
+    return T::add(acc0, acc1);
+}
+
+// Sum over the kTPR consecutive lanes of a row group (all lanes take part).
+template <typename A, typename T>
+__device__ __forceinline__ A group_sum(A v) {
+    for (int o = kTPR / 2; o; o >>= 1) {
+        if constexpr (T::cplx) {
+            v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+            v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+        } else {
+            v += __shfl_xor_sync(0xffffffffu, v, o);
+        }
+    }
+    return v;
+}
+
 // TEAM = false: one CTA per matrix, in place on U (the columns not yet
 // completed are zero, so every product runs over all n columns, as the
 // reference's u @ (u^H v) does; the new column is excluded from the second
 // projection).  TEAM = true: a cooperative team of G CTAs, the kept and
-// completed columns packed into X (row stride n), G > 1.
+// completed columns packed into X (row stride x_stride(n)), G > 1.
 template <typename S, bool TEAM>
-__global__ void __launch_bounds__(kThreads) null_kernel(Params p) {
+__global__ void __launch_bounds__(kThreads, 1) null_kernel(Params p) {
     using T = Tr<S>;
     using A = typename T::A;
+    constexpr int kGroups = kThreads / kTPR;
     extern __shared__ __align__(16) unsigned char smem[];
-    S *rowc = (S *)smem;                                   // row idx of X
+    S *rowc = (S *)smem;                                   // row idx of X; y in the second projection
     __shared__ Slot s_red[kWarps];
     __shared__ double s_dred[kWarps];
     __shared__ int s_flag;
+    __shared__ int64_t s_idx;
+    __shared__ double s_sum;
     const int G = TEAM ? p.G : 1;
     const int g = TEAM ? blockIdx.x : 0;                   // rank in the team
     const int64_t team = TEAM ? 0 : blockIdx.x;
     const int64_t nteams = TEAM ? 1 : gridDim.x;
     const int64_t m = p.m, n = p.n;
+    const int64_t ldx = TEAM ? x_stride(n, sizeof(S)) : n;
     const Layout L = layout(m, n, sizeof(S), sizeof(A), G);
     unsigned char *base = p.ws + team * p.team_bytes;
     double *lev = (double *)(base + L.lev);
@@ -250,11 +378,12 @@ __global__ void __launch_bounds__(kThreads) null_kernel(Params p) {
     int *cmap = (int *)(base + L.cmap);
     Slot *slots = (Slot *)(base + L.slots);                // [2][G]
     unsigned *bar = (unsigned *)(base + L.bar);
-    int *err = (int *)(bar + 2);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int sub = threadIdx.x % kTPR, grp = threadIdx.x / kTPR;
     const int64_t r0 = m * g / G, r1 = m * (g + 1) / G;   // this CTA's rows
     // cross-CTA data is read through L2 (ld.global.cg): L1 is not coherent
-    auto ldx = [&](const S *q) -> A { return TEAM ? T::ldcg(q) : T::ld(q); };
+    auto ldx_ = [&](const S *q) -> A { return TEAM ? T::ldcg(q) : T::ld(q); };
+    auto ldy = [&](const A *q) -> A { return TEAM ? T::ldcgA(q) : *q; };
     int64_t z = team;
     for (; z < p.batch; z += nteams) {
         S *U = (S *)p.U + z * m * n;
@@ -276,6 +405,7 @@ __global__ void __launch_bounds__(kThreads) null_kernel(Params p) {
         const int nkept = s_flag;
         if (nkept < 0) {                                   // nothing to complete
             if (g == 0 && threadIdx.x == 0) p.status[z] = JB_ST_OK;
+            __syncthreads();                               // s_flag is rewritten for the next matrix
             continue;
         }
         // Zero U's missing columns (primitives.py:436), pack the kept ones
@@ -290,7 +420,7 @@ __global__ void __launch_bounds__(kThreads) null_kernel(Params p) {
                 else acc += T::norm2(T::ld(urow + c));
             }
             if (TEAM)
-                for (int k = lane; k < nkept; k += 32) X[i * n + k] = urow[cmap[k]];
+                for (int k = lane; k < nkept; k += 32) X[i * ldx + k] = urow[cmap[k]];
             for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
             const double lv = 1.0 - acc;
             if (lane == 0) lev[i] = lv;
@@ -298,57 +428,53 @@ __global__ void __launch_bounds__(kThreads) null_kernel(Params p) {
         }
         Slot sb = cta_argmax(best, bidx, s_red);
         if (threadIdx.x == 0) slots[g] = sb;
-        if (!team_sync(bar, err, G)) goto timeout;
+        if (!team_sync(bar, G)) goto timeout;
         {
             int a = nkept;                                 // packed columns (TEAM)
-            const int span = TEAM ? 0 : (int)n;            // columns a product runs over (in place)
             bool failed = false;
             for (int64_t c = 0; c < n; ++c) {
                 if (keep[c]) continue;
-                const int na = TEAM ? a : span;
+                const int na = TEAM ? a : (int)n;          // columns a product runs over
                 const int64_t col = TEAM ? a : c;          // where v is built
                 // idx = team-wide first argmax of the leverage
-                Slot b = {-1e300, 0};
-                for (int q = 0; q < G; ++q) {
-                    Slot s;
-                    if (TEAM) { s.val = __ldcg(&slots[q].val); s.idx = __ldcg(&slots[q].idx); }
-                    else s = slots[q];
-                    if (s.val > b.val || (s.val == b.val && s.idx < b.idx)) b = s;
-                }
-                const int64_t idx = b.idx;
-                for (int k = threadIdx.x; k < na; k += kThreads) T::st(rowc + k, ldx(X + idx * n + k));
+                const int64_t idx = team_argmax(slots, G, TEAM, &s_idx);
+                for (int k = threadIdx.x; k < na; k += kThreads) T::st(rowc + k, ldx_(X + idx * ldx + k));
                 __syncthreads();
                 // first projection, row-local: v_i = delta - X_i . conj(X_idx)
                 // (column col of X is still zero in every row)
                 double pn2 = 0.0;
-                for (int64_t i = r0 + warp; i < r1; i += kWarps) {
-                    const S *xrow = X + i * n;
-                    A acc = T::zero();
-                    for (int k = lane; k < na; k += 32) acc = T::fma_(acc, T::ld(xrow + k), T::conj(T::ld(rowc + k)));
-                    acc = T::shfl_sum(acc);
-                    if (lane == 0) {
-                        T::st(X + i * n + col, T::sub(i == idx ? T::unit() : T::zero(), acc));
-                        pn2 += T::norm2(T::ld(X + i * n + col));
+                for (int64_t i0 = r0; i0 < r1; i0 += kGroups) {
+                    const int64_t i = i0 + grp;
+                    A acc = i < r1 ? row_dot<S, TEAM, true>(X + i * ldx, rowc, na, sub) : T::zero();
+                    acc = group_sum<A, T>(acc);
+                    if (sub == 0 && i < r1) {
+                        T::st(X + i * ldx + col, T::sub(i == idx ? T::unit() : T::zero(), acc));
+                        pn2 += T::norm2(T::ld(X + i * ldx + col));
                     }
                 }
                 double n2 = cta_sum(pn2, s_dred);
                 if (threadIdx.x == 0) slots[G + g].val = n2;
-                if (!team_sync(bar, err, G)) goto timeout;
-                n2 = 0.0;
-                for (int q = 0; q < G; ++q) n2 += TEAM ? __ldcg(&slots[G + q].val) : slots[G + q].val;
+                if (!team_sync(bar, G)) goto timeout;
+                n2 = team_sum(slots + G, G, TEAM, &s_sum);
                 if (p.always_reorth || n2 < 0.5) {
                     // second projection: y = X^H v (without v's own column), v -= X y
                     A *yout = TEAM ? part + (size_t)g * n : y;
                     for (int k = threadIdx.x; k < na; k += kThreads) {
-                        A acc = T::zero();
-                        if (k != col)
-                            for (int64_t i = r0; i < r1; ++i)
-                                acc = T::fma_(acc, T::conj(T::ld(X + i * n + k)), T::ld(X + i * n + col));
-                        yout[k] = acc;
+                        A acc0 = T::zero(), acc1 = T::zero();
+                        if (k != col) {
+                            int64_t i = r0;
+                            for (; i + 1 < r1; i += 2) {
+                                acc0 = T::fma_(acc0, T::conj(T::ld(X + i * ldx + k)), T::ld(X + i * ldx + col));
+                                acc1 = T::fma_(acc1, T::conj(T::ld(X + (i + 1) * ldx + k)),
+                                               T::ld(X + (i + 1) * ldx + col));
+                            }
+                            if (i < r1) acc0 = T::fma_(acc0, T::conj(T::ld(X + i * ldx + k)), T::ld(X + i * ldx + col));
+                        }
+                        yout[k] = T::add(acc0, acc1);
                     }
                     if (TEAM) {
                         // every CTA sums the partials of its slice of y
-                        if (!team_sync(bar, err, G)) goto timeout;
+                        if (!team_sync(bar, G)) goto timeout;
                         const int64_t k0 = (int64_t)na * g / G, k1 = (int64_t)na * (g + 1) / G;
                         for (int64_t k = k0 + threadIdx.x; k < k1; k += kThreads) {
                             A acc = T::zero();
@@ -356,24 +482,24 @@ __global__ void __launch_bounds__(kThreads) null_kernel(Params p) {
                             y[k] = acc;
                         }
                     }
-                    if (!team_sync(bar, err, G)) goto timeout;
+                    if (!team_sync(bar, G)) goto timeout;
+                    // y in the input precision, as the reference's product (rowc is free again)
+                    for (int k = threadIdx.x; k < na; k += kThreads) T::st(rowc + k, ldy(y + k));
+                    __syncthreads();
                     double pn2b = 0.0;
-                    for (int64_t i = r0 + warp; i < r1; i += kWarps) {
-                        const S *xrow = X + i * n;
-                        A acc = T::zero();
-                        for (int k = lane; k < na; k += 32)
-                            acc = T::fma_(acc, T::ld(xrow + k), TEAM ? T::ldcgA(y + k) : y[k]);
-                        acc = T::shfl_sum(acc);
-                        if (lane == 0) {
-                            T::st(X + i * n + col, T::sub(T::ld(X + i * n + col), acc));
-                            pn2b += T::norm2(T::ld(X + i * n + col));
+                    for (int64_t i0 = r0; i0 < r1; i0 += kGroups) {
+                        const int64_t i = i0 + grp;
+                        A acc = i < r1 ? row_dot<S, TEAM, false>(X + i * ldx, rowc, na, sub) : T::zero();
+                        acc = group_sum<A, T>(acc);
+                        if (sub == 0 && i < r1) {
+                            T::st(X + i * ldx + col, T::sub(T::ld(X + i * ldx + col), acc));
+                            pn2b += T::norm2(T::ld(X + i * ldx + col));
                         }
                     }
                     const double s2 = cta_sum(pn2b, s_dred);
                     if (threadIdx.x == 0) slots[G + g].val = s2;
-                    if (!team_sync(bar, err, G)) goto timeout;
-                    n2 = 0.0;
-                    for (int q = 0; q < G; ++q) n2 += TEAM ? __ldcg(&slots[G + q].val) : slots[G + q].val;
+                    if (!team_sync(bar, G)) goto timeout;
+                    n2 = team_sum(slots + G, G, TEAM, &s_sum);
                 }
                 const double len = sqrt(n2);
                 if (len < 10.0 * T::eps) {                 // primitives.py:451-452
@@ -385,8 +511,8 @@ __global__ void __launch_bounds__(kThreads) null_kernel(Params p) {
                 best = -1e300;
                 bidx = 0;
                 for (int64_t i = r0 + threadIdx.x; i < r1; i += kThreads) {
-                    T::st(X + i * n + col, T::scale(T::ld(X + i * n + col), inv));
-                    const double lv = lev[i] - T::norm2(T::ld(X + i * n + col));
+                    T::st(X + i * ldx + col, T::scale(T::ld(X + i * ldx + col), inv));
+                    const double lv = lev[i] - T::norm2(T::ld(X + i * ldx + col));
                     lev[i] = lv;
                     if (lv > best) { best = lv; bidx = i; }
                 }
@@ -396,13 +522,13 @@ __global__ void __launch_bounds__(kThreads) null_kernel(Params p) {
                     if (TEAM && g == 0) cmap[a] = (int)c;
                 }
                 ++a;
-                if (!team_sync(bar, err, G)) goto timeout;
+                if (!team_sync(bar, G)) goto timeout;
             }
             if (TEAM)                                      // completed columns back into U
                 for (int64_t i = r0 + warp; i < r1; i += kWarps)
-                    for (int k = nkept + lane; k < a; k += 32) U[i * n + __ldcg(&cmap[k])] = X[i * n + k];
+                    for (int k = nkept + lane; k < a; k += 32) U[i * n + __ldcg(&cmap[k])] = X[i * ldx + k];
             if (g == 0 && threadIdx.x == 0) p.status[z] = failed ? JB_ST_NULL_FAILED : JB_ST_OK;
-            if (!team_sync(bar, err, G)) goto timeout;
+            if (!team_sync(bar, G)) goto timeout;
         }
     }
     return;
@@ -474,7 +600,7 @@ static int launch(Params &p, const Plan &pl, cudaStream_t st) {
         return JB_ECUDA;
     // the barrier words and the error flag start at zero
     const Layout L = layout(p.m, p.n, sizeof(S), Tr<S>::cplx ? 16 : 8, pl.G);
-    if (cudaMemsetAsync(p.ws + L.bar, 0, 16, st) != cudaSuccess) return JB_ECUDA;
+    if (cudaMemsetAsync(p.ws + L.bar, 0, 256, st) != cudaSuccess) return JB_ECUDA;
     int per_sm = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, pl.smem) != cudaSuccess)
         return JB_ECUDA;

@@ -644,6 +644,8 @@ def _block_svd(a, full_matrices, values_only, return_info, rank, opts):
         plan = _block_plans.get(key)
         if plan is None:
             plan = _block_plans[key] = BlockJacobi(mt, nt, used, device=dev)
+            # launch choices timed once per shape, on the first matrix (preparation)
+            plan.tune((x[0] if m >= n else x[0].t()).contiguous())
         us, ss, vs, sweeps = [], [], [], 0
         for z in range(x.shape[0]):
             xt = x[z] if m >= n else x[z].t()

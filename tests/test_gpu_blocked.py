@@ -90,34 +90,35 @@ def test_block_eig_f64(n):
 
 
 @pytest.mark.parametrize("n", [64, 128])
-@pytest.mark.parametrize("sweeps", [1, 2])
-def test_block_eig_cluster_equals_register_kernel(n, sweeps):
-    """The cluster eigen-solve (one cluster of 8 CTAs per slot, distributed
-    shared memory) runs the register kernel's rotations: the same Q^T parts,
-    off, dmax, bit for bit, on graded Grams."""
+def test_block_eig_variants_agree(n):
+    """The register-resident odd-even kernel at 4, 8 and 16 columns per warp
+    and the shared-memory round-robin kernel (jb_block_eig_f64_ex variants 4,
+    8, 16 and 1) diagonalise the same graded Grams: the register layouts run
+    the same rotations (each build may contract multiply-adds differently,
+    so Q^T agrees to FP32 rounding); the round robin (a different pair order)
+    gives the same eigenvectors up to sign within the FP32 accumulation of Q."""
     N = importlib.import_module("pavel-s_svd_b200.native")
-    g = torch.Generator(device="cuda").manual_seed(n + sweeps)
-    P = 16
+    g = torch.Generator(device="cuda").manual_seed(n)
+    P = 8
     x = torch.randn(P, n, 2 * n, device="cuda", generator=g, dtype=torch.float64)
     x = x * torch.logspace(0, -4, n, device="cuda", dtype=torch.float64)[:, None]
     G = (x @ x.transpose(1, 2)).float().contiguous()
-    live = torch.full((1,), 1e-12, dtype=torch.float64, device="cuda")
     st = torch.cuda.current_stream().cuda_stream
     outs = []
-    for variant in (1, 2):
-        qt = [torch.full((P, n, n), 7.0, dtype=torch.bfloat16, device="cuda") for _ in range(3)]
+    for variant in (8, 1, 4, 16):
+        qt = [torch.empty(P, n, n, dtype=torch.bfloat16, device="cuda") for _ in range(3)]
         off = torch.zeros(P, device="cuda")
         dmax = torch.zeros(P, device="cuda")
         sw = torch.zeros(P, dtype=torch.int32, device="cuda")
         N.check(N.lib().jb_block_eig_f64_ex(G.data_ptr(), qt[0].data_ptr(), qt[1].data_ptr(), qt[2].data_ptr(),
-                                            off.data_ptr(), dmax.data_ptr(), sw.data_ptr(), P, n, sweeps, 1e-7,
-                                            live.data_ptr(), variant, st), "jb_block_eig_f64_ex")
+                                            off.data_ptr(), dmax.data_ptr(), sw.data_ptr(), P, n, 12, 1e-12, None,
+                                            variant, st), "jb_block_eig_f64_ex")
         torch.cuda.synchronize()
-        outs.append((qt, off, dmax))
-    (qa, offa, da), (qb, offb, db) = outs
-    for a, b in zip(qa, qb):
-        assert torch.equal(a, b)
-    assert torch.equal(offa, offb) and torch.equal(da, db)
+        outs.append(sum(q.double() for q in qt))
+    dots = (outs[0] * outs[1]).sum(-1).abs()                  # |<row of Q1^T, row of Q2^T>|
+    assert float((dots - 1).abs().max()) <= 1e-5
+    for other in outs[2:]:
+        torch.testing.assert_close(other, outs[0], rtol=0, atol=2e-6)
 
 
 def test_block_jacobi_drop_in():

@@ -7,6 +7,7 @@ tests start two processes that take the same steps bench.py takes under
 torchrun, without a GPU."""
 import json
 import os
+import re
 import socket
 import subprocess
 import sys
@@ -120,6 +121,6 @@ def test_bench_starts_one_rank_per_gpu(tmp_path):
                          capture_output=True, text=True, timeout=240,
                          env=dict(os.environ, OMP_NUM_THREADS="1"))
     assert out.returncode == 0, out.stderr[-2000:]
-    ranks = sorted((json.loads(x[5:]) for x in out.stdout.splitlines() if x.startswith("RANK ")),
-                   key=lambda r: r["rank"])
+    # the two ranks write to one stream, so their lines may interleave
+    ranks = sorted((json.loads(x) for x in re.findall(r"RANK (\{[^{}]*\})", out.stdout)), key=lambda r: r["rank"])
     assert [(r["rank"], r["world"], r["local"], r["sum"]) for r in ranks] == [(0, 2, 0, 3.0), (1, 2, 1, 3.0)]
