@@ -285,7 +285,10 @@ JB_API int jb_block_eig_f64(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_l
  * width up to 256), 4 / 8 / 16 = one CTA per slot with G and Q in registers
  * (slot widths 64 and 128, odd-even order), that many columns per warp
  * (n / variant warps; the same outputs, a different latency / occupancy
- * balance, chosen by the blocked solver's autotuner). */
+ * balance, chosen by the blocked solver's autotuner).  Adding JB_EIG_FP32 to
+ * a register variant (or to 0) rotates G in FP32 instead of FP64: for the
+ * sweeps whose Gram is itself only ~16-bit accurate (two-part operands). */
+#define JB_EIG_FP32 128
 JB_API int jb_block_eig_f64_ex(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
                                int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps, double tol,
                                const double *live_floor, int32_t variant, void *stream);

@@ -129,6 +129,9 @@ class BlockJacobi:
         self.gram_split = max(1, torch.cuda.get_device_properties(dev).multi_processor_count // self.P)
         # layout of the register eigen-solve: columns of G per warp (4, 8 or 16)
         self.eig_variant = 8
+        # the two-part sweeps' Grams carry ~16-bit accuracy: their eigen-solves
+        # may rotate G in FP32 (jb_block_eig_f64_ex with JB_EIG_FP32)
+        self.eig_fp32_two_part = False
         self.tuned = None
         self._graphs, self._seen = {}, set()
 
@@ -174,7 +177,7 @@ class BlockJacobi:
                                             self.Qt[2].data_ptr() if parts == 3 else None, self.off[r].data_ptr(),
                                             self.dmax[r].data_ptr(), self.isweeps.data_ptr(), P, 2 * b,
                                             inner_sweeps, inner_tol, self.live.data_ptr(),
-                                            self.eig_variant if 2 * b in (64, 128) else 0, st), "jb_block_eig_f64_ex")
+                                            self._eig_variant(parts), st), "jb_block_eig_f64_ex")
             # X_k <- vv^T X_k (rows of W^T), same for V, each rotated row
             # written (as BF16 parts) straight into its next-round slot.
             nxt = 1 - cur
@@ -183,12 +186,17 @@ class BlockJacobi:
             cur = nxt
         return cur
 
+    def _eig_variant(self, parts):
+        if 2 * self.b not in (64, 128):
+            return 0
+        return self.eig_variant | (N.EIG_FP32 if parts == 2 and self.eig_fp32_two_part else 0)
+
     def _run_sweep(self, cur, parts, inner_sweeps, inner_tol, use_graphs):
         """One sweep, replayed from a CUDA graph after its first (eager) run:
         the ~4 (nb - 1) launches of a sweep then cost one host call.  The
         graphs hold only this plan's buffers; the live floor is read on the
         device (self.live)."""
-        key = (cur, parts, inner_sweeps, inner_tol, self.eig_variant, self.gram_split)
+        key = (cur, parts, inner_sweeps, inner_tol, self._eig_variant(parts), self.gram_split)
         if not use_graphs or key not in self._seen:
             self._seen.add(key)
             return self._sweep(cur, parts, inner_sweeps, inner_tol)

@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(kEigThreads) eig_kernel(const float *Gin, __nv
 // diagonal d and superdiagonal e (published in shared memory by their
 // owners), one barrier, rotations, (odd rounds: boundary exchange, one
 // barrier), new d / e, one barrier.
-template <int RPT, int CB>
+template <int RPT, int CB, typename TG>
 __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *Gin, __nv_bfloat16 *Qt_hi,
                                                             __nv_bfloat16 *Qt_lo, __nv_bfloat16 *Qt_lo2,
                                                             float *off_out, float *dmax_out, int *sweeps_out,
@@ -247,11 +247,11 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
     constexpr int NW = n / CB;                 // warps
     static_assert(CB % 2 == 0 && NW >= RPT / 2, "columns per warp");
     extern __shared__ __align__(16) unsigned char smem[];
-    double *sd = (double *)smem;               // d[x] = G[x][x]
-    double *se = sd + n;                       // e[x] = G[x][x + 1]
-    double *sc = se + n;                       // c of the pair starting at position p
-    double *ss = sc + n;                       // s of the pair starting at position p
-    double *bg = ss + n;                       // [NW][2][n] boundary columns of G (first, last)
+    TG *sd = (TG *)smem;               // d[x] = G[x][x]
+    TG *se = sd + n;                       // e[x] = G[x][x + 1]
+    TG *sc = se + n;                       // c of the pair starting at position p
+    TG *ss = sc + n;                       // s of the pair starting at position p
+    TG *bg = ss + n;                       // [NW][2][n] boundary columns of G (first, last)
     float *bq = (float *)(bg + (size_t)NW * 2 * n);  // [NW][2][n] boundary columns of Q
     float *Qs = bq + (size_t)NW * 2 * n;       // n x n, Q[col * n + row] (write-out)
     int *perm = (int *)(Qs + (size_t)n * n);   // n
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
     const double live_floor = live_floor_ptr ? *live_floor_ptr : 0.0;
     const float *g_in = Gin + (size_t)k * n * n;
 
-    double g[RPT][CB];
+    TG g[RPT][CB];
     float q[RPT][CB];
 #pragma unroll
     for (int i = 0; i < RPT; ++i)
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
         for (int j = 0; j < CB; ++j) {
             const int r = r0 + i, c = c0 + j;
             // symmetrise (the tensor-core Gram is symmetric up to rounding)
-            g[i][j] = 0.5 * ((double)g_in[(size_t)r * n + c] + (double)g_in[(size_t)c * n + r]);
+            g[i][j] = (TG)(0.5 * ((double)g_in[(size_t)r * n + c] + (double)g_in[(size_t)c * n + r]));
             q[i][j] = (r == c) ? 1.f : 0.f;
         }
     auto publish_de = [&]() {
@@ -290,14 +290,16 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
     if (threadIdx.x == 0) s_first_off = 0.0;
     __syncthreads();
     double dm = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) dm = fmax(dm, sd[i]);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dm = fmax(dm, (double)sd[i]);
     for (int o = 16; o; o >>= 1) dm = fmax(dm, __shfl_xor_sync(0xffffffffu, dm, o));
     if (lane == 0) s_red[warp] = dm;
     __syncthreads();
     double gmax = 0.0;
 #pragma unroll
     for (int w = 0; w < NW; ++w) gmax = fmax(gmax, s_red[w]);
-    const double floor_ = 2.220446049250313e-16 * 2.220446049250313e-16 * gmax;
+    // eps of the arithmetic squared times the largest diagonal: the active floor
+    constexpr double eps_g = sizeof(TG) == 8 ? 2.220446049250313e-16 : 1.1920928955078125e-07;
+    const double floor_ = eps_g * eps_g * gmax;
     const double tol2 = tol * tol;
     int sweep = 0;
     for (sweep = 1; sweep <= max_sweeps; ++sweep) {
@@ -312,22 +314,31 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
                     if (t >= n / 2 - par) goto angles_done;
                     const int p = 2 * t + par;
                     const double app = sd[p], aqq = sd[p + 1], apq = se[p];
-                    double c = 1.0, sn = 0.0;
+                    TG c = 1, sn = 0;
                     const double prod = app * aqq, apq2 = apq * apq;
                     if (apq2 > tol2 * prod && fmin(app, aqq) > floor_) {
                         // off over live columns only (solvers.py:55-57)
                         if (fmin(app, aqq) > live_floor && apq2 * offd > offn * prod) { offn = apq2; offd = prod; }
-                        const double d = aqq - app, a2 = 2.0 * fabs(apq);
-                        const int ex = (__double2hiint(fmax(fabs(d), a2)) >> 20) & 0x7ff;
-                        const double scl = __hiloint2double((2046 - ex) << 20, 0);
-                        const float df = fabsf((float)(d * scl)), af = (float)(a2 * scl);
-                        const float tf = __fdividef(af, df + sqrtf(df * df + af * af));
-                        const double tt = d < 0.0 ? -(double)tf : (double)tf;
-                        // c = 1 / sqrt(1 + t^2): FP32 estimate and one Newton step in FP64
-                        const double x = 1.0 + tt * tt;
-                        const double c0 = (double)rsqrtf(1.f + tf * tf);
-                        c = c0 * (1.5 - 0.5 * x * c0 * c0);
-                        sn = tt * c;
+                        if constexpr (sizeof(TG) == 8) {
+                            const double d = aqq - app, a2 = 2.0 * fabs(apq);
+                            const int ex = (__double2hiint(fmax(fabs(d), a2)) >> 20) & 0x7ff;
+                            const double scl = __hiloint2double((2046 - ex) << 20, 0);
+                            const float df = fabsf((float)(d * scl)), af = (float)(a2 * scl);
+                            const float tf = __fdividef(af, df + sqrtf(df * df + af * af));
+                            const double tt = d < 0.0 ? -(double)tf : (double)tf;
+                            // c = 1 / sqrt(1 + t^2): FP32 estimate and one Newton step in FP64
+                            const double x = 1.0 + tt * tt;
+                            const double c0 = (double)rsqrtf(1.f + tf * tf);
+                            c = c0 * (1.5 - 0.5 * x * c0 * c0);
+                            sn = tt * c;
+                        } else {
+                            // FP32 G (the two-part stage): the same angle, all in FP32
+                            const float d = (float)(aqq - app), a2 = 2.f * fabsf((float)apq);
+                            const float tf = __fdividef(a2, fabsf(d) + sqrtf(d * d + a2 * a2));
+                            const float tt = d < 0.f ? -tf : tf;
+                            c = rsqrtf(1.f + tt * tt);
+                            sn = tt * c;
+                        }
                         if (apq < 0.0) sn = -sn;
                         s_any = 1;
                     }
@@ -341,32 +352,32 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
             if (par == 0) {
 #pragma unroll
                 for (int i = 0; i < RPT; i += 2) {
-                    const double c = sc[r0 + i], sn = ss[r0 + i];
+                    const TG c = sc[r0 + i], sn = ss[r0 + i];
 #pragma unroll
                     for (int j = 0; j < CB; ++j) {
-                        const double x = g[i][j], y = g[i + 1][j];
+                        const TG x = g[i][j], y = g[i + 1][j];
                         g[i][j] = sn * x + c * y;
                         g[i + 1][j] = c * x - sn * y;
                     }
                 }
             } else {
                 const bool has_up = lane > 0, has_down = lane < 31;
-                const double cu = has_up ? sc[r0 - 1] : 1.0, su = has_up ? ss[r0 - 1] : 0.0;
-                const double cd = has_down ? sc[r0 + RPT - 1] : 1.0, sdn = has_down ? ss[r0 + RPT - 1] : 0.0;
+                const TG cu = has_up ? sc[r0 - 1] : (TG)1, su = has_up ? ss[r0 - 1] : (TG)0;
+                const TG cd = has_down ? sc[r0 + RPT - 1] : (TG)1, sdn = has_down ? ss[r0 + RPT - 1] : (TG)0;
 #pragma unroll
                 for (int j = 0; j < CB; ++j) {
-                    const double up = __shfl_up_sync(0xffffffffu, g[RPT - 1][j], 1);   // row r0 - 1
-                    const double dn = __shfl_down_sync(0xffffffffu, g[0][j], 1);       // row r0 + RPT
-                    const double first = g[0][j], last = g[RPT - 1][j];
+                    const TG up = __shfl_up_sync(0xffffffffu, g[RPT - 1][j], 1);   // row r0 - 1
+                    const TG dn = __shfl_down_sync(0xffffffffu, g[0][j], 1);       // row r0 + RPT
+                    const TG first = g[0][j], last = g[RPT - 1][j];
                     if (has_up) g[0][j] = cu * up - su * first;                         // second of pair (r0 - 1, r0)
                     if (has_down) g[RPT - 1][j] = sdn * last + cd * dn;                 // first of pair (r0 + RPT - 1, r0 + RPT)
                 }
 #pragma unroll
                 for (int i = 1; i + 1 < RPT; i += 2) {
-                    const double c = sc[r0 + i], sn = ss[r0 + i];
+                    const TG c = sc[r0 + i], sn = ss[r0 + i];
 #pragma unroll
                     for (int j = 0; j < CB; ++j) {
-                        const double x = g[i][j], y = g[i + 1][j];
+                        const TG x = g[i][j], y = g[i + 1][j];
                         g[i][j] = sn * x + c * y;
                         g[i + 1][j] = c * x - sn * y;
                     }
@@ -376,11 +387,11 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
             if (par == 0) {
 #pragma unroll
                 for (int j = 0; j < CB; j += 2) {
-                    const double c = sc[c0 + j], sn = ss[c0 + j];
+                    const TG c = sc[c0 + j], sn = ss[c0 + j];
                     const float fc = (float)c, fs = (float)sn;
 #pragma unroll
                     for (int i = 0; i < RPT; ++i) {
-                        const double x = g[i][j], y = g[i][j + 1];
+                        const TG x = g[i][j], y = g[i][j + 1];
                         g[i][j] = sn * x + c * y;
                         g[i][j + 1] = c * x - sn * y;
                         const float u = q[i][j], v = q[i][j + 1];
@@ -399,19 +410,19 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
                 }
                 __syncthreads();
                 const bool has_left = warp > 0, has_right = warp < NW - 1;
-                const double cl = has_left ? sc[c0 - 1] : 1.0, sl = has_left ? ss[c0 - 1] : 0.0;
-                const double cr = has_right ? sc[c0 + CB - 1] : 1.0, sr = has_right ? ss[c0 + CB - 1] : 0.0;
+                const TG cl = has_left ? sc[c0 - 1] : (TG)1, sl = has_left ? ss[c0 - 1] : (TG)0;
+                const TG cr = has_right ? sc[c0 + CB - 1] : (TG)1, sr = has_right ? ss[c0 + CB - 1] : (TG)0;
 #pragma unroll
                 for (int i = 0; i < RPT; ++i) {
                     const int row = r0 + i;
                     if (has_left) {                // pair (c0 - 1, c0): this warp holds the second
-                        const double x = bg[((size_t)(warp - 1) * 2 + 1) * n + row];
+                        const TG x = bg[((size_t)(warp - 1) * 2 + 1) * n + row];
                         const float u = bq[((size_t)(warp - 1) * 2 + 1) * n + row];
                         g[i][0] = cl * x - sl * g[i][0];
                         q[i][0] = (float)cl * u - (float)sl * q[i][0];
                     }
                     if (has_right) {               // pair (c0 + CB - 1, c0 + CB): this warp holds the first
-                        const double y = bg[((size_t)(warp + 1) * 2 + 0) * n + row];
+                        const TG y = bg[((size_t)(warp + 1) * 2 + 0) * n + row];
                         const float v = bq[((size_t)(warp + 1) * 2 + 0) * n + row];
                         g[i][CB - 1] = sr * g[i][CB - 1] + cr * y;
                         q[i][CB - 1] = (float)sr * q[i][CB - 1] + (float)cr * v;
@@ -419,11 +430,11 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
                 }
 #pragma unroll
                 for (int j = 1; j + 1 < CB; j += 2) {
-                    const double c = sc[c0 + j], sn = ss[c0 + j];
+                    const TG c = sc[c0 + j], sn = ss[c0 + j];
                     const float fc = (float)c, fs = (float)sn;
 #pragma unroll
                     for (int i = 0; i < RPT; ++i) {
-                        const double x = g[i][j], y = g[i][j + 1];
+                        const TG x = g[i][j], y = g[i][j + 1];
                         g[i][j] = sn * x + c * y;
                         g[i][j + 1] = c * x - sn * y;
                         const float u = q[i][j], v = q[i][j + 1];
@@ -487,7 +498,7 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
     }
 }
 
-__host__ inline size_t eig_reg_smem_bytes(int n, int cb) {
+__host__ inline size_t eig_reg_smem_bytes(int n, int cb) {   // sized for FP64 G (enough for FP32)
     const int nw = n / cb;
     return (size_t)4 * n * 8 + (size_t)nw * 2 * n * 8 + (size_t)nw * 2 * n * 4 + (size_t)n * n * 4 + (size_t)n * 4 +
            16;
@@ -627,19 +638,37 @@ __global__ void __launch_bounds__(256) gemm_f64acc_kernel(const float *A, const 
     }
 }
 
-template <int RPT, int CB>
+template <int RPT, int CB, typename TG>
 static int launch_eig_reg(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
                           int32_t *sweeps, int64_t pairs, int32_t max_sweeps, double tol, const double *live_floor,
                           cudaStream_t st) {
     constexpr int n = 32 * RPT;
     const size_t smem = eig_reg_smem_bytes(n, CB);
-    auto kern = eig_reg_kernel<RPT, CB>;
+    auto kern = eig_reg_kernel<RPT, CB, TG>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return JB_ECUDA;
     kern<<<(unsigned)pairs, 32 * (n / CB), smem, st>>>(G, (__nv_bfloat16 *)Qt_hi, (__nv_bfloat16 *)Qt_lo,
                                                       (__nv_bfloat16 *)Qt_lo2, off, dmax, sweeps, max_sweeps, tol,
                                                       live_floor);
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+}
+
+template <typename TG>
+static int dispatch_eig_reg(int n, int cb, const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off,
+                            float *dmax, int32_t *sweeps, int64_t pairs, int32_t max_sweeps, double tol,
+                            const double *live_floor, cudaStream_t st) {
+#define JB_EIG_CASE(NN, RPT, CBV)                                                                               \
+    if (n == NN && cb == CBV)                                                                                   \
+        return launch_eig_reg<RPT, CBV, TG>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps, tol, \
+                                            live_floor, st);
+    JB_EIG_CASE(64, 2, 4)
+    JB_EIG_CASE(64, 2, 8)
+    JB_EIG_CASE(64, 2, 16)
+    JB_EIG_CASE(128, 4, 4)
+    JB_EIG_CASE(128, 4, 8)
+    JB_EIG_CASE(128, 4, 16)
+#undef JB_EIG_CASE
+    return JB_EINVAL;
 }
 
 }  // namespace blk
@@ -652,21 +681,20 @@ extern "C" {
 int jb_block_eig_f64_ex(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
                         int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps, double tol,
                         const double *live_floor, int32_t variant, void *stream) {
+    const int lay = variant & ~JB_EIG_FP32;
     if (!G || !Qt_hi || !Qt_lo || pairs < 1 || n < 2 || (n & 1) || max_sweeps < 1 ||
-        !(variant == 0 || variant == 1 || variant == 4 || variant == 8 || variant == 16))
+        !(lay == 0 || lay == 1 || lay == 4 || lay == 8 || lay == 16) || (variant & ~(JB_EIG_FP32 | 31)) ||
+        ((variant & JB_EIG_FP32) && !((n == 64 || n == 128) && lay != 1)))
         return JB_EINVAL;
     cudaStream_t st = (cudaStream_t)stream;
-    if ((n == 64 || n == 128) && variant != 1) {
-        const int cb = variant == 0 ? 8 : variant;
-        switch (n * 100 + cb) {
-            case 6404: return launch_eig_reg<2, 4>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps, tol, live_floor, st);
-            case 6408: return launch_eig_reg<2, 8>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps, tol, live_floor, st);
-            case 6416: return launch_eig_reg<2, 16>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps, tol, live_floor, st);
-            case 12804: return launch_eig_reg<4, 4>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps, tol, live_floor, st);
-            case 12808: return launch_eig_reg<4, 8>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps, tol, live_floor, st);
-            case 12816: return launch_eig_reg<4, 16>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps, tol, live_floor, st);
-            default: return JB_EINVAL;
-        }
+    const bool g32 = (variant & JB_EIG_FP32) != 0;
+    const int layout = variant & ~JB_EIG_FP32;
+    if ((n == 64 || n == 128) && layout != 1) {
+        const int cb = layout == 0 ? 8 : layout;
+        return g32 ? dispatch_eig_reg<float>(n, cb, G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps,
+                                             tol, live_floor, st)
+                   : dispatch_eig_reg<double>(n, cb, G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps,
+                                              tol, live_floor, st);
     }
     if (n > 256) return JB_ETOOBIG;                  // players are stored as bytes
     const size_t smem = eig_smem_bytes(n);

@@ -18,11 +18,14 @@
 // column; products accumulate in FP64 (complex: FP64 pairs).
 //   * Many matrices (team of one CTA per matrix): the second projection
 //     always runs, as in the reference.
-//   * Few large matrices: one team of CTAs (about one per SM, cooperative
-//     launch, rows split evenly) handles one matrix after another, with two
-//     grid-wide barriers per column.  The second projection runs when the
-//     first left ||v||^2 < 1/2 (Kahan-Parlett "twice is enough": otherwise
-//     v is already orthogonal to the columns to working accuracy).
+//   * Few large matrices: one team of CTAs (about 64 rows each, at most one
+//     per SM, cooperative launch) handles one matrix after another.  The
+//     first projection's length^2 equals the pivot's leverage (v = P e_idx,
+//     P the projector onto the complement), so while that leverage is at
+//     least 1/2 a column costs one grid-wide barrier: v is normalised by it
+//     directly (Kahan-Parlett "twice is enough": v is then orthogonal to the
+//     columns to working accuracy and needs no second projection).  Below
+//     1/2 the second projection runs, with the norm reduced over the team.
 // Every barrier wait is bounded (about two seconds of globaltimer); a wait
 // that runs out marks the team's matrix JB_ST_TIMEOUT and the CTAs return.
 #include <cuda_runtime.h>
@@ -216,7 +219,7 @@ __device__ __forceinline__ double cta_sum(double v, double *red) {
 
 // Team-wide reductions over the G slots, read by warp 0 only (one L2 read
 // per slot per CTA) and broadcast through shared memory.
-__device__ __forceinline__ int64_t team_argmax(const Slot *slots, int G, bool team, int64_t *s_idx) {
+__device__ __forceinline__ Slot team_argmax(const Slot *slots, int G, bool team, Slot *s_slot) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (warp == 0) {
         double best = -1e300;
@@ -231,10 +234,10 @@ __device__ __forceinline__ int64_t team_argmax(const Slot *slots, int G, bool te
             const int64_t oi = __shfl_xor_sync(0xffffffffu, bidx, o);
             if (ob > best || (ob == best && oi < bidx)) { best = ob; bidx = oi; }
         }
-        if (lane == 0) *s_idx = bidx;
+        if (lane == 0) *s_slot = {best, bidx};
     }
     __syncthreads();
-    const int64_t r = *s_idx;
+    const Slot r = *s_slot;
     __syncthreads();
     return r;
 }
@@ -362,7 +365,7 @@ __global__ void __launch_bounds__(kThreads, 1) null_kernel(Params p) {
     __shared__ Slot s_red[kWarps];
     __shared__ double s_dred[kWarps];
     __shared__ int s_flag;
-    __shared__ int64_t s_idx;
+    __shared__ Slot s_piv;
     __shared__ double s_sum;
     const int G = TEAM ? p.G : 1;
     const int g = TEAM ? blockIdx.x : 0;                   // rank in the team
@@ -437,20 +440,47 @@ __global__ void __launch_bounds__(kThreads, 1) null_kernel(Params p) {
                 const int na = TEAM ? a : (int)n;          // columns a product runs over
                 const int64_t col = TEAM ? a : c;          // where v is built
                 // idx = team-wide first argmax of the leverage
-                const int64_t idx = team_argmax(slots, G, TEAM, &s_idx);
+                const Slot piv = team_argmax(slots, G, TEAM, &s_piv);
+                const int64_t idx = piv.idx;
+                // The first projection's length^2 is the pivot's leverage (v = P e_idx
+                // with P the projector onto the complement, so |v|^2 = P_idx,idx).  A
+                // team that needs no second projection (leverage >= 1/2) normalises
+                // by it at once and saves the team-wide norm reduction.
+                const bool fast = TEAM && piv.val >= 0.5;
+                const double inv_fast = fast ? 1.0 / sqrt(piv.val) : 0.0;
                 for (int k = threadIdx.x; k < na; k += kThreads) T::st(rowc + k, ldx_(X + idx * ldx + k));
                 __syncthreads();
                 // first projection, row-local: v_i = delta - X_i . conj(X_idx)
                 // (column col of X is still zero in every row)
                 double pn2 = 0.0;
+                best = -1e300;
+                bidx = 0;
                 for (int64_t i0 = r0; i0 < r1; i0 += kGroups) {
                     const int64_t i = i0 + grp;
                     A acc = i < r1 ? row_dot<S, TEAM, true>(X + i * ldx, rowc, na, sub) : T::zero();
                     acc = group_sum<A, T>(acc);
                     if (sub == 0 && i < r1) {
-                        T::st(X + i * ldx + col, T::sub(i == idx ? T::unit() : T::zero(), acc));
-                        pn2 += T::norm2(T::ld(X + i * ldx + col));
+                        const A v = T::sub(i == idx ? T::unit() : T::zero(), acc);
+                        if (fast) {
+                            T::st(X + i * ldx + col, T::scale(v, inv_fast));
+                            const double lv = lev[i] - T::norm2(T::ld(X + i * ldx + col));
+                            lev[i] = lv;
+                            if (lv > best) { best = lv; bidx = i; }
+                        } else {
+                            T::st(X + i * ldx + col, v);
+                            pn2 += T::norm2(T::ld(X + i * ldx + col));
+                        }
                     }
+                }
+                if (fast) {
+                    sb = cta_argmax(best, bidx, s_red);
+                    if (threadIdx.x == 0) {
+                        slots[g] = sb;
+                        if (g == 0) cmap[a] = (int)c;
+                    }
+                    ++a;
+                    if (!team_sync(bar, G)) goto timeout;
+                    continue;
                 }
                 double n2 = cta_sum(pn2, s_dred);
                 if (threadIdx.x == 0) slots[G + g].val = n2;
@@ -554,14 +584,14 @@ static int dev_sms() {
 }
 
 // One CTA per matrix unless the batch has few large matrices: then one
-// cooperative team of about one CTA per SM (at least 16 rows each).
+// cooperative team of up to one CTA per SM (about 64 rows each).
 static Plan make_plan(int dtype, int64_t batch, int64_t m, int64_t n) {
     Plan pl;
     const int sms = dev_sms();
     const int esz = esize(dtype), asz = dtype >= 2 ? 16 : 8;
     const bool large = batch * 4 < sms && m * n >= (1 << 16) && m >= 256;
     if (large) {
-        int64_t G = m / 16;
+        int64_t G = m / 64;                         // about 64 rows per CTA
         if (G > sms) G = sms;
         if (G < 2) G = 2;
         pl.G = (int)G;
