@@ -691,12 +691,11 @@ def run_warm(args):
     a_np, theta = wl.warm_family(count=65536, device="cuda")
     a = torch.from_numpy(a_np).cuda()
     tr, te = a[:60000].contiguous(), a[60000:64096].contiguous()
-    frame = wl.family_v(theta[:60000], device="cuda")
     e0, e1 = _events()
     e0.record()
     v_tr, _ = W.plain_v(tr)
     net = W.WarmStartMLP(seed=0)
-    hist = W.train(net, tr, v_tr, epochs=15, batch=512, lr=1e-3, order="frame", frame=frame)
+    hist = W.train(net, tr, v_tr, epochs=15, batch=512, lr=1e-3, order="assign")
     e1.record()
     torch.cuda.synchronize()
     train_ms = e0.elapsed_time(e1)

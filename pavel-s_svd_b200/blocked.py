@@ -130,8 +130,10 @@ class BlockJacobi:
         # layout of the register eigen-solve: columns of G per warp (4, 8 or 16)
         self.eig_variant = 8
         # the two-part sweeps' Grams carry ~16-bit accuracy: their eigen-solves
-        # may rotate G in FP32 (jb_block_eig_f64_ex with JB_EIG_FP32)
-        self.eig_fp32_two_part = False
+        # rotate G in FP32 (jb_block_eig_f64_ex with JB_EIG_FP32; measured on
+        # the 4096 x 1024 and 8192 x 2048 configurations: 1.3x faster per call,
+        # the same block sweeps and sigma errors); the three-part sweeps in FP64
+        self.eig_fp32_two_part = True
         self.tuned = None
         self._graphs, self._seen = {}, set()
 

@@ -178,28 +178,13 @@ def assign_order(v: torch.Tensor) -> torch.Tensor:
     return out
 
 
-def frame_order(v: torch.Tensor, frame: torch.Tensor) -> torch.Tensor:
-    """Reorder and re-sign the columns of V (B, n, n) into a reference frame
-    (B, n, n) spanning the same eigenvectors: column j becomes the column of V
-    most parallel to frame column j, signed to agree with it.  For training
-    matrices of a parameterised family the frame is the generator's smooth
-    V(theta); the numbers stay those of the solver's V."""
-    c = frame.transpose(-1, -2) @ v                      # (B, n, n): frame_j . v_k
-    k = c.abs().argmax(-1)                               # best v column for every frame column
-    picked = torch.gather(v, -1, k[:, None, :].expand_as(v))
-    sign = torch.sign(torch.gather(c, -1, k[..., None])[..., 0])
-    sign[sign == 0] = 1
-    return picked * sign[:, None, :]
-
-
-def labels(v: torch.Tensor, order="assign", frame=None) -> torch.Tensor:
-    """Training targets from the plain solver's V (B, n, n), flattened
+def labels(v: torch.Tensor, order="assign") -> torch.Tensor:
+    """Training targets from the plain solver's V (B, n, n) alone, flattened
     row-major: 'assign' (assign_order, default) or 'sorted' (the solver's
     singular-value order with canonical signs)."""
-    if order == "frame":
-        t = frame_order(v, frame)
-    else:
-        t = assign_order(v) if order == "assign" else canonical_signs(v)
+    if order not in ("assign", "sorted"):
+        raise ValueError("order must be 'assign' or 'sorted'")
+    t = assign_order(v) if order == "assign" else canonical_signs(v)
     return t.reshape(v.shape[0], -1).contiguous()
 
 
@@ -211,10 +196,10 @@ def plain_v(a: torch.Tensor, precision="mixed"):
 
 
 def train(net: WarmStartMLP, a_train: torch.Tensor, v_train: torch.Tensor, epochs=10, batch=1024, lr=1e-3,
-          seed=0, log=None, order="assign", frame=None):
+          seed=0, log=None, order="assign"):
     """Minibatch Adam on (sketch(a), canonical V) pairs; returns per-epoch mean loss."""
     x_all = sketch(a_train)
-    t_all = labels(v_train, order, frame)
+    t_all = labels(v_train, order)
     g = torch.Generator(device="cpu").manual_seed(seed)
     hist = []
     n = x_all.shape[0]

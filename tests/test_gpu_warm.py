@@ -85,34 +85,52 @@ def test_exact_and_garbage_starts(W, workloads):
 
 
 def test_trained_network_saves_sweeps(W, workloads):
-    """The configured split: train on 60000 matrices of the family (labels:
-    the plain solver's V, columns aligned to the generator's frame), evaluate
-    4096 held-out matrices.  The trained start must lower the Gram off-norm,
-    be kept for most matrices and save sweeps; the ideal start (the frame
-    itself) bounds what a perfect network could save."""
+    """The configured split: train on 60000 matrices of the family with labels
+    taken only from the plain solver's V (columns in the label-only canonical
+    order of assign_order), evaluate 4096 held-out matrices.  The trained
+    start must lower the Gram off-norm, be kept for most matrices and save
+    sweeps, with the same singular values; the ideal start (the generator's
+    own V(theta), used here only as a bound) shows what a perfect network
+    could save.  The gain in matrices/s is measured and printed, not
+    asserted: on this family the saved sweeps (~4 %) do not pay for the
+    network and the start's preparation (warm ~3 % slower than plain), and
+    only the overhead is bounded here."""
     a_np, theta = workloads.warm_family(count=65536, device="cuda")
     a = torch.from_numpy(a_np).cuda()
     tr, te = a[:60000].contiguous(), a[60000:64096].contiguous()
-    frame = workloads.family_v(theta[:60000], device="cuda")
     v_tr, _ = W.plain_v(tr)
     net = W.WarmStartMLP(seed=0)
-    hist = W.train(net, tr, v_tr, epochs=15, batch=512, lr=1e-3, order="frame", frame=frame)
-    assert hist[-1] < 0.2 * hist[0]
+    hist = W.train(net, tr, v_tr, epochs=15, batch=512, lr=1e-3, order="assign")
+    assert hist[-1] < 0.5 * hist[0]
     solver = W.WarmSolver(net, m=128, n=64, batch=4096)
     eye = torch.eye(64, device="cuda").expand(4096, 64, 64).contiguous()
-    solver.launch(te, v0=eye)
+
+    def timed(v0):
+        solver.launch(te, v0=v0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            solver.launch(te, v0=v0)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 3
+
+    ms_plain = timed(eye)
     n_plain, used0 = solver.check()
     s_plain = solver.S.clone()
     assert used0.sum() == 0
-    solver.launch(te)
+    ms_warm = timed(None)
     sweeps, used = solver.check()
     off0, off1 = float(solver.off[0].mean()), float(solver.off[1].mean())
     s_warm = solver.S.clone()
     solver.launch(te, v0=workloads.family_v(theta[60000:64096], device="cuda").contiguous())
     ideal, _ = solver.check()
-    print(f"held-out sweeps: plain {n_plain.mean():.2f}, trained {sweeps.mean():.2f} (kept {used.mean():.2f}, "
-          f"off-norm {off0:.3f} -> {off1:.3f}), ideal start {ideal.mean():.2f}")
+    print(f"held-out sweeps: plain {n_plain.mean():.2f} ({ms_plain:.2f} ms), trained {sweeps.mean():.2f} "
+          f"({ms_warm:.2f} ms, kept {used.mean():.2f}, off-norm {off0:.3f} -> {off1:.3f}), ideal start "
+          f"{ideal.mean():.2f}")
     assert float(((s_warm - s_plain).abs() / s_plain[:, :1]).max()) <= 1e-5
     assert used.mean() > 0.5
     assert off1 < off0
     assert sweeps.mean() < n_plain.mean()
+    assert ms_warm <= 1.15 * ms_plain
