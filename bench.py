@@ -673,7 +673,9 @@ def run_blocked(args, name):
             "scaling": "none (single matrix)", "vs_baseline": None,
             "dtype": "f32 in/out; bf16x3/bf16x6 tensor; f64 eig",
             "config": {"workload": name, "m": m, "n": n, "block_size": b,
-                       "launch": {"eig_cols_per_warp": plan.eig_variant, "gram_split": plan.gram_split},
+                       "launch": {"eig_cols_per_warp": plan.eig_variant, "gram_split": plan.gram_split,
+                                  "schedule": plan.schedule, "slot_split": plan.slot_split,
+                                  "eig_fp32_two_part": plan.eig_fp32_two_part},
                        "autotuner_ms_per_sweep": {k: round(v, 3) for k, v in tune_ms.items()}},
             "data": ("synthetic (seeded: Haar U, V; 64 clusters x 16, cond 1e6)" if name == "clustered_large"
                      else "synthetic (seeded: rank-64 Gaussian product + N(0, 1e-6) noise)"),

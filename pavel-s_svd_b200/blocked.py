@@ -134,6 +134,11 @@ class BlockJacobi:
         # the 4096 x 1024 and 8192 x 2048 configurations: 1.3x faster per call,
         # the same block sweeps and sigma errors); the three-part sweeps in FP64
         self.eig_fp32_two_part = True
+        # "batched": every round's products as one launch per kind; "dataflow":
+        # per-slot launches on per-slot streams with only the true dependencies
+        # (_sweep_dataflow), so products overlap other slots' eigen-solves
+        self.schedule = "batched"
+        self.slot_split = 1            # K split of a per-slot Gram (1: the fewest CTAs TMEM allows)
         self.tuned = None
         self._graphs, self._seen = {}, set()
 
@@ -188,6 +193,82 @@ class BlockJacobi:
             cur = nxt
         return cur
 
+    def _dataflow_deps(self):
+        """Per round r (of a sweep) and next-round slot k: src[r][k], the
+        round-r slots whose updates write slot k's rows of round r + 1; war[r][k],
+        the round-r slots that read the rows slot k's round r + 1 update
+        overwrites (its blocks' positions two rounds on, in the buffer round r
+        read).  Both sets have at most two slots."""
+        if getattr(self, "_deps", None) is None:
+            R, pos = self.nb - 1, self.pos
+            src, war = [], []
+            for r in range(R):
+                nr, nnr = (r + 1) % R, (r + 2) % R
+                src.append([sorted({int(pos[r, i, 0]), int(pos[r, j, 0])}) for i, j in self.sched[nr]])
+                war.append([sorted({int(pos[nnr, i, 0]), int(pos[nnr, j, 0])}) for i, j in self.sched[nr]])
+            self._deps = (src, war)
+        return self._deps
+
+    def _sweep_dataflow(self, cur, parts, inner_sweeps, inner_tol):
+        """One sweep as a per-slot dataflow: slot k's Gram, eigen-solve and
+        W / V updates run on stream k; the Gram of next-round slot k waits only
+        for the two updates that write its rows, and an update waits for the
+        round-before readers of the rows it overwrites.  Captured into a CUDA
+        graph, one slot's products run on the SMs the other slots'
+        eigen-solves leave free, instead of every round's products waiting for
+        the slowest eigen-solve.  The same kernels and arithmetic per slot as
+        _sweep."""
+        lib = N.lib()
+        P, b, R = self.P, self.b, self.nb - 1
+        L = 2 * b
+        src, war = self._dataflow_deps()
+        main = torch.cuda.current_stream(self.device)
+        if getattr(self, "_slot_streams", None) is None:
+            self._slot_streams = [torch.cuda.Stream(self.device) for _ in range(P)]
+        streams = self._slot_streams
+        fork = torch.cuda.Event()
+        fork.record(main)
+        for st in streams:
+            st.wait_event(fork)
+        ev_w = [[torch.cuda.Event() for _ in range(P)] for _ in range(R)]
+        ev_v = [[torch.cuda.Event() for _ in range(P)] for _ in range(R)]
+        eigv = self._eig_variant(parts)
+        for r in range(R):
+            nxt = 1 - cur
+            Wp = [x.view(P, L, self.mpad) for x in self.W[cur][:parts]]
+            Vp = [x.view(P, L, self.npad) for x in self.V[cur][:parts]]
+            for k in range(P):
+                st = streams[k]
+                with torch.cuda.stream(st):
+                    if r > 0:
+                        for q in src[r - 1][k]:
+                            st.wait_event(ev_w[r - 1][q])
+                    gemm_parts([x[k:k + 1] for x in Wp], None, self.G[k:k + 1], syrk=True, chain128=True,
+                               split_k=self.slot_split)
+                    qt = [x[k:k + 1] for x in self.Qt[:parts]]
+                    N.check(lib.jb_block_eig_f64_ex(self.G[k].data_ptr(), qt[0].data_ptr(), qt[1].data_ptr(),
+                                                    qt[2].data_ptr() if parts == 3 else None,
+                                                    self.off[r, k:].data_ptr(), self.dmax[r, k:].data_ptr(),
+                                                    self.isweeps[k:].data_ptr(), 1, L, inner_sweeps, inner_tol,
+                                                    self.live.data_ptr(), eigv, st.cuda_stream),
+                            "jb_block_eig_f64_ex")
+                    if r > 0:
+                        for q in war[r - 1][k]:
+                            st.wait_event(ev_w[r - 1][q])
+                    rows = self.maps[r][k * L:(k + 1) * L]
+                    gemm_parts_rows(qt, [x[k:k + 1] for x in Wp], self.W[nxt][:parts], rows, b_mn=True)
+                    ev_w[r][k].record(st)
+                    if r > 0:
+                        for q in war[r - 1][k]:
+                            st.wait_event(ev_v[r - 1][q])
+                    gemm_parts_rows(qt, [x[k:k + 1] for x in Vp], self.V[nxt][:parts], rows, b_mn=True)
+                    ev_v[r][k].record(st)
+            cur = nxt
+        for k in range(P):
+            main.wait_event(ev_w[R - 1][k])
+            main.wait_event(ev_v[R - 1][k])
+        return cur
+
     def _eig_variant(self, parts):
         if 2 * self.b not in (64, 128):
             return 0
@@ -198,15 +279,17 @@ class BlockJacobi:
         the ~4 (nb - 1) launches of a sweep then cost one host call.  The
         graphs hold only this plan's buffers; the live floor is read on the
         device (self.live)."""
-        key = (cur, parts, inner_sweeps, inner_tol, self._eig_variant(parts), self.gram_split)
+        key = (cur, parts, inner_sweeps, inner_tol, self._eig_variant(parts), self.gram_split, self.schedule,
+               self.slot_split)
+        sweep = self._sweep_dataflow if self.schedule == "dataflow" else self._sweep
         if not use_graphs or key not in self._seen:
             self._seen.add(key)
-            return self._sweep(cur, parts, inner_sweeps, inner_tol)
+            return sweep(cur, parts, inner_sweeps, inner_tol)
         g = self._graphs.get(key)
         if g is None:
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g):
-                self._sweep(cur, parts, inner_sweeps, inner_tol)
+                sweep(cur, parts, inner_sweeps, inner_tol)
             self._graphs[key] = g
         g.replay()
         return 1 - cur
@@ -237,33 +320,51 @@ class BlockJacobi:
         return ap, at, e
 
     def tune(self, a: torch.Tensor, *, repeats=2):
-        """Autotuner of the launch choices: the register eigen-solve's layout
-        (4, 8 or 16 columns of G per warp; slot widths 64 and 128) and the
-        Gram's split along K (about one wave of CTAs over the SMs, or twice
-        that).  Each choice times `repeats` sweeps of the two-part stage on a
-        (CUDA events, after one warm-up sweep); the fastest is kept for every
-        later solve.  The choices change no result beyond rounding.  Returns
-        {choice: ms per sweep}."""
+        """Autotuner of the launch choices, on a's two-part sweeps (CUDA
+        events, after a warm-up sweep); the fastest of each is kept for every
+        later solve, and no choice changes a result beyond rounding:
+          * the register eigen-solve's layout (4, 8 or 16 columns of G per
+            warp; slot widths 64 and 128) and the Gram's split along K (about
+            one wave of CTAs over the SMs, or twice that), timed as eager
+            launches of the batched schedule;
+          * then the schedule, batched or per-slot dataflow (with the per-slot
+            Gram split the fewest CTAs TMEM allows, or twice that), timed as
+            replays of the captured sweep graph.
+        Returns {choice: ms per sweep}."""
         base_split = self.gram_split
         variants = (4, 8, 16) if 2 * self.b in (64, 128) else (8,)
-        splits = (base_split, 2 * base_split)
         times = {}
         _, at, _ = self._load(a)
         self.live.fill_(1e-4 * float((at * at).sum(1).max()))     # the two-part stage's live floor
+        self.schedule = "batched"
         cur = 0
+
+        def timed(step, warm=1):                                   # ms per sweep
+            nonlocal cur
+            for _ in range(warm):
+                cur = step(cur)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(repeats):
+                cur = step(cur)
+            e1.record()
+            torch.cuda.synchronize(self.device)
+            return e0.elapsed_time(e1) / repeats
+
         for v in variants:
-            for sp in splits:
+            for sp in (base_split, 2 * base_split):
                 self.eig_variant, self.gram_split = v, sp
-                cur = self._sweep(cur, 2, 1, 1e-7)
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record()
-                for _ in range(repeats):
-                    cur = self._sweep(cur, 2, 1, 1e-7)
-                e1.record()
-                torch.cuda.synchronize(self.device)
-                times[f"eig_cols_per_warp={v},gram_split={sp}"] = e0.elapsed_time(e1) / repeats
+                times[f"eig_cols_per_warp={v},gram_split={sp}"] = timed(lambda c: self._sweep(c, 2, 1, 1e-7))
         best = min(times, key=times.get)
         self.eig_variant, self.gram_split = [int(x.split("=")[1]) for x in best.split(",")]
+        graph_times = {}
+        for sched, split in (("batched", 1), ("dataflow", 1), ("dataflow", 2)):
+            self.schedule, self.slot_split = sched, split
+            # a sweep has an odd number of rounds, so the buffer parity alternates:
+            # two eager sweeps and two captures before the timed replays
+            graph_times[(sched, split)] = timed(lambda c: self._run_sweep(c, 2, 1, 1e-7, True), warm=4)
+            times[f"graph schedule={sched},slot_split={split}"] = graph_times[(sched, split)]
+        self.schedule, self.slot_split = min(graph_times, key=graph_times.get)
         self.tuned = times
         return times
 

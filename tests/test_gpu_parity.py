@@ -303,3 +303,26 @@ def test_uneven_size_classes_each_solved_once(pkg, precision):
         u2, s2, vh2 = pkg.svd(torch.from_numpy(a).to(DEV), precision=precision)
         torch.testing.assert_close(s, s2, rtol=0, atol=1e-6 * float(s2[0]))
         reference_check(a, u.cpu().numpy(), s.cpu().numpy(), vh.cpu().numpy(), 3e-4)
+
+
+def test_sharded_uneven_equals_single_plan(pkg, workloads):
+    """batch.ShardedUneven splits one uneven batch by cost into one share per
+    device (shard_by_cost) and solves every share with no exchange.  With
+    two shares on the one device of this run, every matrix's singular values
+    and sweeps equal those of the single-plan solve (the same kernels per
+    matrix), and every matrix is solved exactly once."""
+    from importlib import import_module
+    B = import_module("pavel-s_svd_b200.batch")
+    mats = workloads.uneven_batch(512)
+    B_, flat, m, n, plan = _plan(pkg, mats, "mixed")
+    plan.launch(flat)
+    sweeps = plan.check()
+    sh = B.ShardedUneven(m, n, [DEV, DEV], precision="mixed")
+    assert sorted(np.concatenate(sh.shards).tolist()) == list(range(len(mats)))
+    sh.launch(sh.pack(mats))
+    sw2 = sh.check()
+    assert np.array_equal(sw2, sweeps)
+    for i in range(len(mats)):
+        _, s1, _ = plan.result(i)
+        _, s2, _ = sh.result(i)
+        assert torch.equal(s1, s2), i
