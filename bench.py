@@ -675,7 +675,7 @@ def run_blocked(args, name):
             "config": {"workload": name, "m": m, "n": n, "block_size": b,
                        "launch": {"eig_cols_per_warp": plan.eig_variant, "gram_split": plan.gram_split,
                                   "schedule": plan.schedule, "slot_split": plan.slot_split,
-                                  "eig_fp32_two_part": plan.eig_fp32_two_part},
+                                  "eig_fp32_two_part": plan.eig_fp32_two_part, "eig_defer_q": plan.eig_defer_q},
                        "autotuner_ms_per_sweep": {k: round(v, 3) for k, v in tune_ms.items()}},
             "data": ("synthetic (seeded: Haar U, V; 64 clusters x 16, cond 1e6)" if name == "clustered_large"
                      else "synthetic (seeded: rank-64 Gaussian product + N(0, 1e-6) noise)"),

@@ -289,6 +289,20 @@ JB_API int jb_block_eig_f64(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_l
  * a register variant (or to 0) rotates G in FP32 instead of FP64: for the
  * sweeps whose Gram is itself only ~16-bit accurate (two-part operands). */
 #define JB_EIG_FP32 128
+
+/* jb_block_eig_f64_ex with a workspace, for JB_EIG_DEFER_Q: the register
+ * eigen-solve records its rotations instead of accumulating Q, and a second
+ * kernel forms Q^T from them, one warp per row of Q over the whole GPU (the
+ * eigen-solve itself then issues fewer instructions per round on its one SM
+ * per slot).  The same Q^T to FP32 rounding.  Register variants only (slot
+ * widths 64 and 128).  Workspace: jb_block_eig_workspace_bytes(pairs, n,
+ * max_sweeps) bytes (8 max_sweeps n^2 + 4 n per slot, rounded). */
+#define JB_EIG_DEFER_Q 256
+JB_API size_t jb_block_eig_workspace_bytes(int64_t pairs, int32_t n, int32_t max_sweeps);
+JB_API int jb_block_eig_ws(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
+                           int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps, double tol,
+                           const double *live_floor, int32_t variant, void *workspace, size_t workspace_bytes,
+                           void *stream);
 JB_API int jb_block_eig_f64_ex(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
                                int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps, double tol,
                                const double *live_floor, int32_t variant, void *stream);

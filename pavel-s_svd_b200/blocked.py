@@ -139,6 +139,10 @@ class BlockJacobi:
         # (_sweep_dataflow), so products overlap other slots' eigen-solves
         self.schedule = "batched"
         self.slot_split = 1            # K split of a per-slot Gram (1: the fewest CTAs TMEM allows)
+        # Q of the register eigen-solve formed by a separate all-GPU kernel from
+        # the recorded rotations (JB_EIG_DEFER_Q), with a workspace per slot
+        self.eig_defer_q = False
+        self._eig_ws, self._eig_ws_slot = None, 0
         self.tuned = None
         self._graphs, self._seen = {}, set()
 
@@ -180,11 +184,7 @@ class BlockJacobi:
             Vp = [x.view(P, 2 * b, self.npad) for x in self.V[cur][:parts]]
             # Grams of every slot: G_k = X_k X_k^T with X_k = 2b rows of W^T.
             gemm_parts(Wp, None, self.G, syrk=True, chain128=True, split_k=self.gram_split)
-            N.check(lib.jb_block_eig_f64_ex(self.G.data_ptr(), self.Qt[0].data_ptr(), self.Qt[1].data_ptr(),
-                                            self.Qt[2].data_ptr() if parts == 3 else None, self.off[r].data_ptr(),
-                                            self.dmax[r].data_ptr(), self.isweeps.data_ptr(), P, 2 * b,
-                                            inner_sweeps, inner_tol, self.live.data_ptr(),
-                                            self._eig_variant(parts), st), "jb_block_eig_f64_ex")
+            self._eig(0, P, parts, r, inner_sweeps, inner_tol, st)
             # X_k <- vv^T X_k (rows of W^T), same for V, each rotated row
             # written (as BF16 parts) straight into its next-round slot.
             nxt = 1 - cur
@@ -232,7 +232,6 @@ class BlockJacobi:
             st.wait_event(fork)
         ev_w = [[torch.cuda.Event() for _ in range(P)] for _ in range(R)]
         ev_v = [[torch.cuda.Event() for _ in range(P)] for _ in range(R)]
-        eigv = self._eig_variant(parts)
         for r in range(R):
             nxt = 1 - cur
             Wp = [x.view(P, L, self.mpad) for x in self.W[cur][:parts]]
@@ -245,13 +244,7 @@ class BlockJacobi:
                             st.wait_event(ev_w[r - 1][q])
                     gemm_parts([x[k:k + 1] for x in Wp], None, self.G[k:k + 1], syrk=True, chain128=True,
                                split_k=self.slot_split)
-                    qt = [x[k:k + 1] for x in self.Qt[:parts]]
-                    N.check(lib.jb_block_eig_f64_ex(self.G[k].data_ptr(), qt[0].data_ptr(), qt[1].data_ptr(),
-                                                    qt[2].data_ptr() if parts == 3 else None,
-                                                    self.off[r, k:].data_ptr(), self.dmax[r, k:].data_ptr(),
-                                                    self.isweeps[k:].data_ptr(), 1, L, inner_sweeps, inner_tol,
-                                                    self.live.data_ptr(), eigv, st.cuda_stream),
-                            "jb_block_eig_f64_ex")
+                    qt = self._eig(k, 1, parts, r, inner_sweeps, inner_tol, st.cuda_stream)
                     if r > 0:
                         for q in war[r - 1][k]:
                             st.wait_event(ev_w[r - 1][q])
@@ -272,7 +265,30 @@ class BlockJacobi:
     def _eig_variant(self, parts):
         if 2 * self.b not in (64, 128):
             return 0
-        return self.eig_variant | (N.EIG_FP32 if parts == 2 and self.eig_fp32_two_part else 0)
+        return (self.eig_variant | (N.EIG_FP32 if parts == 2 and self.eig_fp32_two_part else 0)
+                | (N.EIG_DEFER_Q if self.eig_defer_q else 0))
+
+    def _eig(self, k, count, parts, r, inner_sweeps, inner_tol, stream):
+        """Eigen-solves of slots k .. k + count - 1 of round r (jb_block_eig_ws),
+        with slot k's workspace region when Q is deferred."""
+        lib = N.lib()
+        L = 2 * self.b
+        variant = self._eig_variant(parts)
+        ws, ws_bytes = None, 0
+        if variant & N.EIG_DEFER_Q:
+            per = int(lib.jb_block_eig_workspace_bytes(1, L, inner_sweeps))
+            if self._eig_ws is None or self._eig_ws_slot < per:
+                self._eig_ws = torch.empty(self.P * per, dtype=torch.uint8, device=self.device)
+                self._eig_ws_slot = per
+            per = self._eig_ws_slot
+            ws, ws_bytes = self._eig_ws.data_ptr() + k * per, count * per
+        qt = [x[k:k + count] for x in self.Qt[:parts]]
+        N.check(lib.jb_block_eig_ws(self.G[k].data_ptr(), qt[0].data_ptr(), qt[1].data_ptr(),
+                                    qt[2].data_ptr() if parts == 3 else None, self.off[r, k:].data_ptr(),
+                                    self.dmax[r, k:].data_ptr(), self.isweeps[k:].data_ptr(), count, L, inner_sweeps,
+                                    inner_tol, self.live.data_ptr(), variant, ws, ws_bytes, stream),
+                "jb_block_eig_ws")
+        return qt
 
     def _run_sweep(self, cur, parts, inner_sweeps, inner_tol, use_graphs):
         """One sweep, replayed from a CUDA graph after its first (eager) run:
@@ -351,12 +367,15 @@ class BlockJacobi:
             torch.cuda.synchronize(self.device)
             return e0.elapsed_time(e1) / repeats
 
-        for v in variants:
-            for sp in (base_split, 2 * base_split):
-                self.eig_variant, self.gram_split = v, sp
-                times[f"eig_cols_per_warp={v},gram_split={sp}"] = timed(lambda c: self._sweep(c, 2, 1, 1e-7))
+        for dq in ((False, True) if 2 * self.b in (64, 128) else (False,)):
+            for v in variants:
+                for sp in (base_split, 2 * base_split):
+                    self.eig_variant, self.gram_split, self.eig_defer_q = v, sp, dq
+                    times[f"eig_cols_per_warp={v},gram_split={sp},defer_q={int(dq)}"] = timed(
+                        lambda c: self._sweep(c, 2, 1, 1e-7))
         best = min(times, key=times.get)
-        self.eig_variant, self.gram_split = [int(x.split("=")[1]) for x in best.split(",")]
+        v, sp, dq = [int(x.split("=")[1]) for x in best.split(",")]
+        self.eig_variant, self.gram_split, self.eig_defer_q = v, sp, bool(dq)
         graph_times = {}
         for sched, split in (("batched", 1), ("dataflow", 1), ("dataflow", 2)):
             self.schedule, self.slot_split = sched, split

@@ -238,11 +238,18 @@ __global__ void __launch_bounds__(kEigThreads) eig_kernel(const float *Gin, __nv
 // diagonal d and superdiagonal e (published in shared memory by their
 // owners), one barrier, rotations, (odd rounds: boundary exchange, one
 // barrier), new d / e, one barrier.
-template <int RPT, int CB, typename TG>
+// DQ (deferred Q): Q is not accumulated here.  The angle threads record every
+// applied (c, s) as FP32 pairs, cs_out[(k * max_sweeps + sweep) * n + r][p]
+// by the pair's first position p, and the kernel writes the eigenvalues'
+// sorted position of every column (pos_out[k * n + j]); q_apply_kernel then
+// forms Q^T from them on other SMs, so this latency-bound kernel issues
+// about a quarter fewer instructions per round.
+template <int RPT, int CB, typename TG, bool DQ = false>
 __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *Gin, __nv_bfloat16 *Qt_hi,
                                                             __nv_bfloat16 *Qt_lo, __nv_bfloat16 *Qt_lo2,
                                                             float *off_out, float *dmax_out, int *sweeps_out,
-                                                            int max_sweeps, double tol, const double *live_floor_ptr) {
+                                                            int max_sweeps, double tol, const double *live_floor_ptr,
+                                                            float2 *cs_out, int *pos_out) {
     constexpr int n = 32 * RPT;
     constexpr int NW = n / CB;                 // warps
     static_assert(CB % 2 == 0 && NW >= RPT / 2, "columns per warp");
@@ -344,6 +351,8 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
                     }
                     sc[p] = c;
                     ss[p] = sn;
+                    if constexpr (DQ)
+                        cs_out[(((size_t)k * max_sweeps + (sweep - 1)) * n + r) * n + p] = make_float2((float)c, (float)sn);
                 }
             angles_done:;
             }
@@ -394,9 +403,11 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
                         const TG x = g[i][j], y = g[i][j + 1];
                         g[i][j] = sn * x + c * y;
                         g[i][j + 1] = c * x - sn * y;
-                        const float u = q[i][j], v = q[i][j + 1];
-                        q[i][j] = fs * u + fc * v;
-                        q[i][j + 1] = fc * u - fs * v;
+                        if constexpr (!DQ) {
+                            const float u = q[i][j], v = q[i][j + 1];
+                            q[i][j] = fs * u + fc * v;
+                            q[i][j + 1] = fc * u - fs * v;
+                        }
                     }
                 }
             } else {
@@ -405,8 +416,10 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
                 for (int i = 0; i < RPT; ++i) {
                     bg[((size_t)warp * 2 + 0) * n + r0 + i] = g[i][0];
                     bg[((size_t)warp * 2 + 1) * n + r0 + i] = g[i][CB - 1];
-                    bq[((size_t)warp * 2 + 0) * n + r0 + i] = q[i][0];
-                    bq[((size_t)warp * 2 + 1) * n + r0 + i] = q[i][CB - 1];
+                    if constexpr (!DQ) {
+                        bq[((size_t)warp * 2 + 0) * n + r0 + i] = q[i][0];
+                        bq[((size_t)warp * 2 + 1) * n + r0 + i] = q[i][CB - 1];
+                    }
                 }
                 __syncthreads();
                 const bool has_left = warp > 0, has_right = warp < NW - 1;
@@ -417,15 +430,19 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
                     const int row = r0 + i;
                     if (has_left) {                // pair (c0 - 1, c0): this warp holds the second
                         const TG x = bg[((size_t)(warp - 1) * 2 + 1) * n + row];
-                        const float u = bq[((size_t)(warp - 1) * 2 + 1) * n + row];
                         g[i][0] = cl * x - sl * g[i][0];
-                        q[i][0] = (float)cl * u - (float)sl * q[i][0];
+                        if constexpr (!DQ) {
+                            const float u = bq[((size_t)(warp - 1) * 2 + 1) * n + row];
+                            q[i][0] = (float)cl * u - (float)sl * q[i][0];
+                        }
                     }
                     if (has_right) {               // pair (c0 + CB - 1, c0 + CB): this warp holds the first
                         const TG y = bg[((size_t)(warp + 1) * 2 + 0) * n + row];
-                        const float v = bq[((size_t)(warp + 1) * 2 + 0) * n + row];
                         g[i][CB - 1] = sr * g[i][CB - 1] + cr * y;
-                        q[i][CB - 1] = (float)sr * q[i][CB - 1] + (float)cr * v;
+                        if constexpr (!DQ) {
+                            const float v = bq[((size_t)(warp + 1) * 2 + 0) * n + row];
+                            q[i][CB - 1] = (float)sr * q[i][CB - 1] + (float)cr * v;
+                        }
                     }
                 }
 #pragma unroll
@@ -437,9 +454,11 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
                         const TG x = g[i][j], y = g[i][j + 1];
                         g[i][j] = sn * x + c * y;
                         g[i][j + 1] = c * x - sn * y;
-                        const float u = q[i][j], v = q[i][j + 1];
-                        q[i][j] = fs * u + fc * v;
-                        q[i][j + 1] = fc * u - fs * v;
+                        if constexpr (!DQ) {
+                            const float u = q[i][j], v = q[i][j + 1];
+                            q[i][j] = fs * u + fc * v;
+                            q[i][j + 1] = fc * u - fs * v;
+                        }
                     }
                 }
             }
@@ -464,10 +483,12 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
         if (!any) break;
     }
     // Q to shared memory (column-major) for the sorted write-out.
+    if constexpr (!DQ) {
 #pragma unroll
-    for (int i = 0; i < RPT; ++i)
+        for (int i = 0; i < RPT; ++i)
 #pragma unroll
-        for (int j = 0; j < CB; ++j) Qs[(size_t)(c0 + j) * n + r0 + i] = q[i][j];
+            for (int j = 0; j < CB; ++j) Qs[(size_t)(c0 + j) * n + r0 + i] = q[i][j];
+    }
     __syncthreads();
     // Eigenvalues descending (stable), Q^T rows in that order.
     for (int j = threadIdx.x; j < n; j += blockDim.x) {
@@ -478,10 +499,11 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
             rk += (di > dj) || (di == dj && i < j);
         }
         perm[rk] = j;
+        if constexpr (DQ) pos_out[(size_t)k * n + j] = rk;
     }
     __syncthreads();
     __nv_bfloat16 *qh = Qt_hi + (size_t)k * n * n, *ql = Qt_lo + (size_t)k * n * n;
-    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+    for (int t = threadIdx.x; t < (DQ ? 0 : n * n); t += blockDim.x) {
         const int rrow = t / n, i = t - rrow * n;       // Q^T row rrow = column perm[rrow] of Q
         const float x = Qs[(size_t)perm[rrow] * n + i];
         const __nv_bfloat16 h = __float2bfloat16_rn(x);
@@ -495,6 +517,70 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
         if (off_out) off_out[k] = (float)s_first_off;
         if (dmax_out) dmax_out[k] = (float)gmax;
         if (sweeps_out) sweeps_out[k] = sweep > max_sweeps ? max_sweeps : sweep;
+    }
+}
+
+// Q^T of every slot from the rotations eig_reg_kernel<..., DQ = true>
+// recorded.  Warp (k, i) forms row i of Q = prod_r J_r P_r with the same FP32
+// column updates the register kernel applies to its Q tiles (lane l holds
+// columns RPT l .. RPT l + RPT - 1; in odd rounds the pairs that straddle two
+// lanes take the neighbour's value by a shuffle), then writes it as column i
+// of Q^T in eigenvalue order (row pos[j] for column j), as hi / lo (/ lo2)
+// BF16 parts.  Rows are independent, so the whole grid works at once.
+template <int RPT>
+__global__ void __launch_bounds__(256) q_apply_kernel(const float2 *cs, const int *sweeps, const int *pos,
+                                                      __nv_bfloat16 *Qt_hi, __nv_bfloat16 *Qt_lo,
+                                                      __nv_bfloat16 *Qt_lo2, int pairs, int max_sweeps) {
+    constexpr int n = 32 * RPT;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (gw >= (int64_t)pairs * n) return;                  // whole warps
+    const int k = (int)(gw / n), i = (int)(gw - (int64_t)k * n);
+    const int c0 = lane * RPT;
+    float q[RPT];
+#pragma unroll
+    for (int e = 0; e < RPT; ++e) q[e] = (c0 + e == i) ? 1.f : 0.f;
+    int ns = sweeps[k];
+    if (ns > max_sweeps) ns = max_sweeps;
+    const float2 *ck = cs + (size_t)k * max_sweeps * n * n;
+    for (int rr = 0; rr < ns * n; ++rr) {
+        const float2 *c_r = ck + (size_t)rr * n;
+        if ((rr & 1) == 0) {
+#pragma unroll
+            for (int e = 0; e < RPT; e += 2) {
+                const float2 t = c_r[c0 + e];
+                const float u = q[e], v = q[e + 1];
+                q[e] = t.y * u + t.x * v;
+                q[e + 1] = t.x * u - t.y * v;
+            }
+        } else {
+            const bool has_up = lane > 0, has_down = lane < 31;
+            const float2 tu = has_up ? c_r[c0 - 1] : make_float2(1.f, 0.f);
+            const float2 td = has_down ? c_r[c0 + RPT - 1] : make_float2(1.f, 0.f);
+            const float up = __shfl_up_sync(0xffffffffu, q[RPT - 1], 1);    // column c0 - 1
+            const float dn = __shfl_down_sync(0xffffffffu, q[0], 1);        // column c0 + RPT
+            const float first = q[0], last = q[RPT - 1];
+            if (has_up) q[0] = tu.x * up - tu.y * first;                      // second of (c0 - 1, c0)
+            if (has_down) q[RPT - 1] = td.y * last + td.x * dn;               // first of (c0 + RPT - 1, c0 + RPT)
+#pragma unroll
+            for (int e = 1; e + 1 < RPT; e += 2) {
+                const float2 t = c_r[c0 + e];
+                const float u = q[e], v = q[e + 1];
+                q[e] = t.y * u + t.x * v;
+                q[e + 1] = t.x * u - t.y * v;
+            }
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < RPT; ++e) {
+        const size_t t = (size_t)k * n * n + (size_t)pos[(size_t)k * n + c0 + e] * n + i;
+        const float x = q[e];
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        Qt_hi[t] = h;
+        const float rem = x - __bfloat162float(h);
+        const __nv_bfloat16 l = __float2bfloat16_rn(rem);
+        Qt_lo[t] = l;
+        if (Qt_lo2) Qt_lo2[t] = __float2bfloat16_rn(rem - __bfloat162float(l));
     }
 }
 
@@ -638,29 +724,54 @@ __global__ void __launch_bounds__(256) gemm_f64acc_kernel(const float *A, const 
     }
 }
 
+// Workspace of the deferred-Q form: the recorded (c, s) of every round and
+// the sorted positions, per slot.
+__host__ inline size_t eig_dq_cs_bytes(int64_t pairs, int n, int max_sweeps) {
+    return ((size_t)pairs * max_sweeps * n * n * sizeof(float2) + 255) & ~(size_t)255;
+}
+__host__ inline size_t eig_dq_bytes(int64_t pairs, int n, int max_sweeps) {
+    return eig_dq_cs_bytes(pairs, n, max_sweeps) + (((size_t)pairs * n * 4 + 255) & ~(size_t)255);
+}
+
 template <int RPT, int CB, typename TG>
 static int launch_eig_reg(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
                           int32_t *sweeps, int64_t pairs, int32_t max_sweeps, double tol, const double *live_floor,
-                          cudaStream_t st) {
+                          unsigned char *dq_ws, cudaStream_t st) {
     constexpr int n = 32 * RPT;
     const size_t smem = eig_reg_smem_bytes(n, CB);
-    auto kern = eig_reg_kernel<RPT, CB, TG>;
+    if (!dq_ws) {
+        auto kern = eig_reg_kernel<RPT, CB, TG>;
+        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return JB_ECUDA;
+        kern<<<(unsigned)pairs, 32 * (n / CB), smem, st>>>(G, (__nv_bfloat16 *)Qt_hi, (__nv_bfloat16 *)Qt_lo,
+                                                          (__nv_bfloat16 *)Qt_lo2, off, dmax, sweeps, max_sweeps, tol,
+                                                          live_floor, nullptr, nullptr);
+        return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+    }
+    float2 *cs = (float2 *)dq_ws;
+    int *pos = (int *)(dq_ws + eig_dq_cs_bytes(pairs, n, max_sweeps));
+    auto kern = eig_reg_kernel<RPT, CB, TG, true>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return JB_ECUDA;
     kern<<<(unsigned)pairs, 32 * (n / CB), smem, st>>>(G, (__nv_bfloat16 *)Qt_hi, (__nv_bfloat16 *)Qt_lo,
                                                       (__nv_bfloat16 *)Qt_lo2, off, dmax, sweeps, max_sweeps, tol,
-                                                      live_floor);
+                                                      live_floor, cs, pos);
+    if (cudaGetLastError() != cudaSuccess) return JB_ECUDA;
+    const int64_t warps = pairs * n;
+    q_apply_kernel<RPT><<<(unsigned)((warps + 7) / 8), 256, 0, st>>>(cs, sweeps, pos, (__nv_bfloat16 *)Qt_hi,
+                                                                     (__nv_bfloat16 *)Qt_lo, (__nv_bfloat16 *)Qt_lo2,
+                                                                     (int)pairs, max_sweeps);
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
 }
 
 template <typename TG>
 static int dispatch_eig_reg(int n, int cb, const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off,
                             float *dmax, int32_t *sweeps, int64_t pairs, int32_t max_sweeps, double tol,
-                            const double *live_floor, cudaStream_t st) {
+                            const double *live_floor, unsigned char *dq_ws, cudaStream_t st) {
 #define JB_EIG_CASE(NN, RPT, CBV)                                                                               \
     if (n == NN && cb == CBV)                                                                                   \
         return launch_eig_reg<RPT, CBV, TG>(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps, tol, \
-                                            live_floor, st);
+                                            live_floor, dq_ws, st);
     JB_EIG_CASE(64, 2, 4)
     JB_EIG_CASE(64, 2, 8)
     JB_EIG_CASE(64, 2, 16)
@@ -678,23 +789,34 @@ using namespace jb::blk;
 
 extern "C" {
 
-int jb_block_eig_f64_ex(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
-                        int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps, double tol,
-                        const double *live_floor, int32_t variant, void *stream) {
+size_t jb_block_eig_workspace_bytes(int64_t pairs, int32_t n, int32_t max_sweeps) {
+    if (pairs < 1 || n < 2 || max_sweeps < 1) return 0;
+    return eig_dq_bytes(pairs, n, max_sweeps);
+}
+
+int jb_block_eig_ws(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
+                    int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps, double tol,
+                    const double *live_floor, int32_t variant, void *workspace, size_t workspace_bytes,
+                    void *stream) {
+    const bool dq = (variant & JB_EIG_DEFER_Q) != 0;
+    variant &= ~JB_EIG_DEFER_Q;
     const int lay = variant & ~JB_EIG_FP32;
     if (!G || !Qt_hi || !Qt_lo || pairs < 1 || n < 2 || (n & 1) || max_sweeps < 1 ||
         !(lay == 0 || lay == 1 || lay == 4 || lay == 8 || lay == 16) || (variant & ~(JB_EIG_FP32 | 31)) ||
-        ((variant & JB_EIG_FP32) && !((n == 64 || n == 128) && lay != 1)))
+        ((variant & JB_EIG_FP32) && !((n == 64 || n == 128) && lay != 1)) ||
+        (dq && !((n == 64 || n == 128) && lay != 1)))
         return JB_EINVAL;
+    if (dq && (!workspace || workspace_bytes < eig_dq_bytes(pairs, n, max_sweeps))) return JB_EWORKSPACE;
     cudaStream_t st = (cudaStream_t)stream;
     const bool g32 = (variant & JB_EIG_FP32) != 0;
     const int layout = variant & ~JB_EIG_FP32;
+    unsigned char *dq_ws = dq ? (unsigned char *)workspace : nullptr;
     if ((n == 64 || n == 128) && layout != 1) {
         const int cb = layout == 0 ? 8 : layout;
         return g32 ? dispatch_eig_reg<float>(n, cb, G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps,
-                                             tol, live_floor, st)
+                                             tol, live_floor, dq_ws, st)
                    : dispatch_eig_reg<double>(n, cb, G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, max_sweeps,
-                                              tol, live_floor, st);
+                                              tol, live_floor, dq_ws, st);
     }
     if (n > 256) return JB_ETOOBIG;                  // players are stored as bytes
     const size_t smem = eig_smem_bytes(n);
@@ -705,6 +827,14 @@ int jb_block_eig_f64_ex(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, 
                                                            (__nv_bfloat16 *)Qt_lo2, off, dmax, sweeps, n, max_sweeps,
                                                            tol, live_floor);
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
+}
+
+int jb_block_eig_f64_ex(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,
+                        int32_t *sweeps, int64_t pairs, int32_t n, int32_t max_sweeps, double tol,
+                        const double *live_floor, int32_t variant, void *stream) {
+    if (variant & JB_EIG_DEFER_Q) return JB_EWORKSPACE;  // the deferred-Q form needs jb_block_eig_ws
+    return jb_block_eig_ws(G, Qt_hi, Qt_lo, Qt_lo2, off, dmax, sweeps, pairs, n, max_sweeps, tol, live_floor, variant,
+                           nullptr, 0, stream);
 }
 
 int jb_block_eig_f64(const float *G, void *Qt_hi, void *Qt_lo, void *Qt_lo2, float *off, float *dmax,

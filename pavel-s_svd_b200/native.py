@@ -27,7 +27,8 @@ SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_bat
            "jb_svd_batched_f64", "jb_uneven_workspace_bytes", "jb_svd_uneven_f32", "jb_svd_uneven_f32_ex",
            "jb_gemm_bf16", "jb_gemm_bf16x", "jb_gemm_bf16x_rows", "jb_split_bf16", "jb_split3_bf16",
            "jb_warm_prep_f32", "jb_svd_warm_f32", "jb_transpose_bf16", "jb_bias_act", "jb_relu_backward",
-           "jb_col_sum", "jb_mse_grad", "jb_adam", "jb_gram_sketch", "jb_block_eig_f64", "jb_block_eig_f64_ex", "jb_rows_scatter",
+           "jb_col_sum", "jb_mse_grad", "jb_adam", "jb_gram_sketch", "jb_block_eig_f64", "jb_block_eig_workspace_bytes",
+           "jb_block_eig_ws", "jb_block_eig_f64_ex", "jb_rows_scatter",
            "jb_rows_combine", "jb_gemm_f64acc", "jb_block_finish", "jb_eigh_workspace_bytes", "jb_eigh_f32",
            "jb_eigh_f64", "jb_eigh_complex_workspace_bytes", "jb_eigh_c64", "jb_eigh_c128",
            "jb_qr_workspace_bytes", "jb_qr_f32", "jb_qr_f64", "jb_qr_c64", "jb_qr_c128",
@@ -36,6 +37,7 @@ SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_bat
            "jb_svd_batched_f32_noalloc")
 GEMM_PLAIN, GEMM_SPLIT3, GEMM_SPLIT6, GEMM_B_MN, GEMM_CHAIN128, GEMM_SYRK = 0, 1, 2, 4, 8, 16
 EIG_FP32 = 128  # JB_EIG_FP32
+EIG_DEFER_Q = 256  # JB_EIG_DEFER_Q
 NOALLOC_SCRATCH_BYTES = 16 << 20  # JB_NOALLOC_SCRATCH_BYTES
 
 
@@ -116,6 +118,7 @@ def _declare(l):
                        ("jb_gram_sketch", [P, P, I64, I32, I32, P]),
                        ("jb_block_eig_f64", [P, P, P, P, P, P, P, I64, I32, I32, F64, P, P]),
                        ("jb_block_eig_f64_ex", [P, P, P, P, P, P, P, I64, I32, I32, F64, P, I32, P]),
+                       ("jb_block_eig_ws", [P, P, P, P, P, P, P, I64, I32, I32, F64, P, I32, P, SZ, P]),
                        ("jb_rows_scatter", [P, P, P, P, P, P, I64, I64, P]),
                        ("jb_rows_combine", [P, P, P, P, P, I64, I64, P]),
                        ("jb_gemm_f64acc", [P, P, P, I64, I64, I64, I64, I64, I64, P]),
@@ -123,6 +126,8 @@ def _declare(l):
         f = getattr(l, name)
         f.restype = ctypes.c_int
         f.argtypes = args
+    l.jb_block_eig_workspace_bytes.restype = SZ
+    l.jb_block_eig_workspace_bytes.argtypes = [I64, I32, I32]
     l.jb_complete_null_workspace_bytes.restype = SZ
     l.jb_complete_null_workspace_bytes.argtypes = [I32, I64, I64, I64]
     l.jb_complete_null.restype = ctypes.c_int

@@ -147,6 +147,44 @@ def test_dataflow_schedule_matches_batched(BJ, m, n, b):
     assert float(np.abs(sb - sd).max() / sb[0]) <= 2e-6
 
 
+@pytest.mark.parametrize("n", [64, 128])
+@pytest.mark.parametrize("layout,fp32", [(4, False), (8, False), (16, False), (8, True)])
+@pytest.mark.parametrize("sweeps", [1, 2])
+def test_block_eig_deferred_q_matches(n, layout, fp32, sweeps):
+    """JB_EIG_DEFER_Q: the register eigen-solve records its rotations and
+    q_apply_kernel forms Q^T from them.  The same Q^T as the eigen-solve that
+    accumulates Q itself (the same FP32 updates; to rounding), the same off,
+    dmax and sweep counts."""
+    N = importlib.import_module("pavel-s_svd_b200.native")
+    lib = N.lib()
+    g = torch.Generator(device="cuda").manual_seed(3 * n + layout)
+    P = 6
+    x = torch.randn(P, n, 2 * n, device="cuda", generator=g, dtype=torch.float64)
+    x = x * torch.logspace(0, -3, n, device="cuda", dtype=torch.float64)[:, None]
+    G = (x @ x.transpose(1, 2)).float().contiguous()
+    st = torch.cuda.current_stream().cuda_stream
+    ws = torch.empty(int(lib.jb_block_eig_workspace_bytes(P, n, sweeps)), dtype=torch.uint8, device="cuda")
+    outs = []
+    for dq in (False, True):
+        variant = layout | (N.EIG_FP32 if fp32 else 0) | (N.EIG_DEFER_Q if dq else 0)
+        qt = [torch.full((P, n, n), 3.0, dtype=torch.bfloat16, device="cuda") for _ in range(3)]
+        off = torch.zeros(P, device="cuda")
+        dmax = torch.zeros(P, device="cuda")
+        sw = torch.zeros(P, dtype=torch.int32, device="cuda")
+        N.check(lib.jb_block_eig_ws(G.data_ptr(), qt[0].data_ptr(), qt[1].data_ptr(), qt[2].data_ptr(),
+                                    off.data_ptr(), dmax.data_ptr(), sw.data_ptr(), P, n, sweeps, 1e-9, None, variant,
+                                    ws.data_ptr(), ws.numel(), st), "jb_block_eig_ws")
+        torch.cuda.synchronize()
+        outs.append((sum(q.double() for q in qt), off, dmax, sw))
+    (qa, offa, da, swa), (qb, offb, db, swb) = outs
+    torch.testing.assert_close(qb, qa, rtol=0, atol=2e-6)
+    assert torch.equal(offa, offb) and torch.equal(da, db) and torch.equal(swa, swb)
+    with pytest.raises(RuntimeError):                       # the deferred form needs its workspace
+        N.check(lib.jb_block_eig_ws(G.data_ptr(), qt[0].data_ptr(), qt[1].data_ptr(), None, off.data_ptr(),
+                                    dmax.data_ptr(), sw.data_ptr(), P, n, sweeps, 1e-9, None,
+                                    layout | N.EIG_DEFER_Q, None, 0, st), "jb_block_eig_ws")
+
+
 def test_block_jacobi_drop_in():
     """svd(a, 'block_jacobi', ...) through the drop-in API: tall and wide
     inputs, the reference's defaults (block_size 4 -> width 32 here), the
