@@ -417,15 +417,16 @@ def time_replays(graph, flush, stream, steps):
     (outside the events)."""
     import torch
     times = []
-    for step in range(steps):
-        flush.fill_(step & 0xff)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        graph.replay()
-        e1.record(stream)
-        times.append((e0, e1))
-    torch.cuda.synchronize()
+    with _timed_range():
+        for step in range(steps):
+            flush.fill_(step & 0xff)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            graph.replay()
+            e1.record(stream)
+            times.append((e0, e1))
+        torch.cuda.synchronize()
     return [a.elapsed_time(b) for a, b in times]
 
 
@@ -571,6 +572,19 @@ def _events():
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
 
+class _timed_range:
+    """NVTX push/pop range "timed" around a timed region, so a profiler's
+    launch list can be restricted to it (ncu --nvtx --nvtx-include timed/)."""
+
+    def __enter__(self):
+        import torch
+        torch.cuda.nvtx.range_push("timed")
+
+    def __exit__(self, *exc):
+        import torch
+        torch.cuda.nvtx.range_pop()
+
+
 def lapack_check(a, U, S, Vh, cut_width):
     """Accuracy against FP64 LAPACK of the same float32 input; 'resolved'
     values are those above twice the reference cut eps32 * cut_width * sigma_1."""
@@ -654,13 +668,14 @@ def run_blocked(args, name):
         U, S, Vh, info = plan.solve(a)
     torch.cuda.synchronize()
     times = []
-    for _ in range(args.steps):
-        e0, e1 = _events()
-        e0.record()
-        U, S, Vh, info = plan.solve(a)
-        e1.record()
-        torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1))
+    with _timed_range():
+        for _ in range(args.steps):
+            e0, e1 = _events()
+            e0.record()
+            U, S, Vh, info = plan.solve(a, use_graphs=not args.eager)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
     ms = float(np.median(times))
     R, P, mp, npd = plan.nb - 1, plan.P, plan.mpad, plan.npad
     per_round = P * (2 * mp * (2 * b) ** 2 * 2 + 2 * npd * (2 * b) ** 2)       # Gram + W and V updates
@@ -900,6 +915,9 @@ def main():
                     help="reference arm: skip timing the reference's own PyTorch CPU Jacobi")
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--eager", action="store_true",
+                    help="blocked workloads: launch the timed solve's kernels one by one instead of replaying the "
+                         "captured sweep graphs (for a profiler's launch list; the line is then no bench number)")
     ap.add_argument("--full-check", action="store_true")
     ap.add_argument("--traffic-bytes", type=float, default=None,
                     help="per-launch DRAM bytes from an ncu capture, reported as roofline.traffic")

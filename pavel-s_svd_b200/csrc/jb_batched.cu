@@ -403,14 +403,17 @@ __device__ inline bool next_ticket(int *counter, int &s_idx, int64_t &idx) {
 }
 
 // C (M x N) = alpha * A (M x K) * B (K x N), column-major, in shared memory;
-// M and N multiples of 4.  Each thread owns 4 x 4 tiles of C, consecutive
-// lanes take consecutive row tiles (contiguous A loads, B loads broadcast).
+// M and N multiples of 4.  Each thread owns a 4 x 4 tile of C: rows
+// i0, i0 + M/4, i0 + 2M/4, i0 + 3M/4 (consecutive lanes take consecutive i0,
+// so every A load and C store of a warp is one contiguous run of shared
+// memory, free of bank conflicts) and columns j0 .. j0 + 3 (B loads
+// broadcast across the lanes of one j0).
 template <typename TA, typename TC = double, typename TB = double>
 __device__ void gemm_nn(TC *C, int ldc, const TA *A, int lda, const TB *B, int ldb, int M, int N, int K,
                         TC alpha) {
     const int tm = M >> 2, tn = N >> 2;
     for (int t = threadIdx.x; t < tm * tn; t += blockDim.x) {
-        const int i0 = (t % tm) << 2, j0 = (t / tm) << 2;
+        const int i0 = t % tm, j0 = (t / tm) << 2;
         TC acc[4][4];
 #pragma unroll
         for (int r = 0; r < 4; ++r)
@@ -419,7 +422,7 @@ __device__ void gemm_nn(TC *C, int ldc, const TA *A, int lda, const TB *B, int l
         for (int k = 0; k < K; ++k) {
             TC a[4], b[4];
 #pragma unroll
-            for (int r = 0; r < 4; ++r) a[r] = (TC)A[(size_t)k * lda + i0 + r];
+            for (int r = 0; r < 4; ++r) a[r] = (TC)A[(size_t)k * lda + i0 + r * tm];
 #pragma unroll
             for (int c = 0; c < 4; ++c) b[c] = (TC)B[(size_t)(j0 + c) * ldb + k];
 #pragma unroll
@@ -430,7 +433,21 @@ __device__ void gemm_nn(TC *C, int ldc, const TA *A, int lda, const TB *B, int l
 #pragma unroll
         for (int r = 0; r < 4; ++r)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) C[(size_t)(j0 + c) * ldc + i0 + r] = alpha * acc[r][c];
+            for (int c = 0; c < 4; ++c) C[(size_t)(j0 + c) * ldc + i0 + r * tm] = alpha * acc[r][c];
+    }
+}
+
+// T (ld) = transpose of S (ld), n x n, column-major in shared memory.  The
+// 32 lanes of a warp take one diagonal of a 32 x 32 block (row i = lane,
+// column (lane + s) mod 32), so both the read of S and the write of T hit 32
+// different banks instead of one (a column-major stride of ld words).
+__device__ inline void transpose_sq(double *T, const double *S, int n, int ld) {
+    const int nbk = (n + 31) >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int job = warp; job < nbk * nbk * 32; job += nw) {
+        const int s = job & 31, blk = job >> 5;
+        const int i = ((blk % nbk) << 5) + lane, c = ((blk / nbk) << 5) + ((lane + s) & 31);
+        if (i < n && c < n) T[(size_t)i * ld + c] = S[(size_t)c * ld + i];
     }
 }
 
@@ -438,10 +455,7 @@ __device__ void gemm_nn(TC *C, int ldc, const TA *A, int lda, const TB *B, int l
 // factor of V), n x n with ld; VT, H, Vn: n x n scratch (ld).  Returns
 // max |V^T V - I| before the step.
 __device__ double polar_step(double *V, int n, int ld, double *VT, double *H, double *Vn, Aux &ax) {
-    for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
-        const int c = k / n, i = k - c * n;
-        VT[(size_t)i * ld + c] = V[(size_t)c * ld + i];
-    }
+    transpose_sq(VT, V, n, ld);
     __syncthreads();
     gemm_nn<double>(H, ld, VT, ld, V, ld, n, n, n, 1.0);
     __syncthreads();
@@ -462,6 +476,20 @@ __device__ double polar_step(double *V, int n, int ld, double *VT, double *H, do
     }
     __syncthreads();
     return err;
+}
+
+// Hand-off word from the FP32 to the FP64 launch of the mixed register path:
+// bit 30 set, the input's scale exponent e + 1024 in bits 12..22, the FP32
+// sweeps in bits 0..11.  A sweep count or exponent out of that range is
+// passed as the plain sweep count, and the FP64 launch then scans the input.
+__device__ __forceinline__ int pack_handoff(int ns, int e) {
+    return (ns >= 0 && ns < 4096 && e > -1024 && e < 1024) ? (1 << 30) | ((e + 1024) << 12) | ns : ns;
+}
+__device__ __forceinline__ bool unpack_handoff(int w, int &ns, int &e) {
+    if (!(w & (1 << 30))) { ns = w; return false; }
+    ns = w & 0xfff;
+    e = ((w >> 12) & 0x7ff) - 1024;
+    return true;
 }
 
 // K1: FP32 sweeps.  MIXED: store the FP32 V (nt x nt) in the scratch for K2;
@@ -485,7 +513,7 @@ __global__ void __launch_bounds__(THREADS, (BW == kB32 && MR <= kMaxR) ? 512 / T
         if (!class_takes(d, p.cls)) continue;  // the other size class's launch solves it
         if (threadIdx.x < 4) ax.flag[threadIdx.x] = 0;
         __syncthreads();
-        int ns = 0, st = JB_ST_OK;
+        int ns = 0, st = JB_ST_OK, e_in = 0;
         if (!rdesc_fits(d, BW, 4, p, MIXED, MR, MRV)) {
             st = JB_ST_BAD_DESC;
         } else {
@@ -496,6 +524,7 @@ __global__ void __launch_bounds__(THREADS, (BW == kB32 && MR <= kMaxR) ? 512 / T
             float *V = (float *)(region + align16((size_t)r.ldw * r.ncp * 4));
             bool bad;
             const int e = scan_input(A, g.m * g.n, ax, bad);
+            e_in = e;
             if (bad) {
                 st = JB_ST_NONFINITE_IN;
             } else {
@@ -552,7 +581,11 @@ __global__ void __launch_bounds__(THREADS, (BW == kB32 && MR <= kMaxR) ? 512 / T
         }
         if (threadIdx.x == 0) {
             if (p.status) p.status[mat] = st;
-            if (p.sweeps) p.sweeps[mat] = ns;
+            // Mixed, register tiles: the FP64 phase (rb64_kernel) takes over a
+            // matrix this launch solved; the sweeps word then also carries the
+            // input's scale exponent, so that rb64 need not scan the input again.
+            if (p.sweeps)
+                p.sweeps[mat] = (MIXED && MR <= kMaxR && st == JB_ST_OK) ? pack_handoff(ns, e_in) : ns;
         }
         __syncthreads();
     }
@@ -580,10 +613,11 @@ __global__ void __launch_bounds__(THREADS, kT64 / THREADS) rb64_kernel(Params p)
         if (!class_takes(d, p.cls)) continue;  // the other size class's launch solves it
         if (threadIdx.x < 4) ax.flag[threadIdx.x] = 0;
         __syncthreads();
-        int prev = JB_ST_OK, s1 = 0;
+        int prev = JB_ST_OK, s1 = 0, e_k1 = 0;
+        bool have_e = false;
         if (MIXED && threadIdx.x == 0) { ax.flag[3] = p.status[mat]; ax.flag[2] = p.sweeps[mat]; }
         __syncthreads();
-        if (MIXED) { prev = ax.flag[3]; s1 = ax.flag[2]; }
+        if (MIXED) { prev = ax.flag[3]; have_e = unpack_handoff(ax.flag[2], s1, e_k1); }
         __syncthreads();
         if (threadIdx.x == 0) ax.flag[2] = 0;
         __syncthreads();
@@ -598,8 +632,9 @@ __global__ void __launch_bounds__(THREADS, kT64 / THREADS) rb64_kernel(Params p)
             const TI *A = (const TI *)p.A + d.a_off;
             double *W = (double *)region;
             double *V = (double *)(region + align16((size_t)r.ldw * r.ncp * 8));
-            bool bad;
-            const int e = scan_input(A, g.m * g.n, ax, bad);
+            bool bad = false;
+            // the FP32 launch already checked the input and found its scale
+            const int e = have_e ? e_k1 : scan_input(A, g.m * g.n, ax, bad);
             if (bad) {
                 st = JB_ST_NONFINITE_IN;
             } else {

@@ -39,7 +39,8 @@ template <typename T, int B, int R, int RV>
 struct Tile {
     T w[2 * B][R];
     T v[2 * B][RV];
-    T nrm[2 * B];   // column norms squared (norm-update sweeps only), same on every lane
+    T nrm[2 * B];   // column norms squared (norm-update sweeps, intra steps), same on every lane
+    T nx, ny;       // norm-update cross steps: the squared norms of the lane group's pair (x_i, y_i)
 };
 
 // Warp reduce-scatter of NV (power of two <= 32) values: afterwards x[0] on
@@ -176,24 +177,29 @@ __device__ __forceinline__ int rot_params_exact(double app, double aqq, double a
     return 1 | (apq2 > big2 * prod ? 2 : 0) | (apq2 > ex2 * prod ? 4 : 0);
 }
 
-// Packed FP32 (two rows per instruction): a += x * y for (a0, a1), and the
-// rotation pair (x, y) <- (c x - s y, s x + c y) for two rows at once.
+// Packed FP32 (two rows per instruction, the sm_100 float2 intrinsics, so
+// that the compiler sees the operations and keeps operand pairs in register
+// pairs): a += x * y for (a0, a1), and the rotation pair
+// (x, y) <- (c x - s y, s x + c y) for two rows at once, with the packed
+// (c, c), (s, s), (-s, -s) built once per pair by the caller.
 __device__ __forceinline__ void fma2(float &a0, float &a1, float x0, float x1, float y0, float y1) {
-    asm("{\n\t.reg .b64 ra, rx, ry;\n\t"
-        "mov.b64 ra, {%0, %1};\n\tmov.b64 rx, {%2, %3};\n\tmov.b64 ry, {%4, %5};\n\t"
-        "fma.rn.f32x2 ra, rx, ry, ra;\n\tmov.b64 {%0, %1}, ra;\n\t}"
-        : "+f"(a0), "+f"(a1) : "f"(x0), "f"(x1), "f"(y0), "f"(y1));
+    const float2 r = __ffma2_rn(make_float2(x0, x1), make_float2(y0, y1), make_float2(a0, a1));
+    a0 = r.x;
+    a1 = r.y;
 }
-__device__ __forceinline__ void rot2(float &x0, float &x1, float &y0, float &y1, float c, float s) {
-    asm("{\n\t.reg .b64 rx, ry, rc, rs, rn, t1, t2;\n\t"
-        "mov.b64 rx, {%0, %1};\n\tmov.b64 ry, {%2, %3};\n\t"
-        "mov.b64 rc, {%4, %4};\n\tmov.b64 rs, {%5, %5};\n\tmov.b64 rn, {%6, %6};\n\t"
-        "mul.rn.f32x2 t1, rn, ry;\n\t"          // -s y
-        "fma.rn.f32x2 t1, rc, rx, t1;\n\t"      // c x - s y
-        "mul.rn.f32x2 t2, rc, ry;\n\t"          // c y
-        "fma.rn.f32x2 t2, rs, rx, t2;\n\t"      // s x + c y
-        "mov.b64 {%0, %1}, t1;\n\tmov.b64 {%2, %3}, t2;\n\t}"
-        : "+f"(x0), "+f"(x1), "+f"(y0), "+f"(y1) : "f"(c), "f"(s), "f"(-s));
+struct Rot2 {
+    float2 c, s, ns;
+    __device__ __forceinline__ Rot2(float c_, float s_)
+        : c(make_float2(c_, c_)), s(make_float2(s_, s_)), ns(make_float2(-s_, -s_)) {}
+};
+__device__ __forceinline__ void rot2(float &x0, float &x1, float &y0, float &y1, const Rot2 &g) {
+    const float2 x = make_float2(x0, x1), y = make_float2(y0, y1);
+    const float2 t1 = __ffma2_rn(g.c, x, __fmul2_rn(g.ns, y));   // c x - s y
+    const float2 t2 = __ffma2_rn(g.s, x, __fmul2_rn(g.c, y));    // s x + c y
+    x0 = t1.x;
+    x1 = t1.y;
+    y0 = t2.x;
+    y1 = t2.y;
 }
 
 // Register column of the first / second member of pair i in a step.
@@ -262,12 +268,13 @@ __device__ __forceinline__ void step(Tile<T, B, R, RV> &t, T tol2, T big2, T ex2
         const T ci = __shfl_sync(FULL, c, src), si = __shfl_sync(FULL, s, src);
         const int p = pair_p<INTRA, B>(i), q = pair_q<INTRA, B>(i);
         if constexpr (PACK) {
+            const Rot2 g((float)ci, (float)si);
 #pragma unroll
             for (int r = 0; r < R; r += 2)
-                if (r < nr) rot2(t.w[p][r], t.w[p][r + 1], t.w[q][r], t.w[q][r + 1], ci, si);
+                if (r < nr) rot2(t.w[p][r], t.w[p][r + 1], t.w[q][r], t.w[q][r + 1], g);
 #pragma unroll
             for (int r = 0; r < RV; r += 2)
-                if (r < nv) rot2(t.v[p][r], t.v[p][r + 1], t.v[q][r], t.v[q][r + 1], ci, si);
+                if (r < nv) rot2(t.v[p][r], t.v[p][r + 1], t.v[q][r], t.v[q][r + 1], g);
         } else {
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -289,11 +296,16 @@ __device__ __forceinline__ void step(Tile<T, B, R, RV> &t, T tol2, T big2, T ex2
     }
 }
 
-// Norm-update step: the squared column norms come from t.nrm instead of two
-// more dot products, and each rotation updates them as it changes them; only
-// w_p^T w_q is reduced across the warp.  FP32 (packed tiles): app - t|apq|,
-// aqq + t|apq|.  FP64: the expansion c^2 app - 2cs apq + s^2 aqq (and its
-// mirror) with the applied c and s, exact whatever the accuracy of the angle.
+// Norm-update step: the squared column norms come from the tile instead of
+// two more dot products, and each rotation updates them as it changes them;
+// only w_p^T w_q is reduced across the warp.  FP32 (packed tiles):
+// app - t|apq|, aqq + t|apq|.  FP64: the expansion c^2 app - 2cs apq + s^2 aqq
+// (and its mirror) with the applied c and s, exact whatever the accuracy of
+// the angle.  INTRA steps read and update the replicated t.nrm (every lane
+// holds all 2B norms: the updated pair norms are broadcast).  CROSS steps
+// pair x_i with y_i in lane group i, which holds just those two norms
+// (t.nx, t.ny) and updates them itself, so they cost no broadcast; shift_y
+// passes ny on to the neighbouring group.
 template <bool INTRA, typename T, int B, int R, int RV>
 __device__ __forceinline__ void step_upd(Tile<T, B, R, RV> &t, T tol2, T big2, T ex2, T floor_, int &fl,
                                          bool rotate, int lane, int nr, int nv) {
@@ -319,12 +331,19 @@ __device__ __forceinline__ void step_upd(Tile<T, B, R, RV> &t, T tol2, T big2, T
         }
     }
     reduce_scatter<T, B>(pc, lane);
-    // this lane's pair (lane >> (5 - LB)): its two norms from the tile
-    const int li = lane >> (5 - LB);
-    T app = t.nrm[pair_p<INTRA, B>(0)], aqq = t.nrm[pair_q<INTRA, B>(0)];
+    // this lane's pair (lane >> (5 - LB)): its two norms
+    T app, aqq;
+    if constexpr (INTRA) {
+        const int li = lane >> (5 - LB);
+        app = t.nrm[pair_p<INTRA, B>(0)];
+        aqq = t.nrm[pair_q<INTRA, B>(0)];
 #pragma unroll
-    for (int i = 1; i < B; ++i)
-        if (li == i) { app = t.nrm[pair_p<INTRA, B>(i)]; aqq = t.nrm[pair_q<INTRA, B>(i)]; }
+        for (int i = 1; i < B; ++i)
+            if (li == i) { app = t.nrm[pair_p<INTRA, B>(i)]; aqq = t.nrm[pair_q<INTRA, B>(i)]; }
+    } else {
+        app = t.nx;
+        aqq = t.ny;
+    }
     T c, s, sh;
     const int f = rot_params<T>(app, aqq, pc[0], tol2, big2, ex2, floor_, c, s, &sh);
     fl |= f;
@@ -338,20 +357,27 @@ __device__ __forceinline__ void step_upd(Tile<T, B, R, RV> &t, T tol2, T big2, T
         np_ = dfma(cc, app, dfma(ss, aqq, -x2));
         nq_ = dfma(ss, app, dfma(cc, aqq, x2));
     }
+    if constexpr (!INTRA) {
+        t.nx = np_;
+        t.ny = nq_;
+    }
 #pragma unroll
     for (int i = 0; i < B; ++i) {
         const int src = i << (5 - LB);
         const T ci = __shfl_sync(FULL, c, src), si = __shfl_sync(FULL, s, src);
         const int p = pair_p<INTRA, B>(i), q = pair_q<INTRA, B>(i);
-        t.nrm[p] = __shfl_sync(FULL, np_, src);
-        t.nrm[q] = __shfl_sync(FULL, nq_, src);
+        if constexpr (INTRA) {
+            t.nrm[p] = __shfl_sync(FULL, np_, src);
+            t.nrm[q] = __shfl_sync(FULL, nq_, src);
+        }
         if constexpr (PACK) {
+            const Rot2 g((float)ci, (float)si);
 #pragma unroll
             for (int r = 0; r < R; r += 2)
-                if (r < nr) rot2(t.w[p][r], t.w[p][r + 1], t.w[q][r], t.w[q][r + 1], ci, si);
+                if (r < nr) rot2(t.w[p][r], t.w[p][r + 1], t.w[q][r], t.w[q][r + 1], g);
 #pragma unroll
             for (int r = 0; r < RV; r += 2)
-                if (r < nv) rot2(t.v[p][r], t.v[p][r + 1], t.v[q][r], t.v[q][r + 1], ci, si);
+                if (r < nv) rot2(t.v[p][r], t.v[p][r + 1], t.v[q][r], t.v[q][r + 1], g);
         } else {
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -373,14 +399,26 @@ __device__ __forceinline__ void step_upd(Tile<T, B, R, RV> &t, T tol2, T big2, T
     }
 }
 
-// y_i <- y_(i+1) (cyclic): the next CROSS step pairs x_i with the old y_(i+1).
-template <int UPD, typename T, int B, int R, int RV>
-__device__ __forceinline__ void shift_y(Tile<T, B, R, RV> &t) {
-    if constexpr (UPD != 0) {
-        const T f = t.nrm[B];
+// Cross-step norms from / to the replicated form: lane group i takes the
+// norms of x_i (column i of the tile) and y_i (column B + i).
+template <typename T, int B, int R, int RV>
+__device__ __forceinline__ void norms_to_pairs(Tile<T, B, R, RV> &t, int lane) {
+    constexpr int LB = Log2<B>::value;
+    const int li = lane >> (5 - LB);
+    t.nx = t.nrm[0];
+    t.ny = t.nrm[B];
 #pragma unroll
-        for (int i = 0; i < B - 1; ++i) t.nrm[B + i] = t.nrm[B + i + 1];
-        t.nrm[2 * B - 1] = f;
+    for (int i = 1; i < B; ++i)
+        if (li == i) { t.nx = t.nrm[i]; t.ny = t.nrm[B + i]; }
+}
+
+// y_i <- y_(i+1) (cyclic): the next CROSS step pairs x_i with the old y_(i+1).
+// Norm-update sweeps: lane group i takes the norm of y_(i+1) from group i + 1.
+template <int UPD, typename T, int B, int R, int RV>
+__device__ __forceinline__ void shift_y(Tile<T, B, R, RV> &t, int lane) {
+    if constexpr (UPD != 0) {
+        constexpr int LB = Log2<B>::value;
+        t.ny = __shfl_sync(FULL, t.ny, (lane + (32 >> LB)) & 31);
     }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -606,6 +644,8 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
                          T *xbuf = nullptr) {
     const int nr = ldw >> 5, nv = ldv >> 5;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int LB = Log2<B>::value;
+    const int li = lane >> (5 - LB);   // the lane's pair in the cross steps
     const int nw = nwarps();
     const bool act = warp < nb / 2;
     Tile<T, B, R, RV> t;
@@ -652,6 +692,9 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
                 circle_shift<UPD>(t);
             }
         }
+        if constexpr (UPD != 0) {
+            if (act) norms_to_pairs(t, lane);   // the cross steps keep each pair's norms in its lane group
+        }
         for (int br = 0; br < nb - 1; ++br) {
             if (br > 0 || sweep > 1) {
                 if (act) {
@@ -661,9 +704,9 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
                             if constexpr (UPD == 1) {
                                 // the updated norms travel with the tiles
                                 T *xn = xbuf + (size_t)nb * B * 32 * (R + RV);
-                                if (lane == 0) {
-#pragma unroll
-                                    for (int c = 0; c < 2 * B; ++c) xn[c < B ? X * B + c : Y * B + (c - B)] = t.nrm[c];
+                                if ((lane & ((32 >> LB) - 1)) == 0) {
+                                    xn[X * B + li] = t.nx;
+                                    xn[Y * B + li] = t.ny;
                                 }
                             }
                         } else {
@@ -673,10 +716,9 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
                         tile_io(t, W, ldw, V, ldv, X, Y, lane, true, nr, nv);
                     }
                     if constexpr (UPD == 2) {
-                        if (lane == 0) {
-#pragma unroll
-                            for (int c = 0; c < 2 * B; ++c)
-                                colnorm[c < B ? X * B + c : Y * B + (c - B)] = (double)t.nrm[c];
+                        if ((lane & ((32 >> LB) - 1)) == 0) {
+                            colnorm[X * B + li] = (double)t.nx;
+                            colnorm[Y * B + li] = (double)t.ny;
                         }
                     }
                 }
@@ -694,16 +736,18 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
                     if constexpr (UPD == 1) {
                         if (xbuf) {
                             const T *xn = xbuf + (size_t)nb * B * 32 * (R + RV);
-#pragma unroll
-                            for (int c = 0; c < 2 * B; ++c) t.nrm[c] = xn[c < B ? X * B + c : Y * B + (c - B)];
+                            t.nx = xn[X * B + li];
+                            t.ny = xn[Y * B + li];
                         } else {
+                            // nrm[0] on lane l: column l >> (5 - log2 2B) of the tile
                             T nrm[2 * B];
                             tile_col_norms(t, nrm, lane, nr);
-                            spread_norms(t, nrm[0]);
+                            t.nx = __shfl_sync(FULL, nrm[0], li << (4 - LB));
+                            t.ny = __shfl_sync(FULL, nrm[0], (B + li) << (4 - LB));
                         }
                     } else if constexpr (UPD == 2) {
-#pragma unroll
-                        for (int c = 0; c < 2 * B; ++c) t.nrm[c] = (T)colnorm[c < B ? X * B + c : Y * B + (c - B)];
+                        t.nx = (T)colnorm[X * B + li];
+                        t.ny = (T)colnorm[Y * B + li];
                     }
                 }
             }
@@ -712,7 +756,7 @@ __device__ int rb_sweeps(T *W, int ldw, T *V, int ldv, int nb, int live, T tol, 
                 for (int j = 0; j < B; ++j) {
                     if constexpr (UPD != 0) step_upd<false>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
                     else step<false>(t, tol2, big2, ex2, floor_, fl, rotate, lane, nr, nv);
-                    shift_y<UPD>(t);
+                    shift_y<UPD>(t, lane);
                 }
             }
         }
