@@ -132,6 +132,7 @@ struct Params {
     size_t team_bytes;
     int G;               // CTAs per team (1: every CTA is a team)
     int always_reorth;
+    int blocked;         // team path, real types: the blocked pass may run (block_pass)
 };
 
 __device__ __forceinline__ unsigned long long gtimer() {
@@ -265,24 +266,62 @@ __host__ __device__ inline int64_t x_stride(int64_t n, int esz) {
     return (n + v - 1) / v * v;
 }
 
+// Blocked pass of the team path (block_pass): the most candidate rows of a
+// block, columns per block at most, K chunk of its row products, and the
+// most rows a CTA may hold for it (its local sort).
+constexpr int kCandMax = 256;
+constexpr int kBlk = 32;
+constexpr int kKC = 128;
+constexpr int kSortMax = 1024;
+static_assert(kCandMax % 64 == 0 && kBlk == 32 && kSortMax >= 64, "blocked pass sizes");
+
 // Per-team workspace layout (byte offsets from the team's base).  X, the
-// packed columns, exists only for multi-CTA teams.
+// packed columns, and the blocked pass's areas exist only for multi-CTA teams:
+// cand (every CTA's best rows), bm (the candidate block of the projector,
+// kCandMax^2), bl (kBlk^2 triangular factor), bp (pivot rows), bv (pivot
+// leverages), bmeta.
 struct Layout {
-    size_t x, lev, y, part, cmap, slots, bar, total;
+    size_t x, lev, y, part, cmap, slots, bar, cand, bm, bl, bp, bv, bmeta, total;
 };
 __host__ __device__ inline size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
 __host__ __device__ inline Layout layout(int64_t m, int64_t n, int esz, int asz, int G) {
     Layout L;
     size_t o = 0;
-    L.x = o;     o += G > 1 ? al256((size_t)m * x_stride(n, esz) * esz) : 0;
+    const bool team = G > 1;
+    L.x = o;     o += team ? al256((size_t)m * x_stride(n, esz) * esz) : 0;
     L.lev = o;   o += al256((size_t)m * 8);
     L.y = o;     o += al256((size_t)n * asz);
-    L.part = o;  o += G > 1 ? al256((size_t)G * n * asz) : 0;
+    L.part = o;  o += team ? al256((size_t)G * n * asz) : 0;
     L.cmap = o;  o += al256((size_t)n * 4);
     L.slots = o; o += al256((size_t)2 * G * sizeof(Slot));
     L.bar = o;   o += 256;
+    L.cand = o;  o += team ? al256((size_t)kCandMax * sizeof(Slot)) : 0;
+    L.bm = o;    o += team ? al256((size_t)kCandMax * kCandMax * 8) : 0;
+    L.bl = o;    o += team ? al256((size_t)kBlk * kBlk * 8) : 0;
+    L.bp = o;    o += team ? al256((size_t)kBlk * 8) : 0;
+    L.bv = o;    o += team ? al256((size_t)kBlk * 8) : 0;
+    L.bmeta = o; o += team ? 256 : 0;
     L.total = o;
     return L;
+}
+
+// Candidates each CTA of a team of G contributes (its best rows) and the
+// candidate count padded to whole 64-row tiles: G q <= kCandMax.
+__host__ __device__ inline int cand_per_cta(int G) {
+    int q = kCandMax / G;
+    return q > 64 ? 64 : (q < 1 ? 1 : q);
+}
+__host__ __device__ inline int cand_count(int G) { return (G * cand_per_cta(G) + 63) & ~63; }
+
+// Dynamic shared memory of the blocked pass: the candidates (row, leverage),
+// then the largest of its phases' work areas.
+__host__ __device__ constexpr size_t block_smem() {
+    constexpr size_t sort = (size_t)kSortMax * 16;
+    constexpr size_t chol = (size_t)kCandMax * (kBlk + 1) * 8 + kCandMax * 8 + kBlk * 4 * 2 + 64;
+    constexpr size_t rows = (size_t)kBlk * kBlk * 8 + kBlk * 8 * 2 + (size_t)(64 + kBlk) * (kKC + 1) * 8 +
+                            (size_t)64 * (kBlk + 1) * 8 + 64 * 8 + kSortMax;
+    constexpr size_t w = sort > chol ? (sort > rows ? sort : rows) : (chol > rows ? chol : rows);
+    return (size_t)kCandMax * 16 + w;
 }
 
 // Rows are processed TPR threads per row, THREADS / TPR rows at a time, so a
@@ -348,6 +387,399 @@ __device__ __forceinline__ A group_sum(A v) {
         }
     }
     return v;
+}
+
+// Order of the candidate rows: the larger leverage first, then the smaller
+// row index (the reference's argmax takes the first of equal values).
+__device__ __forceinline__ bool before(double va, int64_t ia, double vb, int64_t ib) {
+    return va > vb || (va == vb && ia < ib);
+}
+
+// Rows rowA[0..64) (entries of INT64_MAX are zero rows) times rows
+// rowB[0..32) of X over its first `a` columns, in FP64: Yb (64 x 32, ld
+// kBlk + 1) = X_A X_B^T.  Staged through shared memory in FP64, kKC columns
+// at a time, the next chunk's loads in flight (registers) while the current
+// one is multiplied: warp w stages rows w + 16 j, lanes the columns.  Each
+// thread owns 4 x 4 outputs (rows r + 16 v, four consecutive columns) of one
+// quarter of the chunk's columns, the quarters summed at the end.  All
+// threads of the CTA call it.
+template <typename S>
+__device__ void rows_dot(const S *X, int64_t ldx, int a, const int64_t *rowA, const int64_t *rowB, double *Xr,
+                         double *Xs, double *Yb) {
+    constexpr int LDK = kKC + 1, LDY = kBlk + 1, NW = kThreads / 32;
+    constexpr int KC = sizeof(S) == 8 ? kKC / 2 : kKC;     // chunk: FP64 storage keeps half in flight
+    constexpr int RA = 64 / NW, RB = kBlk / NW, KL = KC / 32;    // rows per warp, columns per lane
+    static_assert(kThreads == 512 && kKC % 32 == 0, "rows_dot layout");
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int kq = tid >> 7, t7 = tid & 127, rr = t7 & 15, cg = t7 >> 4;   // K quarter, row, column group
+    const S *pa[RA], *pb[RB];
+#pragma unroll
+    for (int j = 0; j < RA; ++j) {
+        const int64_t row = rowA[warp + NW * j];
+        pa[j] = row != INT64_MAX ? X + row * ldx : nullptr;
+    }
+#pragma unroll
+    for (int j = 0; j < RB; ++j) {
+        const int64_t row = rowB[warp + NW * j];
+        pb[j] = row != INT64_MAX ? X + row * ldx : nullptr;
+    }
+    S va[RA][KL], vb[RB][KL];                              // the next chunk, in the storage type
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int u = 0; u < KL; ++u) {
+            const int k = k0 + lane + 32 * u;
+            const bool in = k < a;
+#pragma unroll
+            for (int j = 0; j < RA; ++j) va[j][u] = in && pa[j] ? __ldcg(pa[j] + k) : S(0);
+#pragma unroll
+            for (int j = 0; j < RB; ++j) vb[j][u] = in && pb[j] ? __ldcg(pb[j] + k) : S(0);
+        }
+    };
+    auto stage = [&]() {
+#pragma unroll
+        for (int u = 0; u < KL; ++u) {
+#pragma unroll
+            for (int j = 0; j < RA; ++j) Xr[(warp + NW * j) * LDK + lane + 32 * u] = (double)va[j][u];
+#pragma unroll
+            for (int j = 0; j < RB; ++j) Xs[(warp + NW * j) * LDK + lane + 32 * u] = (double)vb[j][u];
+        }
+    };
+    double acc[4][4];
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc[v][u] = 0.0;
+    fetch(0);
+    stage();
+    __syncthreads();
+    for (int k0 = 0; k0 < a; k0 += KC) {
+        const int kc = (a - k0) < KC ? (a - k0) : KC;
+        const bool more = k0 + KC < a;
+        if (more) fetch(k0 + KC);                          // in flight during the products
+        for (int k = kq; k < kc; k += 4) {
+            double x[4], y[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) x[v] = Xr[(rr + 16 * v) * LDK + k];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) y[u] = Xs[(4 * cg + u) * LDK + k];
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) acc[v][u] = fma(x[v], y[u], acc[v][u]);
+        }
+        __syncthreads();
+        if (more) {
+            stage();
+            __syncthreads();
+        }
+    }
+    // the four quarters, summed in a fixed order
+    for (int q4 = 0; q4 < 4; ++q4) {
+        if (kq == q4)
+#pragma unroll
+            for (int v = 0; v < 4; ++v)
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    double *y = Yb + (rr + 16 * v) * LDY + 4 * cg + u;
+                    *y = q4 ? *y + acc[v][u] : acc[v][u];
+                }
+        __syncthreads();
+    }
+}
+
+// This CTA's best q rows by leverage ("before" order: bitonic sort of its
+// nrow <= kSortMax rows in `work`), written to out[0..q).
+__device__ void publish_best(const double *lev, int64_t r0, int nrow, int q, Slot *out, unsigned char *work) {
+    double *kv = (double *)work;
+    int64_t *ki = (int64_t *)(work + (size_t)kSortMax * 8);
+    const int tid = threadIdx.x;
+    int np2 = 64;
+    while (np2 < nrow || np2 < q) np2 <<= 1;
+    for (int i = tid; i < np2; i += kThreads) {
+        kv[i] = i < nrow ? lev[r0 + i] : -1e300;
+        ki[i] = i < nrow ? r0 + i : INT64_MAX;
+    }
+    __syncthreads();
+    for (int k = 2; k <= np2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < np2; i += kThreads) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const bool up = (i & k) == 0;
+                    const bool sw = up ? before(kv[ixj], ki[ixj], kv[i], ki[i]) : before(kv[i], ki[i], kv[ixj], ki[ixj]);
+                    if (sw) {
+                        const double tv = kv[i];
+                        kv[i] = kv[ixj];
+                        kv[ixj] = tv;
+                        const int64_t ti = ki[i];
+                        ki[i] = ki[ixj];
+                        ki[ixj] = ti;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int i = tid; i < q; i += kThreads) out[i] = {kv[i], ki[i]};
+    __syncthreads();
+}
+
+// Blocked pass of the team path (real types).  The missing columns are the
+// pivoted Cholesky factor of the projector P = I - X X^T onto the complement
+// of the packed columns X, pivot = the largest leverage (P's remaining
+// diagonal), exactly as the per-column loop builds them: column k =
+// P_k e_p / sqrt(lev_p).  A block of up to kBlk columns is built
+// speculatively on a candidate set C (every CTA's best rows), then checked:
+//   P2  M = P[C, C] (diagonal: the tracked leverages; off-diagonal
+//       -X_i . X_j in FP64), shared out over the team in 64 x 32 tiles;
+//   P3  CTA 0: the pivoted Cholesky of M, pivot = the best remaining
+//       leverage in C, until kBlk columns, the missing columns run out, or
+//       the best is below 1/2 (the per-column loop then takes that column,
+//       with its second projection);
+//   P4  every CTA forms its rows of the block, Y = E_S - X X_S^T and
+//       N = Y L_SS^-T (forward substitution with the factor's pivot rows),
+//       stores N as the next packed columns, and checks every row outside C
+//       step by step: a row whose leverage at step s ranks before the
+//       pivot's would have been step s's pivot, so the block keeps only the
+//       steps before the first such s (step 0 always stands: the best row of
+//       every CTA is in C);
+//   P5  the leverages lowered by |N_i|^2 over the kept steps, the slots and
+//       the next block's candidates published.
+// The kept pivots and columns are, in exact arithmetic, the per-column
+// loop's, at four team barriers per block instead of one per column.
+// `fresh`: the candidate lists match the current leverages (else P1
+// publishes them first).  Returns the columns completed (0: the per-column
+// loop takes the next one), or -1 when a barrier wait ran out; `slow` is set
+// when the block ended on a leverage below 1/2.
+template <typename S>
+__device__ int block_pass(const Params &p, const Layout &L, unsigned char *base, S *X, int64_t ldx, double *lev,
+                          int a, const uint8_t *keep, int64_t c, int *cmap, Slot *slots, unsigned *bar,
+                          unsigned char *smem, int G, int g, int64_t r0, int64_t r1, bool &fresh, bool &slow,
+                          Slot *s_red) {
+    using T = Tr<S>;
+    constexpr unsigned FULL = 0xffffffffu;
+    constexpr int LDK = kKC + 1, LDY = kBlk + 1;
+    const int64_t n = p.n;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int q = cand_per_cta(G), nc = cand_count(G), nreal = G * q;
+    Slot *cand = (Slot *)(base + L.cand);
+    double *bm = (double *)(base + L.bm);
+    double *bl = (double *)(base + L.bl);
+    int64_t *bp = (int64_t *)(base + L.bp);
+    double *bpv = (double *)(base + L.bv);
+    int *bmeta = (int *)(base + L.bmeta);
+    int64_t *cidx = (int64_t *)smem;                       // candidates: row, leverage
+    double *cval = (double *)(smem + kCandMax * 8);
+    unsigned char *work = smem + kCandMax * 16;
+    __shared__ int s_nmiss, s_fail;
+    const int nrow = (int)(r1 - r0);
+    slow = false;
+
+    if (!fresh) {                                          // P1
+        publish_best(lev, r0, nrow, q, cand + (size_t)g * q, work);
+        if (!team_sync(bar, G)) return -1;
+    }
+    fresh = false;
+    // P2
+    for (int i = tid; i < nc; i += kThreads) {
+        cidx[i] = i < nreal ? __ldcg(&cand[i].idx) : INT64_MAX;
+        cval[i] = i < nreal ? __ldcg(&cand[i].val) : -1e300;
+    }
+    __syncthreads();
+    {
+        double *Xr = (double *)work, *Xs = Xr + 64 * LDK, *Yb = Xs + kBlk * LDK;
+        const int tcol = nc / kBlk, tiles = (nc / 64) * tcol;
+        for (int tt = g; tt < tiles; tt += G) {
+            const int i0 = 64 * (tt / tcol), j0 = kBlk * (tt % tcol);
+            rows_dot<S>(X, ldx, a, cidx + i0, cidx + j0, Xr, Xs, Yb);
+            for (int e = tid; e < 64 * kBlk; e += kThreads) {
+                const int r = e / kBlk, cc = e - r * kBlk, ia = i0 + r, jb = j0 + cc;
+                const bool ok = cidx[ia] != INT64_MAX && cidx[jb] != INT64_MAX;
+                bm[(size_t)ia * nc + jb] = ia == jb ? (ok ? cval[ia] : 0.0) : (ok ? -Yb[r * LDY + cc] : 0.0);
+            }
+            __syncthreads();
+        }
+    }
+    if (!team_sync(bar, G)) return -1;
+
+    // P3: CTA 0, the pivoted Cholesky of M
+    if (g == 0) {
+        constexpr int LDL = kBlk + 1;                      // odd: candidates' rows in different banks
+        double *Lc = (double *)work;                       // L[t][s], nc x kBlk (ld LDL)
+        double *d = Lc + (size_t)kCandMax * LDL;           // remaining leverage of candidate t
+        int *pa = (int *)(d + kCandMax);                   // candidate of pivot s
+        int *cols = pa + kBlk;                             // U column of pivot s
+        for (int i = tid; i < nc * LDL; i += kThreads) Lc[i] = 0.0;
+        for (int i = tid; i < nc; i += kThreads) d[i] = cidx[i] != INT64_MAX ? cval[i] : -1e300;
+        if (tid == 0) {
+            int k = 0;
+            for (int64_t cc = c; cc < n && k < kBlk; ++cc)
+                if (!keep[cc]) cols[k++] = (int)cc;
+            s_nmiss = k;
+        }
+        __syncthreads();
+        const int nmax = s_nmiss;
+        int ns = 0, stop_slow = 0;
+        // the best remaining candidate: each warp's best of its 32 (after the
+        // step's update), then the warps' bests in shared memory
+        __shared__ double s_wv[kWarps];
+        __shared__ int64_t s_wi[kWarps];
+        __shared__ int s_wa[kWarps];
+        auto warp_best = [&]() {
+            double bv = -1e300;
+            int64_t bi = INT64_MAX;
+            int ba = -1;
+            for (int t = tid; t < nc; t += kThreads)
+                if (d[t] > -1e299 && before(d[t], cidx[t], bv, bi)) { bv = d[t]; bi = cidx[t]; ba = t; }
+            for (int o = 16; o; o >>= 1) {
+                const double ov = __shfl_xor_sync(FULL, bv, o);
+                const int64_t oi = __shfl_xor_sync(FULL, bi, o);
+                const int oa = __shfl_xor_sync(FULL, ba, o);
+                if (before(ov, oi, bv, bi)) { bv = ov; bi = oi; ba = oa; }
+            }
+            if (lane == 0) { s_wv[warp] = bv; s_wi[warp] = bi; s_wa[warp] = ba; }
+        };
+        auto cta_best = [&](double &bv, int &ba) {
+            bv = s_wv[0];
+            int64_t bi = s_wi[0];
+            ba = s_wa[0];
+            for (int w = 1; w < kWarps; ++w)
+                if (before(s_wv[w], s_wi[w], bv, bi)) { bv = s_wv[w]; bi = s_wi[w]; ba = s_wa[w]; }
+        };
+        warp_best();
+        __syncthreads();
+        for (; ns < nmax; ++ns) {
+            double bv;
+            int pb;
+            cta_best(bv, pb);
+            if (pb < 0 || bv < 0.5) {
+                stop_slow = pb >= 0;
+                break;
+            }
+            const double lpp = sqrt(bv);
+            for (int t = tid; t < nc; t += kThreads) {
+                if (t == pb) {
+                    Lc[t * LDL + ns] = lpp;
+                    d[t] = -1e300;                         // pivoted
+                } else if (d[t] > -1e299) {
+                    const double mt = __ldcg(bm + (size_t)pb * nc + t);   // row pb of M (symmetric), in flight
+                    double acc0 = 0.0, acc1 = 0.0;
+                    int u = 0;
+                    for (; u + 1 < ns; u += 2) {
+                        acc0 = fma(Lc[t * LDL + u], Lc[pb * LDL + u], acc0);
+                        acc1 = fma(Lc[t * LDL + u + 1], Lc[pb * LDL + u + 1], acc1);
+                    }
+                    if (u < ns) acc0 = fma(Lc[t * LDL + u], Lc[pb * LDL + u], acc0);
+                    const double l = (mt - (acc0 + acc1)) / lpp;
+                    Lc[t * LDL + ns] = l;
+                    d[t] -= l * l;
+                }
+            }
+            if (tid == 0) {
+                pa[ns] = pb;
+                bpv[ns] = bv;
+            }
+            __syncthreads();                               // everyone has read this step's s_w*
+            warp_best();                                   // each thread's candidates are its own: no barrier before
+            __syncthreads();
+        }
+        for (int i = tid; i < ns * kBlk; i += kThreads) {
+            const int s2 = i / kBlk, t = i - s2 * kBlk;
+            bl[i] = t <= s2 ? Lc[pa[s2] * LDL + t] : 0.0;
+        }
+        for (int i = tid; i < ns; i += kThreads) {
+            bp[i] = cidx[pa[i]];
+            cmap[a + i] = cols[i];
+        }
+        if (tid == 0) {
+            bmeta[0] = ns;
+            bmeta[1] = stop_slow;
+            bmeta[2] = ns;                                 // the first failing step (P4), at most ns
+        }
+    }
+    if (!team_sync(bar, G)) return -1;
+    const int ns = __ldcg(bmeta);
+    if (ns == 0) {
+        slow = __ldcg(bmeta + 1) != 0;
+        fresh = true;                                      // the leverages did not change
+        return 0;
+    }
+
+    // P4: this CTA's rows of the block, 64 at a time, and the check
+    double *Ls = (double *)work;                           // kBlk x kBlk
+    int64_t *Sv = (int64_t *)(Ls + kBlk * kBlk);           // pivot rows
+    double *Pv = (double *)(Sv + kBlk);                    // pivot leverages
+    double *Xr = Pv + kBlk;                                // 64 x kKC (ld LDK)
+    double *Xs = Xr + 64 * LDK;                            // kBlk x kKC (ld LDK)
+    double *Yb = Xs + kBlk * LDK;                          // 64 x kBlk (ld LDY)
+    int64_t *rowsA = (int64_t *)(Yb + 64 * LDY);           // this chunk's rows
+    unsigned char *incand = (unsigned char *)(rowsA + 64); // own rows in C
+    for (int i = tid; i < ns * kBlk; i += kThreads) Ls[i] = __ldcg(bl + i);
+    for (int i = tid; i < kBlk; i += kThreads) {
+        Sv[i] = i < ns ? __ldcg(bp + i) : INT64_MAX;
+        Pv[i] = i < ns ? __ldcg(bpv + i) : 0.0;
+    }
+    for (int i = tid; i < nrow; i += kThreads) incand[i] = 0;
+    if (tid == 0) s_fail = ns;
+    __syncthreads();
+    for (int i = tid; i < nc; i += kThreads)
+        if (cidx[i] >= r0 && cidx[i] < r1) incand[cidx[i] - r0] = 1;
+    __syncthreads();
+    int fail = ns;
+    for (int64_t rc = r0; rc < r1; rc += 64) {
+        const int nr = (int)((r1 - rc) < 64 ? (r1 - rc) : 64);
+        if (tid < 64) rowsA[tid] = tid < nr ? rc + tid : INT64_MAX;
+        __syncthreads();
+        rows_dot<S>(X, ldx, a, rowsA, Sv, Xr, Xs, Yb);
+        if (tid < nr) {
+            const int64_t i = rc + tid;
+            double *yr = Yb + tid * LDY;
+            const bool check = !incand[i - r0];
+            double lv = lev[i];
+            for (int s2 = 0; s2 < ns; ++s2) {
+                if (check && s2 < fail && before(lv, i, Pv[s2], Sv[s2])) fail = s2;
+                double y0 = (i == Sv[s2] ? 1.0 : 0.0) - yr[s2], y1 = 0.0;
+                int t = 0;
+                for (; t + 1 < s2; t += 2) {
+                    y0 = fma(-yr[t], Ls[s2 * kBlk + t], y0);
+                    y1 = fma(-yr[t + 1], Ls[s2 * kBlk + t + 1], y1);
+                }
+                if (t < s2) y0 = fma(-yr[t], Ls[s2 * kBlk + t], y0);
+                const double y = (y0 + y1) / Ls[s2 * kBlk + s2];
+                yr[s2] = y;
+                const S ys = (S)y;                         // the stored value, as the leverage sees it
+                X[i * ldx + a + s2] = ys;
+                lv -= (double)ys * (double)ys;
+            }
+        }
+        __syncthreads();
+    }
+    if (fail < ns) atomicMin(&s_fail, fail);
+    __syncthreads();
+    if (tid == 0 && s_fail < ns) atomicMin(bmeta + 2, s_fail);
+    if (!team_sync(bar, G)) return -1;
+    const int kept = __ldcg(bmeta + 2);
+
+    // P5: leverages over the kept steps, slots, the next candidates
+    double best = -1e300;
+    int64_t bidx = 0;
+    for (int64_t i = r0 + tid; i < r1; i += kThreads) {
+        double lv = lev[i];
+        const S *xi = X + i * ldx + a;
+#pragma unroll 8
+        for (int s2 = 0; s2 < kept; ++s2) {
+            const double x = (double)__ldcg(xi + s2);
+            lv -= x * x;
+        }
+        lev[i] = lv;
+        if (lv > best) { best = lv; bidx = i; }
+    }
+    const Slot sb = cta_argmax(best, bidx, s_red);
+    if (tid == 0) slots[g] = sb;
+    publish_best(lev, r0, nrow, q, cand + (size_t)g * q, work);
+    if (!team_sync(bar, G)) return -1;
+    fresh = true;
+    slow = kept == ns && __ldcg(bmeta + 1) != 0;
+    return kept;
 }
 
 // TEAM = false: one CTA per matrix, in place on U (the columns not yet
@@ -435,8 +867,25 @@ __global__ void __launch_bounds__(kThreads, 1) null_kernel(Params p) {
         {
             int a = nkept;                                 // packed columns (TEAM)
             bool failed = false;
+            bool blocked = TEAM && !T::cplx && p.blocked;  // block_pass while it applies
+            bool fresh = false;                            // its candidate lists are current
             for (int64_t c = 0; c < n; ++c) {
                 if (keep[c]) continue;
+                if constexpr (TEAM && !T::cplx) {
+                    if (blocked) {
+                        bool slow = false;
+                        const int done = block_pass<S>(p, L, base, X, ldx, lev, a, keep, c, cmap, slots, bar, smem, G,
+                                                       g, r0, r1, fresh, slow, s_red);
+                        if (done < 0) goto timeout;
+                        if (slow) blocked = false;
+                        if (done > 0) {
+                            a += done;
+                            c = __ldcg(&cmap[a - 1]);              // the last column of the block
+                            continue;
+                        }
+                    }
+                    fresh = false;                         // the per-column step changes the leverages
+                }
                 const int na = TEAM ? a : (int)n;          // columns a product runs over
                 const int64_t col = TEAM ? a : c;          // where v is built
                 // idx = team-wide first argmax of the leverage
@@ -569,7 +1018,7 @@ timeout:
 }
 
 struct Plan {
-    int G;
+    int G, blocked;
     int64_t grid;
     size_t team_bytes, bytes, smem;
 };
@@ -590,6 +1039,7 @@ static Plan make_plan(int dtype, int64_t batch, int64_t m, int64_t n) {
     const int sms = dev_sms();
     const int esz = esize(dtype), asz = dtype >= 2 ? 16 : 8;
     const bool large = batch * 4 < sms && m * n >= (1 << 16) && m >= 256;
+    pl.blocked = 0;
     if (large) {
         int64_t G = m / 64;                         // about 64 rows per CTA
         if (G > sms) G = sms;
@@ -598,6 +1048,8 @@ static Plan make_plan(int dtype, int64_t batch, int64_t m, int64_t n) {
         pl.grid = G;
         pl.team_bytes = layout(m, n, esz, asz, pl.G).total;
         pl.bytes = pl.team_bytes;
+        // real types, at most kSortMax rows per CTA: the blocked pass
+        pl.blocked = dtype <= 1 && (m + G - 1) / G <= kSortMax;
     } else {
         pl.G = 1;
         int64_t grid = (int64_t)sms * 4;
@@ -608,6 +1060,7 @@ static Plan make_plan(int dtype, int64_t batch, int64_t m, int64_t n) {
         pl.bytes = pl.team_bytes * (size_t)grid;
     }
     pl.smem = (size_t)n * esz;
+    if (pl.blocked && pl.smem < block_smem()) pl.smem = block_smem();
     return pl;
 }
 
@@ -616,6 +1069,7 @@ static int launch(Params &p, const Plan &pl, cudaStream_t st) {
     p.G = pl.G;
     p.team_bytes = pl.team_bytes;
     p.always_reorth = pl.G == 1;
+    p.blocked = pl.blocked;
     if (pl.G == 1) {
         auto kern = null_kernel<S, false>;
         if (pl.smem > 48 * 1024 &&

@@ -5,8 +5,9 @@ Bars: the pivot rows are integers and must be the oracle's; the completed
 columns agree with the oracle's within 1e-12 (float64 / complex128) and
 5e-5 (float32 / complex64); kept columns come back unchanged.  Cases cover
 the one-CTA-per-matrix path (many matrices), the multi-CTA team path (one
-tall matrix), a full basis that needs the second projection, the all-zero
-input, and the reference's failure when the columns cannot be completed."""
+tall matrix), its blocked pass (most columns missing), a full basis that
+needs the second projection, the all-zero input, and the reference's
+failure when the columns cannot be completed."""
 import importlib
 
 import numpy as np
@@ -72,6 +73,23 @@ def test_team_path_tall(S, dtype):
     assert np.array_equal(np.abs(got[0][:, miss]).argmax(0), np.abs(want[0][:, miss]).argmax(0))
     err = np.abs(got.astype(np.float64) - want).max()
     assert err <= (1e-11 if dtype == np.float64 else 5e-5), err
+
+
+@pytest.mark.parametrize("dtype,m,n,kept", [(np.float64, 4096, 1024, 32), (np.float32, 4096, 512, 16)])
+def test_blocked_pass(S, dtype, m, n, kept):
+    """A tall matrix with most columns missing: the team path completes them
+    in blocks (candidate rows, pivoted Cholesky of their projector block);
+    the pivots and columns must be the per-column algorithm's."""
+    rng = np.random.default_rng(m + n)
+    u, keep = _case(rng, 1, m, n, kept, dtype)
+    want = O.complete_null_columns(u.astype(np.float64), keep)
+    got = S._complete_null_columns(torch.from_numpy(u).cuda(), torch.from_numpy(keep).cuda()).cpu().numpy()
+    miss = ~keep[0]
+    assert np.array_equal(np.abs(got[0][:, miss]).argmax(0), np.abs(want[0][:, miss]).argmax(0))
+    err = np.abs(got.astype(np.float64) - want).max()
+    assert err <= (1e-11 if dtype == np.float64 else 5e-5), err
+    g64 = got[0].astype(np.float64)
+    assert np.abs(g64.T @ g64 - np.eye(n)).max() <= (1e-12 if dtype == np.float64 else 2e-5)
 
 
 def test_team_path_full_basis(S):
