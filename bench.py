@@ -65,9 +65,9 @@ COUNT = 8192
 # this workload, the four launches of the two size classes (rb32_kernel_t
 # 256- and 128-thread, rb64_kernel 512- and 256-thread), from one ncu capture
 # (those metrics only) of `bench.py --steps 1 --warmup 3 --no-cpu-baseline`.
-MEASURED_TRAFFIC_PER_SOLVE = 289.5e6
+MEASURED_TRAFFIC_PER_SOLVE = 289.0e6
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the four solve launches of one step, "
-                  "captured at the library of commit 520108d (profiles/rb_uneven_batch_8192.md)")
+                  "captured at the library of commit 013b917 (profiles/rb_uneven_batch_8192.md)")
 
 
 MIXED = ("mixed (FP32 sweeps, then FP64 sweeps from the Newton-Schulz orthogonalised V, "
