@@ -256,10 +256,10 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
     extern __shared__ __align__(16) unsigned char smem[];
     TG *sd = (TG *)smem;               // d[x] = G[x][x]
     TG *se = sd + n;                       // e[x] = G[x][x + 1]
-    TG *sc = se + n;                       // c of the pair starting at position p
-    TG *ss = sc + n;                       // s of the pair starting at position p
-    TG *bg = ss + n;                       // [NW][2][n] boundary columns of G (first, last)
-    float *bq = (float *)(bg + (size_t)NW * 2 * n);  // [NW][2][n] boundary columns of Q
+    TG *sc = se + n;                       // c of the pair starting at position p, at cs_at(p)
+    TG *ss = sc + n;                       // s of the pair starting at position p, at cs_at(p)
+    TG *bg = ss + n;                       // [NW][2][RPT][32] boundary columns of G (first, last), lane-major
+    float *bq = (float *)(bg + (size_t)NW * 2 * n);  // [NW][2][RPT][32] boundary columns of Q, lane-major
     float *Qs = bq + (size_t)NW * 2 * n;       // n x n, Q[col * n + row] (write-out)
     int *perm = (int *)(Qs + (size_t)n * n);   // n
     __shared__ int s_any;
@@ -267,6 +267,11 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
     __shared__ double s_red[NW];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int r0 = lane * RPT, c0 = warp * CB;
+    // Shared-memory slots of per-row data, lane-major: row x = RPT l + i (lane l's i-th row) at
+    // 32 i + l, so that the 32 lanes reading "their" i-th row hit 32 consecutive words instead of
+    // one bank RPT-fold; a warp-uniform row is a broadcast either way.
+    auto cs_at = [](int x) { return (x % RPT) * 32 + x / RPT; };
+    auto bnd_at = [](int w, int side, int i, int l) { return ((w * 2 + side) * RPT + i) * 32 + l; };
     const int k = blockIdx.x;
     const double live_floor = live_floor_ptr ? *live_floor_ptr : 0.0;
     const float *g_in = Gin + (size_t)k * n * n;
@@ -349,8 +354,8 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
                         if (apq < 0.0) sn = -sn;
                         s_any = 1;
                     }
-                    sc[p] = c;
-                    ss[p] = sn;
+                    sc[cs_at(p)] = c;
+                    ss[cs_at(p)] = sn;
                     if constexpr (DQ)
                         cs_out[(((size_t)k * max_sweeps + (sweep - 1)) * n + r) * n + p] = make_float2((float)c, (float)sn);
                 }
@@ -361,7 +366,7 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
             if (par == 0) {
 #pragma unroll
                 for (int i = 0; i < RPT; i += 2) {
-                    const TG c = sc[r0 + i], sn = ss[r0 + i];
+                    const TG c = sc[32 * i + lane], sn = ss[32 * i + lane];       // pair at row r0 + i
 #pragma unroll
                     for (int j = 0; j < CB; ++j) {
                         const TG x = g[i][j], y = g[i + 1][j];
@@ -371,8 +376,11 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
                 }
             } else {
                 const bool has_up = lane > 0, has_down = lane < 31;
-                const TG cu = has_up ? sc[r0 - 1] : (TG)1, su = has_up ? ss[r0 - 1] : (TG)0;
-                const TG cd = has_down ? sc[r0 + RPT - 1] : (TG)1, sdn = has_down ? ss[r0 + RPT - 1] : (TG)0;
+                // pairs at rows r0 - 1 (lane - 1's last row) and r0 + RPT - 1 (this lane's last row)
+                const TG cu = has_up ? sc[32 * (RPT - 1) + lane - 1] : (TG)1,
+                         su = has_up ? ss[32 * (RPT - 1) + lane - 1] : (TG)0;
+                const TG cd = has_down ? sc[32 * (RPT - 1) + lane] : (TG)1,
+                         sdn = has_down ? ss[32 * (RPT - 1) + lane] : (TG)0;
 #pragma unroll
                 for (int j = 0; j < CB; ++j) {
                     const TG up = __shfl_up_sync(0xffffffffu, g[RPT - 1][j], 1);   // row r0 - 1
@@ -383,7 +391,7 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
                 }
 #pragma unroll
                 for (int i = 1; i + 1 < RPT; i += 2) {
-                    const TG c = sc[r0 + i], sn = ss[r0 + i];
+                    const TG c = sc[32 * i + lane], sn = ss[32 * i + lane];       // pair at row r0 + i
 #pragma unroll
                     for (int j = 0; j < CB; ++j) {
                         const TG x = g[i][j], y = g[i + 1][j];
@@ -396,7 +404,7 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
             if (par == 0) {
 #pragma unroll
                 for (int j = 0; j < CB; j += 2) {
-                    const TG c = sc[c0 + j], sn = ss[c0 + j];
+                    const TG c = sc[cs_at(c0 + j)], sn = ss[cs_at(c0 + j)];
                     const float fc = (float)c, fs = (float)sn;
 #pragma unroll
                     for (int i = 0; i < RPT; ++i) {
@@ -414,40 +422,40 @@ __global__ void __launch_bounds__(RPT * 1024 / CB) eig_reg_kernel(const float *G
                 // publish this warp's first and last columns (after the row rotation)
 #pragma unroll
                 for (int i = 0; i < RPT; ++i) {
-                    bg[((size_t)warp * 2 + 0) * n + r0 + i] = g[i][0];
-                    bg[((size_t)warp * 2 + 1) * n + r0 + i] = g[i][CB - 1];
+                    bg[bnd_at(warp, 0, i, lane)] = g[i][0];
+                    bg[bnd_at(warp, 1, i, lane)] = g[i][CB - 1];
                     if constexpr (!DQ) {
-                        bq[((size_t)warp * 2 + 0) * n + r0 + i] = q[i][0];
-                        bq[((size_t)warp * 2 + 1) * n + r0 + i] = q[i][CB - 1];
+                        bq[bnd_at(warp, 0, i, lane)] = q[i][0];
+                        bq[bnd_at(warp, 1, i, lane)] = q[i][CB - 1];
                     }
                 }
                 __syncthreads();
                 const bool has_left = warp > 0, has_right = warp < NW - 1;
-                const TG cl = has_left ? sc[c0 - 1] : (TG)1, sl = has_left ? ss[c0 - 1] : (TG)0;
-                const TG cr = has_right ? sc[c0 + CB - 1] : (TG)1, sr = has_right ? ss[c0 + CB - 1] : (TG)0;
+                const TG cl = has_left ? sc[cs_at(c0 - 1)] : (TG)1, sl = has_left ? ss[cs_at(c0 - 1)] : (TG)0;
+                const TG cr = has_right ? sc[cs_at(c0 + CB - 1)] : (TG)1,
+                         sr = has_right ? ss[cs_at(c0 + CB - 1)] : (TG)0;
 #pragma unroll
                 for (int i = 0; i < RPT; ++i) {
-                    const int row = r0 + i;
                     if (has_left) {                // pair (c0 - 1, c0): this warp holds the second
-                        const TG x = bg[((size_t)(warp - 1) * 2 + 1) * n + row];
+                        const TG x = bg[bnd_at(warp - 1, 1, i, lane)];
                         g[i][0] = cl * x - sl * g[i][0];
                         if constexpr (!DQ) {
-                            const float u = bq[((size_t)(warp - 1) * 2 + 1) * n + row];
+                            const float u = bq[bnd_at(warp - 1, 1, i, lane)];
                             q[i][0] = (float)cl * u - (float)sl * q[i][0];
                         }
                     }
                     if (has_right) {               // pair (c0 + CB - 1, c0 + CB): this warp holds the first
-                        const TG y = bg[((size_t)(warp + 1) * 2 + 0) * n + row];
+                        const TG y = bg[bnd_at(warp + 1, 0, i, lane)];
                         g[i][CB - 1] = sr * g[i][CB - 1] + cr * y;
                         if constexpr (!DQ) {
-                            const float v = bq[((size_t)(warp + 1) * 2 + 0) * n + row];
+                            const float v = bq[bnd_at(warp + 1, 0, i, lane)];
                             q[i][CB - 1] = (float)sr * q[i][CB - 1] + (float)cr * v;
                         }
                     }
                 }
 #pragma unroll
                 for (int j = 1; j + 1 < CB; j += 2) {
-                    const TG c = sc[c0 + j], sn = ss[c0 + j];
+                    const TG c = sc[cs_at(c0 + j)], sn = ss[cs_at(c0 + j)];
                     const float fc = (float)c, fs = (float)sn;
 #pragma unroll
                     for (int i = 0; i < RPT; ++i) {
