@@ -732,6 +732,94 @@ __global__ void __launch_bounds__(256) gemm_f64acc_kernel(const float *A, const 
     }
 }
 
+// The same product for 16-byte aligned rows (A, B 16-byte aligned; lda, ldb
+// and K multiples of 4): the next 16-deep K slice is fetched with float4
+// loads into registers while the current slice's FMAs run, then stored as
+// FP64 into the other half of a double-buffered shared tile, so each slice
+// costs one barrier and no exposed global latency.  Thread (ty, tx) owns rows
+// 2 ty + 32 i + {0, 1} and columns 2 tx + 32 j + {0, 1} (i, j < 4): its
+// operands are double2 loads from shared memory.
+constexpr int kF64KC = 16;
+constexpr size_t kF64AccSmem = 2 * 2 * kF64KC * 128 * sizeof(double);   // [A, B][2][16][128]
+
+__global__ void __launch_bounds__(256) gemm_f64acc_vec_kernel(const float *A, const float *B, float *C, int64_t M,
+                                                              int64_t N, int64_t K, int64_t lda, int64_t ldb,
+                                                              int64_t ldc, int m_fast) {
+    extern __shared__ __align__(16) double f64acc_smem[];
+    double *As = f64acc_smem;                      // As[buf][k][row] at (buf * kF64KC + k) * 128 + row
+    double *Bs = f64acc_smem + 2 * kF64KC * 128;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    // m_fast: consecutive CTAs take consecutive row tiles of C, so the tile of
+    // B (the larger operand) they share is read from DRAM once
+    const int64_t m0 = (int64_t)(m_fast ? blockIdx.x : blockIdx.y) * 128,
+                  n0 = (int64_t)(m_fast ? blockIdx.y : blockIdx.x) * 128;
+    // loader: row lrow of the tile, K offsets lk and lk + 8 of the slice
+    const int lrow = threadIdx.x & 127, lk = (threadIdx.x >> 7) * 4;
+    const bool arow = m0 + lrow < M, brow = n0 + lrow < N;
+    const float *ap = A + (arow ? (m0 + lrow) * lda : 0), *bp = B + (brow ? (n0 + lrow) * ldb : 0);
+    float4 pa[2], pb[2];
+    auto fetch = [&](int64_t k0) {
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            const int64_t ka = k0 + lk + 8 * l;
+            const bool kin = ka < K;               // K % 4 == 0: a float4 is wholly in or out
+            pa[l] = (arow && kin) ? *(const float4 *)(ap + ka) : make_float4(0.f, 0.f, 0.f, 0.f);
+            pb[l] = (brow && kin) ? *(const float4 *)(bp + ka) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    };
+    auto stash = [&](int buf) {
+#pragma unroll
+        for (int l = 0; l < 2; ++l) {
+            double *a = As + ((size_t)buf * kF64KC + lk + 8 * l) * 128 + lrow;
+            double *b = Bs + ((size_t)buf * kF64KC + lk + 8 * l) * 128 + lrow;
+            a[0] = pa[l].x; a[128] = pa[l].y; a[256] = pa[l].z; a[384] = pa[l].w;
+            b[0] = pb[l].x; b[128] = pb[l].y; b[256] = pb[l].z; b[384] = pb[l].w;
+        }
+    };
+    double acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    const int64_t nk = (K + kF64KC - 1) / kF64KC;
+    fetch(0);
+    stash(0);
+    __syncthreads();
+    for (int64_t kb = 0; kb < nk; ++kb) {
+        const int buf = (int)(kb & 1);
+        if (kb + 1 < nk) fetch((kb + 1) * kF64KC);
+        const double *a_s = As + (size_t)buf * kF64KC * 128, *b_s = Bs + (size_t)buf * kF64KC * 128;
+#pragma unroll
+        for (int k = 0; k < kF64KC; ++k) {
+            double a[8], b[8];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const double2 x = *(const double2 *)(a_s + k * 128 + 2 * ty + 32 * i);
+                const double2 y = *(const double2 *)(b_s + k * 128 + 2 * tx + 32 * i);
+                a[2 * i] = x.x; a[2 * i + 1] = x.y;
+                b[2 * i] = y.x; b[2 * i + 1] = y.y;
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        // The other half was last read in the previous slice, before its barrier.
+        if (kb + 1 < nk) stash(buf ^ 1);
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int64_t r = m0 + 2 * ty + 32 * (i >> 1) + (i & 1);
+        if (r >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int64_t c = n0 + 2 * tx + 32 * (j >> 1) + (j & 1);
+            if (c < N) C[r * ldc + c] = (float)acc[i][j];
+        }
+    }
+}
+
 // Workspace of the deferred-Q form: the recorded (c, s) of every round and
 // the sorted positions, per slot.
 __host__ inline size_t eig_dq_cs_bytes(int64_t pairs, int n, int max_sweeps) {
@@ -888,7 +976,19 @@ int jb_gemm_f64acc(const float *A, const float *B, float *C, int64_t M, int64_t 
     if (!A || !B || !C || M < 1 || N < 1 || K < 1 || lda < K || ldb < K || ldc < N) return JB_EINVAL;
     if ((M + 127) / 128 > 65535) return JB_ETOOBIG;
     dim3 grid((unsigned)((N + 127) / 128), (unsigned)((M + 127) / 128));
-    gemm_f64acc_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(A, B, C, M, N, K, lda, ldb, ldc);
+    const bool vec = ((uintptr_t)A & 15) == 0 && ((uintptr_t)B & 15) == 0 && lda % 4 == 0 && ldb % 4 == 0 &&
+                     K % 4 == 0;
+    if (vec) {
+        const int m_fast = N > M && (N + 127) / 128 <= 65535;
+        if (m_fast) grid = dim3((unsigned)((M + 127) / 128), (unsigned)((N + 127) / 128));
+        if (cudaFuncSetAttribute(gemm_f64acc_vec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kF64AccSmem) != cudaSuccess)
+            return JB_ECUDA;
+        gemm_f64acc_vec_kernel<<<grid, 256, kF64AccSmem, (cudaStream_t)stream>>>(A, B, C, M, N, K, lda, ldb, ldc,
+                                                                                   m_fast);
+    } else {
+        gemm_f64acc_kernel<<<grid, 256, 0, (cudaStream_t)stream>>>(A, B, C, M, N, K, lda, ldb, ldc);
+    }
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
 }
 

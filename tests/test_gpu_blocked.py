@@ -51,6 +51,42 @@ def test_blocked_matches_lapack(BJ, m, n, b, cond):
     assert err1 <= 5e-6 and relbig <= 1e-5 and rec <= 2e-5 and ou <= max(2e-5, 2e-7 * cond) and ov <= 2e-5
 
 
+@pytest.mark.parametrize("M,N,K,lda", [(300, 520, 1000, 1000), (256, 384, 1004, 1012), (129, 77, 37, 37),
+                                        (130, 200, 64, 66)])
+def test_gemm_f64acc_against_fp64(M, N, K, lda):
+    """jb_gemm_f64acc (C = A B^T, exact float products summed in FP64):
+    equal to the FP64 product rounded once to float, on the float4 path
+    (16-byte rows: K, lda multiples of 4, ragged K slices and tiles) and on
+    the scalar path (odd lda or K).  The inputs cancel heavily, so an
+    FP32-accumulated product misses this bound by orders of magnitude."""
+    N_ = importlib.import_module("pavel-s_svd_b200.native")
+    g = torch.Generator().manual_seed(M + N + K)
+    a_full = torch.randn(M, lda, generator=g)
+    b_full = torch.randn(N, lda, generator=g)
+    # cancellation: columns h..2h-1 of A are minus columns 0..h-1 (scaled by
+    # 1e3) plus O(1), and the same columns of B repeat columns 0..h-1, so
+    # every entry of C is O(1) made from terms of size 1e3
+    h = K // 2
+    a_full[:, :h] *= 1e3
+    a_full[:, h:2 * h] = -a_full[:, :h] + a_full[:, h:2 * h]
+    b_full[:, h:2 * h] = b_full[:, :h]
+    a = a_full[:, :K]
+    b = b_full[:, :K]
+    A = a_full.cuda()
+    B = b_full.cuda()
+    C = torch.empty(M, N, device="cuda")
+    N_.check(N_.lib().jb_gemm_f64acc(A.data_ptr(), B.data_ptr(), C.data_ptr(), M, N, K, lda, lda, N,
+                                     torch.cuda.current_stream().cuda_stream), "jb_gemm_f64acc")
+    torch.cuda.synchronize()
+    ref = (a.double() @ b.double().T)
+    scale = a.double().abs() @ b.double().abs().T
+    err = (C.cpu().double() - ref).abs()
+    bound = 2.5e-7 * ref.abs() + 1e-14 * scale
+    assert bool((err <= bound).all()), float((err / bound).max())
+    f32 = (a @ b.T).double()                               # FP32 accumulation, for contrast
+    assert float((f32 - ref).abs().max()) > 10 * float(bound.max())
+
+
 @pytest.mark.parametrize("n", [64, 128, 48])
 def test_block_eig_f64(n):
     """jb_block_eig_f64 alone: Qt (hi + lo + lo2) orthogonal, Qt G Qt^T
