@@ -67,7 +67,7 @@ COUNT = 8192
 # (those metrics only) of `bench.py --steps 1 --warmup 3 --no-cpu-baseline`.
 MEASURED_TRAFFIC_PER_SOLVE = 289.0e6
 TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the four solve launches of one step, "
-                  "captured at the library of commit 013b917 (profiles/rb_uneven_batch_8192.md)")
+                  "captured at the library of commit 013b917 (the FP32 and FP64 solve kernels unchanged since)")
 
 
 MIXED = ("mixed (FP32 sweeps, then FP64 sweeps from the Newton-Schulz orthogonalised V, "
@@ -652,6 +652,26 @@ def run_plain_single(args):
     print(json.dumps(line), flush=True)
 
 
+def cpu_sweep_sample(a_np, width):
+    """CPU cost of one sweep of the plain one-sided Jacobi on a (the C
+    restatement of the reference's jacobi_svd, oracle/): disjoint blocks of
+    `width` columns, one per host thread, each run for one sweep at once; a
+    sweep's pairs are independent within a round, so the full sweep on the
+    same threads is extrapolated as (pairs of a) / (pairs of a block) x the
+    wall time / the blocks run side by side.  Returns (seconds per sweep,
+    threads, wall seconds, blocks)."""
+    from oracle import c_oracle
+    m, n = a_np.shape
+    threads = c_oracle.max_threads()
+    blocks = max(1, min(threads, n // width))
+    sub = np.stack([a_np[:, k * width:(k + 1) * width] for k in range(blocks)])
+    t = time.perf_counter()
+    c_oracle.svd_batched(sub, values_only=True, max_sweeps=1, threads=blocks)
+    wall = time.perf_counter() - t
+    per_sweep = wall * (n * (n - 1)) / (width * (width - 1)) / blocks
+    return per_sweep, blocks, wall, blocks
+
+
 def run_blocked(args, name):
     import torch
     wl = importlib.import_module("pavel-s_svd_b200.workloads")
@@ -698,6 +718,49 @@ def run_blocked(args, name):
             "converged": info["converged"], "reached_tol": info["reached_tol"],
             "tensor_flop_per_solve": tensor_flop, "tensor_tflops_whole_solve": tensor_flop / (ms / 1e3) / 1e12,
             "accuracy": acc}
+    pk = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    peak, kind = (float(pk["bf16_tflops_sustained"]), "measured sustained") if "bf16_tflops_sustained" in pk \
+        else (1400.0, "fallback sustained")
+    achieved = tensor_flop / (ms / 1e3) / 1e12
+    line["roofline"] = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                        "frac": achieved / peak, "peak_kind": kind, "traffic": None,
+                        "note": "tensor flops of the Gram and update products (3 or 6 BF16 terms) over the whole "
+                                "solve; the solve is bound by the 16-slot eigen-solves that set each round's pace"}
+    if not args.no_plain:
+        # the plain FP32 CUDA path at the same shape: the reference's block
+        # rounds (solvers.py:30-68), every pair's inner one-sided Jacobi in
+        # FP32 on the CUDA cores (pair QR first), updates as FP32 GEMMs
+        S_ = importlib.import_module("pavel-s_svd_b200.solvers")
+        e0, e1 = _events()
+        torch.cuda.synchronize()
+        e0.record()
+        try:
+            u2, s2, vh2, st2 = S_._composed_svd(a[None], "block_jacobi", False, False, True, n,
+                                                {"block_size": b, "precision": "fp32"})
+            e1.record()
+            torch.cuda.synchronize()
+            pms = e0.elapsed_time(e1)
+            acc2 = lapack_check(a_np, u2[0], s2[0], vh2[0], max(m, n))
+            line["plain_fp32"] = {
+                "matrices_per_s": 1e3 / pms, "ms": pms, "block_sweeps": st2.get("block_sweeps"),
+                "inner_jacobi_sweeps_max": st2.get("jacobi_sweeps"), "accuracy": acc2,
+                "meets_1e-5": bool(acc2["resolved_spectrum_max_relative_error"] <= 1e-5),
+                "tensor_over_plain_fp32": pms / ms,
+                "note": "svd(a, 'block_jacobi', block_size=b) through the block rounds with precision='fp32': "
+                        "the reference's algorithm on this library's FP32 CUDA-core kernels, one call"}
+        except RuntimeError as err:
+            torch.cuda.synchronize()
+            line["plain_fp32"] = {"failed": str(err)}
+    if not args.no_cpu_baseline:
+        per_sweep, thr, wall, blocks = cpu_sweep_sample(a_np, 128)
+        k = line.get("plain_fp32", {}).get("block_sweeps") or info["block_sweeps"]
+        line["cpu_baseline"] = {
+            "value": 1.0 / (per_sweep * k), "unit": "matrices/s", "cores": thr, "kind": "port", "cpu": cpu_model(),
+            "seconds_per_sweep_extrapolated": per_sweep,
+            "sample": f"one sweep of the plain one-sided Jacobi (C restatement) on {blocks} disjoint {m}x128 column "
+                      f"blocks at once ({wall:.1f} s), extrapolated by pair count to one sweep of the whole matrix, "
+                      f"times {k} sweeps (the block sweeps of the plain FP32 path; a block sweep of the reference "
+                      f"does at least one sweep's work, so this overstates the CPU's throughput)"}
     print(json.dumps(line), flush=True)
 
 
@@ -915,6 +978,8 @@ def main():
                     help="reference arm: skip timing the reference's own PyTorch CPU Jacobi")
     ap.add_argument("--ref-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true",
+                    help="blocked workloads: skip the plain FP32 CUDA block-rounds comparison")
     ap.add_argument("--eager", action="store_true",
                     help="blocked workloads: launch the timed solve's kernels one by one instead of replaying the "
                          "captured sweep graphs (for a profiler's launch list; the line is then no bench number)")

@@ -11,7 +11,7 @@ standalone suite.  Each test skips, saying why, when its part is absent.
     spec and run_one() on a CUDA device; the row must come back "ok" with
     the reference's own validate() metrics within its bounds.
   * The reference's Standalone test case with SVD_TEST_DEVICE=cuda and
-    svdbench.standalone.svd replaced by the INTEGRATION.md shim: CUDA input
+    svdbench.standalone.svd replaced by the integration shim: CUDA input
     of the families this library builds goes to pavel_s_svd_b200.svd, the
     rest to the reference's own torch code.
 """
@@ -96,7 +96,7 @@ def test_reference_standalone_suite_through_shim(ref):
     SS = importlib.import_module("svdbench.standalone")
     torch_svd = SS.svd
 
-    def svd(a, algorithm='jacobi', **kw):                 # the INTEGRATION.md shim
+    def svd(a, algorithm='jacobi', **kw):                 # the integration shim
         if a.is_cuda and algorithm in b200.ALGORITHMS and (
                 not a.is_complex() or algorithm in b200.COMPLEX_ALGORITHMS):
             return b200.svd(a, algorithm, **kw)
