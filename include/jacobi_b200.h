@@ -61,6 +61,11 @@ extern "C" {
 #define JB_BLOCK_WIDTH_8    8   /* uneven batches: FP32 register sweeps with
                                    8-column blocks (4 warps per 64 columns)
                                    instead of 4-column blocks                   */
+#define JB_ONE_SIZE_CLASS  16   /* uneven batches: no second launch per phase
+                                   for the matrices of at most 32 columns (tall
+                                   view) in half-size CTAs; every matrix runs
+                                   in the full-size CTAs.  Same results; a
+                                   choice for the autotuner                     */
 
 /* ---- arithmetic of the solve ------------------------------------------- */
 #define JB_PREC_NATIVE      0   /* sweeps in the input precision (f32 or f64)   */

@@ -82,7 +82,8 @@ def shard_by_cost(m, n, parts):
 
 class Launch:
     """Launch choices of an uneven solve: ``flags`` (ROUND_ROBIN pair order,
-    BLOCK_WIDTH_8 register blocks) and ``exit_ratio`` (the FP32 phase of a
+    BLOCK_WIDTH_8 register blocks, ONE_SIZE_CLASS: no separate half-size
+    launch for matrices of at most 32 columns) and ``exit_ratio`` (the FP32 phase of a
     mixed solve hands over once no pair ratio of a sweep exceeds it; 0 = the
     library default 1e-2, < 0 = the FP32 phase runs to tol).  Every choice
     converges to the same tolerance; they differ only in speed."""
@@ -91,7 +92,8 @@ class Launch:
         self.flags, self.exit_ratio = int(flags), float(exit_ratio)
 
     def __repr__(self):
-        names = [n for n, b in (("round_robin", N.ROUND_ROBIN), ("block_width_8", N.BLOCK_WIDTH_8)) if self.flags & b]
+        names = [n for n, b in (("round_robin", N.ROUND_ROBIN), ("block_width_8", N.BLOCK_WIDTH_8),
+                                ("one_size_class", N.ONE_SIZE_CLASS)) if self.flags & b]
         return f"Launch({'|'.join(names) or 'default'}, exit_ratio={self.exit_ratio:g})"
 
     def key(self):
@@ -100,7 +102,7 @@ class Launch:
 
 # Candidates the autotuner times (the first is the library default).
 TUNE_CANDIDATES = (Launch(), Launch(exit_ratio=3e-3), Launch(exit_ratio=-1.0), Launch(N.BLOCK_WIDTH_8),
-                   Launch(N.ROUND_ROBIN))
+                   Launch(N.ONE_SIZE_CLASS), Launch(N.ROUND_ROBIN))
 _tune_cache = {}
 
 

@@ -276,7 +276,7 @@ constexpr int kB32L = 4;  // block width of the large-tile FP32 kernel (16 warps
 // and one confirming sweep, as it does from a fully converged FP32 phase.
 constexpr float kMixedExitRatio = 1e-2f;
 // Launch choices jb_svd_uneven_f32_ex accepts in `flags` (an autotuner picks among them).
-constexpr int kTuneFlags = JB_ROUND_ROBIN | JB_BLOCK_WIDTH_8;
+constexpr int kTuneFlags = JB_ROUND_ROBIN | JB_BLOCK_WIDTH_8 | JB_ONE_SIZE_CLASS;
 constexpr int kB64 = 2;   // block width of the FP64 sweeps (16 warps for 64 columns)
 constexpr int kT32 = 256, kT64 = 512;  // threads of the two kernels
 constexpr int kMaxR = 4;  // rows per lane: mt <= 128
@@ -978,7 +978,7 @@ static Plan make_plan(int max_mt, int max_nt, int elem, int precision, int flags
         pl.smem32 = aux_bytes(pl.d32) + pl.reg32 + pl.xbytes32;
         pl.smem64 = aux_bytes(pl.d64) + pl.reg64;
         if (pl.smem64 > kSmemLimit || pl.smem32 > kSmemLimit) pl.reg = false;
-        pl.split = pl.reg && pl.bw == kB32 && max_nt > kNarrowN;
+        pl.split = pl.reg && pl.bw == kB32 && max_nt > kNarrowN && !(flags & JB_ONE_SIZE_CLASS);
         if (pl.split) {
             const RGeo r32n = rgeo(max_mt, kNarrowN, kB32, flags);
             pl.d32n = raux_dims(r32n);

@@ -16,7 +16,7 @@ from .build import library_path
 JB_OK, JB_EINVAL, JB_ETOOBIG, JB_EWORKSPACE, JB_ECUDA = 0, 1, 2, 3, 4
 ST_OK, ST_NOT_CONVERGED, ST_NONFINITE_IN, ST_NULL_FAILED, ST_NONFINITE_OUT, ST_BAD_DESC, ST_TIMEOUT = (
     0, 1, 2, 3, 4, 5, 6)
-FULL_MATRICES, VALUES_ONLY, ROUND_ROBIN, BLOCK_WIDTH_8 = 1, 2, 4, 8
+FULL_MATRICES, VALUES_ONLY, ROUND_ROBIN, BLOCK_WIDTH_8, ONE_SIZE_CLASS = 1, 2, 4, 8, 16
 PREC_NATIVE, PREC_MIXED = 0, 1
 
 RC_NAMES = {JB_EINVAL: "invalid argument", JB_ETOOBIG: "shape too large for this entry point",

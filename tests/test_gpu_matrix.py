@@ -8,11 +8,13 @@ Tolerances, stated once (relative to sigma_1): sigma 2e-5 for single
 precision (the 'fp32' and complex64 arithmetic of the reference), 1e-11 for
 double precision; orthonormal columns and reconstruction 10x those, scaled
 by max(1, size / 64).  gram_jacobi squares the condition number cond: sigma
-within 10 eps cond, vectors within 10 eps cond^2 (checked where that is
-below 1e-2).  The projected solvers run with rank = min(m, n) and no power
+within 10 eps cond (or reported as 0 within a factor 2 of the reference's
+eigenvalue cut), vectors within 10 eps cond^2 (checked where that is below
+1e-2).  The projected solvers run with rank = min(m, n) and no power
 iterations, where their range basis is exact."""
 import importlib
 import itertools
+import zlib
 
 import numpy as np
 import pytest
@@ -44,7 +46,8 @@ def pkg():
 
 @pytest.mark.parametrize("alg,dt,shape,form", _cases())
 def test_routes_against_lapack(pkg, alg, dt, shape, form):
-    rng = np.random.default_rng(abs(hash((alg, np.dtype(dt).name, shape))) % 2**32)
+    # a seed fixed per case (Python's hash of strings changes per process)
+    rng = np.random.default_rng(zlib.crc32(f"{alg}-{np.dtype(dt).name}-{shape}".encode()))
     a = rng.standard_normal(shape)
     if np.issubdtype(dt, np.complexfloating):
         a = a + 1j * rng.standard_normal(shape)
@@ -77,7 +80,14 @@ def test_routes_against_lapack(pkg, alg, dt, shape, form):
         vec_scale = max(1.0, eps * cond ** 2 / tol)
     s = s.cpu().numpy().astype(np.float64)
     assert s.shape == (*shape[:-2], r)
-    assert float(np.abs(s - truth[..., :r]).max() / truth.max()) <= sig_tol
+    err = np.abs(s - truth[..., :r])
+    allowed = sig_tol * truth.max()
+    if alg == "gram_jacobi":
+        # the reference reports 0 for Gram eigenvalues below eps n w_max
+        # (solvers.py:_gram): values near that cut may come back as 0
+        cut = truth[..., :1] * np.sqrt(2.0 * eps * n)
+        allowed = np.where(truth[..., :r] < cut, np.maximum(truth[..., :r], allowed), allowed)
+    assert bool((err <= allowed).all()), float((err - allowed).max())
     if form == "values":
         assert u is None and vh is None
         return

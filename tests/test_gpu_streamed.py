@@ -48,8 +48,9 @@ def test_streamed_raises_on_nonfinite_input():
 
 def test_launch_choices_and_autotuner():
     """Every launch choice the autotuner varies (pair order, block width,
-    FP32-phase exit ratio) converges to the same singular values within the
-    mixed path's bound; tune() returns the fastest of them and caches it."""
+    FP32-phase exit ratio, one size class instead of two) converges to the
+    same singular values within the mixed path's bound; tune() returns the
+    fastest of them and caches it."""
     B = importlib.import_module("pavel-s_svd_b200.batch")
     N = importlib.import_module("pavel-s_svd_b200.native")
     wl = importlib.import_module("pavel-s_svd_b200.workloads")
@@ -72,3 +73,4 @@ def test_launch_choices_and_autotuner():
     assert times[repr(best)] == min(times.values())
     assert B.tune(m, n, x)[0] is best                      # cached
     assert B.Launch(N.ROUND_ROBIN | N.BLOCK_WIDTH_8).flags == 12
+    assert repr(B.Launch(N.ONE_SIZE_CLASS)) == "Launch(one_size_class, exit_ratio=0)"
