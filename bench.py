@@ -700,7 +700,8 @@ def run_blocked(args, name):
     R, P, mp, npd = plan.nb - 1, plan.P, plan.mpad, plan.npad
     per_round = P * (2 * mp * (2 * b) ** 2 * 2 + 2 * npd * (2 * b) ** 2)       # Gram + W and V updates
     terms = [3 if p == 2 else 6 for _, p in info["off_per_sweep"]]
-    tensor_flop = sum(R * per_round * t for t in terms)
+    # the sweeps' Gram and update products, and the post-sweep Gram of the whole W
+    tensor_flop = sum(R * per_round * t + 2 * npd * npd * mp * t for t in terms)
     acc = lapack_check(a_np, U, S, Vh, max(m, n))
     line = {"metric": f"blocked Jacobi SVD matrices/s ({m}x{n}, b={b})", "value": 1e3 / ms, "unit": "matrices/s",
             "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 2), "ms_per_step": ms,
@@ -715,6 +716,7 @@ def run_blocked(args, name):
             "data": ("synthetic (seeded: Haar U, V; 64 clusters x 16, cond 1e6)" if name == "clustered_large"
                      else "synthetic (seeded: rank-64 Gaussian product + N(0, 1e-6) noise)"),
             "block_sweeps": info["block_sweeps"], "off_per_sweep": info["off_per_sweep"],
+            "post_sweep_off": info["post_sweep_off"],
             "converged": info["converged"], "reached_tol": info["reached_tol"],
             "tensor_flop_per_solve": tensor_flop, "tensor_tflops_whole_solve": tensor_flop / (ms / 1e3) / 1e12,
             "accuracy": acc}

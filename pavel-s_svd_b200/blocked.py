@@ -123,6 +123,8 @@ class BlockJacobi:
         self.Qt = [torch.empty(self.P, 2 * b, 2 * b, **bf) for _ in range(3)]
         self.off = torch.zeros(R, self.P, **f32)
         self.dmax = torch.zeros(R, self.P, **f32)
+        self.Gfull = torch.empty(self.npad, self.npad, **f32)      # post-sweep Gram of the whole W
+        self.post_off = torch.zeros(1, **f32)
         self.isweeps = torch.zeros(self.P, dtype=torch.int32, device=dev)
         self.live = torch.zeros(1, dtype=torch.float64, device=dev)   # live-column floor of the sweep
         # CTAs along K of the Gram products: about one wave over the SMs
@@ -290,22 +292,49 @@ class BlockJacobi:
                 "jb_block_eig_ws")
         return qt
 
-    def _run_sweep(self, cur, parts, inner_sweeps, inner_tol, use_graphs):
+    def _post_sweep_off(self, cur, parts, live_rel):
+        """The reference's convergence test after a sweep (solvers.py:51-58),
+        on the device into self.post_off: the largest |g_pq| / sqrt(g_pp g_qq)
+        over pairs of live columns (g_pp > live_rel * max g) of G = W^T W, G
+        formed on the tensor cores from the stored parts of W (all rows of W^T
+        at once; their slot order does not change the maximum).  The in-sweep
+        off of the eigen-solves sees a pair only when its slot meets it in the
+        next sweep, one sweep later than this test.  No host sync: it is
+        captured with the sweep."""
+        w = list(self.W[cur][:parts])
+        g = gemm_parts(w, w, self.Gfull, chain128=True)
+        d = g.diagonal().clamp_min(0)
+        live = d > live_rel * d.max()
+        sd = d.sqrt()
+        corr = g.abs() / (sd[:, None] * sd[None, :]).clamp_min(torch.finfo(torch.float32).tiny)
+        corr.fill_diagonal_(0)
+        corr = torch.where(live[:, None] & live[None, :], corr, torch.zeros_like(corr))
+        self.post_off.copy_(corr.max().reshape(1))
+
+    def _run_sweep(self, cur, parts, inner_sweeps, inner_tol, use_graphs, post_rel=None):
         """One sweep, replayed from a CUDA graph after its first (eager) run:
         the ~4 (nb - 1) launches of a sweep then cost one host call.  The
         graphs hold only this plan's buffers; the live floor is read on the
-        device (self.live)."""
+        device (self.live).  post_rel: also run the post-sweep test
+        (_post_sweep_off) with that live floor, in the same graph."""
         key = (cur, parts, inner_sweeps, inner_tol, self._eig_variant(parts), self.gram_split, self.schedule,
-               self.slot_split)
+               self.slot_split, post_rel)
         sweep = self._sweep_dataflow if self.schedule == "dataflow" else self._sweep
+
+        def body():
+            nxt = sweep(cur, parts, inner_sweeps, inner_tol)
+            if post_rel is not None:
+                self._post_sweep_off(nxt, parts, post_rel)
+            return nxt
+
         if not use_graphs or key not in self._seen:
             self._seen.add(key)
-            return sweep(cur, parts, inner_sweeps, inner_tol)
+            return body()
         g = self._graphs.get(key)
         if g is None:
             g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g):
-                sweep(cur, parts, inner_sweeps, inner_tol)
+                body()
             self._graphs[key] = g
         g.replay()
         return 1 - cur
@@ -388,7 +417,8 @@ class BlockJacobi:
         return times
 
     def solve(self, a: torch.Tensor, *, tol_phase1=5e-6, switch=5e-2, max_sweeps=30, max_two_part=12,
-              inner_sweeps=1, inner_tol=1e-7, polar_steps=2, require_convergence=True, use_graphs=True):
+              inner_sweeps=1, inner_tol=1e-7, polar_steps=2, require_convergence=True, use_graphs=True,
+              post_check=True):
         """SVD of a (m x n float32, CUDA).  Returns U (m x n), S (n), Vh (n x n),
         info dict.
 
@@ -403,7 +433,11 @@ class BlockJacobi:
         off <= tol_phase1, the reference's 40 eps32 (solvers.py:41).  Early
         sweeps are not monotone (columns migrate between blocks while the
         per-pair sort settles), so a stall -- off not halving for two sweeps
-        -- only ends the solve once off < 1e-4, the FP32 floor regime."""
+        -- only ends the solve once off < 1e-4, the FP32 floor regime.
+        post_check: after every sweep also run the reference's own test on
+        the Gram of the whole W (_post_sweep_off); the stage switch and the
+        end of the solve then come one sweep sooner, the end only when that
+        off is below half of tol_phase1 (room for the Gram's rounding)."""
         lib = N.lib()
         dev, st = self.device, _st(self.device)
         m, n, b, P, R = self.m, self.n, self.b, self.P, self.nb - 1
@@ -415,21 +449,26 @@ class BlockJacobi:
         live_rel = (np.finfo(np.float32).eps * max(m, n)) ** 2
         dmax = float((at * at).sum(1).max())
         best, stall, converged, stage_sweeps = float("inf"), 0, False, 0
+        post_hist = []
         for sweeps in range(1, max_sweeps + 1):
             self.live.fill_((live_rel if parts == 3 else 1e-4) * dmax)
             stage_sweeps += 1
-            cur = self._run_sweep(cur, parts, inner_sweeps, inner_tol, use_graphs)
-            off = float(self.off.max())
-            dmax = max(dmax, float(self.dmax.max()))
+            cur = self._run_sweep(cur, parts, inner_sweeps, inner_tol, use_graphs,
+                                  (live_rel if parts == 3 else 1e-4) if post_check else None)
+            vals = torch.stack([self.off.max(), self.dmax.max(), self.post_off[0]]).cpu()   # one sync
+            off = float(vals[0])
+            dmax = max(dmax, float(vals[1]))
             off_hist.append((off, parts))
+            post = float(vals[2]) if post_check else math.inf
+            post_hist.append(post)
             if off < 0.5 * best:
                 best, stall = off, 0
             elif off < 1e-4:
                 stall += 1
-            if parts == 3 and (off <= tol_phase1 or stall >= 2):
+            if parts == 3 and (off <= tol_phase1 or post <= 0.5 * tol_phase1 or stall >= 2):
                 converged = True
                 break
-            if parts == 2 and (off <= switch or stage_sweeps >= max_two_part):
+            if parts == 2 and (off <= switch or post <= switch or stage_sweeps >= max_two_part):
                 # Re-synchronise before the accurate sweeps: V made orthogonal,
                 # W = A V recomputed from the exact input (the 16-bit sweeps
                 # left W's small columns off by ~2^-16 sigma_1 / sigma_j).
@@ -460,7 +499,8 @@ class BlockJacobi:
         from .solvers import _complete_null_columns
         U = _complete_null_columns(U[:m][None], (S > 0)[None])[0]
         info = {"algorithm": "block_jacobi", "block_sweeps": sweeps, "off_per_sweep": off_hist,
-                "converged": converged, "reached_tol": off_hist[-1][0] <= tol_phase1,
+                "post_sweep_off": post_hist, "converged": converged,
+                "reached_tol": off_hist[-1][0] <= tol_phase1 or post_hist[-1] <= 0.5 * tol_phase1,
                 "precision": "tensor-core sweeps (3xBF16 then 6xBF16) with FP64 block eigen-solves; "
                              "6xBF16 Newton-Schulz V, FP64-accumulated W = A V"}
         return U, S, Vh[:, :n].contiguous(), info
