@@ -64,6 +64,11 @@ def schedule(nb):
     return out
 
 
+# W = A V at the stage switch and the finish runs on the tensor cores when the
+# columns the reference's cut keeps span at most this ratio (else FP64 sums)
+TENSOR_W_COND = 32.0
+
+
 class BlockJacobi:
     """Plan + buffers for one m x n (m >= n) float32 matrix, block width b."""
 
@@ -167,8 +172,28 @@ class BlockJacobi:
             vt = gemm_parts(split3_bf16(h), vp, b_mn=True, chain128=True)[0]
         return vt
 
-    def _w_from_v(self, vt, ap):
-        """W^T = V^T A^T with FP64 accumulation of exact float products."""
+    def _cond_kept(self, cur, parts):
+        """sigma_1 / the smallest column norm of W (buffer `cur`) that the
+        reference's cut eps32 * max(m, n) * sigma_1 keeps (solvers.py:18-21)."""
+        w = self.W[cur][0].float()
+        for x in self.W[cur][1:parts]:
+            w += x.float()
+        nrm = w.pow(2).sum(1).sqrt()
+        s1 = nrm.max()
+        kept = nrm[nrm > np.finfo(np.float32).eps * max(self.m, self.n) * s1]
+        return float(s1 / kept.min()) if kept.numel() else math.inf
+
+    def _w_from_v(self, vt, ap, cond_kept=math.inf, ap_parts=None):
+        """W^T = V^T A^T.  Exact float products summed in FP64
+        (jb_gemm_f64acc) in general: a small kept column sigma_j carries the
+        product's error times sigma_1 / sigma_j.  When every column the cut
+        keeps is within TENSOR_W_COND of sigma_1, the six-term BF16 product on
+        the tensor cores instead (hi, mid, lo splits of both operands, FP32
+        chains of at most 128): about 2^-24 sigma_1 absolute in each column,
+        so at most TENSOR_W_COND x 2^-24 (2e-6) relative to a kept one."""
+        if cond_kept <= TENSOR_W_COND:
+            return gemm_parts(list(split3_bf16(vt)), list(ap_parts if ap_parts is not None else split3_bf16(ap)),
+                              chain128=True)[0]
         wt = torch.empty(self.npad, self.mpad, dtype=torch.float32, device=self.device)
         N.check(N.lib().jb_gemm_f64acc(vt.data_ptr(), ap.data_ptr(), wt.data_ptr(), self.npad, self.mpad, self.npad,
                                        self.npad, self.npad, self.mpad, _st(self.device)), "jb_gemm_f64acc")
@@ -454,6 +479,7 @@ class BlockJacobi:
         dmax = float((at * at).sum(1).max())
         best, stall, converged, stage_sweeps = float("inf"), 0, False, 0
         post_hist = []
+        ap_parts = None
         for sweeps in range(1, max_sweeps + 1):
             self.live.fill_((live_rel if parts == 3 else 1e-4) * dmax)
             stage_sweeps += 1
@@ -476,11 +502,13 @@ class BlockJacobi:
                 # Re-synchronise before the accurate sweeps: V made orthogonal,
                 # W = A V recomputed from the exact input (the 16-bit sweeps
                 # left W's small columns off by ~2^-16 sigma_1 / sigma_j).
-                parts = 3
+                parts_before, parts = parts, 3
                 best, stall, stage_sweeps = float("inf"), 0, 0
                 vt = self._combine_v(cur)
                 vt = self._polar(vt, polar_steps)
-                wt = self._w_from_v(vt, ap)
+                ck = self._cond_kept(cur, parts_before)
+                ap_parts = split3_bf16(ap) if ck <= TENSOR_W_COND else None
+                wt = self._w_from_v(vt, ap, ck, ap_parts)
                 for buf, src, L in ((self.W[cur], wt, self.mpad), (self.V[cur], vt, self.npad)):
                     N.check(lib.jb_rows_scatter(src.data_ptr(), self.init_map.data_ptr(), buf[0].data_ptr(),
                                                 buf[1].data_ptr(), buf[2].data_ptr(), None, self.npad, L, st),
@@ -489,7 +517,9 @@ class BlockJacobi:
             raise RuntimeError("block Jacobi did not converge")
         # The data now sits in round 0's layout of the next sweep.
         vt = self._polar(self._combine_v(cur), polar_steps)
-        wt = self._w_from_v(vt, ap)                                       # npad x mpad
+        ck = self._cond_kept(cur, parts)
+        wt = self._w_from_v(vt, ap, ck, ap_parts if ck <= TENSOR_W_COND else None)   # npad x mpad
+        w_product = "six-term BF16 (tensor cores)" if ck <= TENSOR_W_COND else "FP64-accumulated"
         U = torch.empty(self.mpad, n, dtype=torch.float32, device=dev)
         S = torch.empty(n, dtype=torch.float32, device=dev)
         Vh = torch.empty(n, self.npad, dtype=torch.float32, device=dev)
@@ -506,5 +536,6 @@ class BlockJacobi:
                 "post_sweep_off": post_hist, "converged": converged,
                 "reached_tol": off_hist[-1][0] <= tol_phase1 or post_hist[-1] <= post_end * tol_phase1,
                 "precision": "tensor-core sweeps (3xBF16 then 6xBF16) with FP64 block eigen-solves; "
-                             "6xBF16 Newton-Schulz V, FP64-accumulated W = A V"}
+                             f"6xBF16 Newton-Schulz V, {w_product} W = A V",
+                "cond_kept": ck}
         return U, S, Vh[:, :n].contiguous(), info
