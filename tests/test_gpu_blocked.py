@@ -87,6 +87,27 @@ def test_gemm_f64acc_against_fp64(M, N, K, lda):
     assert float((f32 - ref).abs().max()) > 10 * float(bound.max())
 
 
+def test_w_from_v_tensor_matches_fp64(BJ):
+    """W^T = V^T A^T of the blocked solver's stage switch and finish: the
+    six-term BF16 tensor-core product (taken when every kept column is within
+    TENSOR_W_COND of sigma_1) agrees with the FP64-accumulated one to ~2^-24
+    of the largest column norm in every entry, and the cond_kept measure
+    picks the path as stated."""
+    m, n, b = 600, 256, 32
+    plan = BJ.BlockJacobi(m, n, b)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    ap = torch.zeros(plan.mpad, plan.npad, device="cuda")
+    ap[:m, :n] = torch.randn(m, n, device="cuda", generator=g)
+    vt = torch.linalg.qr(torch.randn(plan.npad, plan.npad, device="cuda", generator=g, dtype=torch.float64))[0]
+    vt = vt.float().contiguous()
+    w64 = plan._w_from_v(vt, ap)
+    wtc = plan._w_from_v(vt, ap, cond_kept=1.0)
+    scale = float(ap.norm(dim=0).max())
+    assert float((wtc - w64).abs().max()) <= 2e-6 * scale
+    assert float((wtc - w64).abs().max()) > 0.0             # a different product was taken
+    assert BJ.TENSOR_W_COND == 32.0
+
+
 @pytest.mark.parametrize("n", [64, 128, 48])
 def test_block_eig_f64(n):
     """jb_block_eig_f64 alone: Qt (hi + lo + lo2) orthogonal, Qt G Qt^T
