@@ -210,6 +210,19 @@ JB_API int jb_gemm_bf16x_rows(const void *const *A, const void *const *B, int32_
                               int64_t ldb, int64_t batch, int64_t strideA, int64_t strideB,
                               float alpha, int32_t *error_flag, void *stream);
 
+/* Two jb_gemm_bf16x_rows products in one launch that share A, K, the split
+ * parts, mode and row map: alpha A B^T into out (N columns, rows ld_out long)
+ * and alpha A B2^T into out2 (N2 columns, rows ld_out2 long); B2 has the
+ * layout of B with its own ldb2 and strideB2.  The blocked Jacobi's rotation
+ * update of W^T and of V^T with the same Q^T (solvers.py:49-50), each rotated
+ * row moved to its next-round slot, without a second launch. */
+JB_API int jb_gemm_bf16x_rows2(const void *const *A, const void *const *B, const void *const *B2,
+                               int32_t mode, void *const *out, void *const *out2, int32_t nparts,
+                               const int32_t *row_map, int64_t ld_out, int64_t ld_out2, int64_t M,
+                               int64_t N, int64_t N2, int64_t K, int64_t lda, int64_t ldb,
+                               int64_t ldb2, int64_t batch, int64_t strideA, int64_t strideB,
+                               int64_t strideB2, float alpha, int32_t *error_flag, void *stream);
+
 /* hi = bf16(X), lo = bf16(X - hi) for n floats (lo may be NULL). */
 JB_API int jb_split_bf16(const float *X, void *hi, void *lo, int64_t n, void *stream);
 

@@ -40,7 +40,7 @@ import numpy as np
 import torch
 
 from . import native as N
-from .tensor import gemm_parts, gemm_parts_rows, split3_bf16
+from .tensor import gemm_parts, gemm_parts_rows, gemm_parts_rows2, split3_bf16
 
 
 def _st(dev):
@@ -214,9 +214,10 @@ class BlockJacobi:
             self._eig(0, P, parts, r, inner_sweeps, inner_tol, st)
             # X_k <- vv^T X_k (rows of W^T), same for V, each rotated row
             # written (as BF16 parts) straight into its next-round slot.
+            # (one launch for both: the same Q^T and row map)
             nxt = 1 - cur
-            gemm_parts_rows(self.Qt[:parts], Wp, self.W[nxt][:parts], self.maps[r], b_mn=True)
-            gemm_parts_rows(self.Qt[:parts], Vp, self.V[nxt][:parts], self.maps[r], b_mn=True)
+            gemm_parts_rows2(self.Qt[:parts], Wp, self.W[nxt][:parts], Vp, self.V[nxt][:parts], self.maps[r],
+                             b_mn=True)
             cur = nxt
         return cur
 

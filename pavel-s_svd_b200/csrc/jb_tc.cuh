@@ -31,7 +31,7 @@ constexpr uint32_t A_TILE = BM * BK * 2;  // 16 KiB
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz
 
 struct TcParams {
-    CUtensorMap ta[3], tb[3];
+    CUtensorMap ta[3], tb[6];   // tb[3..5]: the B parts of a second product (nx1 > 0)
     float *C;
     long long ldc, sC;
     int M, N, K;
@@ -56,6 +56,13 @@ struct TcParams {
     int out_nparts;
     const int *out_map;
     long long out_ld;
+    // A second product in the same launch (row-mapped output only): the
+    // column tiles blockIdx.x >= nx1 (nx1 > 0) compute alpha * A B2^T (B2's
+    // parts in tb[3..5]) with the same A, K and row map into out_part2, N2
+    // columns, rows out_ld2 long.
+    int nx1, N2;
+    __nv_bfloat16 *out_part2[3];
+    long long out_ld2;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -167,8 +174,10 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 
 // Stores 32 consecutive values of one output row as hi / mid / lo BF16
 // parts (16-byte stores when the row segment is 16-byte aligned and whole).
-__device__ __forceinline__ void store_parts32(const TcParams &p, long long base, int col0, const float (&v)[32]) {
-    const bool vec = col0 + 32 <= p.N && ((base + col0) & 7) == 0;
+__device__ __forceinline__ void store_parts32(__nv_bfloat16 *out0, __nv_bfloat16 *out1, __nv_bfloat16 *out2,
+                                              int nparts, int N, float alpha, long long base, int col0,
+                                              const float (&v)[32]) {
+    const bool vec = col0 + 32 <= N && ((base + col0) & 7) == 0;
     if (vec) {
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
@@ -178,7 +187,7 @@ __device__ __forceinline__ void store_parts32(const TcParams &p, long long base,
                 wh[i] = wm[i] = wl[i] = 0u;
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
-                    const float x = p.alpha * v[g * 8 + i * 2 + e];
+                    const float x = alpha * v[g * 8 + i * 2 + e];
                     const __nv_bfloat16 h = __float2bfloat16_rn(x);
                     const float r1 = x - __bfloat162float(h);
                     const __nv_bfloat16 m = __float2bfloat16_rn(r1);
@@ -189,19 +198,21 @@ __device__ __forceinline__ void store_parts32(const TcParams &p, long long base,
                 }
             }
             const long long o = base + col0 + g * 8;
-            *(uint4 *)(p.out_part[0] + o) = make_uint4(wh[0], wh[1], wh[2], wh[3]);
-            if (p.out_nparts > 1) *(uint4 *)(p.out_part[1] + o) = make_uint4(wm[0], wm[1], wm[2], wm[3]);
-            if (p.out_nparts > 2) *(uint4 *)(p.out_part[2] + o) = make_uint4(wl[0], wl[1], wl[2], wl[3]);
+            *(uint4 *)(out0 + o) = make_uint4(wh[0], wh[1], wh[2], wh[3]);
+            if (nparts > 1) *(uint4 *)(out1 + o) = make_uint4(wm[0], wm[1], wm[2], wm[3]);
+            if (nparts > 2) *(uint4 *)(out2 + o) = make_uint4(wl[0], wl[1], wl[2], wl[3]);
         }
     } else {
-        for (int i = 0; i < 32 && col0 + i < p.N; ++i) {
-            const float x = p.alpha * v[i];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+            if (col0 + i >= N) break;
+            const float x = alpha * v[i];
             const __nv_bfloat16 h = __float2bfloat16_rn(x);
             const float r1 = x - __bfloat162float(h);
             const __nv_bfloat16 m = __float2bfloat16_rn(r1);
-            p.out_part[0][base + col0 + i] = h;
-            if (p.out_nparts > 1) p.out_part[1][base + col0 + i] = m;
-            if (p.out_nparts > 2) p.out_part[2][base + col0 + i] = __float2bfloat16_rn(r1 - __bfloat162float(m));
+            out0[base + col0 + i] = h;
+            if (nparts > 1) out1[base + col0 + i] = m;
+            if (nparts > 2) out2[base + col0 + i] = __float2bfloat16_rn(r1 - __bfloat162float(m));
         }
     }
 }
@@ -222,7 +233,17 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
     __shared__ int s_err;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
+    // the launch's second product (nx1 > 0): its column tiles follow the first's
+    const bool second = p.nx1 > 0 && (int)blockIdx.x >= p.nx1;
+    const int n0 = (second ? (int)blockIdx.x - p.nx1 : (int)blockIdx.x) * BN, m0 = blockIdx.y * BM;
+    const int Ncols = second ? p.N2 : p.N;
+    const int tb0 = second ? 3 : 0;
+    // (scalars selected here: a pointer into the parameter arrays chosen at run
+    // time would make the compiler copy them to local memory)
+    __nv_bfloat16 *const out0 = second ? p.out_part2[0] : p.out_part[0];
+    __nv_bfloat16 *const out1 = second ? p.out_part2[1] : p.out_part[1];
+    __nv_bfloat16 *const out2 = second ? p.out_part2[2] : p.out_part[2];
+    const long long out_ld = second ? p.out_ld2 : p.out_ld;
     const int batch = blockIdx.z / p.splits, split = blockIdx.z % p.splits;
     const int kbeg = split * p.kchunk;
     const int kend = min(p.K, kbeg + p.kchunk);
@@ -265,10 +286,10 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
                 for (int b = 0; b < p.nb; ++b) {
                     unsigned char *bt = st + p.na * A_TILE + b * B_TILE;
                     if (!p.b_mn) {
-                        tma_load_3d(bt, &p.tb[b], kx, n0, batch, &full[s]);
+                        tma_load_3d(bt, &p.tb[b + tb0], kx, n0, batch, &full[s]);
                     } else {
                         for (int g = 0; g < BN / 64; ++g)
-                            tma_load_3d(bt + g * 8192, &p.tb[b], n0 + 64 * g, kx, batch, &full[s]);
+                            tma_load_3d(bt + g * 8192, &p.tb[b + tb0], n0 + 64 * g, kx, batch, &full[s]);
                     }
                 }
             }
@@ -313,7 +334,7 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
     if (__all_sync(0xffffffffu, have && !s_err)) {
         const long long obase = p.out_nparts
             ? (long long)(p.out_map && row < p.M ? p.out_map[(long long)batch * p.M + row]
-                                                 : (long long)batch * p.M + row) * p.out_ld
+                                                 : (long long)batch * p.M + row) * out_ld
             : 0;
         float *crow = p.C ? p.C + (long long)batch * p.sC + (long long)row * p.ldc : nullptr;
 #pragma unroll 1
@@ -326,10 +347,10 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
 #pragma unroll
                 for (int i = 0; i < 32; ++i) v[i] += w[i];
             }
-            if (row >= p.M || n0 + c0 >= p.N) continue;
+            if (row >= p.M || n0 + c0 >= Ncols) continue;
             if (p.out_nparts) {
-                store_parts32(p, obase, n0 + c0, v);
-            } else if (p.splits == 1 && n0 + c0 + 32 <= p.N && (((uintptr_t)(crow + n0 + c0)) & 15) == 0) {
+                store_parts32(out0, out1, out2, p.out_nparts, Ncols, p.alpha, obase, n0 + c0, v);
+            } else if (p.splits == 1 && n0 + c0 + 32 <= Ncols && (((uintptr_t)(crow + n0 + c0)) & 15) == 0) {
 #pragma unroll
                 for (int g = 0; g < 8; ++g) {
                     float4 *dst = (float4 *)(crow + n0 + c0 + 4 * g);
@@ -345,7 +366,7 @@ __global__ void __launch_bounds__(128, 1) tc_gemm_kernel(const __grid_constant__
 #pragma unroll
                 for (int i = 0; i < 32; ++i) {
                     const int col = n0 + c0 + i;
-                    if (col < p.N) {
+                    if (col < Ncols) {
                         const float x = p.alpha * v[i];
                         if (p.splits > 1) atomicAdd(&crow[col], x);
                         else crow[col] = p.beta != 0.f ? crow[col] + x : x;

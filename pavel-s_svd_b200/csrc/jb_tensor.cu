@@ -65,7 +65,9 @@ static int launch(TcParams &p, int64_t batch, cudaStream_t st) {
     auto kern = tc_gemm_kernel<BN>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return JB_ECUDA;
-    dim3 grid((unsigned)((p.N + BN - 1) / BN), (unsigned)((p.M + BM - 1) / BM), (unsigned)(batch * p.splits));
+    // the column tiles of the first product, then (nx1 > 0) those of the second
+    const int gx = (p.N + BN - 1) / BN + (p.nx1 > 0 ? (p.N2 + BN - 1) / BN : 0);
+    dim3 grid((unsigned)gx, (unsigned)((p.M + BM - 1) / BM), (unsigned)(batch * p.splits));
     kern<<<grid, 128, smem, st>>>(p);
     return cudaGetLastError() == cudaSuccess ? JB_OK : JB_ECUDA;
 }
@@ -229,6 +231,44 @@ int jb_gemm_bf16x_rows(const void *const *A, const void *const *B, int32_t mode,
     p.out_nparts = nparts;
     p.out_map = row_map;
     p.out_ld = ld_out;
+    return tc::dispatch(p, bn, batch, (cudaStream_t)stream);
+}
+
+int jb_gemm_bf16x_rows2(const void *const *A, const void *const *B, const void *const *B2, int32_t mode,
+                        void *const *out, void *const *out2, int32_t nparts, const int32_t *row_map, int64_t ld_out,
+                        int64_t ld_out2, int64_t M, int64_t N, int64_t N2, int64_t K, int64_t lda, int64_t ldb,
+                        int64_t ldb2, int64_t batch, int64_t strideA, int64_t strideB, int64_t strideB2, float alpha,
+                        int32_t *error_flag, void *stream) {
+    if (!out || !out2 || !B2 || nparts < 1 || nparts > 3 || N2 < 1 || ld_out < N || ld_out % 8 || ld_out2 < N2 ||
+        ld_out2 % 8)
+        return JB_EINVAL;
+    for (int i = 0; i < nparts; ++i)
+        if (!out[i] || ((uintptr_t)out[i] & 15) || !out2[i] || ((uintptr_t)out2[i] & 15)) return JB_EINVAL;
+    tc::TcParams p;
+    int bn = 0;
+    const int rc = tc::setup(A, B, mode, M, N, K, lda, ldb, batch, strideA, strideB, 1, alpha, error_flag, p, bn);
+    if (rc != JB_OK) return rc;
+    if (p.splits != 1 || p.a_as_b) return JB_ETOOBIG;   // one CTA along K; B given
+    // the second product: the same A, K, mode and split parts, its own B2
+    if (ldb2 % 8 || (p.b_mn ? ldb2 < N2 : ldb2 < K) || (batch > 1 && strideB2 % 8) || N2 > (1 << 30))
+        return JB_EINVAL;
+    for (int i = 0; i < p.nb; ++i) {
+        if (!B2[i] || ((uintptr_t)B2[i] & 15)) return JB_EINVAL;
+        const bool ok = p.b_mn ? tc::make_map(&p.tb[3 + i], B2[i], N2, K, ldb2, batch, strideB2, tc::BK)
+                               : tc::make_map(&p.tb[3 + i], B2[i], K, N2, ldb2, batch, strideB2, bn);
+        if (!ok) return JB_ECUDA;
+    }
+    for (int i = 0; i < nparts; ++i) {
+        p.out_part[i] = (__nv_bfloat16 *)out[i];
+        p.out_part2[i] = (__nv_bfloat16 *)out2[i];
+    }
+    p.out_nparts = nparts;
+    p.out_map = row_map;
+    p.out_ld = ld_out;
+    p.out_ld2 = ld_out2;
+    p.nx1 = (int)((N + bn - 1) / bn);
+    p.N2 = (int)N2;
+    if ((int64_t)p.nx1 + (N2 + bn - 1) / bn > 0x7fffffff) return JB_ETOOBIG;
     return tc::dispatch(p, bn, batch, (cudaStream_t)stream);
 }
 

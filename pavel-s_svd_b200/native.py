@@ -25,7 +25,7 @@ RC_NAMES = {JB_EINVAL: "invalid argument", JB_ETOOBIG: "shape too large for this
 # Exported symbols, in declaration order of include/jacobi_b200.h.
 SYMBOLS = ("jb_version", "jb_device_sm_count", "jb_workspace_bytes", "jb_svd_batched_f32",
            "jb_svd_batched_f64", "jb_uneven_workspace_bytes", "jb_svd_uneven_f32", "jb_svd_uneven_f32_ex",
-           "jb_gemm_bf16", "jb_gemm_bf16x", "jb_gemm_bf16x_rows", "jb_split_bf16", "jb_split3_bf16",
+           "jb_gemm_bf16", "jb_gemm_bf16x", "jb_gemm_bf16x_rows", "jb_gemm_bf16x_rows2", "jb_split_bf16", "jb_split3_bf16",
            "jb_warm_prep_f32", "jb_svd_warm_f32", "jb_transpose_bf16", "jb_bias_act", "jb_relu_backward",
            "jb_col_sum", "jb_mse_grad", "jb_adam", "jb_gram_sketch", "jb_block_eig_f64", "jb_block_eig_workspace_bytes",
            "jb_block_eig_ws", "jb_block_eig_f64_ex", "jb_rows_scatter",
@@ -106,6 +106,10 @@ def _declare(l):
     l.jb_gemm_bf16x_rows.argtypes = [ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p), I32,
                                      ctypes.POINTER(ctypes.c_void_p), I32, P, I64, I64, I64, I64, I64, I64, I64,
                                      I64, I64, ctypes.c_float, P, P]
+    VP = ctypes.POINTER(ctypes.c_void_p)
+    l.jb_gemm_bf16x_rows2.restype = ctypes.c_int
+    l.jb_gemm_bf16x_rows2.argtypes = [VP, VP, VP, I32, VP, VP, I32, P, I64, I64, I64, I64, I64, I64, I64, I64, I64,
+                                      I64, I64, I64, I64, ctypes.c_float, P, P]
     FL = ctypes.c_float
     for name, args in (("jb_warm_prep_f32", [P, P, P, P, P, P, I64, I32, I32, P]),
                        ("jb_svd_warm_f32", [P, P, P, P, P, I64, I32, I32, I32, I32, F64, I32, I32, P, P, P, SZ, P]),

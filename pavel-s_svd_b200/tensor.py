@@ -91,6 +91,25 @@ def gemm_parts_rows(a_parts, b_parts, out_parts, row_map=None, *, b_mn=False, al
     N.check(rc, "jb_gemm_bf16x_rows")
 
 
+def gemm_parts_rows2(a_parts, b_parts, out_parts, b2_parts, out2_parts, row_map=None, *, b_mn=False, alpha=1.0,
+                     chain128=True, error_flag=None):
+    """Two gemm_parts_rows products sharing A and the row map, in one launch
+    (jb_gemm_bf16x_rows2): alpha A B^T into out_parts and alpha A B2^T into
+    out2_parts."""
+    a0, b0, c0 = a_parts[0], b_parts[0], b2_parts[0]
+    bsz, M, K = a0.shape
+    Nn = b0.shape[-1] if b_mn else b0.shape[-2]
+    N2 = c0.shape[-1] if b_mn else c0.shape[-2]
+    ns = len(a_parts)
+    arr = lambda xs: (ctypes.c_void_p * 3)(*[x.data_ptr() for x in xs] + [None] * (3 - len(xs)))
+    rc = N.lib().jb_gemm_bf16x_rows2(arr(a_parts), arr(b_parts), arr(b2_parts), _mode(ns, b_mn, chain128, False),
+                                     arr(out_parts), arr(out2_parts), len(out_parts), _ptr(row_map),
+                                     out_parts[0].shape[-1], out2_parts[0].shape[-1], M, Nn, N2, K, a0.stride(1),
+                                     b0.stride(1), c0.stride(1), bsz, a0.stride(0), b0.stride(0), c0.stride(0),
+                                     float(alpha), _ptr(error_flag), torch.cuda.current_stream(a0.device).cuda_stream)
+    N.check(rc, "jb_gemm_bf16x_rows2")
+
+
 def gemm(a, b, c=None, *, a_lo=None, b_lo=None, alpha=1.0, beta=0.0, split_k=1, error_flag=None):
     """C = alpha * A @ B^T (+ beta C) on the tensor cores.
 

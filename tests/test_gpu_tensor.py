@@ -150,3 +150,29 @@ def test_rows_output_parts_and_map(T, parts):
     assert float(((got - expect).abs() / expect.abs().clamp_min(1e-30)).max()) <= tol
     for o in out:  # the padding past N is untouched
         assert bool((o[:, L:] == 7.0).all())
+
+
+@pytest.mark.parametrize("parts", [2, 3])
+def test_rows2_equals_two_rows_calls(T, parts):
+    """jb_gemm_bf16x_rows2: the two products of one launch (shared A and row
+    map, each B with its own width and leading dimension) write exactly what
+    two jb_gemm_bf16x_rows calls write, and leave the padding untouched."""
+    g = torch.Generator(device="cuda").manual_seed(10 + parts)
+    batch, M, K, L1, L2 = 6, 64, 64, 1000, 328          # B rows 16-byte aligned (TMA strides)
+    a = torch.randn(batch, M, K, device="cuda", generator=g)
+    b1 = torch.randn(batch, K, L1, device="cuda", generator=g)
+    b2 = torch.randn(batch, K, L2, device="cuda", generator=g)
+    sa, s1, s2 = (list(T.split3_bf16(x)[:parts]) for x in (a, b1, b2))
+    rows = batch * M
+    perm = torch.randperm(rows, generator=torch.Generator().manual_seed(3)).to(torch.int32).cuda()
+    fused1 = [torch.full((rows, 1008), 7.0, dtype=torch.bfloat16, device="cuda") for _ in range(parts)]
+    fused2 = [torch.full((rows, 336), 7.0, dtype=torch.bfloat16, device="cuda") for _ in range(parts)]
+    sep1 = [x.clone() for x in fused1]
+    sep2 = [x.clone() for x in fused2]
+    T.gemm_parts_rows2(sa, s1, fused1, s2, fused2, perm, b_mn=True, alpha=0.5)
+    T.gemm_parts_rows(sa, s1, sep1, perm, b_mn=True, alpha=0.5)
+    T.gemm_parts_rows(sa, s2, sep2, perm, b_mn=True, alpha=0.5)
+    torch.cuda.synchronize()
+    for f, s_ in zip(fused1 + fused2, sep1 + sep2):
+        assert torch.equal(f, s_)
+    assert bool((fused2[0][:, L2:] == 7.0).all())
