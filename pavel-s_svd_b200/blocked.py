@@ -151,7 +151,7 @@ class BlockJacobi:
         self.eig_defer_q = False
         self._eig_ws, self._eig_ws_slot = None, 0
         self.tuned = None
-        self._graphs, self._seen = {}, set()
+        self._graphs, self._seen, self._pool = {}, set(), None
 
     def _combine_v(self, cur):
         """V^T (npad x npad, FP32) from the slots of buffer `cur` (round 0 layout)."""
@@ -171,6 +171,30 @@ class BlockJacobi:
             h = (3.0 * eye - g) * 0.5
             vt = gemm_parts(split3_bf16(h), vp, b_mn=True, chain128=True)[0]
         return vt
+
+    def _polish_kept(self, U, r):
+        """Re-orthogonalise the r kept columns of U (mpad x n, in place,
+        columns in descending sigma) by one first-order Gram-Schmidt step
+        against the larger columns: u_j <- u_j - sum_{k<j} (u_k . u_j) u_k,
+        then unit length (SPLIT6 products).  U = A V / sigma carries V's
+        FP32-level error times sigma_1 / sigma_j into a small column's
+        direction (eps32 * cond from orthogonal); the step leaves the square
+        of that.  Only the smaller column of each pair moves, by about its
+        own error, so A - U S V^T changes by about eps32 sigma_1 (a symmetric
+        polar step would move the large columns as much and cost sigma_1
+        times the error)."""
+        if r < 2:
+            return
+        r8 = -(-r // 8) * 8                                   # 16-byte rows for the products
+        ut = torch.zeros(r8, self.mpad, dtype=torch.float32, device=self.device)
+        ut[:r] = U[:, :r].T
+        up = split3_bf16(ut)
+        g = gemm_parts(list(up), list(up), chain128=True)[0]  # U^T U
+        h = -torch.tril(g, diagonal=-1)                        # row j: -(u_k . u_j), k < j
+        h.diagonal().fill_(1.0)
+        h[r:], h[:, r:] = 0.0, 0.0
+        ut = gemm_parts(list(split3_bf16(h.contiguous())), list(up), b_mn=True, chain128=True)[0][:r]
+        U[:, :r] = (ut / ut.norm(dim=1, keepdim=True)).T
 
     def _cond_kept(self, cur, parts):
         """sigma_1 / the smallest column norm of W (buffer `cur`) that the
@@ -331,10 +355,10 @@ class BlockJacobi:
         g = gemm_parts(w, w, self.Gfull, chain128=True)
         d = g.diagonal().clamp_min(0)
         live = d > live_rel * d.max()
-        sd = d.sqrt()
-        corr = g.abs() / (sd[:, None] * sd[None, :]).clamp_min(torch.finfo(torch.float32).tiny)
+        # 1 / sqrt(g_pp) for live columns, 0 for the others (which drops their pairs)
+        inv = torch.where(live, d.sqrt(), torch.full_like(d, math.inf)).reciprocal()
+        corr = g.abs().mul_(inv[:, None]).mul_(inv[None, :])
         corr.fill_diagonal_(0)
-        corr = torch.where(live[:, None] & live[None, :], corr, torch.zeros_like(corr))
         self.post_off.copy_(corr.max().reshape(1))
 
     def _run_sweep(self, cur, parts, inner_sweeps, inner_tol, use_graphs, post_rel=None):
@@ -358,8 +382,12 @@ class BlockJacobi:
             return body()
         g = self._graphs.get(key)
         if g is None:
+            # the plan's graphs replay one at a time on one stream: one memory
+            # pool serves the temporaries of all of them
+            if self._pool is None:
+                self._pool = torch.cuda.graph_pool_handle()
             g = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(g):
+            with torch.cuda.graph(g, pool=self._pool):
                 body()
             self._graphs[key] = g
         g.replay()
@@ -463,11 +491,9 @@ class BlockJacobi:
         post_check: after every sweep also run the reference's own test on
         the Gram of the whole W (_post_sweep_off); the stage switch and the
         end of the solve then come one sweep sooner, the end only when that
-        off is below post_end * tol_phase1.  The sweep that this skips would
-        rotate pairs below tol_phase1 too, which still sharpens the small
-        columns' directions (U = A V / sigma at the finish carries V's error
-        times sigma_1 / sigma_j): 0.05 keeps U as orthogonal as the full
-        count of sweeps gives on the clustered 4096 x 1024 case."""
+        off is below post_end * tol_phase1 (0.05: a margin for the Gram's
+        FP32-level rounding; on the configured cases 0.5 gives the same sweep
+        counts and accuracy)."""
         lib = N.lib()
         dev, st = self.device, _st(self.device)
         m, n, b, P, R = self.m, self.n, self.b, self.P, self.nb - 1
@@ -529,6 +555,7 @@ class BlockJacobi:
         N.check(lib.jb_block_finish(wt.data_ptr(), vt.data_ptr(), U.data_ptr(), S.data_ptr(), Vh.data_ptr(),
                                     sig.data_ptr(), perm.data_ptr(), self.mpad, self.npad, n, e, max(m, n), st),
                 "jb_block_finish")
+        self._polish_kept(U, int((S > 0).sum()))
         # Columns of cut sigma: the reference's completion vectors (_finish_columns,
         # solvers.py:18-21 -> primitives.py:430-455), on the device.
         from .solvers import _complete_null_columns

@@ -5,9 +5,9 @@ Stated bounds for this mixed-precision path (3xBF16 sweeps, FP64 block
 eigen-solves, ~FP32-accurate 6xBF16 finish): |sigma_i - sigma_i(FP64)| <=
 5e-6 sigma_1 (spectrum_error_over_sigma1), relative error <= 1e-5 for
 sigma_i >= 0.1 sigma_1, reconstruction ||A - U S V^T|| / ||A|| <= 2e-5,
-max |V^T V - I| <= 2e-5, max |U^T U - I| <= max(2e-5, 2e-7 cond) (the
-columns of U for small sigma carry the FP32-level error eps32 * cond of the
-accurate sweeps, as in the reference's FP32 solver)."""
+max |V^T V - I| <= 2e-5, max |U^T U - I| <= 2e-5 (U = A V / sigma carries
+eps32 * cond into the small columns' directions; the finish re-orthogonalises
+the kept columns against the larger ones)."""
 import importlib
 
 import numpy as np
@@ -48,7 +48,7 @@ def test_blocked_matches_lapack(BJ, m, n, b, cond):
     U, S, Vh, info = plan.solve(torch.from_numpy(a).cuda())
     err1, relbig, rec, ou, ov = check(a, U, S, Vh)
     print(m, n, b, info["block_sweeps"], ["%.1e/%d" % x for x in info["off_per_sweep"]], err1, relbig, rec, ou, ov)
-    assert err1 <= 5e-6 and relbig <= 1e-5 and rec <= 2e-5 and ou <= max(2e-5, 2e-7 * cond) and ov <= 2e-5
+    assert err1 <= 5e-6 and relbig <= 1e-5 and rec <= 2e-5 and ou <= 2e-5 and ov <= 2e-5
 
 
 @pytest.mark.parametrize("M,N,K,lda", [(300, 520, 1000, 1000), (256, 384, 1004, 1012), (129, 77, 37, 37),
@@ -392,9 +392,8 @@ def test_configured_sizes_against_lapack(pkg, name, b):
       * values below cut / 2 are reported as 0, every reported value is
         within 1e-5 sigma_1 of the truth;
       * |V^T V - I| <= 2e-5;
-      * U (kept and completed columns): |U^T U - I| <= max(2e-5,
-        2e-7 sigma_1 / sigma_min kept), the FP32-level error of the
-        smallest kept column's direction;
+      * U (kept and completed columns): |U^T U - I| <= 2e-5 (the kept
+        columns re-orthogonalised at the finish);
       * ||A - U S V^T|| / ||A|| within 2e-5 of the cut values' own share;
       * the completed columns are the oracle's completion of the kept ones
         (first 40 missing columns, FP64 oracle: same pivots, 1e-5)."""
@@ -418,9 +417,8 @@ def test_configured_sizes_against_lapack(pkg, name, b):
     u64, vh64, a64 = u.double(), vh.double(), a.double()
     eye = torch.eye(n, dtype=torch.float64, device="cuda")
     assert float((vh64 @ vh64.T - eye).abs().max()) <= 2e-5
-    smin_kept = float(s_np[rep].min())
     ou = float((u64.T @ u64 - eye).abs().max())
-    assert ou <= max(2e-5, 2e-7 * sr[0] / smin_kept), ou
+    assert ou <= 2e-5, ou
     s64 = torch.from_numpy(s_np).cuda()
     rec = float((a64 - (u64 * s64) @ vh64).norm() / a64.norm())
     cut_share = float(np.sqrt((sr[~rep] ** 2).sum()) / np.sqrt((sr ** 2).sum()))
