@@ -702,6 +702,12 @@ def run_blocked(args, name):
     terms = [3 if p == 2 else 6 for _, p in info["off_per_sweep"]]
     # the sweeps' Gram and update products, and the post-sweep Gram of the whole W
     tensor_flop = sum(R * per_round * t + 2 * npd * npd * mp * t for t in terms)
+    # outside the sweeps, all six-term: Newton-Schulz steps on V (two npad^3
+    # products each), W = A V on the tensor cores, the two products of U's
+    # re-orthogonalisation (kept columns rounded up to 8)
+    r8 = -(-info["kept_columns"] // 8) * 8 if info["kept_columns"] > 1 else 0
+    tensor_flop += 6 * (info["polar_steps"] * 2 * 2 * npd ** 3 + info["tensor_w_products"] * 2 * npd * mp * npd
+                        + 2 * 2 * r8 * r8 * mp)
     acc = lapack_check(a_np, U, S, Vh, max(m, n))
     line = {"metric": f"blocked Jacobi SVD matrices/s ({m}x{n}, b={b})", "value": 1e3 / ms, "unit": "matrices/s",
             "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 2), "ms_per_step": ms,
@@ -726,8 +732,10 @@ def run_blocked(args, name):
     achieved = tensor_flop / (ms / 1e3) / 1e12
     line["roofline"] = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                         "frac": achieved / peak, "peak_kind": kind, "traffic": None,
-                        "note": "tensor flops of the Gram and update products (3 or 6 BF16 terms) over the whole "
-                                "solve; the solve is bound by the 16-slot eigen-solves that set each round's pace"}
+                        "note": "tensor flops over the whole solve (every BF16 term counted): the sweeps' Gram and "
+                                "update products, the post-sweep Grams, the Newton-Schulz steps, W = A V where it "
+                                "runs on the tensor cores, U's re-orthogonalisation; the solve is bound by the "
+                                "16-slot eigen-solves that set each round's pace"}
     if not args.no_plain:
         # the plain FP32 CUDA path at the same shape: the reference's block
         # rounds (solvers.py:30-68), every pair's inner one-sided Jacobi in

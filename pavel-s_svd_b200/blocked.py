@@ -507,6 +507,7 @@ class BlockJacobi:
         best, stall, converged, stage_sweeps = float("inf"), 0, False, 0
         post_hist = []
         ap_parts = None
+        n_polar = n_wtensor = 0            # tensor-core products outside the sweeps, for info
         for sweeps in range(1, max_sweeps + 1):
             self.live.fill_((live_rel if parts == 3 else 1e-4) * dmax)
             stage_sweeps += 1
@@ -536,6 +537,8 @@ class BlockJacobi:
                 ck = self._cond_kept(cur, parts_before)
                 ap_parts = split3_bf16(ap) if ck <= TENSOR_W_COND else None
                 wt = self._w_from_v(vt, ap, ck, ap_parts)
+                n_polar += polar_steps
+                n_wtensor += int(ck <= TENSOR_W_COND)
                 for buf, src, L in ((self.W[cur], wt, self.mpad), (self.V[cur], vt, self.npad)):
                     N.check(lib.jb_rows_scatter(src.data_ptr(), self.init_map.data_ptr(), buf[0].data_ptr(),
                                                 buf[1].data_ptr(), buf[2].data_ptr(), None, self.npad, L, st),
@@ -555,7 +558,10 @@ class BlockJacobi:
         N.check(lib.jb_block_finish(wt.data_ptr(), vt.data_ptr(), U.data_ptr(), S.data_ptr(), Vh.data_ptr(),
                                     sig.data_ptr(), perm.data_ptr(), self.mpad, self.npad, n, e, max(m, n), st),
                 "jb_block_finish")
-        self._polish_kept(U, int((S > 0).sum()))
+        kept = int((S > 0).sum())
+        self._polish_kept(U, kept)
+        n_polar += polar_steps
+        n_wtensor += int(ck <= TENSOR_W_COND)
         # Columns of cut sigma: the reference's completion vectors (_finish_columns,
         # solvers.py:18-21 -> primitives.py:430-455), on the device.
         from .solvers import _complete_null_columns
@@ -565,5 +571,8 @@ class BlockJacobi:
                 "reached_tol": off_hist[-1][0] <= tol_phase1 or post_hist[-1] <= post_end * tol_phase1,
                 "precision": "tensor-core sweeps (3xBF16 then 6xBF16) with FP64 block eigen-solves; "
                              f"6xBF16 Newton-Schulz V, {w_product} W = A V",
-                "cond_kept": ck}
+                "cond_kept": ck, "kept_columns": kept,
+                # the tensor-core products outside the sweeps: Newton-Schulz
+                # steps on V, W = A V products, the re-orthogonalisation of U
+                "polar_steps": n_polar, "tensor_w_products": n_wtensor}
         return U, S, Vh[:, :n].contiguous(), info
