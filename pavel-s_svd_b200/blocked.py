@@ -141,6 +141,9 @@ class BlockJacobi:
         # the 4096 x 1024 and 8192 x 2048 configurations: 1.3x faster per call,
         # the same block sweeps and sigma errors); the three-part sweeps in FP64
         self.eig_fp32_two_part = True
+        # the three-part sweeps' eigen-solves in FP32 too when every column the
+        # cut keeps is within TENSOR_W_COND of sigma_1 (set at the stage switch)
+        self._eig_fp32_three_part = False
         # "batched": every round's products as one launch per kind; "dataflow":
         # per-slot launches on per-slot streams with only the true dependencies
         # (_sweep_dataflow), so products overlap other slots' eigen-solves
@@ -317,8 +320,8 @@ class BlockJacobi:
     def _eig_variant(self, parts):
         if 2 * self.b not in (64, 128):
             return 0
-        return (self.eig_variant | (N.EIG_FP32 if parts == 2 and self.eig_fp32_two_part else 0)
-                | (N.EIG_DEFER_Q if self.eig_defer_q else 0))
+        fp32 = (parts == 2 and self.eig_fp32_two_part) or (parts == 3 and self._eig_fp32_three_part)
+        return self.eig_variant | (N.EIG_FP32 if fp32 else 0) | (N.EIG_DEFER_Q if self.eig_defer_q else 0)
 
     def _eig(self, k, count, parts, r, inner_sweeps, inner_tol, stream):
         """Eigen-solves of slots k .. k + count - 1 of round r (jb_block_eig_ws),
@@ -505,6 +508,7 @@ class BlockJacobi:
         live_rel = (np.finfo(np.float32).eps * max(m, n)) ** 2
         dmax = float((at * at).sum(1).max())
         best, stall, converged, stage_sweeps = float("inf"), 0, False, 0
+        self._eig_fp32_three_part = False
         post_hist = []
         ap_parts = None
         n_polar = n_wtensor = 0            # tensor-core products outside the sweeps, for info
@@ -539,6 +543,7 @@ class BlockJacobi:
                 wt = self._w_from_v(vt, ap, ck, ap_parts)
                 n_polar += polar_steps
                 n_wtensor += int(ck <= TENSOR_W_COND)
+                self._eig_fp32_three_part = ck <= TENSOR_W_COND
                 for buf, src, L in ((self.W[cur], wt, self.mpad), (self.V[cur], vt, self.npad)):
                     N.check(lib.jb_rows_scatter(src.data_ptr(), self.init_map.data_ptr(), buf[0].data_ptr(),
                                                 buf[1].data_ptr(), buf[2].data_ptr(), None, self.npad, L, st),
