@@ -713,7 +713,8 @@ def run_blocked(args, name):
             "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 2), "ms_per_step": ms,
             "higher_is_better": True,
             "scaling": "none (single matrix)", "vs_baseline": None,
-            "dtype": "f32 in/out; bf16x3/bf16x6 tensor; f64 eig",
+            "dtype": "f32 in/out; bf16x3/bf16x6 tensor; " + "/".join(sorted({x.lower() for x in info["eig_precision"]}))
+                     + " eig",
             "config": {"workload": name, "m": m, "n": n, "block_size": b,
                        "launch": {"eig_cols_per_warp": plan.eig_variant, "gram_split": plan.gram_split,
                                   "schedule": plan.schedule, "slot_split": plan.slot_split,

@@ -563,6 +563,8 @@ class BlockJacobi:
         N.check(lib.jb_block_finish(wt.data_ptr(), vt.data_ptr(), U.data_ptr(), S.data_ptr(), Vh.data_ptr(),
                                     sig.data_ptr(), perm.data_ptr(), self.mpad, self.npad, n, e, max(m, n), st),
                 "jb_block_finish")
+        eig2 = "FP32" if self.eig_fp32_two_part else "FP64"
+        eig3 = "FP32" if self._eig_fp32_three_part else "FP64"
         kept = int((S > 0).sum())
         self._polish_kept(U, kept)
         n_polar += polar_steps
@@ -574,8 +576,9 @@ class BlockJacobi:
         info = {"algorithm": "block_jacobi", "block_sweeps": sweeps, "off_per_sweep": off_hist,
                 "post_sweep_off": post_hist, "converged": converged,
                 "reached_tol": off_hist[-1][0] <= tol_phase1 or post_hist[-1] <= post_end * tol_phase1,
-                "precision": "tensor-core sweeps (3xBF16 then 6xBF16) with FP64 block eigen-solves; "
-                             f"6xBF16 Newton-Schulz V, {w_product} W = A V",
+                "precision": f"tensor-core sweeps (3xBF16 with {eig2} block eigen-solves, then 6xBF16 with "
+                             f"{eig3} ones); 6xBF16 Newton-Schulz V, {w_product} W = A V",
+                "eig_precision": (eig2, eig3),
                 "cond_kept": ck, "kept_columns": kept,
                 # the tensor-core products outside the sweeps: Newton-Schulz
                 # steps on V, W = A V products, the re-orthogonalisation of U
