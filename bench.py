@@ -795,15 +795,24 @@ def run_warm(args):
     eye = torch.eye(64, device="cuda").expand(4096, 64, 64).contiguous()
     ideal = wl.family_v(theta[60000:64096], device="cuda").contiguous()
     res = {}
-    for label, v0 in (("plain_fp32", eye), ("plain", eye), ("warm", None), ("ideal_start", ideal)):
+    # plain_fp32 / plain: the Jacobi alone from V = I (the plain solvers);
+    # warm: sketch -> network -> in-kernel QR and fallback test -> Jacobi;
+    # identity_through_pipeline: V0 = I through the QR preparation and the
+    # Jacobi (the warm path's cost without the network); ideal_start: the
+    # generator's own V(theta) through the same preparation, and ideal_solve
+    # the Jacobi alone from it (what a perfect network with a free start gives)
+    variants = (("plain_fp32", eye, True), ("plain", eye, True), ("warm", None, False),
+                ("identity_through_pipeline", eye, False), ("ideal_start", ideal, False), ("ideal_solve", ideal, True))
+    for label, v0, direct in variants:
         solver = solver32 if label == "plain_fp32" else W.WarmSolver(net, m=128, n=64, batch=4096)
+        run = (lambda: solver.solve_from(te, v0)) if direct else (lambda: solver.launch(te, v0=v0))
         for _ in range(args.warmup):
-            solver.launch(te, v0=v0)
+            run()
         torch.cuda.synchronize()
         e0, e1 = _events()
         e0.record()
         for _ in range(args.steps):
-            solver.launch(te, v0=v0)
+            run()
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.steps
@@ -815,6 +824,22 @@ def run_warm(args):
             worst = max(worst, float(np.max(np.abs(S[i] - sr) / sr)))
         res[label] = {"ms": ms, "matrices_per_s": 4096 / (ms / 1e3), "sweeps_mean": float(sweeps.mean()),
                       "kept": float(used.mean()), "max_rel_sigma_err_vs_fp64_sample": worst}
+    # the warm path's parts, each timed alone
+    x = W.sketch(te)
+    v0n = net.predict_v0(te).contiguous()
+    sol = W.WarmSolver(net, m=128, n=64, batch=4096)
+    lib = importlib.import_module("pavel-s_svd_b200.native").lib()
+    st = torch.cuda.current_stream().cuda_stream
+
+    def prep():
+        lib.jb_warm_prep_f32(te.data_ptr(), v0n.data_ptr(), sol.vstart.data_ptr(), sol.used.data_ptr(),
+                             sol.off[0].data_ptr(), sol.off[1].data_ptr(), 4096, 128, 64, st)
+    parts = {"sketch": _time_gpu(lambda: W.sketch(te), args.steps, args.warmup),
+             "network": _time_gpu(lambda: net.forward(x), args.steps, args.warmup),
+             "qr_and_fallback_prep": _time_gpu(prep, args.steps, args.warmup)}
+    prep()
+    vs = sol.vstart.transpose(-1, -2).contiguous()     # back to launch's layout (vectors as columns)
+    parts["jacobi_from_prepared_start"] = _time_gpu(lambda: sol.solve_from(te, vs), args.steps, args.warmup)
     line = {"metric": "Jacobi SVD matrices/s, learned warm start vs plain (128x64 family, 4096 held-out)",
             "value": res["warm"]["matrices_per_s"], "unit": "matrices/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": res["warm"]["ms"], "higher_is_better": True, "scaling": "weak",
@@ -822,9 +847,12 @@ def run_warm(args):
             "data": "synthetic (seeded: U Haar, log-uniform s, V = expm(0.3 L(theta)))", "config": {"workload": "warm_family", "train": 60000,
                                                                          "held_out": 4096, "epochs": 15},
             "train_ms": train_ms, "loss_first_last": [hist[0], hist[-1]], "variants": res,
-            "note": "plain_fp32 = the plain FP32 Jacobi from V = I; plain = the mixed-precision solver from V = I; "
-                    "warm = the network's V0 (QR-orthonormalised, identity fallback); ideal_start = the "
-                    "generator's own V(theta): what a perfect network would give"}
+            "warm_over_plain": res["warm"]["matrices_per_s"] / res["plain"]["matrices_per_s"],
+            "warm_parts_ms": parts,
+            "note": "plain_fp32 / plain = the plain FP32 / mixed-precision Jacobi from V = I alone; warm = sketch, "
+                    "network, in-kernel Householder QR of V0 with the identity fallback test, then the Jacobi; "
+                    "identity_through_pipeline = V0 = I through that QR preparation; ideal_start / ideal_solve = "
+                    "the generator's own V(theta) with / without the preparation: what a perfect network would give"}
     print(json.dumps(line), flush=True)
 
 

@@ -254,6 +254,20 @@ class WarmSolver:
                                     self.prec, self.info[0].data_ptr(), self.info[1].data_ptr(), self.ws.data_ptr(),
                                     self.ws.numel(), st), "jb_svd_warm_f32")
 
+    def solve_from(self, a: torch.Tensor, vstart: torch.Tensor):
+        """The Jacobi alone from a given orthonormal start V (B, n, n),
+        row-major with the vectors as columns like launch's v0 (no network,
+        no QR preparation, no fallback test): with the identity, the plain
+        solver; with the generator's own frame, the ceiling of a perfect
+        network."""
+        lib = N.lib()
+        self.vstart.copy_(vstart.transpose(-1, -2))       # the solver reads the columns contiguously
+        k = min(self.m, self.n)
+        N.check(lib.jb_svd_warm_f32(a.data_ptr(), self.vstart.data_ptr(), self.U.data_ptr(), self.S.data_ptr(),
+                                    self.Vh.data_ptr(), self.batch, self.m, self.n, k, 0, self.tol, self.max_sweeps,
+                                    self.prec, self.info[0].data_ptr(), self.info[1].data_ptr(), self.ws.data_ptr(),
+                                    self.ws.numel(), _st(self.device)), "jb_svd_warm_f32")
+
     def check(self):
         host = self.info.cpu()
         raise_for_status(host[1], self.max_sweeps)

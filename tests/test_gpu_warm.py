@@ -92,9 +92,12 @@ def test_trained_network_saves_sweeps(W, workloads):
     sweeps, with the same singular values; the ideal start (the generator's
     own V(theta), used here only as a bound) shows what a perfect network
     could save.  The gain in matrices/s is measured and printed, not
-    asserted: on this family the saved sweeps (~4 %) do not pay for the
-    network and the start's preparation (warm ~3 % slower than plain), and
-    only the overhead is bounded here."""
+    asserted: on this family the saved sweeps (~4 %) pay neither for the
+    network nor for the start's preparation (the in-kernel QR of V0 and the
+    fallback test take about as long as the Jacobi itself), so the warm path
+    is about 2x slower than the plain Jacobi from V = I alone.  What is
+    bounded here is the network's own cost: the warm path against the
+    identity start through the same preparation."""
     a_np, theta = workloads.warm_family(count=65536, device="cuda")
     a = torch.from_numpy(a_np).cuda()
     tr, te = a[:60000].contiguous(), a[60000:64096].contiguous()
@@ -116,7 +119,7 @@ def test_trained_network_saves_sweeps(W, workloads):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / 3
 
-    ms_plain = timed(eye)
+    ms_pipe_identity = timed(eye)                    # V0 = I through the same QR preparation
     n_plain, used0 = solver.check()
     s_plain = solver.S.clone()
     assert used0.sum() == 0
@@ -126,11 +129,20 @@ def test_trained_network_saves_sweeps(W, workloads):
     s_warm = solver.S.clone()
     solver.launch(te, v0=workloads.family_v(theta[60000:64096], device="cuda").contiguous())
     ideal, _ = solver.check()
-    print(f"held-out sweeps: plain {n_plain.mean():.2f} ({ms_plain:.2f} ms), trained {sweeps.mean():.2f} "
-          f"({ms_warm:.2f} ms, kept {used.mean():.2f}, off-norm {off0:.3f} -> {off1:.3f}), ideal start "
-          f"{ideal.mean():.2f}")
+    solver.solve_from(te, eye)                     # the plain Jacobi alone, for the printout
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        solver.solve_from(te, eye)
+    e1.record()
+    torch.cuda.synchronize()
+    ms_plain_alone = e0.elapsed_time(e1) / 3
+    print(f"held-out sweeps: plain {n_plain.mean():.2f} ({ms_plain_alone:.2f} ms alone, {ms_pipe_identity:.2f} ms "
+          f"through the preparation), trained {sweeps.mean():.2f} ({ms_warm:.2f} ms, kept {used.mean():.2f}, "
+          f"off-norm {off0:.3f} -> {off1:.3f}), ideal start {ideal.mean():.2f}")
     assert float(((s_warm - s_plain).abs() / s_plain[:, :1]).max()) <= 1e-5
     assert used.mean() > 0.5
     assert off1 < off0
     assert sweeps.mean() < n_plain.mean()
-    assert ms_warm <= 1.15 * ms_plain
+    assert ms_warm <= 1.15 * ms_pipe_identity
