@@ -141,8 +141,8 @@ JB_API int jb_svd_uneven_f32(const float *A, float *U, float *S, float *Vh,
                       void *workspace, size_t workspace_bytes, void *stream);
 
 /* jb_svd_uneven_f32 with the launch choices an autotuner varies: flags
- * JB_ROUND_ROBIN and/or JB_BLOCK_WIDTH_8 (the workspace query must get the
- * same flags); exit_ratio, the largest pair ratio after which the FP32 phase
+ * JB_ROUND_ROBIN, JB_BLOCK_WIDTH_8 and/or JB_ONE_SIZE_CLASS (the workspace
+ * query must get the same flags); exit_ratio, the largest pair ratio after which the FP32 phase
  * of a mixed solve hands over to the FP64 phase (0: the default 1e-2; < 0:
  * the FP32 phase runs to tol).  Results converge to the same tolerance
  * whatever the choices. */
